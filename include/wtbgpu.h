@@ -1,0 +1,132 @@
+/*
+ * wtbgpu.h -- C-ABI of libwtbgpu.so, the B200 (sm_100a) implementation of the
+ * WanTiBEXOS Bethe-Salpeter exciton + optics path.
+ *
+ * The reference has no plugin or FFI layer: its boundary is the set of Fortran
+ * subroutines that the driver (wtb_main.f90) calls.  Each entry point below
+ * replaces one of those stages and is what a Fortran ISO_C_BINDING interface
+ * (or the bundled C++ driver) binds.  Conventions:
+ *   - arrays are column-major (Fortran order), caller-allocated host memory;
+ *   - complex arrays are interleaved (re, im) doubles, i.e. complex(c_double_complex);
+ *   - every call returns a status: 0 = OK, < 0 = error (see wtbg_error_string);
+ *   - one context = one device + one CUDA stream, used from one host thread;
+ *   - large arrays (H(k) eigenvectors, BSE matrix, reflectors) stay on the device.
+ */
+#ifndef WTBGPU_H
+#define WTBGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum wtbg_status {
+  WTBG_OK = 0,
+  WTBG_ERR_ARG = -1,          /* invalid argument (size, pointer, option)                 */
+  WTBG_ERR_CUDA = -2,         /* CUDA runtime error (message in wtbg_last_error)          */
+  WTBG_ERR_OOM = -3,          /* device allocation failed                                  */
+  WTBG_ERR_NOCONV = -4,       /* an iterative device solver hit its iteration cap          */
+  WTBG_ERR_STATE = -5,        /* call order violated (e.g. solve before build)            */
+  WTBG_ERR_BANDWINDOW = -6,   /* nv > nocp or nc > w - nocp at some k (quantumnumbers2)   */
+  WTBG_ERR_NOEMPTY = -7,      /* no eigenvalue above E_F at some k (nocp undefined)       */
+  WTBG_ERR_UNSUPPORTED = -8,  /* size or option outside what this build supports          */
+  WTBG_ERR_NOCUDA = -9        /* no CUDA device available                                  */
+};
+
+/* Coulomb potential selector: the COULOMB_POT= deck values of matrizelbse
+ * (subroutines/bse_subs.f90:49-93). */
+enum wtbg_coulomb_type {
+  WTBG_V2DK = 1, WTBG_V3D = 2, WTBG_V3DL = 3, WTBG_V2DT = 4, WTBG_V2DT2 = 5,
+  WTBG_V2DOH = 6, WTBG_V2DRK = 7, WTBG_V1DT = 8, WTBG_V0DT = 9
+};
+
+/* Arguments of the coulomb_pot.f90 functions as matrizelbse passes them
+ * (bse_subs.f90:2-93): KTOL, EDIEL_T/EDIEL/EDIEL_B, LC, EDIEL_Z, W_COUL, R_0, ngrid. */
+typedef struct wtbg_coulomb {
+  int coultype;       /* enum wtbg_coulomb_type */
+  int ngrid[3];
+  double ktol;
+  double ediel[3];    /* ediel(1..3) = EDIEL_T, EDIEL, EDIEL_B */
+  double lc, ez, w, r0;
+} wtbg_coulomb;
+
+typedef struct wtbg_ctx wtbg_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+int wtbg_create(wtbg_ctx** ctx, int device);
+int wtbg_destroy(wtbg_ctx* ctx);
+const char* wtbg_error_string(int status);
+const char* wtbg_last_error(const wtbg_ctx* ctx);
+/* Milliseconds spent on the device by the last wtbg_* call on this context
+ * (CUDA events on the context stream around that call's launches). */
+double wtbg_last_device_ms(const wtbg_ctx* ctx);
+
+/* ---- model: replaces the module globals filled by hamiltonian_input_read
+ *      (subroutines/module_input_read.f90:32-176).
+ *      hre/him: hopmatrices/ihopmatrices (nvec,w,w); rvec (nvec,3); deg = ffactor(nvec);
+ *      rlat (3,3) with rlat(i,:) = a_i; efermi; scs (scissors). */
+int wtbg_set_model(wtbg_ctx* ctx, int w, int nvec, const double* hre, const double* him,
+                   const int* rvec, const int* deg, const double* rlat,
+                   double efermi, double scs);
+
+/* ---- bands: replaces the per-k eigsys loop and band selection of bsesolver
+ *      (bse_solver-tool-diel.f90:257-313; eigsys = hamiltonian_tb.f90:2-137).
+ *      kpt (nk,3) Cartesian 1/Angstrom.  Outputs (each may be NULL):
+ *      eigv (nk,nc+nv), vector (nk,nc+nv,w) complex (component 1 real, as ZHEEV('V','L')),
+ *      nocpk (nk), egap (min direct gap).  The selected bands stay on the device. */
+int wtbg_bands(wtbg_ctx* ctx, int nk, const double* kpt, int nv, int nc,
+               double* eigv, double* vector, int* nocpk, double* egap);
+
+/* ---- velocity: replaces the optsp loop (bse_solver-tool-diel.f90:365-396;
+ *      optsp/hlm = optics.f90:1-156).  hr (N,5) complex: hrx, hry, hrz, hrsp, hrsm,
+ *      N = nk*nc*nv in quantumnumbers2 order (k outer, c, v inner).  hr may be NULL. */
+int wtbg_velocity(wtbg_ctx* ctx, double sme, double* hr);
+
+/* ---- single-particle table: replaces vecres + Bubblem
+ *      (bse_solver-tool-diel.f90:379-402, general_subs.f90:405-440).
+ *      vecres (N,15) real(4), rows stably sorted by column 7. */
+int wtbg_sp_table(wtbg_ctx* ctx, float* vecres);
+
+/* ---- BSE kernel build: replaces the matrizelbse double loop
+ *      (bse_solver-tool-diel.f90:431-458; bse_subs.f90:2-124; coulomb_pot.f90:2-432).
+ *      The N x N matrix stays on the device (lower triangle, = conj of the reference's
+ *      upper triangle). */
+int wtbg_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p);
+
+/* Copy the built matrix to the host with the reference's layout: hbse (N,N) complex,
+ * upper triangle j >= i written, strictly lower part zero.  For checks on small N. */
+int wtbg_bse_get_matrix(wtbg_ctx* ctx, double* hbse);
+
+/* ---- dense solve + oscillators: replaces ZHEEV('V','U') and dielbsev/dielbsep
+ *      (bse_solver-tool-diel.f90:485-602; bse_subs.f90:278-378).
+ *      W (N) ascending; act (N,8) = xx, yy, zz, xy, xz, yz, sp, sm
+ *      (xy/xz/yz zero unless dtfull, sp/sm zero unless cpol).  Requires wtbg_velocity. */
+int wtbg_bse_solve(wtbg_ctx* ctx, int dtfull, int cpol, double* W, double* act);
+
+/* Exciton eigenvectors n0..n1 (1-based, inclusive) after wtbg_bse_solve, for the
+ * BSE_WF files (excwf2, bse_subs.f90:534-576).  A (N, n1-n0+1) complex, each vector
+ * normalised with its last component real and >= 0. */
+int wtbg_bse_eigvecs(wtbg_ctx* ctx, int n0, int n1, double* A);
+
+/* ---- spectrum: replaces the omega loop of bsedielraw with optdiel, avgsme and
+ *      imagrenorm (bse_diel-tool.f90:137-210; optics.f90:160-390).
+ *      ebse (n), fosc (n,6) in bse_opt_diel.dat column order xx,yy,zz,xy,xz,yz
+ *      (the values as read back from that file); vcell3d = |(a1 x a2).a3|.
+ *      Outputs omega (nw) and eps (nw,2,6): eps(:,1,c) = real(spinf*Re), eps(:,2,c) =
+ *      real(spinf*Im) as real(4), components in file order xx, yy, zz, xy, xz, yz. */
+int wtbg_spectrum(wtbg_ctx* ctx, int n, const double* ebse, const double* fosc,
+                  const int* ngrid, double vcell3d, double ebse0, double ebsef, double numbse,
+                  double sme, int renorm, double spinf, double* omega, float* eps);
+
+/* ---- exciton band structure: one centre-of-mass Q of bsebnds
+ *      (bse_kpath-tool.f90:246-435; matrizelbsekq = bse_subs_kpath.f90:1-208).
+ *      Uses the k-mesh bands of the last wtbg_bands call; kptq (nk,3) is the k+Q mesh
+ *      of monhkhorst_packq (mhkpack_subs.f90:305-356) and q4 = (distance, qx, qy, qz)
+ *      one row of the kpathbse path.  Builds the Q kernel with its exchange term and
+ *      returns the eigenvalues W (N) ascending (ZHEEV('N','U')). */
+int wtbg_bse_q_eigenvalues(wtbg_ctx* ctx, int nk, const double* kptq, const double* q4,
+                           const wtbg_coulomb* p, double* W);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WTBGPU_H */

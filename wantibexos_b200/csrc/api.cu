@@ -1,0 +1,415 @@
+// C-ABI of libwtbgpu.so: context management, argument checks, host <-> device transfers
+// and the order of kernel launches for each replaced reference stage (see wtbgpu.h).
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+int set_err(wtbg_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_fail(wtbg_ctx* c, cudaError_t e, const char* where) {
+  std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return set_err(c, WTBG_ERR_OOM, m);
+  return set_err(c, WTBG_ERR_CUDA, m);
+}
+
+int ensure(wtbg_ctx* c, DevBuf& b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b.bytes >= bytes) return 0;
+  if (b.p) {
+    cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+  }
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    b.p = nullptr;
+    char msg[160];
+    snprintf(msg, sizeof msg, "device allocation of %zu bytes failed", bytes);
+    return set_err(c, WTBG_ERR_OOM, msg);
+  }
+  b.bytes = bytes;
+  return 0;
+}
+
+namespace {
+
+struct Timer {
+  wtbg_ctx* c;
+  explicit Timer(wtbg_ctx* ctx) : c(ctx) { cudaEventRecord(c->ev0, c->stream); }
+  int stop() {
+    cudaEventRecord(c->ev1, c->stream);
+    cudaError_t e = cudaEventSynchronize(c->ev1);
+    if (e != cudaSuccess) return cuda_fail(c, e, "stream");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->last_ms = ms;
+    return 0;
+  }
+};
+
+void free_buf(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+int set_device(wtbg_ctx* ctx) {
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* wtbg_error_string(int s) {
+  switch (s) {
+    case WTBG_OK: return "ok";
+    case WTBG_ERR_ARG: return "invalid argument";
+    case WTBG_ERR_CUDA: return "CUDA error";
+    case WTBG_ERR_OOM: return "out of device memory";
+    case WTBG_ERR_NOCONV: return "iterative solver did not converge";
+    case WTBG_ERR_STATE: return "call order violated";
+    case WTBG_ERR_BANDWINDOW: return "Number of valence/conduction states higher than occupied/unoccupied states";
+    case WTBG_ERR_NOEMPTY: return "no eigenvalue above the Fermi level";
+    case WTBG_ERR_UNSUPPORTED: return "unsupported size or option";
+    case WTBG_ERR_NOCUDA: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char* wtbg_last_error(const wtbg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+double wtbg_last_device_ms(const wtbg_ctx* ctx) { return ctx ? ctx->last_ms : 0.0; }
+
+int wtbg_create(wtbg_ctx** out, int device) {
+  if (!out) return WTBG_ERR_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return WTBG_ERR_NOCUDA;
+  }
+  if (device < 0 || device >= n) return WTBG_ERR_ARG;
+  wtbg_ctx* ctx = new wtbg_ctx();
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) {
+    cudaGetLastError();
+    delete ctx;
+    return WTBG_ERR_CUDA;
+  }
+  *out = ctx;
+  return WTBG_OK;
+}
+
+int wtbg_destroy(wtbg_ctx* ctx) {
+  if (!ctx) return WTBG_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  DevBuf* bufs[] = {&ctx->HR, &ctx->Rcart, &ctx->Rf32, &ctx->invdeg, &ctx->isR0, &ctx->kpt, &ctx->eig, &ctx->U,
+                    &ctx->nocp, &ctx->kstat, &ctx->kptq, &ctx->eigq, &ctx->Uq, &ctx->nocpq, &ctx->h, &ctx->H,
+                    &ctx->d, &ctx->e, &ctx->tau, &ctx->g, &ctx->Wp, &ctx->slots, &ctx->part, &ctx->scal,
+                    &ctx->yv, &ctx->lam, &ctx->ws, &ctx->act, &ctx->zsel, &ctx->csz, &ctx->sp_in, &ctx->sp_out,
+                    &ctx->sp_om, &ctx->tmp, &ctx->tmp2, &ctx->istat};
+  for (DevBuf* b : bufs) free_buf(*b);
+  cudaEventDestroy(ctx->ev0);
+  cudaEventDestroy(ctx->ev1);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return WTBG_OK;
+}
+
+int wtbg_set_model(wtbg_ctx* ctx, int w, int nvec, const double* hre, const double* him, const int* rvec,
+                   const int* deg, const double* rlat, double efermi, double scs) {
+  if (!ctx) return WTBG_ERR_ARG;
+  if (w <= 0 || nvec <= 0 || !hre || !him || !rvec || !deg || !rlat)
+    return set_err(ctx, WTBG_ERR_ARG, "set_model: bad sizes or null pointers");
+  if (w > WTBG_MAX_W) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "set_model: w exceeds the per-k eigensolver limit");
+  for (int i = 0; i < nvec; ++i)
+    if (deg[i] == 0) return set_err(ctx, WTBG_ERR_ARG, "set_model: zero degeneracy");
+  if (int r = set_device(ctx)) return r;
+  ctx->w = w;
+  ctx->nvec = nvec;
+  for (int i = 0; i < 3; ++i)
+    for (int c = 0; c < 3; ++c) ctx->rlat[i * 3 + c] = rlat[i + 3 * c];   // Fortran rlat(i,c)
+  ctx->efermi = efermi;
+  ctx->scs = scs;
+  const size_t ww = (size_t)w * w;
+  std::vector<double2> hr(nvec * ww);
+  std::vector<double> rc(3 * (size_t)nvec), rf(3 * (size_t)nvec), inv(nvec);
+  std::vector<int> is0(nvec);
+  for (int iR = 0; iR < nvec; ++iR) {
+    for (int n = 0; n < w; ++n)
+      for (int m = 0; m < w; ++m) {
+        const size_t src = (size_t)iR + (size_t)nvec * ((size_t)m + (size_t)w * n);   // hopmatrices(iR,m,n)
+        hr[iR * ww + (size_t)n * w + m] = make_double2(hre[src], him[src]);
+      }
+    const int r1 = rvec[iR], r2 = rvec[iR + nvec], r3 = rvec[iR + 2 * nvec];
+    for (int c = 0; c < 3; ++c) {
+      // (r1*a1c + r2*a2c) + r3*a3c, as the reference's expression is evaluated
+      const double v = (r1 * ctx->rlat[0 * 3 + c] + r2 * ctx->rlat[1 * 3 + c]) + r3 * ctx->rlat[2 * 3 + c];
+      rc[3 * iR + c] = v;
+      rf[3 * iR + c] = (double)(float)v;
+    }
+    inv[iR] = 1.0 / (double)deg[iR];
+    is0[iR] = (r1 == 0 && r2 == 0 && r3 == 0) ? 1 : 0;
+  }
+  ENSURE(ctx->HR, hr.size() * 16);
+  ENSURE(ctx->Rcart, rc.size() * 8);
+  ENSURE(ctx->Rf32, rf.size() * 8);
+  ENSURE(ctx->invdeg, inv.size() * 8);
+  ENSURE(ctx->isR0, is0.size() * 4);
+  CK(cudaMemcpyAsync(ctx->HR.p, hr.data(), hr.size() * 16, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->Rcart.p, rc.data(), rc.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->Rf32.p, rf.data(), rf.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->invdeg.p, inv.data(), inv.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->isR0.p, is0.data(), is0.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->have_bands = ctx->have_velocity = ctx->have_matrix = ctx->have_solution = false;
+  return WTBG_OK;
+}
+
+static int check_kstat(wtbg_ctx* ctx, int nk) {
+  std::vector<int> st(nk);
+  CK(cudaMemcpyAsync(st.data(), ctx->kstat.p, (size_t)nk * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < nk; ++k) {
+    if (st[k] == 1) return set_err(ctx, WTBG_ERR_NOCONV, "bands: Jacobi sweep cap reached at k-point " + std::to_string(k + 1));
+    if (st[k] == 2) return set_err(ctx, WTBG_ERR_NOEMPTY, "bands: no eigenvalue above E_F at k-point " + std::to_string(k + 1));
+    if (st[k] == 3)
+      return set_err(ctx, WTBG_ERR_BANDWINDOW, "bands: nv/nc exceed occupied/unoccupied states at k-point " + std::to_string(k + 1));
+  }
+  return 0;
+}
+
+int wtbg_bands(wtbg_ctx* ctx, int nk, const double* kpt, int nv, int nc, double* eigv, double* vector, int* nocpk,
+               double* egap) {
+  if (!ctx) return WTBG_ERR_ARG;
+  if (ctx->w == 0) return set_err(ctx, WTBG_ERR_STATE, "bands: no model");
+  if (nk <= 0 || nv <= 0 || nc <= 0 || !kpt) return set_err(ctx, WTBG_ERR_ARG, "bands: bad sizes");
+  if (nv + nc > ctx->w) return set_err(ctx, WTBG_ERR_BANDWINDOW, "bands: nv + nc > w");
+  if (int r = set_device(ctx)) return r;
+  ctx->nk = nk;
+  ctx->nv = nv;
+  ctx->nc = nc;
+  const int nb = nv + nc, w = ctx->w;
+  ctx->N = (long long)nk * nc * nv;
+  std::vector<double> kp(3 * (size_t)nk);
+  for (int k = 0; k < nk; ++k)
+    for (int c = 0; c < 3; ++c) kp[3 * k + c] = kpt[k + (size_t)nk * c];
+  ENSURE(ctx->kpt, kp.size() * 8);
+  ENSURE(ctx->eig, (size_t)nk * nb * 8);
+  ENSURE(ctx->U, (size_t)nk * nb * w * 16);
+  ENSURE(ctx->nocp, (size_t)nk * 4);
+  ENSURE(ctx->kstat, (size_t)nk * 4);
+  Timer t(ctx);
+  CK(cudaMemcpyAsync(ctx->kpt.p, kp.data(), kp.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (int r = launch_bands(ctx, false)) return r;
+  if (int r = t.stop()) return r;
+  if (int r = check_kstat(ctx, nk)) return r;
+  ctx->have_bands = true;
+  ctx->have_velocity = ctx->have_matrix = ctx->have_solution = false;
+  std::vector<double> e((size_t)nk * nb);
+  CK(cudaMemcpyAsync(e.data(), ctx->eig.p, e.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  std::vector<int> no(nk);
+  CK(cudaMemcpyAsync(no.data(), ctx->nocp.p, (size_t)nk * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  std::vector<double2> u;
+  if (vector) {
+    u.resize((size_t)nk * nb * w);
+    CK(cudaMemcpyAsync(u.data(), ctx->U.p, u.size() * 16, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  double gap = 50.0;
+  for (int k = 0; k < nk; ++k) {
+    const double gk = e[(size_t)k * nb + nv] - e[(size_t)k * nb + nv - 1];
+    if (gk <= gap) gap = gk;
+  }
+  if (egap) *egap = gap;
+  if (eigv)
+    for (int k = 0; k < nk; ++k)
+      for (int j = 0; j < nb; ++j) eigv[k + (size_t)nk * j] = e[(size_t)k * nb + j];
+  if (nocpk)
+    for (int k = 0; k < nk; ++k) nocpk[k] = no[k];
+  if (vector)
+    for (int k = 0; k < nk; ++k)
+      for (int j = 0; j < nb; ++j)
+        for (int m = 0; m < w; ++m) {
+          const double2 v = u[((size_t)k * nb + j) * w + m];
+          const size_t dst = (size_t)k + (size_t)nk * ((size_t)j + (size_t)nb * m);   // vector(k, j, m)
+          vector[2 * dst] = v.x;
+          vector[2 * dst + 1] = v.y;
+        }
+  return WTBG_OK;
+}
+
+int wtbg_velocity(wtbg_ctx* ctx, double sme, double* hr) {
+  if (!ctx) return WTBG_ERR_ARG;
+  if (!ctx->have_bands) return set_err(ctx, WTBG_ERR_STATE, "velocity: call wtbg_bands first");
+  if (int r = set_device(ctx)) return r;
+  const long long N = ctx->N;
+  ENSURE(ctx->h, (size_t)N * 5 * 16);
+  Timer t(ctx);
+  // cmplx(0.0, sme) without KIND: the broadening enters as float32 (optics.f90:139)
+  if (int r = launch_velocity(ctx, (double)(float)sme)) return r;
+  if (int r = t.stop()) return r;
+  ctx->have_velocity = true;
+  if (hr) CK(cudaMemcpy(hr, ctx->h.p, (size_t)N * 5 * 16, cudaMemcpyDeviceToHost));
+  return WTBG_OK;
+}
+
+int wtbg_sp_table(wtbg_ctx* ctx, float* vecres) {
+  if (!ctx || !vecres) return WTBG_ERR_ARG;
+  if (!ctx->have_velocity) return set_err(ctx, WTBG_ERR_STATE, "sp_table: call wtbg_velocity first");
+  if (int r = set_device(ctx)) return r;
+  const long long N = ctx->N;
+  ENSURE(ctx->sp_in, (size_t)N * 15 * 4);
+  Timer t(ctx);
+  if (int r = launch_sp_table(ctx, ctx->sp_in.as<float>())) return r;
+  if (int r = t.stop()) return r;
+  CK(cudaMemcpy(vecres, ctx->sp_in.p, (size_t)N * 15 * 4, cudaMemcpyDeviceToHost));
+  return WTBG_OK;
+}
+
+int wtbg_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p) {
+  if (!ctx || !p) return WTBG_ERR_ARG;
+  if (!ctx->have_bands) return set_err(ctx, WTBG_ERR_STATE, "bse_build: call wtbg_bands first");
+  if (p->coultype < WTBG_V2DK || p->coultype > WTBG_V0DT) return set_err(ctx, WTBG_ERR_ARG, "Wrong Coulomb Potential");
+  if (int r = set_device(ctx)) return r;
+  const long long N = ctx->N;
+  ENSURE(ctx->H, (size_t)N * N * 16);
+  Timer t(ctx);
+  if (int r = launch_bse_build(ctx, p, nullptr)) return r;
+  if (int r = t.stop()) return r;
+  ctx->have_matrix = true;
+  ctx->have_solution = false;
+  return WTBG_OK;
+}
+
+int wtbg_bse_get_matrix(wtbg_ctx* ctx, double* hbse) {
+  if (!ctx || !hbse) return WTBG_ERR_ARG;
+  if (!ctx->have_matrix || ctx->have_solution) return set_err(ctx, WTBG_ERR_STATE, "bse_get_matrix: no built matrix");
+  if (int r = set_device(ctx)) return r;
+  const long long N = ctx->N;
+  std::vector<double2> L((size_t)N * N);
+  CK(cudaMemcpy(L.data(), ctx->H.p, (size_t)N * N * 16, cudaMemcpyDeviceToHost));
+  for (long long j = 0; j < N; ++j)
+    for (long long i = 0; i < N; ++i) {
+      double2 v = make_double2(0, 0);
+      if (j >= i) {
+        const double2 l = L[j + i * N];   // lower element (j, i)
+        v = make_double2(l.x, -l.y);
+      }
+      hbse[2 * (i + j * N)] = v.x;
+      hbse[2 * (i + j * N) + 1] = v.y;
+    }
+  return WTBG_OK;
+}
+
+int wtbg_bse_solve(wtbg_ctx* ctx, int dtfull, int cpol, double* W, double* act) {
+  if (!ctx) return WTBG_ERR_ARG;
+  if (!ctx->have_matrix) return set_err(ctx, WTBG_ERR_STATE, "bse_solve: call wtbg_bse_build first");
+  if (!ctx->have_velocity && act) return set_err(ctx, WTBG_ERR_STATE, "bse_solve: call wtbg_velocity first");
+  if (int r = set_device(ctx)) return r;
+  const long long N = ctx->N;
+  Timer t(ctx);
+  if (int r = run_tridiagonalise(ctx)) return r;
+  ctx->have_matrix = false;   // overwritten by the reflectors
+  if (int r = run_tridiagonal_solve(ctx, dtfull, cpol, act != nullptr)) return r;
+  if (int r = t.stop()) return r;
+  ctx->have_solution = true;
+  if (W) memcpy(W, ctx->lam_host.data(), (size_t)N * 8);
+  if (act) CK(cudaMemcpy(act, ctx->act.p, (size_t)N * 8 * 8, cudaMemcpyDeviceToHost));
+  return WTBG_OK;
+}
+
+int wtbg_bse_eigvecs(wtbg_ctx* ctx, int n0, int n1, double* A) {
+  if (!ctx || !A) return WTBG_ERR_ARG;
+  if (!ctx->have_solution || ctx->csize_host.empty())
+    return set_err(ctx, WTBG_ERR_STATE, "bse_eigvecs: call wtbg_bse_solve (with act) first");
+  if (n0 < 1 || n1 < n0 || n1 > ctx->N) return set_err(ctx, WTBG_ERR_ARG, "bse_eigvecs: bad range");
+  if (int r = set_device(ctx)) return r;
+  const long long N = ctx->N;
+  ENSURE(ctx->yv, (size_t)N * 32 * 16);
+  double ms = 0.0;
+  for (int a0 = n0; a0 <= n1; a0 += 32) {
+    const int a1 = (a0 + 31 < n1) ? a0 + 31 : n1;
+    const int nvec = a1 - a0 + 1;
+    Timer t(ctx);
+    if (int r = run_eigvecs(ctx, a0, a1, ctx->yv.as<double2>())) return r;
+    if (int r = t.stop()) return r;
+    ms += ctx->last_ms;
+    CK(cudaMemcpy(A + 2 * (size_t)N * (a0 - n0), ctx->yv.p, (size_t)N * nvec * 16, cudaMemcpyDeviceToHost));
+  }
+  ctx->last_ms = ms;
+  return WTBG_OK;
+}
+
+int wtbg_spectrum(wtbg_ctx* ctx, int n, const double* ebse, const double* fosc, const int* ngrid, double vcell3d,
+                  double ebse0, double ebsef, double numbse, double sme, int renorm, double spinf, double* omega,
+                  float* eps) {
+  if (!ctx || !ebse || !fosc || !ngrid || !omega || !eps) return WTBG_ERR_ARG;
+  const int nw = (int)numbse;
+  if (n <= 0 || nw < 2) return set_err(ctx, WTBG_ERR_ARG, "spectrum: bad sizes");
+  if (int r = set_device(ctx)) return r;
+  ENSURE(ctx->sp_in, (size_t)n * 7 * 8);
+  ENSURE(ctx->sp_om, (size_t)nw * 8 + (size_t)nw * 12 * 4 + 64);
+  double* de = ctx->sp_in.as<double>();
+  double* df = de + n;
+  double* dom = ctx->sp_om.as<double>();
+  float* deps = reinterpret_cast<float*>(dom + nw);
+  Timer t(ctx);
+  CK(cudaMemcpyAsync(de, ebse, (size_t)n * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(df, fosc, (size_t)n * 6 * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (int r = launch_spectrum(ctx, n, de, df, ngrid, vcell3d, ebse0, ebsef, numbse, sme, renorm, spinf, dom, deps))
+    return r;
+  CK(cudaMemcpyAsync(omega, dom, (size_t)nw * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(eps, deps, (size_t)nw * 12 * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  if (int r = t.stop()) return r;
+  return WTBG_OK;
+}
+
+int wtbg_bse_q_eigenvalues(wtbg_ctx* ctx, int nk, const double* kptq, const double* q4, const wtbg_coulomb* p,
+                           double* W) {
+  if (!ctx || !kptq || !q4 || !p || !W) return WTBG_ERR_ARG;
+  if (!ctx->have_bands || nk != ctx->nk) return set_err(ctx, WTBG_ERR_STATE, "bse_q: call wtbg_bands on the k-mesh first");
+  if (int r = set_device(ctx)) return r;
+  const int nb = ctx->nv + ctx->nc, w = ctx->w;
+  const long long N = ctx->N;
+  std::vector<double> kq(3 * (size_t)nk);
+  for (int k = 0; k < nk; ++k)
+    for (int c = 0; c < 3; ++c) kq[3 * k + c] = kptq[k + (size_t)nk * c];
+  ENSURE(ctx->kptq, kq.size() * 8);
+  ENSURE(ctx->eigq, (size_t)nk * nb * 8);
+  ENSURE(ctx->Uq, (size_t)nk * nb * w * 16);
+  ENSURE(ctx->nocpq, (size_t)nk * 4);
+  ENSURE(ctx->H, (size_t)N * N * 16);
+  Timer t(ctx);
+  CK(cudaMemcpyAsync(ctx->kptq.p, kq.data(), kq.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (int r = launch_bands(ctx, true)) return r;
+  if (int r = check_kstat(ctx, nk)) return r;
+  if (int r = launch_bse_build(ctx, p, q4)) return r;
+  const bool hv = ctx->have_velocity;
+  ctx->have_velocity = false;   // eigenvalues only: g not needed
+  int r = run_tridiagonalise(ctx);
+  ctx->have_velocity = hv;
+  if (r) return r;
+  if ((r = run_tridiagonal_solve(ctx, 0, 0, false))) return r;
+  if ((r = t.stop())) return r;
+  ctx->have_matrix = false;
+  ctx->have_solution = false;
+  memcpy(W, ctx->lam_host.data(), (size_t)N * 8);
+  return WTBG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,467 @@
+// Kernel (a): Wannier Fourier sum H(k) = sum_R e^{i k.R} H(R)/deg(R) - E_F and the per-k
+// Hermitian eigensolver, one CTA per k-point; plus the velocity matrices dH/dk_alpha
+// and their band matrix elements (optsp), and the single-particle table.
+//
+// Reference: eigsys (subroutines/hamiltonian_tb.f90:2-137), band selection
+// (subprograms/bse_solver-tool-diel.f90:257-313), hlm/optsp (subroutines/optics.f90:1-156),
+// vecres + Bubblem (bse_solver-tool-diel.f90:379-402, general_subs.f90:405-440).
+//
+// Numerics that follow the reference exactly:
+//   * the phase k.R is evaluated in double in the reference's order and rounded to
+//     float32 before exp() (cmplx(0.0, x) without KIND, hamiltonian_tb.f90:64-66);
+//   * E_F enters as float32 (fermilvl, hamiltonian_tb.f90:383);
+//   * ZHEEV('V','Lower') reads the lower triangle and the real part of the diagonal, and
+//     its eigenvectors have a real first component: the matrix is built from its lower
+//     triangle and every eigenvector is rotated so that component 1 is real and >= 0
+//     (the sign is irrelevant for every output of the path);
+//   * the velocity prefactor i*R_alpha is float32-rounded (optics.f90:43-47) and the
+//     optsp scale is Re(1/(E_c - E_v + i*float32(eta))) (REAL factor, optics.f90:114,148).
+// The eigensolver is cyclic complex Jacobi in FP64 with a round-robin parallel ordering
+// (w/2 disjoint rotations per step), converged to a relative threshold; it has an
+// iteration cap and reports non-convergence per k instead of spinning.
+#include <cfloat>
+#include <cub/cub.cuh>
+
+#include "common.cuh"
+
+namespace {
+
+constexpr int kBandsThreads = 256;
+constexpr int kMaxSweeps = 60;
+
+struct Rot {
+  int p, q, active, pad;
+  double cs, sn, ex, ey, ap, aq;
+};
+
+__device__ __forceinline__ double2 phase_of(double kx, double ky, double kz, const double* R) {
+  // (kx*Rx + ky*Ry) + kz*Rz, each product and sum rounded separately (no contraction)
+  double kr = __dadd_rn(__dadd_rn(__dmul_rn(kx, R[0]), __dmul_rn(ky, R[1])), __dmul_rn(kz, R[2]));
+  float kr32 = __double2float_rn(kr);
+  double s, c;
+  sincos((double)kr32, &s, &c);
+  return make_double2(c, s);
+}
+
+struct BandsArgs {
+  const double2* HR;
+  const double* Rcart;
+  const double* invdeg;
+  int nvec, w;
+  const double* kpt;
+  int nk;
+  double ef32, scs;
+  int nv, nc;
+  double* eig;     // [nk][nb]
+  double2* U;      // [nk][nb][w]
+  int* nocp;       // [nk]
+  int* kstat;      // [nk]
+};
+
+__global__ void __launch_bounds__(kBandsThreads) k_bands(BandsArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int w = a.w, nvec = a.nvec, tid = threadIdx.x, bs = blockDim.x;
+  const int ww = w * w;
+  const int m2 = w + (w & 1);
+  const int npair = m2 / 2;
+  double2* ph = reinterpret_cast<double2*>(smem);
+  double2* A = ph + nvec;
+  double2* V = A + ww;
+  Rot* rot = reinterpret_cast<Rot*>(V + ww);
+  double* lam = reinterpret_cast<double*>(rot + npair);
+  int* perm = reinterpret_cast<int*>(lam + w);
+  double* red = reinterpret_cast<double*>(perm + w + (w & 1));  // kBandsThreads/32 doubles
+  __shared__ int s_rotated;
+  __shared__ double s_tolabs;
+  __shared__ int s_nocp, s_stat;
+
+  for (int k = blockIdx.x; k < a.nk; k += gridDim.x) {
+    const double kx = a.kpt[3 * k], ky = a.kpt[3 * k + 1], kz = a.kpt[3 * k + 2];
+    for (int R = tid; R < nvec; R += bs) ph[R] = phase_of(kx, ky, kz, a.Rcart + 3 * R);
+    __syncthreads();
+    // Fourier sum on the lower triangle (ZHEEV 'L' reads nothing else), R in file order
+    double fro = 0.0;
+    for (int el = tid; el < ww; el += bs) {
+      const int m = el % w, n = el / w;
+      double2 acc = make_double2(0.0, 0.0);
+      if (m >= n) {
+        const double2* hp = a.HR + el;
+        for (int R = 0; R < nvec; ++R) {
+          double2 t = cmul(ph[R], hp[(size_t)R * ww]);
+          acc = cadd(acc, cscale(t, a.invdeg[R]));
+        }
+        if (m == n) acc = make_double2(acc.x + (-a.ef32), 0.0);
+        fro += (m == n ? 1.0 : 2.0) * (acc.x * acc.x + acc.y * acc.y);
+      }
+      A[el] = acc;
+      V[el] = make_double2(m == n ? 1.0 : 0.0, 0.0);
+    }
+    // block reduction of the Frobenius norm
+    for (int o = 16; o > 0; o >>= 1) fro += __shfl_xor_sync(0xffffffffu, fro, o);
+    if ((tid & 31) == 0) red[tid >> 5] = fro;
+    __syncthreads();
+    if (tid == 0) {
+      double s = 0.0;
+      for (int i = 0; i < bs / 32; ++i) s += red[i];
+      s_tolabs = DBL_EPSILON * 1e-2 * sqrt(s);
+      s_stat = 1;  // not converged until proven
+    }
+    for (int el = tid; el < ww; el += bs) {
+      const int m = el % w, n = el / w;
+      if (m < n) A[el] = cconj(A[n + m * w]);
+    }
+    __syncthreads();
+
+    for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
+      if (tid == 0) s_rotated = 0;
+      __syncthreads();
+      for (int r = 0; r < m2 - 1; ++r) {
+        if (tid < npair) {
+          const int t = tid;
+          int p = (t == 0) ? (m2 - 1) : ((r + t - 1) % (m2 - 1));
+          int q = (r + (m2 - 1 - t) - 1) % (m2 - 1);
+          Rot ro;
+          ro.active = 0;
+          if (p > q) { int x = p; p = q; q = x; }
+          ro.p = p;
+          ro.q = q;
+          if (q < w) {
+            const double aa = A[p + p * w].x, bb = A[q + q * w].x;
+            const double2 c = A[p + q * w];
+            const double ac = hypot(c.x, c.y);
+            const double thr = fmax(0.5 * DBL_EPSILON * sqrt(fabs(aa * bb)), s_tolabs);
+            if (ac > thr && ac > 0.0) {
+              const double zeta = (bb - aa) / (2.0 * ac);
+              double tt;
+              if (fabs(zeta) > 1e150) tt = 0.5 / zeta;
+              else tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+              const double cs = 1.0 / sqrt(1.0 + tt * tt);
+              ro.cs = cs;
+              ro.sn = tt * cs;
+              ro.ex = c.x / ac;
+              ro.ey = c.y / ac;
+              ro.ap = aa - tt * ac;
+              ro.aq = bb + tt * ac;
+              ro.active = 1;
+              s_rotated = 1;
+            }
+          }
+          rot[t] = ro;
+        }
+        __syncthreads();
+        // rows: A <- J^H A
+        for (int it = tid; it < npair * w; it += bs) {
+          const Rot& ro = rot[it / w];
+          if (!ro.active) continue;
+          const int col = it % w;
+          const double2 e = make_double2(ro.ex, ro.ey);
+          const double2 rp = A[ro.p + col * w], rq = A[ro.q + col * w];
+          A[ro.p + col * w] = csub(cscale(rp, ro.cs), cscale(cmul(e, rq), ro.sn));
+          A[ro.q + col * w] = cadd(cscale(cmulc(e, rp), ro.sn), cscale(rq, ro.cs));
+        }
+        __syncthreads();
+        // columns: A <- A J, V <- V J
+        for (int it = tid; it < npair * w; it += bs) {
+          const Rot& ro = rot[it / w];
+          if (!ro.active) continue;
+          const int row = it % w;
+          const double2 e = make_double2(ro.ex, ro.ey);
+          double2 cp = A[row + ro.p * w], cq = A[row + ro.q * w];
+          A[row + ro.p * w] = csub(cscale(cp, ro.cs), cscale(cmulc(e, cq), ro.sn));
+          A[row + ro.q * w] = cadd(cscale(cmul(e, cp), ro.sn), cscale(cq, ro.cs));
+          cp = V[row + ro.p * w];
+          cq = V[row + ro.q * w];
+          V[row + ro.p * w] = csub(cscale(cp, ro.cs), cscale(cmulc(e, cq), ro.sn));
+          V[row + ro.q * w] = cadd(cscale(cmul(e, cp), ro.sn), cscale(cq, ro.cs));
+        }
+        __syncthreads();
+        if (tid < npair) {
+          const Rot& ro = rot[tid];
+          if (ro.active) {
+            A[ro.p + ro.q * w] = make_double2(0.0, 0.0);
+            A[ro.q + ro.p * w] = make_double2(0.0, 0.0);
+            A[ro.p + ro.p * w] = make_double2(ro.ap, 0.0);
+            A[ro.q + ro.q * w] = make_double2(ro.aq, 0.0);
+          }
+        }
+        __syncthreads();
+      }
+      const int any = s_rotated;
+      __syncthreads();
+      if (!any) {
+        if (tid == 0) s_stat = 0;
+        break;
+      }
+    }
+    __syncthreads();
+    // ascending order (ties by index), nocp, gauge
+    if (tid < w) lam[tid] = A[tid + tid * w].x;
+    __syncthreads();
+    if (tid < w) {
+      const double lj = lam[tid];
+      int rank = 0;
+      for (int i = 0; i < w; ++i) {
+        const double li = lam[i];
+        rank += (li < lj || (li == lj && i < tid)) ? 1 : 0;
+      }
+      perm[rank] = tid;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int nocp = -1;
+      for (int i = 0; i < w; ++i) {
+        if (lam[perm[i]] > 0.0) { nocp = i; break; }
+      }
+      int st = s_stat;
+      if (st == 0) {
+        if (nocp < 0) st = 2;
+        else if (a.nv > nocp || a.nc > w - nocp) st = 3;
+      }
+      s_stat = st;
+      s_nocp = nocp < 0 ? w : nocp;
+      a.kstat[k] = st;
+      a.nocp[k] = s_nocp;
+    }
+    __syncthreads();
+    const int nb = a.nv + a.nc;
+    if (s_stat == 0) {
+      const int nocp = s_nocp;
+      for (int it = tid; it < nb * w; it += bs) {
+        const int sel = it / w, m = it % w;
+        const int src = perm[nocp - a.nv + sel];
+        const double2 v0 = V[src * w];
+        const double r = hypot(v0.x, v0.y);
+        double2 g = make_double2(1.0, 0.0);
+        if (r > 0.0) g = make_double2(v0.x / r, -v0.y / r);
+        a.U[((size_t)k * nb + sel) * w + m] = cmul(V[m + src * w], g);
+        if (m == 0) a.eig[(size_t)k * nb + sel] = lam[src] + (sel >= a.nv ? a.scs : 0.0);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+struct VelArgs {
+  const double2* HR;
+  const double* Rcart;
+  const double* Rf32;
+  const double* invdeg;
+  const int* isR0;
+  int nvec, w;
+  const double* kpt;
+  int nk, nv, nc;
+  const double* eig;
+  const double2* U;
+  double eta32;
+  double inv_sqrt2_f32;
+  double2* h;      // [5][N]
+  long long N;
+};
+
+__global__ void __launch_bounds__(kBandsThreads) k_velocity(VelArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int w = a.w, nvec = a.nvec, tid = threadIdx.x, bs = blockDim.x;
+  const int ww = w * w, nb = a.nv + a.nc;
+  double2* ph = reinterpret_cast<double2*>(smem);
+  double2* HX = ph + nvec;          // 3 matrices, column-major
+  double2* Us = HX + 3 * ww;        // nb x w
+  double2* T = Us + nb * w;         // [3][nv][w] = h_alpha * u_v
+  for (int k = blockIdx.x; k < a.nk; k += gridDim.x) {
+    const double kx = a.kpt[3 * k], ky = a.kpt[3 * k + 1], kz = a.kpt[3 * k + 2];
+    for (int R = tid; R < nvec; R += bs) ph[R] = phase_of(kx, ky, kz, a.Rcart + 3 * R);
+    for (int it = tid; it < nb * w; it += bs) Us[it] = a.U[(size_t)k * nb * w + it];
+    __syncthreads();
+    for (int el = tid; el < ww; el += bs) {
+      const int m = el % w, n = el / w;
+      double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+      const double2* hp = a.HR + el;
+      for (int R = 0; R < nvec; ++R) {
+        if (m == n && a.isR0[R]) continue;   // R=0 diagonal zeroed (optics.f90:59-68)
+        const double2 hr = hp[(size_t)R * ww];
+        const double2 p = ph[R];
+        const double inv = a.invdeg[R];
+#pragma unroll
+        for (int al = 0; al < 3; ++al) {
+          const double ra = a.Rf32[3 * R + al];
+          const double2 pre = make_double2(-ra * p.y, ra * p.x);   // (i*R_alpha) * phase
+          acc[al] = cadd(acc[al], cscale(cmul(pre, hr), inv));
+        }
+      }
+      HX[el] = acc[0];
+      HX[ww + el] = acc[1];
+      HX[2 * ww + el] = acc[2];
+    }
+    __syncthreads();
+    // T[al][v][m] = sum_n H_al[m,n] u_v[n]   (matvec, general_subs.f90:132-160)
+    for (int it = tid; it < 3 * a.nv * w; it += bs) {
+      const int m = it % w, v = (it / w) % a.nv, al = it / (w * a.nv);
+      const double2* Hm = HX + al * ww;
+      const double2* uv = Us + v * w;
+      double2 acc = make_double2(0, 0);
+      for (int n = 0; n < w; ++n) acc = cadd(acc, cmul(Hm[m + n * w], uv[n]));
+      T[it] = acc;
+    }
+    __syncthreads();
+    // h = Re(1/(dE + i eta)) * <c| H_al |v>   for the (c, v) pairs of this k
+    for (int it = tid; it < a.nc * a.nv; it += bs) {
+      const int c = it / a.nv, v = it % a.nv;
+      const double2* uc = Us + (a.nv + c) * w;
+      const double de = a.eig[(size_t)k * nb + a.nv + c] - a.eig[(size_t)k * nb + v];
+      const double factor = de / (de * de + a.eta32 * a.eta32);
+      double2 hr[3];
+#pragma unroll
+      for (int al = 0; al < 3; ++al) {
+        const double2* t = T + (al * a.nv + v) * w;
+        double2 acc = make_double2(0, 0);
+        for (int m = 0; m < w; ++m) acc = cadd(acc, cmulc(uc[m], t[m]));
+        hr[al] = cscale(acc, factor);
+      }
+      const long long i = (long long)k * a.nc * a.nv + c * a.nv + v;
+      a.h[i] = hr[0];
+      a.h[a.N + i] = hr[1];
+      a.h[2 * a.N + i] = hr[2];
+      const double s = a.inv_sqrt2_f32;
+      a.h[3 * a.N + i] = cscale(make_double2(hr[0].x - hr[1].y, hr[0].y + hr[1].x), s);
+      a.h[4 * a.N + i] = cscale(make_double2(hr[0].x + hr[1].y, hr[0].y - hr[1].x), s);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// vecres rows (bse_solver-tool-diel.f90:379-393); key = column 7 (float32 dE)
+__global__ void k_sp_rows(const double* kpt, const double* eig, const int* nocp, const double2* h,
+                          int nk, int nv, int nc, long long N, float* rows, float* key, int* idx) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int ncv = nc * nv, nb = nc + nv;
+  const int k = (int)(i / ncv), c = (int)((i % ncv) / nv), v = (int)(i % nv);
+  const double2 hx = h[i], hy = h[N + i], hz = h[2 * N + i], hp = h[3 * N + i], hm = h[4 * N + i];
+  float* r = rows + i * 15;
+  r[0] = (float)kpt[3 * k];
+  r[1] = (float)kpt[3 * k + 1];
+  r[2] = (float)kpt[3 * k + 2];
+  r[3] = (float)nocp[k];
+  r[4] = (float)(nocp[k] - nv + (nv + c + 1));
+  r[5] = (float)(nocp[k] - nv + (v + 1));
+  r[6] = (float)(eig[(size_t)k * nb + nv + c] - eig[(size_t)k * nb + v]);
+  r[7] = (float)(hx.x * hx.x + hx.y * hx.y);
+  r[8] = (float)(hy.x * hy.x + hy.y * hy.y);
+  r[9] = (float)(hz.x * hz.x + hz.y * hz.y);
+  r[10] = (float)(hx.x * hy.x + hx.y * hy.y);
+  r[11] = (float)(hx.x * hz.x + hx.y * hz.y);
+  r[12] = (float)(hy.x * hz.x + hy.y * hz.y);
+  r[13] = (float)(hp.x * hp.x + hp.y * hp.y);
+  r[14] = (float)(hm.x * hm.x + hm.y * hm.y);
+  key[i] = r[6];
+  idx[i] = (int)i;
+}
+
+__global__ void k_sp_gather(const float* rows, const int* order, long long N, float* out) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const float* r = rows + (long long)order[i] * 15;
+#pragma unroll
+  for (int c = 0; c < 15; ++c) out[c * N + i] = r[c];
+}
+
+}  // namespace
+
+static size_t bands_smem(int w, int nvec) {
+  const int ww = w * w, m2 = w + (w & 1);
+  return (size_t)nvec * 16 + 2 * (size_t)ww * 16 + (size_t)(m2 / 2) * sizeof(Rot) + (size_t)w * 8 +
+         (size_t)(w + (w & 1)) * 4 + 64 * 8;
+}
+
+int launch_bands(wtbg_ctx* ctx, bool q_mesh) {
+  const int w = ctx->w;
+  BandsArgs a;
+  a.HR = ctx->HR.as<double2>();
+  a.Rcart = ctx->Rcart.as<double>();
+  a.invdeg = ctx->invdeg.as<double>();
+  a.nvec = ctx->nvec;
+  a.w = w;
+  a.nk = ctx->nk;
+  a.ef32 = (double)(float)ctx->efermi;
+  a.scs = ctx->scs;
+  a.nv = ctx->nv;
+  a.nc = ctx->nc;
+  if (q_mesh) {
+    a.kpt = ctx->kptq.as<double>();
+    a.eig = ctx->eigq.as<double>();
+    a.U = ctx->Uq.as<double2>();
+    a.nocp = ctx->nocpq.as<int>();
+  } else {
+    a.kpt = ctx->kpt.as<double>();
+    a.eig = ctx->eig.as<double>();
+    a.U = ctx->U.as<double2>();
+    a.nocp = ctx->nocp.as<int>();
+  }
+  a.kstat = ctx->kstat.as<int>();
+  const size_t smem = bands_smem(w, ctx->nvec);
+  if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bands: model too large for shared memory");
+  CK(cudaFuncSetAttribute(k_bands, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int grid = ctx->nk;
+  k_bands<<<grid, kBandsThreads, smem, ctx->stream>>>(a);
+  CKL("k_bands");
+  return 0;
+}
+
+int launch_velocity(wtbg_ctx* ctx, double eta32) {
+  const int w = ctx->w, nb = ctx->nv + ctx->nc;
+  VelArgs a;
+  a.HR = ctx->HR.as<double2>();
+  a.Rcart = ctx->Rcart.as<double>();
+  a.Rf32 = ctx->Rf32.as<double>();
+  a.invdeg = ctx->invdeg.as<double>();
+  a.isR0 = ctx->isR0.as<int>();
+  a.nvec = ctx->nvec;
+  a.w = w;
+  a.kpt = ctx->kpt.as<double>();
+  a.nk = ctx->nk;
+  a.nv = ctx->nv;
+  a.nc = ctx->nc;
+  a.eig = ctx->eig.as<double>();
+  a.U = ctx->U.as<double2>();
+  a.eta32 = eta32;
+  a.inv_sqrt2_f32 = (double)(1.0f / sqrtf(2.0f));
+  a.h = ctx->h.as<double2>();
+  a.N = ctx->N;
+  const size_t smem = (size_t)ctx->nvec * 16 + 3 * (size_t)w * w * 16 + (size_t)nb * w * 16 +
+                      3 * (size_t)ctx->nv * w * 16;
+  if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "velocity: model too large for shared memory");
+  CK(cudaFuncSetAttribute(k_velocity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_velocity<<<ctx->nk, kBandsThreads, smem, ctx->stream>>>(a);
+  CKL("k_velocity");
+  return 0;
+}
+
+int launch_sp_table(wtbg_ctx* ctx, float* d_out) {
+  const long long N = ctx->N;
+  // scratch: rows (N*15 f32), key_in, key_out (N f32), idx_in, idx_out (N int), cub temp
+  size_t cub_bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, (const float*)nullptr, (float*)nullptr,
+                                  (const int*)nullptr, (int*)nullptr, (int)N);
+  const size_t rows_b = (size_t)N * 15 * 4, vec_b = (size_t)N * 4;
+  const size_t total = rows_b + 4 * vec_b + cub_bytes + 1024;
+  ENSURE(ctx->tmp, total);
+  char* base = ctx->tmp.as<char>();
+  float* rows = reinterpret_cast<float*>(base);
+  float* kin = reinterpret_cast<float*>(base + rows_b);
+  float* kout = kin + N;
+  int* iin = reinterpret_cast<int*>(kout + N);
+  int* iout = iin + N;
+  void* ctmp = reinterpret_cast<void*>(((uintptr_t)(iout + N) + 255) & ~(uintptr_t)255);
+  const int th = 256;
+  const int gr = (int)((N + th - 1) / th);
+  k_sp_rows<<<gr, th, 0, ctx->stream>>>(ctx->kpt.as<double>(), ctx->eig.as<double>(), ctx->nocp.as<int>(),
+                                         ctx->h.as<double2>(), ctx->nk, ctx->nv, ctx->nc, N, rows, kin, iin);
+  CKL("k_sp_rows");
+  // LSD radix sort is stable: equal keys keep their original (quantumnumbers2) order,
+  // which is what the strict-greater bubble sort produces.
+  CK(cub::DeviceRadixSort::SortPairs(ctmp, cub_bytes, kin, kout, iin, iout, (int)N, 0, 32, ctx->stream));
+  k_sp_gather<<<gr, th, 0, ctx->stream>>>(rows, iout, N, d_out);
+  CKL("k_sp_gather");
+  return 0;
+}

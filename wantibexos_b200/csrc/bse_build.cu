@@ -1,0 +1,290 @@
+// Kernel (b): the exciton (BSE) kernel build.
+//
+// Reference: matrizelbse (subroutines/bse_subs.f90:2-124) called for every j >= i
+// (subprograms/bse_solver-tool-diel.f90:431-458), and matrizelbsekq
+// (subroutines/bse_subs_kpath.f90:1-208) for a centre-of-mass momentum Q.
+// Element (i, j) with i = (k, c, v), j = (k', c', v') in quantumnumbers2 order:
+//     H_ij = W(k - k') <c_i|c_j> <v_i|v_j>            (i != j; <a|b> = sum_m conj(a_m) b_m)
+//     H_ii = (E_c - E_v) + W(0)
+//   and for Q != 0 additionally  - W(Q) <c_i^{k+Q}|v_i> <v_j|c_j^{k'+Q}>  (exchange).
+// The same expression gives both triangles of the Hermitian matrix, so the device stores
+// the LOWER triangle (column-major, ld = N) that the tridiagonalisation reads.
+//
+// B200 design: one CTA per (k-block, k'-block) tile of the lower triangle.  The overlaps
+// <c|c'> and <v|v'> of the tile are small complex GEMMs (K = w) computed once per tile in
+// shared memory; the Coulomb factor W(k-k') is evaluated once per (k, k') pair; the
+// Kronecker expansion into the (nc*nv) x (nc*nv) blocks happens in the store loop, so every
+// element of the 16*N^2-byte matrix is written to HBM exactly once with coalesced 16-byte
+// stores.  The kernel is bound by the HBM write of the matrix.
+#include <cmath>
+
+#include "common.cuh"
+#include "coulomb.cuh"
+
+namespace {
+
+constexpr int kBuildThreads = 256;
+
+struct BuildArgs {
+  const double2* Uc;    // conduction eigenvectors [nk][nb][w] (k+Q mesh for Q != 0)
+  const double2* Uv;    // valence eigenvectors   [nk][nb][w]
+  const double* eigc;   // [nk][nb]
+  const double* eigv;   // [nk][nb]
+  const double* kpt;    // [nk][3]
+  int nk, nv, nc, w, nb;
+  CoulombDev P;
+  int exch;
+  double vq;
+  const double2* vcv;   // [N] <c^{k+Q}|v> per state (exchange only)
+  double2* H;
+  long long N;
+  int TK, nbk;
+};
+
+__global__ void __launch_bounds__(kBuildThreads) k_bse_build(BuildArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const long long t = blockIdx.x;
+  int bi = (int)floor((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while ((long long)(bi + 1) * (bi + 2) / 2 <= t) ++bi;
+  while ((long long)bi * (bi + 1) / 2 > t) --bi;
+  const int bj = (int)(t - (long long)bi * (bi + 1) / 2);
+  const int TK = a.TK, nc = a.nc, nv = a.nv, w = a.w, nb = a.nb, ncv = nc * nv;
+  const int kr0 = bi * TK, kc0 = bj * TK;
+  const int nkr = min(TK, a.nk - kr0), nkc = min(TK, a.nk - kc0);
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const int RC = TK * nc, RV = TK * nv;
+
+  double2* UcR = reinterpret_cast<double2*>(smem);
+  double2* UcC = UcR + RC * w;
+  double2* UvR = UcC + RC * w;
+  double2* UvC = UvR + RV * w;
+  double2* Mc = UvC + RV * w;          // col-major [RC x RC]
+  double2* Mv = Mc + RC * RC;          // col-major [RV x RV]
+  double* Vt = reinterpret_cast<double*>(Mv + RV * RV);   // [kc][kr]
+  double* dE = Vt + TK * TK;           // [TK*ncv]
+  int* colinfo = reinterpret_cast<int*>(dE + TK * ncv);  // packed (kc, c', v') per tile column
+
+  for (int it = tid; it < RC * w; it += bs) {
+    const int kk = it / (nc * w), rem = it % (nc * w), c = rem / w, m = rem % w;
+    UcR[it] = (kk < nkr) ? a.Uc[((size_t)(kr0 + kk) * nb + nv + c) * w + m] : make_double2(0, 0);
+    UcC[it] = (kk < nkc) ? a.Uc[((size_t)(kc0 + kk) * nb + nv + c) * w + m] : make_double2(0, 0);
+  }
+  for (int it = tid; it < RV * w; it += bs) {
+    const int kk = it / (nv * w), rem = it % (nv * w), v = rem / w, m = rem % w;
+    UvR[it] = (kk < nkr) ? a.Uv[((size_t)(kr0 + kk) * nb + v) * w + m] : make_double2(0, 0);
+    UvC[it] = (kk < nkc) ? a.Uv[((size_t)(kc0 + kk) * nb + v) * w + m] : make_double2(0, 0);
+  }
+  for (int it = tid; it < TK * TK; it += bs) {
+    const int kc = it / TK, kr = it % TK;
+    double v = 0.0;
+    if (kr < nkr && kc < nkc) {
+      const double* k1 = a.kpt + 3 * (size_t)(kr0 + kr);
+      const double* k2 = a.kpt + 3 * (size_t)(kc0 + kc);
+      v = coulomb_eval(a.P, k1[0] - k2[0], k1[1] - k2[1], k1[2] - k2[2]);
+    }
+    Vt[it] = v;
+  }
+  for (int it = tid; it < TK * ncv; it += bs) {
+    const int kr = it / ncv, c = (it % ncv) / nv, v = it % nv;
+    dE[it] = (kr < nkr) ? a.eigc[(size_t)(kr0 + kr) * nb + nv + c] - a.eigv[(size_t)(kr0 + kr) * nb + v] : 0.0;
+    colinfo[it] = (kr << 16) | (c << 8) | v;
+  }
+  __syncthreads();
+  for (int it = tid; it < RC * RC; it += bs) {
+    const int col = it / RC, row = it % RC;
+    const double2* x = UcR + row * w;
+    const double2* y = UcC + col * w;
+    double2 acc = make_double2(0, 0);
+    for (int m = 0; m < w; ++m) acc = cadd(acc, cmulc(x[m], y[m]));
+    Mc[it] = acc;
+  }
+  for (int it = tid; it < RV * RV; it += bs) {
+    const int col = it / RV, row = it % RV;
+    const double2* x = UvR + row * w;
+    const double2* y = UvC + col * w;
+    double2 acc = make_double2(0, 0);
+    for (int m = 0; m < w; ++m) acc = cadd(acc, cmulc(x[m], y[m]));
+    Mv[it] = acc;
+  }
+  __syncthreads();
+
+  const int rows = nkr * ncv, cols = nkc * ncv;
+  const long long N = a.N;
+  const long long I0 = (long long)kr0 * ncv, J0 = (long long)kc0 * ncv;
+  const bool diag_tile = (bi == bj);
+  if (tid >= (bs / rows) * rows) return;
+  const int ii = tid % rows;
+  const int njp = bs / rows;
+  const int kr = ii / ncv, c = (ii % ncv) / nv, v = ii % nv;
+  const long long I = I0 + ii;
+  const double2 vcvI = a.exch ? a.vcv[I] : make_double2(0, 0);
+  const double dEi = dE[ii];
+  const double2* Mc_r = Mc + kr * nc + c;   // + col*RC
+  const double2* Mv_r = Mv + kr * nv + v;   // + col*RV
+  double2* Hcol = a.H + I;
+  for (int jj = tid / rows; jj < cols; jj += njp) {
+    const long long J = J0 + jj;
+    if (diag_tile && I < J) continue;
+    const int ci = colinfo[jj];
+    const int kc = ci >> 16, cc = (ci >> 8) & 0xff, vv = ci & 0xff;
+    const double vk = Vt[kc * TK + kr];
+    double2 val;
+    if (I == J) {
+      val = make_double2(dEi + vk, 0.0);
+    } else {
+      val = cmul(cscale(Mc_r[(kc * nc + cc) * RC], vk), Mv_r[(kc * nv + vv) * RV]);
+    }
+    if (a.exch) {
+      // vvc_j = conj(<c_j|v_j>) exactly
+      const double2 t2 = cmul(cscale(vcvI, a.vq), cconj(a.vcv[J]));
+      val = csub(val, t2);
+    }
+    Hcol[J * N] = val;
+  }
+}
+
+__global__ void k_exchange_overlap(const double2* Uq, const double2* U, int nk, int nv, int nc, int w,
+                                   double2* vcv) {
+  const long long N = (long long)nk * nc * nv;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int nb = nc + nv, ncv = nc * nv;
+  const int k = (int)(i / ncv), c = (int)((i % ncv) / nv), v = (int)(i % nv);
+  const double2* x = Uq + ((size_t)k * nb + nv + c) * w;
+  const double2* y = U + ((size_t)k * nb + v) * w;
+  double2 acc = make_double2(0, 0);
+  for (int m = 0; m < w; ++m) acc = cadd(acc, cmulc(x[m], y[m]));
+  vcv[i] = acc;
+}
+
+size_t build_smem(int TK, int nc, int nv, int w) {
+  const int RC = TK * nc, RV = TK * nv, ncv = nc * nv;
+  return 16ull * (2ull * RC * w + 2ull * RV * w + (size_t)RC * RC + (size_t)RV * RV) + 8ull * TK * TK +
+         8ull * TK * ncv + 4ull * TK * ncv + 64;
+}
+
+}  // namespace
+
+CoulombDev make_coulomb_dev(const wtbg_coulomb* p, const double* L) {
+  CoulombDev P{};
+  P.type = p->coultype;
+  P.ktol = p->ktol;
+  const double a1[3] = {L[0], L[1], L[2]}, a2[3] = {L[3], L[4], L[5]}, a3[3] = {L[6], L[7], L[8]};
+  const double vx[3] = {a1[1] * a2[2] - a1[2] * a2[1], a1[2] * a2[0] - a1[0] * a2[2],
+                        a1[0] * a2[1] - a1[1] * a2[0]};
+  const double vc2 = sqrt((vx[0] * vx[0]) + (vx[1] * vx[1]) + (vx[2] * vx[2]));
+  const double vc3 = fabs(vx[0] * a3[0] + vx[1] * a3[1] + vx[2] * a3[2]);
+  const int nkt = p->ngrid[0] * p->ngrid[1] * p->ngrid[2];
+  P.vbz2d = 1.0 / (nkt * vc2);
+  P.vbz3d = 1.0 / (nkt * vc3);
+  const float cic32 = -(0.0904756f) * 1000.0f;
+  P.cic = (double)cic32;
+  const double pi32 = (double)acosf(-1.0f);
+  // V2DRK (coulomb_pot.f90:311-319)
+  const double epar = p->ediel[1], et = p->ediel[0], eb = p->ediel[2];
+  P.eta = sqrt(epar / p->ez);
+  P.kappa = sqrt(epar * p->ez);
+  P.pb = (eb - P.kappa) / (eb + P.kappa);
+  P.pt = (et - P.kappa) / (et + P.kappa);
+  P.lc = p->lc;
+  P.w = p->w;
+  P.r0 = p->r0;
+  P.ez = p->ez;
+  // V2DK (coulomb_pot.f90:25-42)
+  const double n1 = sqrt(a1[0] * a1[0] + a1[1] * a1[1] + a1[2] * a1[2]);
+  const double n2 = sqrt(a2[0] * a2[0] + a2[1] * a2[1] + a2[2] * a2[2]);
+  const double n3 = sqrt(a3[0] * a3[0] + a3[1] * a3[1] + a3[2] * a3[2]);
+  const double a0 = 0.5 * (n1 + n2);
+  P.v2dk_r0 = ((p->ediel[1] - 1.0) * p->lc) / (p->ediel[0] + p->ediel[2]);
+  const double g1 = (double)(p->ngrid[0] * p->ngrid[1]);
+  const double auxi = (2. * pi32 * P.v2dk_r0) / (a0 * sqrt(g1));
+  P.v2dk_ed = (p->ediel[0] + p->ediel[2]) / (2.0);
+  const double alpha1 = (double)1.76f, alpha2 = 1.0, alpha3 = 0.0;
+  P.v2dk_q0 = P.vbz2d * (P.cic / P.v2dk_ed) * (a0 * sqrt(g1) / (2. * pi32)) *
+              (alpha1 + auxi * alpha2 + alpha3 * auxi * auxi);
+  // V3D / V3DL
+  P.ed3 = (p->coultype == WTBG_V3DL) ? p->ediel[1] : 1.0;
+  // V2DT
+  P.rc = 0.5 * a3[2];
+  // V0DT
+  double cr = n1 < n2 ? n1 : n2;
+  cr = cr < n3 ? cr : n3;
+  P.cr = 0.5 * cr;
+  // V1DT q -> 0 value (coulomb_pot.f90:414)
+  P.v1dt_q0 = (P.vbz3d * P.cic) * ((p->lc * p->lc) / 16.0) * (2.0 * log(p->lc) - 1.0);
+  return P;
+}
+
+// Builds the BSE matrix for Q = 0 (q4 == nullptr) or for a centre-of-mass momentum q4.
+int launch_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p, const double* q4) {
+  const int nc = ctx->nc, nv = ctx->nv, w = ctx->w, ncv = nc * nv;
+  if (ncv > 256) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bse_build: nc*nv > 256");
+  int TK = 128 / ncv;
+  if (TK < 1) TK = 1;
+  while (TK > 1 && build_smem(TK, nc, nv, w) > 96 * 1024) --TK;
+  const size_t smem = build_smem(TK, nc, nv, w);
+  if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bse_build: tile does not fit in shared memory");
+  BuildArgs a;
+  const bool q = (q4 != nullptr);
+  a.Uc = q ? ctx->Uq.as<double2>() : ctx->U.as<double2>();
+  a.Uv = ctx->U.as<double2>();
+  a.eigc = q ? ctx->eigq.as<double>() : ctx->eig.as<double>();
+  a.eigv = ctx->eig.as<double>();
+  a.kpt = ctx->kpt.as<double>();
+  a.nk = ctx->nk;
+  a.nv = nv;
+  a.nc = nc;
+  a.w = w;
+  a.nb = nc + nv;
+  a.P = make_coulomb_dev(p, ctx->rlat);
+  a.exch = 0;
+  a.vq = 0.0;
+  a.vcv = nullptr;
+  a.H = ctx->H.as<double2>();
+  a.N = ctx->N;
+  a.TK = TK;
+  a.nbk = (ctx->nk + TK - 1) / TK;
+  if (q) {
+    const double modq = sqrt((q4[1]) * (q4[1]) + (q4[2]) * (q4[2]) + (q4[3]) * (q4[3]));
+    if (modq != 0.0) {
+      // W(Q) = coulomb(vq, 0) on the host (single value, same formulas)
+      ENSURE(ctx->tmp2, (size_t)ctx->N * 16 + 64);
+      a.vcv = ctx->tmp2.as<double2>();
+      const int th = 256;
+      k_exchange_overlap<<<(int)((ctx->N + th - 1) / th), th, 0, ctx->stream>>>(
+          ctx->Uq.as<double2>(), ctx->U.as<double2>(), ctx->nk, nv, nc, w, ctx->tmp2.as<double2>());
+      CKL("k_exchange_overlap");
+      a.exch = 1;
+    }
+  }
+  if (a.exch) {
+    // evaluate W(Q) with the device formula for exact agreement with the in-kernel values
+    extern int eval_coulomb_single(wtbg_ctx*, const CoulombDev&, double, double, double, double*);
+    double vq = 0.0;
+    int r = eval_coulomb_single(ctx, a.P, q4[1], q4[2], q4[3], &vq);
+    if (r) return r;
+    a.vq = vq;
+  }
+  CK(cudaFuncSetAttribute(k_bse_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long ntile = (long long)a.nbk * (a.nbk + 1) / 2;
+  if (ntile > 0x7fffffffLL) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bse_build: too many tiles");
+  k_bse_build<<<(unsigned)ntile, kBuildThreads, smem, ctx->stream>>>(a);
+  CKL("k_bse_build");
+  return 0;
+}
+
+namespace {
+__global__ void k_coulomb_single(CoulombDev P, double x, double y, double z, double* out) {
+  *out = coulomb_eval(P, x, y, z);
+}
+}  // namespace
+
+int eval_coulomb_single(wtbg_ctx* ctx, const CoulombDev& P, double x, double y, double z, double* out) {
+  ENSURE(ctx->istat, 64);
+  double* d = ctx->istat.as<double>();
+  k_coulomb_single<<<1, 1, 0, ctx->stream>>>(P, x, y, z, d);
+  CKL("k_coulomb_single");
+  CK(cudaMemcpyAsync(out, d, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}

@@ -1,0 +1,133 @@
+// Shared definitions for libwtbgpu.so (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/wtbgpu.h"
+
+#define WTBG_MAX_W 48          // largest orbital count of the per-k shared-memory eigensolver
+#define WTBG_HEMV_TILE 64      // tile edge of the Hermitian matrix-vector kernel
+#define WTBG_PANEL 32          // Householder panel width of the tridiagonalisation
+
+// Device buffer that only grows.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+struct wtbg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0.0;
+  std::string err;
+
+  // model (hamiltonian_input_variables)
+  int w = 0, nvec = 0;
+  double rlat[9] = {0};   // row-major rlat[i*3+c] = a_i component c
+  double efermi = 0.0, scs = 0.0;
+  DevBuf HR;      // [nvec][n][m] double2 : H_mn(R)
+  DevBuf Rcart;   // [nvec][3] double : Cartesian R in the reference evaluation order
+  DevBuf Rf32;    // [nvec][3] double : float32-rounded Cartesian R (velocity prefactor)
+  DevBuf invdeg;  // [nvec] double : 1/deg(R)
+  DevBuf isR0;    // [nvec] int
+
+  // k-mesh bands
+  int nk = 0, nv = 0, nc = 0;
+  DevBuf kpt;     // [nk][3]
+  DevBuf eig;     // [nk][nc+nv]
+  DevBuf U;       // [nk][nc+nv][w] double2
+  DevBuf nocp;    // [nk] int
+  DevBuf kstat;   // [nk] int (per-k status)
+  bool have_bands = false;
+
+  // k+Q bands (exciton band structure)
+  DevBuf kptq, eigq, Uq, nocpq;
+
+  // velocity
+  DevBuf h;       // [5][N] double2
+  bool have_velocity = false;
+
+  // BSE matrix and dense-solve state
+  long long N = 0;
+  DevBuf H;       // N*N double2, lower triangle column-major
+  bool have_matrix = false;
+  DevBuf d, e, tau, g;     // tridiagonal, reflector scalars, g = Q^T h  ([5][N] double2)
+  DevBuf Wp;               // panel W (N x PANEL) double2
+  DevBuf slots;            // hemv partials
+  DevBuf part;             // small partial-reduction area
+  DevBuf scal;             // per-column scalars
+  DevBuf yv;               // hemv result
+  DevBuf lam;              // eigenvalues
+  DevBuf ws;               // inverse-iteration workspace
+  DevBuf act;              // oscillator strengths [8][N]
+  DevBuf zsel;             // selected tridiagonal eigenvectors (for eigvecs)
+  DevBuf csz;              // cluster size per eigenvalue index (leaders), 0 otherwise
+  std::vector<double> lam_host;
+  std::vector<int> csize_host;
+  double tnorm = 0.0;
+  bool have_solution = false;
+
+  // spectrum
+  DevBuf sp_in, sp_out, sp_om;
+
+  // misc
+  DevBuf tmp, tmp2, istat;
+};
+
+// error handling
+int set_err(wtbg_ctx* c, int code, const std::string& msg);
+int cuda_fail(wtbg_ctx* c, cudaError_t e, const char* where);
+int ensure(wtbg_ctx* c, DevBuf& b, size_t bytes);
+
+#define CK(call)                                                  \
+  do {                                                            \
+    cudaError_t _e = (call);                                      \
+    if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call);      \
+  } while (0)
+
+#define CKL(where)                                                \
+  do {                                                            \
+    cudaError_t _e = cudaGetLastError();                          \
+    if (_e != cudaSuccess) return cuda_fail(ctx, _e, where);      \
+  } while (0)
+
+#define ENSURE(buf, bytes)                                        \
+  do {                                                            \
+    int _r = ensure(ctx, (buf), (bytes));                         \
+    if (_r) return _r;                                            \
+  } while (0)
+
+// ---- complex helpers (double2 = re, im)
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // conj(a)*b
+  return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) {
+  return make_double2(a.x - b.x, a.y - b.y);
+}
+__host__ __device__ __forceinline__ double2 cscale(double2 a, double s) {
+  return make_double2(a.x * s, a.y * s);
+}
+__host__ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+
+// ---- kernel launchers (implemented in the .cu files)
+int launch_bands(wtbg_ctx* ctx, bool q_mesh);
+int launch_velocity(wtbg_ctx* ctx, double eta_f32);
+int launch_sp_table(wtbg_ctx* ctx, float* d_out);
+int launch_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p, const double* q4);
+int run_tridiagonalise(wtbg_ctx* ctx);
+int run_tridiagonal_solve(wtbg_ctx* ctx, int dtfull, int cpol, bool vectors);
+int run_eigvecs(wtbg_ctx* ctx, int n0, int n1, double2* d_out);
+int launch_spectrum(wtbg_ctx* ctx, int n, const double* d_e, const double* d_f, const int* ngrid,
+                    double vcell3d, double ebse0, double ebsef, double numbse, double sme,
+                    int renorm, double spinf, double* d_om, float* d_eps);

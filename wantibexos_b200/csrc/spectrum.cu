@@ -1,0 +1,117 @@
+// Kernel (d): broadened dielectric function of the BSE spectrum.
+//
+// Reference: bsedielraw (subprograms/bse_diel-tool.f90:137-210) calling optdiel
+// (subroutines/optics.f90:160-244), avgsme (:302-324) and imagrenorm (:327-390):
+//   eta   = CSHIFT + 10 * sum_{i>=2}(E_i - E_{i-1}) / N          (summed in order)
+//   c     = float32(180.90) / (float32(nk) * V_cell)
+//   Re eps(w) = delta + c * sum_n f_n (E_n - w) / ((w - E_n)^2 + eta^2)
+//   Im eps(w) =         c * sum_n f_n  eta      / ((w - E_n)^2 + eta^2)
+//   then (RNMD) Im is zeroed below E_1 - float32(0.15) and shifted down by its value at
+//   the next grid point (clamped at 0), and every value is written as real(spinf * x).
+// One warp per photon energy reduces over the excitons with shuffles; the six tensor
+// components share the two divisions of each (w, n) term.
+#include "common.cuh"
+
+namespace {
+
+__global__ void k_avgsme(const double* e, int n, double sme, double* eta_out) {
+  // sequential, in the reference's order (one thread)
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0.0;
+  for (int i = 1; i < n; ++i) s = s + e[i] - e[i - 1];
+  *eta_out = 10.0 * (s / (double)n) + sme;
+}
+
+__global__ void __launch_bounds__(256) k_spectrum(const double* __restrict__ E, const double* __restrict__ F, int n,
+                                                  const double* __restrict__ eta_p, double ebse0, double ebsef,
+                                                  double numbse, int nw, double caux, double* om, double* re,
+                                                  double* im) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= nw) return;
+  const int j = warp + 1;
+  const double w = ebse0 + (((ebsef - ebse0) * (j - 1)) / (numbse - 1.));
+  const double eta = *eta_p;
+  const double eta2 = eta * eta;
+  double r[6] = {0, 0, 0, 0, 0, 0}, a[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = lane; i < n; i += 32) {
+    const double e = E[i];
+    const double eaux = ((w - e) * (w - e)) + eta2;
+    const double d1 = (e - w) / eaux;
+    const double d2 = eta / eaux;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      const double f = F[(long long)c * n + i];
+      r[c] += f * d1;
+      a[c] += f * d2;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      r[c] += __shfl_xor_sync(0xffffffffu, r[c], o);
+      a[c] += __shfl_xor_sync(0xffffffffu, a[c], o);
+    }
+  }
+  if (lane == 0) {
+    om[warp] = w;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      const double delta = (c < 3) ? 1.0 : 0.0;
+      re[(long long)c * nw + warp] = delta + (r[c] * caux);
+      im[(long long)c * nw + warp] = a[c] * caux;
+    }
+  }
+}
+
+// imagrenorm per component + real(spinf*x) output, eps(nw,2,6)
+__global__ void k_renorm_out(const double* E, const double* om, const double* re, double* im, int nw, int renorm,
+                             double spinf, float* eps) {
+  const int c = threadIdx.x;
+  if (c >= 6) return;
+  double* ic = im + (long long)c * nw;
+  if (renorm) {
+    const double aux = E[0] - (double)0.15f;
+    if (!(aux <= 0.000)) {
+      int ibegin = 1;
+      for (int i = 1; i <= nw; ++i) {
+        if (om[i - 1] <= aux) ibegin = i;
+        else break;
+      }
+      const double aux3 = (ibegin < nw) ? ic[ibegin] : 0.0;   // dielf(ibegin+1,3)
+      for (int i = 1; i <= ibegin; ++i) ic[i - 1] = 0.0;
+      for (int i = ibegin + 1; i <= nw; ++i) {
+        const double v = ic[i - 1] - aux3;
+        ic[i - 1] = (v < 0.0) ? 0.0 : v;
+      }
+    }
+  }
+  for (int i = 0; i < nw; ++i) {
+    eps[(long long)i + (long long)nw * (0 + 2 * c)] = (float)(spinf * re[(long long)c * nw + i]);
+    eps[(long long)i + (long long)nw * (1 + 2 * c)] = (float)(spinf * ic[i]);
+  }
+}
+
+}  // namespace
+
+int launch_spectrum(wtbg_ctx* ctx, int n, const double* d_e, const double* d_f, const int* ngrid, double vcell3d,
+                    double ebse0, double ebsef, double numbse, double sme, int renorm, double spinf, double* d_om,
+                    float* d_eps) {
+  const int nw = (int)numbse;
+  ENSURE(ctx->sp_out, (size_t)12 * nw * 8 + 64);
+  double* re = ctx->sp_out.as<double>();
+  double* im = re + 6 * (size_t)nw;
+  double* eta = im + 6 * (size_t)nw;
+  const double baux = (double)(float)(ngrid[0] * ngrid[1] * ngrid[2]) * vcell3d;
+  const double caux = (double)180.90f / (baux * 1.0);
+  k_avgsme<<<1, 32, 0, ctx->stream>>>(d_e, n, sme, eta);
+  CKL("k_avgsme");
+  const int threads = 256;
+  const int blocks = (nw * 32 + threads - 1) / threads;
+  k_spectrum<<<blocks, threads, 0, ctx->stream>>>(d_e, d_f, n, eta, ebse0, ebsef, numbse, nw, caux, d_om, re, im);
+  CKL("k_spectrum");
+  k_renorm_out<<<1, 32, 0, ctx->stream>>>(d_e, d_om, re, im, nw, renorm, spinf, d_eps);
+  CKL("k_renorm_out");
+  return 0;
+}

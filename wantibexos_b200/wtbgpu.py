@@ -1,0 +1,224 @@
+"""ctypes binding of libwtbgpu.so (the C-ABI declared in include/wtbgpu.h).
+
+This is the Python view of the same entry points a Fortran ISO_C_BINDING interface binds;
+tests and the benchmark drive the library through it.  There is no fallback: if the
+shared library is missing or no CUDA device is present, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwtbgpu.so")
+
+COULOMB_TYPES = {"V2DK": 1, "V3D": 2, "V3DL": 3, "V2DT": 4, "V2DT2": 5, "V2DOH": 6,
+                 "V2DRK": 7, "V1DT": 8, "V0DT": 9}
+
+# every entry point of include/wtbgpu.h
+EXPORTS = ["wtbg_create", "wtbg_destroy", "wtbg_error_string", "wtbg_last_error",
+           "wtbg_last_device_ms", "wtbg_set_model", "wtbg_bands", "wtbg_velocity",
+           "wtbg_sp_table", "wtbg_bse_build", "wtbg_bse_get_matrix", "wtbg_bse_solve",
+           "wtbg_bse_eigvecs", "wtbg_spectrum", "wtbg_bse_q_eigenvalues"]
+
+
+class WtbgError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"wtbg status {status}: {message}")
+        self.status = status
+
+
+class Coulomb(C.Structure):
+    _fields_ = [("coultype", C.c_int), ("ngrid", C.c_int * 3), ("ktol", C.c_double),
+                ("ediel", C.c_double * 3), ("lc", C.c_double), ("ez", C.c_double),
+                ("w", C.c_double), ("r0", C.c_double)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libwtbgpu.so and declare the signatures (raises if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built (run python -m wantibexos_b200.build)")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int)
+    fp = C.POINTER(C.c_float)
+    sig = {
+        "wtbg_create": (C.c_int, [C.POINTER(P), C.c_int]),
+        "wtbg_destroy": (C.c_int, [P]),
+        "wtbg_error_string": (C.c_char_p, [C.c_int]),
+        "wtbg_last_error": (C.c_char_p, [P]),
+        "wtbg_last_device_ms": (C.c_double, [P]),
+        "wtbg_set_model": (C.c_int, [P, C.c_int, C.c_int, dp, dp, ip, ip, dp, C.c_double, C.c_double]),
+        "wtbg_bands": (C.c_int, [P, C.c_int, dp, C.c_int, C.c_int, dp, dp, ip, dp]),
+        "wtbg_velocity": (C.c_int, [P, C.c_double, dp]),
+        "wtbg_sp_table": (C.c_int, [P, fp]),
+        "wtbg_bse_build": (C.c_int, [P, C.POINTER(Coulomb)]),
+        "wtbg_bse_get_matrix": (C.c_int, [P, dp]),
+        "wtbg_bse_solve": (C.c_int, [P, C.c_int, C.c_int, dp, dp]),
+        "wtbg_bse_eigvecs": (C.c_int, [P, C.c_int, C.c_int, dp]),
+        "wtbg_spectrum": (C.c_int, [P, C.c_int, dp, dp, ip, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_double, C.c_int, C.c_double, dp, fp]),
+        "wtbg_bse_q_eigenvalues": (C.c_int, [P, C.c_int, dp, dp, C.POINTER(Coulomb), dp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _dp(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _f64(a) -> np.ndarray:
+    return np.asfortranarray(np.asarray(a, dtype=np.float64))
+
+
+def coulomb_params(coultype: str, ngrid, ktol, ediel, lc, ez, w, r0) -> Coulomb:
+    t = coultype.strip()
+    if t not in COULOMB_TYPES:
+        raise ValueError("Wrong Coulomb Potential")
+    c = Coulomb()
+    c.coultype = COULOMB_TYPES[t]
+    for i in range(3):
+        c.ngrid[i] = int(ngrid[i])
+        c.ediel[i] = float(ediel[i])
+    c.ktol, c.lc, c.ez, c.w, c.r0 = float(ktol), float(lc), float(ez), float(w), float(r0)
+    return c
+
+
+class Context:
+    """One device context (wtbg_create/wtbg_destroy)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        self.h = C.c_void_p()
+        st = self.lib.wtbg_create(C.byref(self.h), device)
+        if st != 0:
+            raise WtbgError(st, self.lib.wtbg_error_string(st).decode())
+        self.N = 0
+        self.nk = 0
+
+    def close(self):
+        if self.h:
+            self.lib.wtbg_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int):
+        if st != 0:
+            msg = self.lib.wtbg_last_error(self.h).decode()
+            raise WtbgError(st, f"{self.lib.wtbg_error_string(st).decode()}: {msg}")
+
+    @property
+    def last_ms(self) -> float:
+        return float(self.lib.wtbg_last_device_ms(self.h))
+
+    # ---------------------------------------------------------------- stages
+    def set_model(self, model) -> None:
+        # (nvec, w, w) arrays in Fortran order = hopmatrices(iR, m, n)
+        hre = np.asfortranarray(model.hre)
+        him = np.asfortranarray(model.him)
+        rvec = np.asfortranarray(model.rvec.astype(np.int32))
+        deg = np.ascontiguousarray(model.deg.astype(np.int32))
+        rlat = _f64(model.rlat)
+        self.w = model.w
+        self._check(self.lib.wtbg_set_model(self.h, model.w, model.nvec, _dp(hre), _dp(him), _ip(rvec),
+                                            _ip(deg), _dp(rlat), float(model.efermi), float(model.scs)))
+
+    def bands(self, kpt: np.ndarray, nv: int, nc: int, want_vectors: bool = True):
+        kpt = _f64(kpt)
+        nk = kpt.shape[0]
+        nb = nv + nc
+        eigv = np.zeros((nk, nb), order="F")
+        vec = np.zeros((nk, nb, self.w), dtype=np.complex128, order="F") if want_vectors else None
+        nocp = np.zeros(nk, dtype=np.int32)
+        gap = np.zeros(1)
+        vp = vec.ctypes.data_as(C.POINTER(C.c_double)) if vec is not None else None
+        self._check(self.lib.wtbg_bands(self.h, nk, _dp(kpt), nv, nc, _dp(eigv), vp, _ip(nocp), _dp(gap)))
+        self.nk, self.nv, self.nc = nk, nv, nc
+        self.N = nk * nc * nv
+        return eigv, vec, nocp, float(gap[0])
+
+    def velocity(self, sme: float, want: bool = True):
+        h = np.zeros((self.N, 5), dtype=np.complex128, order="F") if want else None
+        hp = h.ctypes.data_as(C.POINTER(C.c_double)) if h is not None else None
+        self._check(self.lib.wtbg_velocity(self.h, float(sme), hp))
+        return h
+
+    def sp_table(self):
+        out = np.zeros((self.N, 15), dtype=np.float32, order="F")
+        self._check(self.lib.wtbg_sp_table(self.h, _fp(out)))
+        return out
+
+    def bse_build(self, coul: Coulomb) -> None:
+        self._check(self.lib.wtbg_bse_build(self.h, C.byref(coul)))
+
+    def bse_get_matrix(self):
+        H = np.zeros((self.N, self.N), dtype=np.complex128, order="F")
+        self._check(self.lib.wtbg_bse_get_matrix(self.h, H.ctypes.data_as(C.POINTER(C.c_double))))
+        return H
+
+    def bse_solve(self, dtfull: bool = False, cpol: bool = False, want_act: bool = True):
+        W = np.zeros(self.N)
+        act = np.zeros((self.N, 8), order="F") if want_act else None
+        self._check(self.lib.wtbg_bse_solve(self.h, int(dtfull), int(cpol), _dp(W), _dp(act)))
+        return W, act
+
+    def bse_eigvecs(self, n0: int, n1: int):
+        A = np.zeros((self.N, n1 - n0 + 1), dtype=np.complex128, order="F")
+        self._check(self.lib.wtbg_bse_eigvecs(self.h, n0, n1, A.ctypes.data_as(C.POINTER(C.c_double))))
+        return A
+
+    def spectrum(self, E, F, ngrid, vcell3d, ebse0, ebsef, numbse, sme, renorm, spinf):
+        E = _f64(E)
+        F = _f64(F)
+        n = E.shape[0]
+        nw = int(numbse)
+        ng = np.array(ngrid, dtype=np.int32)
+        om = np.zeros(nw)
+        eps = np.zeros((nw, 2, 6), dtype=np.float32, order="F")
+        self._check(self.lib.wtbg_spectrum(self.h, n, _dp(E), _dp(F), _ip(ng), float(vcell3d), float(ebse0),
+                                           float(ebsef), float(numbse), float(sme), int(bool(renorm)),
+                                           float(spinf), _dp(om), _fp(eps)))
+        return om, eps
+
+    def bse_q_eigenvalues(self, kptq, q4, coul: Coulomb):
+        kq = _f64(kptq)
+        q = np.ascontiguousarray(np.asarray(q4, dtype=np.float64))
+        W = np.zeros(self.N)
+        self._check(self.lib.wtbg_bse_q_eigenvalues(self.h, kq.shape[0], _dp(kq), _dp(q), C.byref(coul), _dp(W)))
+        return W
