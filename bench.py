@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""Benchmark: BSE time-to-spectrum of the B200 path on the synthetic plain-method workload.
+
+One step = the whole BSE=T + SPEC=T path for one deck: bands on the k-mesh, velocities,
+single-particle table, BSE kernel build, dense FP64 solve + oscillator strengths, and the
+broadened eps(omega) of the BSE and single-particle spectra.
+
+  value  device time of one step with the model resident in HBM (sum of the CUDA-event
+         times of the stages, inputs already on the device), seconds (lower is better)
+  e2e    the same step end to end through the deck-level C entry wtb_run (libwtbdriver.so):
+         deck parse, params-file read, host->device model upload, every device stage, the
+         device->host reads and all output files written
+  roofline  the dominant kernel (the Hermitian matrix-vector product of the
+         tridiagonalisation) timed per launch with CUDA events inside the timed steps
+  cpu_baseline  the CPU oracle (numpy restatement of the reference, LAPACK ZHEEV with the
+         reference's minimum workspace) on bounded samples of the same workload, scaled
+
+Multi-GPU: the dense solve of one deck does not shard; --gpus N runs N independent
+replicas (one per rank) and reports the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from wantibexos_b200 import synth, wtbgpu  # noqa: E402
+from wantibexos_b200 import build as wbuild  # noqa: E402
+
+WORKLOADS = {
+    # name: (model, mesh n, nv, nc, r0, cshift, ebsef, nespec)
+    "c2": dict(model="c2", n=48, nv=4, nc=4, r0=30.0, cshift=0.03, ebsef=6.0, nespec=2001,
+               desc="config 2: w=24, 91 cells, 48x48x1 mesh, nv=nc=4, N=36864, V2DRK r0=30, eps 0-6 eV x2001"),
+    "c5": dict(model="c4_w16", n=60, nv=2, nc=2, r0=35.0, cshift=0.03, ebsef=6.0, nespec=2001,
+               desc="config 5 size: w=16, 61 cells, 60x60x1 mesh, nv=nc=2, N=14400, V2DRK r0=35"),
+    "c1": dict(model="c1", n=12, nv=2, nc=2, r0=40.0, cshift=0.05, ebsef=5.0, nespec=1001,
+               desc="config 1: w=8, 37 cells, 12x12x1 mesh, nv=nc=2, N=576, V2DRK r0=40, eps 0-5 eV x1001"),
+}
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def deck_text(wl, workdir):
+    return f"""BSE= T
+SPEC= T
+NGX= {wl['n']}
+NGY= {wl['n']}
+NGZ= 1
+NBANDSV= {wl['nv']}
+NBANDSC= {wl['nc']}
+COULOMB_POT= V2DRK
+R_0= {wl['r0']}
+EDIEL_T= 1
+EDIEL= 1
+EDIEL_B= 1
+EDIEL_Z= 1
+W_COUL= 0
+LC= 1
+KTOL= 0.001
+CSHIFT= {wl['cshift']}
+ENSPECI= 0
+ENSPECF= {wl['ebsef']}
+NESPEC= {wl['nespec']}
+DTDIAG= F
+CPOL= F
+RNMD= T
+SYSDIM= "2D"
+OUTPUT= "{workdir}/"
+CALC_DATA= "{workdir}/"
+PARAMS_FILE= "{workdir}/tb_synthetic.dat"
+"""
+
+
+# ----------------------------------------------------------------------------- host helpers
+def recvec(rlat):
+    pi32 = float(np.float32(np.pi))
+    a1, a2, a3 = rlat
+    v23, v31, v12 = np.cross(a2, a3), np.cross(a3, a1), np.cross(a1, a2)
+    vol = abs(a1 @ v23)
+    s = (2.0 * pi32) / vol
+    return s * v23, s * v31, s * v12
+
+
+def kmesh(n, rlat):
+    b1, b2, b3 = recvec(rlat)
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    k = (b1[None, None, :] / n) * i[..., None] + (b2[None, None, :] / n) * j[..., None]
+    return k.reshape(-1, 3)
+
+
+def vcell3d(rlat):
+    return abs(np.cross(rlat[0], rlat[1]) @ rlat[2])
+
+
+def f154(x):
+    """The value read back from an F15.4 field (the reference's file round trip)."""
+    return np.array([float(f"{v:15.4f}") for v in np.ravel(x)]).reshape(np.shape(x))
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if shutil.which("nvidia-smi") is None:
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                      "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        loaded = sorted(sm)[len(sm) // 2:] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- device step
+def device_step(ctx, model, kpt, wl, c):
+    """One step with the model resident; returns device seconds per stage."""
+    t = {}
+    ctx.bands(kpt, wl["nv"], wl["nc"], want_vectors=False)
+    t["bands"] = ctx.last_ms
+    h = ctx.velocity(wl["cshift"], want=False)
+    t["velocity"] = ctx.last_ms
+    sp = ctx.sp_table()
+    t["sp_table"] = ctx.last_ms
+    ctx.bse_build(c)
+    t["build"] = ctx.last_ms
+    W, act = ctx.bse_solve(False, False)
+    t["solve"] = ctx.last_ms
+    E = f154(W)
+    F = f154(act[:, :6])
+    ng = [wl["n"], wl["n"], 1]
+    ctx.spectrum(E, F, ng, vcell3d(model.rlat), 0.0, wl["ebsef"], float(wl["nespec"]), wl["cshift"], True, 2.0)
+    t["spectrum_bse"] = ctx.last_ms
+    Es = f154(sp[:, 6].astype(np.float64))
+    Fs = f154(sp[:, 7:13].astype(np.float64))
+    ctx.spectrum(Es, Fs, ng, vcell3d(model.rlat), 0.0, wl["ebsef"], float(wl["nespec"]), wl["cshift"], True, 2.0)
+    t["spectrum_sp"] = ctx.last_ms
+    return {k: v / 1e3 for k, v in t.items()}
+
+
+def e2e_run(workdir, wl):
+    lib = C.CDLL(wbuild.DRIVER_LIB)
+
+    class Timings(C.Structure):
+        _fields_ = [(n, C.c_double) for n in ("bands", "sp", "build", "solve", "write_opt", "spectrum", "total")]
+
+    lib.wtb_run.restype = C.c_int
+    lib.wtb_run.argtypes = [C.c_char_p, C.c_int, C.POINTER(Timings), C.c_char_p, C.c_int]
+    tm = Timings()
+    err = C.create_string_buffer(1024)
+    t0 = time.perf_counter()
+    rc = lib.wtb_run(deck_text(wl, workdir).encode(), 0, C.byref(tm), err, 1024)
+    t1 = time.perf_counter()
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    return t1 - t0, {n: getattr(tm, n) for n, _ in Timings._fields_}
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+def cpu_baseline(wl, model, budget_s=30.0):
+    """Time the CPU oracle on bounded samples of the workload and scale to the full step."""
+    from oracle import wtb_oracle as O
+    import scipy.linalg.lapack as lapack
+    n = wl["n"]
+    nk = n * n
+    nv, nc = wl["nv"], wl["nc"]
+    N = nk * nc * nv
+    kpts = O.monkhorst_pack(n, n, 1, [0, 0, 0], model.rlat)
+    parts = {}
+    # bands: eigsys on a sample of k-points
+    ks = min(nk, 48)
+    t0 = time.perf_counter()
+    eigv, vec, nocp, _ = O.bands(model, kpts[:ks], nv, nc)
+    parts["bands"] = (time.perf_counter() - t0) * nk / ks
+    # velocities: the reference recomputes hlm for every (c, v, k) state
+    t0 = time.perf_counter()
+    O.optsp_all(model, kpts[:8], eigv[:8], vec[:8], nv, nc, wl["cshift"])
+    parts["velocity"] = (time.perf_counter() - t0) * nk / 8 * 1.0
+    # BSE build: a block of rows against all columns, scaled to the upper triangle
+    kb = min(nk, 64)
+    eig_all, vec_all, _, _ = O.bands(model, kpts[:kb], nv, nc)
+    p = O.CoulombParams("V2DRK", 1e-3, [1, 1, 1], 1.0, 1.0, 0.0, wl["r0"], [n, n, 1], model.rlat)
+    t0 = time.perf_counter()
+    O.bse_matrix(p, kpts[:kb], eig_all, vec_all, nv, nc)
+    tb = time.perf_counter() - t0
+    parts["build"] = tb * (N / (kb * nc * nv)) ** 2
+    # dense ZHEEV (minimum workspace): two sizes, N^3 fit
+    sizes = [576, 1152] if N > 1152 else [N]
+    ts = []
+    rng = np.random.default_rng(0)
+    for s in sizes:
+        X = rng.standard_normal((s, s)) + 1j * rng.standard_normal((s, s))
+        Hs = np.asfortranarray(X + X.conj().T)
+        t0 = time.perf_counter()
+        lapack.zheev(Hs, compute_v=1, lower=0, lwork=max(2 * s - 1, 1))
+        ts.append(time.perf_counter() - t0)
+    coef = float(np.mean([t / s ** 3 for t, s in zip(ts, sizes)]))
+    parts["zheev"] = coef * N ** 3
+    # oscillators: N^2 complex MACs per component (3 components), from the largest sample
+    s = sizes[-1]
+    A = np.asfortranarray(rng.standard_normal((s, s)) + 1j * rng.standard_normal((s, s)))
+    hv = rng.standard_normal(s) + 1j * rng.standard_normal(s)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        O.dielbsev(A, hv)
+    parts["oscillators"] = (time.perf_counter() - t0) * (N / s) ** 2
+    # spectrum: a slice of the photon grid, scaled (BSE + SP spectra)
+    E = np.sort(rng.uniform(0.5, 6, N))
+    F = rng.uniform(0, 1, (N, 6))
+    om = O.omega_grid(0.0, wl["ebsef"], float(wl["nespec"]))[:50]
+    t0 = time.perf_counter()
+    for c in range(6):
+        O.optdiel_grid(1, vcell3d(model.rlat), [n, n, 1], om, E, F[:, c], wl["cshift"])
+    parts["spectrum"] = 2 * (time.perf_counter() - t0) * wl["nespec"] / 50
+    total = sum(parts.values())
+    return total, parts, sizes
+
+
+# ----------------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=os.environ.get("WTB_BENCH_WORKLOAD", "c2"), choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # plumbing only: barrier + max over ranks
+        dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=1800))
+
+    metric = "BSE time-to-spectrum (s) at <=0.5 meV vs FP64"
+    unit = "s"
+    cfg = {"workload": wl["desc"], "nk": wl["n"] ** 2, "N_bse": wl["n"] ** 2 * wl["nv"] * wl["nc"],
+           "precision": "fp64 plain method", "parallelism": f"replicas{args.gpus}",
+           "l2": "inputs larger than L2 (BSE matrix %.1f GB)" % ((wl["n"] ** 2 * wl["nv"] * wl["nc"]) ** 2 * 16 / 1e9)}
+    model = synth.config_model(wl["model"])
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cores = os.cpu_count()
+        vals = []
+        for _ in range(args.warmup):
+            cpu_baseline(wl, model)
+        parts = None
+        for _ in range(max(1, args.steps)):
+            v, parts, sizes = cpu_baseline(wl, model)
+            vals.append(v)
+        val = float(np.median(vals))
+        sample = (f"oracle port on samples: bands 48 k-points, velocities 8 k-points, BSE build 64 k-point "
+                  f"row/column block, ZHEEV(lwork=2N-1) at N={sizes}, oscillators N={sizes[-1]}, spectrum 50 "
+                  f"photon energies; each scaled to the full workload (N^3 for ZHEEV, N^2 for build/oscillators)")
+        print(json.dumps({"impl": "reference", "metric": metric, "value": val, "unit": unit, "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+                          "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": "port",
+                                           "sample": sample, "parts_s": parts},
+                          "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    wbuild.build()
+    ctx = wtbgpu.Context(0)
+    ctx.set_model(model)
+    kpt = kmesh(wl["n"], model.rlat)
+    c = wtbgpu.coulomb_params("V2DRK", [wl["n"], wl["n"], 1], 1e-3, [1, 1, 1], 1.0, 1.0, 0.0, wl["r0"])
+    for _ in range(args.warmup):
+        device_step(ctx, model, kpt, wl, c)
+    if dist:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    ctx.reset_stats()
+    ctx.set_profiling(True)
+    steps = []
+    for _ in range(args.steps):
+        steps.append(device_step(ctx, model, kpt, wl, c))
+    ctx.set_profiling(False)
+    st = ctx.stats()
+    ck = clocks.stop()
+    per_step = [sum(s.values()) for s in steps]
+    t_dev = float(np.mean(per_step))
+    ctx.close()
+    # e2e through the deck-level C entry (host buffers, files)
+    workdir = tempfile.mkdtemp(prefix="wtb_bench_")
+    synth.write_params(model, os.path.join(workdir, "tb_synthetic.dat"))
+    e2e_times = []
+    e2e_parts = None
+    for _ in range(max(1, min(args.steps, 2))):
+        t, e2e_parts = e2e_run(workdir, wl)
+        e2e_times.append(t)
+    shutil.rmtree(workdir, ignore_errors=True)
+    t_e2e = float(np.mean(e2e_times))
+    if dist:
+        import torch
+        tt = torch.tensor([t_dev, t_e2e], dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_dev, t_e2e = float(tt[0]), float(tt[1])
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    hemv_gbs = st["hemv_bytes"] / (st["hemv_ms"] / 1e3) / 1e9 if st["hemv_ms"] > 0 else None
+    build_gbs = st["build_bytes"] / (st["build_ms"] / 1e3) / 1e9 if st["build_ms"] > 0 else None
+    N = cfg["N_bse"]
+    nk = cfg["nk"]
+    out = {
+        "metric": metric, "value": t_dev, "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_dev * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded hexagonal Wannier model)",
+        "config": cfg,
+        "stages_s": {k: float(np.mean([s[k] for s in steps])) for k in steps[0]},
+        "e2e": {"value": t_e2e, "unit": unit,
+                "h2d_bytes_per_step": int(model.hre.size * 16 + model.rvec.size * 4 + nk * 24 + N * 7 * 8 * 2),
+                "d2h_bytes_per_step": int(nk * (wl["nv"] + wl["nc"]) * 8 + N * 5 * 16 + N * 15 * 4 + N * 8 * 9
+                                          + wl["nespec"] * (8 + 48) * 2),
+                "stages_s": e2e_parts, "path": "wtb_run (libwtbdriver.so) -> libwtbgpu.so C-ABI, files written"},
+        "roofline": {"kernel": "tridiagonalisation Hermitian mat-vec (k_hemv)", "bound": "hbm",
+                     "achieved": hemv_gbs, "peak": hbm, "unit": "GB/s",
+                     "frac": (hemv_gbs / hbm) if hemv_gbs else None, "traffic": None,
+                     "peak_source": "measured" if peaks else "fallback",
+                     "algorithmic_bytes": "16 B x (n'(n'+1)/2) per launch, n' = trailing order",
+                     "launches": st["hemv_launches"], "avg_launch_ms": st["hemv_ms"] / max(1, st["hemv_launches"]),
+                     "build_kernel": {"achieved": build_gbs, "frac": (build_gbs / hbm) if build_gbs else None,
+                                      "algorithmic_bytes": "16 B x N(N+1)/2 (lower triangle written once)"}},
+        "gpu_launches": int(st["launches"] / max(1, args.steps)),
+        "clocks": ck,
+    }
+    if not args.no_cpu_baseline:
+        v, parts, sizes = cpu_baseline(wl, model)
+        out["cpu_baseline"] = {"value": v, "unit": unit, "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"oracle on samples (bands 48 k, velocity 8 k, build 64-k block, ZHEEV "
+                                         f"lwork=2N-1 at N={sizes} fitted N^3, oscillators, 50 photon energies), "
+                                         f"scaled to the full workload", "parts_s": parts}
+    print(json.dumps(out))
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

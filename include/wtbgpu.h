@@ -60,6 +60,23 @@ const char* wtbg_last_error(const wtbg_ctx* ctx);
  * (CUDA events on the context stream around that call's launches). */
 double wtbg_last_device_ms(const wtbg_ctx* ctx);
 
+/* Counters of the device work issued by this context since the last reset: kernel
+ * launches, and (when profiling is on) CUDA-event time and algorithmic HBM bytes of the
+ * two bandwidth-bound kernels of the path, the Hermitian matrix-vector product of the
+ * tridiagonalisation and the BSE matrix build. */
+typedef struct wtbg_stats {
+  long long launches;
+  long long hemv_launches;
+  double hemv_ms;
+  double hemv_bytes;
+  long long build_launches;
+  double build_ms;
+  double build_bytes;
+} wtbg_stats;
+int wtbg_set_profiling(wtbg_ctx* ctx, int on);
+int wtbg_get_stats(const wtbg_ctx* ctx, wtbg_stats* out);
+int wtbg_reset_stats(wtbg_ctx* ctx);
+
 /* ---- model: replaces the module globals filled by hamiltonian_input_read
  *      (subroutines/module_input_read.f90:32-176).
  *      hre/him: hopmatrices/ihopmatrices (nvec,w,w); rvec (nvec,3); deg = ffactor(nvec);
@@ -108,14 +125,17 @@ int wtbg_bse_solve(wtbg_ctx* ctx, int dtfull, int cpol, double* W, double* act);
 int wtbg_bse_eigvecs(wtbg_ctx* ctx, int n0, int n1, double* A);
 
 /* ---- spectrum: replaces the omega loop of bsedielraw with optdiel, avgsme and
- *      imagrenorm (bse_diel-tool.f90:137-210; optics.f90:160-390).
- *      ebse (n), fosc (n,6) in bse_opt_diel.dat column order xx,yy,zz,xy,xz,yz
- *      (the values as read back from that file); vcell3d = |(a1 x a2).a3|.
- *      Outputs omega (nw) and eps (nw,2,6): eps(:,1,c) = real(spinf*Re), eps(:,2,c) =
- *      real(spinf*Im) as real(4), components in file order xx, yy, zz, xy, xz, yz. */
-int wtbg_spectrum(wtbg_ctx* ctx, int n, const double* ebse, const double* fosc,
-                  const int* ngrid, double vcell3d, double ebse0, double ebsef, double numbse,
-                  double sme, int renorm, double spinf, double* omega, float* eps);
+ *      imagrenorm (bse_diel-tool.f90:137-210; optics.f90:160-390), and the same loop of
+ *      bsedielrawpol, spdielraw and spdielrawpol (bse_diel-tool-pol.f90, sp_diel-tool.f90,
+ *      sp_diel-tool-pol.f90).  ebse (n) and fosc (n,ncomp) are the values as read back from
+ *      bse_opt_diel.dat / sp_optics.dat (and the -pol files); rtype (ncomp) is optdiel's
+ *      rtype per column (1: Re eps includes the +1, 0: off-diagonal); vcell3d = |(a1 x a2).a3|.
+ *      Outputs omega (nw) and eps (nw,2,ncomp) as real(4): eps(:,1,c) = real(spinf*Re),
+ *      eps(:,2,c) = real(spinf*Im).  ncomp <= 8, nw = int(numbse). */
+int wtbg_spectrum(wtbg_ctx* ctx, int n, int ncomp, const double* ebse, const double* fosc,
+                  const int* rtype, const int* ngrid, double vcell3d, double ebse0,
+                  double ebsef, double numbse, double sme, int renorm, double spinf,
+                  double* omega, float* eps);
 
 /* ---- exciton band structure: one centre-of-mass Q of bsebnds
  *      (bse_kpath-tool.f90:246-435; matrizelbsekq = bse_subs_kpath.f90:1-208).

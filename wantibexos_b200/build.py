@@ -39,6 +39,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + \
         [os.path.join(ROOT, "include", "wtbgpu.h")]
     if not force and _newer(LIB, deps):
+        build_driver(verbose=verbose)
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
@@ -53,7 +54,36 @@ def build(force: bool = False, verbose: bool = False) -> str:
     cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", LIB + ".tmp"] + objs
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)
+    build_driver(force=True, verbose=verbose)
     return LIB
+
+
+DRIVER_LIB = os.path.join(HERE, "libwtbdriver.so")
+DRIVER_EXE = os.path.join(HERE, "wtb_bse")
+
+
+def build_driver(force: bool = False, verbose: bool = False) -> str:
+    """Compile the C++ host driver (libwtbdriver.so + the wtb_bse executable) against libwtbgpu.so."""
+    src = os.path.join(HERE, "driver", "wtb_driver.cpp")
+    main = os.path.join(HERE, "driver", "wtb_main.cpp")
+    hdrs = [os.path.join(ROOT, "include", "wtb_driver.h"), os.path.join(ROOT, "include", "wtbgpu.h")]
+    if not force and _newer(DRIVER_LIB, [src] + hdrs + [LIB]) and _newer(DRIVER_EXE, [main, DRIVER_LIB]):
+        return DRIVER_LIB
+    gxx = shutil.which("g++") or "g++"
+    rpath = "-Wl,-rpath,$ORIGIN"
+    cmd = [gxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-I" + os.path.join(ROOT, "include"), src,
+           "-o", DRIVER_LIB + ".tmp", "-L" + HERE, "-lwtbgpu", rpath]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(DRIVER_LIB + ".tmp", DRIVER_LIB)
+    cmd = [gxx, "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), main, "-o", DRIVER_EXE + ".tmp",
+           "-L" + HERE, "-lwtbdriver", "-lwtbgpu", rpath]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(DRIVER_EXE + ".tmp", DRIVER_EXE)
+    return DRIVER_LIB
 
 
 if __name__ == "__main__":

@@ -70,7 +70,35 @@ int set_device(wtbg_ctx* ctx) {
 
 }  // namespace
 
+int ensure_events(wtbg_ctx* ctx, size_t n) {
+  while (ctx->evpool.size() < n) {
+    cudaEvent_t e;
+    cudaError_t r = cudaEventCreate(&e);
+    if (r != cudaSuccess) return cuda_fail(ctx, r, "cudaEventCreate");
+    ctx->evpool.push_back(e);
+  }
+  return 0;
+}
+
 extern "C" {
+
+int wtbg_set_profiling(wtbg_ctx* ctx, int on) {
+  if (!ctx) return WTBG_ERR_ARG;
+  ctx->profiling = on ? 1 : 0;
+  return WTBG_OK;
+}
+
+int wtbg_get_stats(const wtbg_ctx* ctx, wtbg_stats* out) {
+  if (!ctx || !out) return WTBG_ERR_ARG;
+  *out = ctx->stats;
+  return WTBG_OK;
+}
+
+int wtbg_reset_stats(wtbg_ctx* ctx) {
+  if (!ctx) return WTBG_ERR_ARG;
+  ctx->stats = wtbg_stats{};
+  return WTBG_OK;
+}
 
 const char* wtbg_error_string(int s) {
   switch (s) {
@@ -123,6 +151,7 @@ int wtbg_destroy(wtbg_ctx* ctx) {
                     &ctx->yv, &ctx->lam, &ctx->ws, &ctx->act, &ctx->zsel, &ctx->csz, &ctx->sp_in, &ctx->sp_out,
                     &ctx->sp_om, &ctx->tmp, &ctx->tmp2, &ctx->istat};
   for (DevBuf* b : bufs) free_buf(*b);
+  for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   cudaStreamDestroy(ctx->stream);
@@ -355,26 +384,27 @@ int wtbg_bse_eigvecs(wtbg_ctx* ctx, int n0, int n1, double* A) {
   return WTBG_OK;
 }
 
-int wtbg_spectrum(wtbg_ctx* ctx, int n, const double* ebse, const double* fosc, const int* ngrid, double vcell3d,
-                  double ebse0, double ebsef, double numbse, double sme, int renorm, double spinf, double* omega,
-                  float* eps) {
-  if (!ctx || !ebse || !fosc || !ngrid || !omega || !eps) return WTBG_ERR_ARG;
+int wtbg_spectrum(wtbg_ctx* ctx, int n, int ncomp, const double* ebse, const double* fosc, const int* rtype,
+                  const int* ngrid, double vcell3d, double ebse0, double ebsef, double numbse, double sme, int renorm,
+                  double spinf, double* omega, float* eps) {
+  if (!ctx || !ebse || !fosc || !rtype || !ngrid || !omega || !eps) return WTBG_ERR_ARG;
   const int nw = (int)numbse;
-  if (n <= 0 || nw < 2) return set_err(ctx, WTBG_ERR_ARG, "spectrum: bad sizes");
+  if (n <= 0 || nw < 2 || ncomp < 1 || ncomp > 8) return set_err(ctx, WTBG_ERR_ARG, "spectrum: bad sizes");
   if (int r = set_device(ctx)) return r;
-  ENSURE(ctx->sp_in, (size_t)n * 7 * 8);
-  ENSURE(ctx->sp_om, (size_t)nw * 8 + (size_t)nw * 12 * 4 + 64);
+  ENSURE(ctx->sp_in, (size_t)n * (ncomp + 1) * 8);
+  ENSURE(ctx->sp_om, (size_t)nw * 8 + (size_t)nw * 2 * ncomp * 4 + 64);
   double* de = ctx->sp_in.as<double>();
   double* df = de + n;
   double* dom = ctx->sp_om.as<double>();
   float* deps = reinterpret_cast<float*>(dom + nw);
   Timer t(ctx);
   CK(cudaMemcpyAsync(de, ebse, (size_t)n * 8, cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemcpyAsync(df, fosc, (size_t)n * 6 * 8, cudaMemcpyHostToDevice, ctx->stream));
-  if (int r = launch_spectrum(ctx, n, de, df, ngrid, vcell3d, ebse0, ebsef, numbse, sme, renorm, spinf, dom, deps))
+  CK(cudaMemcpyAsync(df, fosc, (size_t)n * ncomp * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (int r = launch_spectrum(ctx, n, ncomp, de, df, rtype, ngrid, vcell3d, ebse0, ebsef, numbse, sme, renorm, spinf,
+                              dom, deps))
     return r;
   CK(cudaMemcpyAsync(omega, dom, (size_t)nw * 8, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaMemcpyAsync(eps, deps, (size_t)nw * 12 * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(eps, deps, (size_t)nw * 2 * ncomp * 4, cudaMemcpyDeviceToHost, ctx->stream));
   if (int r = t.stop()) return r;
   return WTBG_OK;
 }

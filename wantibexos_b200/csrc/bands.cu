@@ -403,7 +403,7 @@ int launch_bands(wtbg_ctx* ctx, bool q_mesh) {
   if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bands: model too large for shared memory");
   CK(cudaFuncSetAttribute(k_bands, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int grid = ctx->nk;
-  k_bands<<<grid, kBandsThreads, smem, ctx->stream>>>(a);
+  k_bands<<<grid, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
   CKL("k_bands");
   return 0;
 }
@@ -432,7 +432,7 @@ int launch_velocity(wtbg_ctx* ctx, double eta32) {
                       3 * (size_t)ctx->nv * w * 16;
   if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "velocity: model too large for shared memory");
   CK(cudaFuncSetAttribute(k_velocity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_velocity<<<ctx->nk, kBandsThreads, smem, ctx->stream>>>(a);
+  k_velocity<<<ctx->nk, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
   CKL("k_velocity");
   return 0;
 }
@@ -456,12 +456,12 @@ int launch_sp_table(wtbg_ctx* ctx, float* d_out) {
   const int th = 256;
   const int gr = (int)((N + th - 1) / th);
   k_sp_rows<<<gr, th, 0, ctx->stream>>>(ctx->kpt.as<double>(), ctx->eig.as<double>(), ctx->nocp.as<int>(),
-                                         ctx->h.as<double2>(), ctx->nk, ctx->nv, ctx->nc, N, rows, kin, iin);
+                                         ctx->h.as<double2>(), ctx->nk, ctx->nv, ctx->nc, N, rows, kin, iin); WTBG_COUNT(ctx, 1);
   CKL("k_sp_rows");
   // LSD radix sort is stable: equal keys keep their original (quantumnumbers2) order,
   // which is what the strict-greater bubble sort produces.
   CK(cub::DeviceRadixSort::SortPairs(ctmp, cub_bytes, kin, kout, iin, iout, (int)N, 0, 32, ctx->stream));
-  k_sp_gather<<<gr, th, 0, ctx->stream>>>(rows, iout, N, d_out);
+  k_sp_gather<<<gr, th, 0, ctx->stream>>>(rows, iout, N, d_out); WTBG_COUNT(ctx, 1);
   CKL("k_sp_gather");
   return 0;
 }

@@ -53,12 +53,13 @@ __global__ void __launch_bounds__(kBuildThreads) k_bse_build(BuildArgs a) {
   const int nkr = min(TK, a.nk - kr0), nkc = min(TK, a.nk - kc0);
   const int tid = threadIdx.x, bs = blockDim.x;
   const int RC = TK * nc, RV = TK * nv;
+  const int ws = w | 1;   // odd row stride: conflict-free 16-byte shared loads across rows
 
   double2* UcR = reinterpret_cast<double2*>(smem);
-  double2* UcC = UcR + RC * w;
-  double2* UvR = UcC + RC * w;
-  double2* UvC = UvR + RV * w;
-  double2* Mc = UvC + RV * w;          // col-major [RC x RC]
+  double2* UcC = UcR + RC * ws;
+  double2* UvR = UcC + RC * ws;
+  double2* UvC = UvR + RV * ws;
+  double2* Mc = UvC + RV * ws;         // col-major [RC x RC]
   double2* Mv = Mc + RC * RC;          // col-major [RV x RV]
   double* Vt = reinterpret_cast<double*>(Mv + RV * RV);   // [kc][kr]
   double* dE = Vt + TK * TK;           // [TK*ncv]
@@ -66,13 +67,15 @@ __global__ void __launch_bounds__(kBuildThreads) k_bse_build(BuildArgs a) {
 
   for (int it = tid; it < RC * w; it += bs) {
     const int kk = it / (nc * w), rem = it % (nc * w), c = rem / w, m = rem % w;
-    UcR[it] = (kk < nkr) ? a.Uc[((size_t)(kr0 + kk) * nb + nv + c) * w + m] : make_double2(0, 0);
-    UcC[it] = (kk < nkc) ? a.Uc[((size_t)(kc0 + kk) * nb + nv + c) * w + m] : make_double2(0, 0);
+    const int row = kk * nc + c;
+    UcR[row * ws + m] = (kk < nkr) ? a.Uc[((size_t)(kr0 + kk) * nb + nv + c) * w + m] : make_double2(0, 0);
+    UcC[row * ws + m] = (kk < nkc) ? a.Uc[((size_t)(kc0 + kk) * nb + nv + c) * w + m] : make_double2(0, 0);
   }
   for (int it = tid; it < RV * w; it += bs) {
     const int kk = it / (nv * w), rem = it % (nv * w), v = rem / w, m = rem % w;
-    UvR[it] = (kk < nkr) ? a.Uv[((size_t)(kr0 + kk) * nb + v) * w + m] : make_double2(0, 0);
-    UvC[it] = (kk < nkc) ? a.Uv[((size_t)(kc0 + kk) * nb + v) * w + m] : make_double2(0, 0);
+    const int row = kk * nv + v;
+    UvR[row * ws + m] = (kk < nkr) ? a.Uv[((size_t)(kr0 + kk) * nb + v) * w + m] : make_double2(0, 0);
+    UvC[row * ws + m] = (kk < nkc) ? a.Uv[((size_t)(kc0 + kk) * nb + v) * w + m] : make_double2(0, 0);
   }
   for (int it = tid; it < TK * TK; it += bs) {
     const int kc = it / TK, kr = it % TK;
@@ -92,16 +95,16 @@ __global__ void __launch_bounds__(kBuildThreads) k_bse_build(BuildArgs a) {
   __syncthreads();
   for (int it = tid; it < RC * RC; it += bs) {
     const int col = it / RC, row = it % RC;
-    const double2* x = UcR + row * w;
-    const double2* y = UcC + col * w;
+    const double2* x = UcR + row * ws;
+    const double2* y = UcC + col * ws;
     double2 acc = make_double2(0, 0);
     for (int m = 0; m < w; ++m) acc = cadd(acc, cmulc(x[m], y[m]));
     Mc[it] = acc;
   }
   for (int it = tid; it < RV * RV; it += bs) {
     const int col = it / RV, row = it % RV;
-    const double2* x = UvR + row * w;
-    const double2* y = UvC + col * w;
+    const double2* x = UvR + row * ws;
+    const double2* y = UvC + col * ws;
     double2 acc = make_double2(0, 0);
     for (int m = 0; m < w; ++m) acc = cadd(acc, cmulc(x[m], y[m]));
     Mv[it] = acc;
@@ -158,8 +161,8 @@ __global__ void k_exchange_overlap(const double2* Uq, const double2* U, int nk, 
 }
 
 size_t build_smem(int TK, int nc, int nv, int w) {
-  const int RC = TK * nc, RV = TK * nv, ncv = nc * nv;
-  return 16ull * (2ull * RC * w + 2ull * RV * w + (size_t)RC * RC + (size_t)RV * RV) + 8ull * TK * TK +
+  const int RC = TK * nc, RV = TK * nv, ncv = nc * nv, ws = w | 1;
+  return 16ull * (2ull * RC * ws + 2ull * RV * ws + (size_t)RC * RC + (size_t)RV * RV) + 8ull * TK * TK +
          8ull * TK * ncv + 4ull * TK * ncv + 64;
 }
 
@@ -252,7 +255,7 @@ int launch_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p, const double* q4) {
       a.vcv = ctx->tmp2.as<double2>();
       const int th = 256;
       k_exchange_overlap<<<(int)((ctx->N + th - 1) / th), th, 0, ctx->stream>>>(
-          ctx->Uq.as<double2>(), ctx->U.as<double2>(), ctx->nk, nv, nc, w, ctx->tmp2.as<double2>());
+          ctx->Uq.as<double2>(), ctx->U.as<double2>(), ctx->nk, nv, nc, w, ctx->tmp2.as<double2>()); WTBG_COUNT(ctx, 1);
       CKL("k_exchange_overlap");
       a.exch = 1;
     }
@@ -268,8 +271,22 @@ int launch_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p, const double* q4) {
   CK(cudaFuncSetAttribute(k_bse_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const long long ntile = (long long)a.nbk * (a.nbk + 1) / 2;
   if (ntile > 0x7fffffffLL) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bse_build: too many tiles");
-  k_bse_build<<<(unsigned)ntile, kBuildThreads, smem, ctx->stream>>>(a);
+  const bool prof = ctx->profiling != 0;
+  if (prof) {
+    if (int r = ensure_events(ctx, 2)) return r;
+    cudaEventRecord(ctx->evpool[0], ctx->stream);
+  }
+  k_bse_build<<<(unsigned)ntile, kBuildThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
   CKL("k_bse_build");
+  if (prof) {
+    cudaEventRecord(ctx->evpool[1], ctx->stream);
+    CK(cudaEventSynchronize(ctx->evpool[1]));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, ctx->evpool[0], ctx->evpool[1]));
+    ctx->stats.build_ms += t;
+    ctx->stats.build_bytes += (double)ctx->N * ((double)ctx->N + 1.0) * 0.5 * 16.0;
+    ctx->stats.build_launches += 1;
+  }
   return 0;
 }
 
@@ -282,7 +299,7 @@ __global__ void k_coulomb_single(CoulombDev P, double x, double y, double z, dou
 int eval_coulomb_single(wtbg_ctx* ctx, const CoulombDev& P, double x, double y, double z, double* out) {
   ENSURE(ctx->istat, 64);
   double* d = ctx->istat.as<double>();
-  k_coulomb_single<<<1, 1, 0, ctx->stream>>>(P, x, y, z, d);
+  k_coulomb_single<<<1, 1, 0, ctx->stream>>>(P, x, y, z, d); WTBG_COUNT(ctx, 1);
   CKL("k_coulomb_single");
   CK(cudaMemcpyAsync(out, d, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));

@@ -77,7 +77,18 @@ struct wtbg_ctx {
 
   // misc
   DevBuf tmp, tmp2, istat;
+
+  // counters
+  wtbg_stats stats{};
+  int profiling = 0;
+  std::vector<cudaEvent_t> evpool;   // event pairs for per-launch timing when profiling
 };
+
+// make sure the event pool holds at least n events
+int ensure_events(wtbg_ctx* ctx, size_t n);
+
+// launch accounting: count every kernel launch issued through a context
+#define WTBG_COUNT(ctx, n) ((ctx)->stats.launches += (n))
 
 // error handling
 int set_err(wtbg_ctx* c, int code, const std::string& msg);
@@ -128,6 +139,6 @@ int launch_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p, const double* q4);
 int run_tridiagonalise(wtbg_ctx* ctx);
 int run_tridiagonal_solve(wtbg_ctx* ctx, int dtfull, int cpol, bool vectors);
 int run_eigvecs(wtbg_ctx* ctx, int n0, int n1, double2* d_out);
-int launch_spectrum(wtbg_ctx* ctx, int n, const double* d_e, const double* d_f, const int* ngrid,
-                    double vcell3d, double ebse0, double ebsef, double numbse, double sme,
+int launch_spectrum(wtbg_ctx* ctx, int n, int ncomp, const double* d_e, const double* d_f, const int* rtype,
+                    const int* ngrid, double vcell3d, double ebse0, double ebsef, double numbse, double sme,
                     int renorm, double spinf, double* d_om, float* d_eps);

@@ -22,10 +22,17 @@ __global__ void k_avgsme(const double* e, int n, double sme, double* eta_out) {
   *eta_out = 10.0 * (s / (double)n) + sme;
 }
 
+constexpr int kMaxComp = 8;
+
+struct SpecRtype {
+  int rt[kMaxComp];
+};
+
+template <int NCOMP>
 __global__ void __launch_bounds__(256) k_spectrum(const double* __restrict__ E, const double* __restrict__ F, int n,
                                                   const double* __restrict__ eta_p, double ebse0, double ebsef,
-                                                  double numbse, int nw, double caux, double* om, double* re,
-                                                  double* im) {
+                                                  double numbse, int nw, double caux, SpecRtype rt, double* om,
+                                                  double* re, double* im) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= nw) return;
@@ -33,21 +40,23 @@ __global__ void __launch_bounds__(256) k_spectrum(const double* __restrict__ E, 
   const double w = ebse0 + (((ebsef - ebse0) * (j - 1)) / (numbse - 1.));
   const double eta = *eta_p;
   const double eta2 = eta * eta;
-  double r[6] = {0, 0, 0, 0, 0, 0}, a[6] = {0, 0, 0, 0, 0, 0};
+  double r[NCOMP], a[NCOMP];
+#pragma unroll
+  for (int c = 0; c < NCOMP; ++c) r[c] = a[c] = 0.0;
   for (int i = lane; i < n; i += 32) {
     const double e = E[i];
     const double eaux = ((w - e) * (w - e)) + eta2;
     const double d1 = (e - w) / eaux;
     const double d2 = eta / eaux;
 #pragma unroll
-    for (int c = 0; c < 6; ++c) {
+    for (int c = 0; c < NCOMP; ++c) {
       const double f = F[(long long)c * n + i];
       r[c] += f * d1;
       a[c] += f * d2;
     }
   }
 #pragma unroll
-  for (int c = 0; c < 6; ++c) {
+  for (int c = 0; c < NCOMP; ++c) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       r[c] += __shfl_xor_sync(0xffffffffu, r[c], o);
@@ -57,8 +66,8 @@ __global__ void __launch_bounds__(256) k_spectrum(const double* __restrict__ E, 
   if (lane == 0) {
     om[warp] = w;
 #pragma unroll
-    for (int c = 0; c < 6; ++c) {
-      const double delta = (c < 3) ? 1.0 : 0.0;
+    for (int c = 0; c < NCOMP; ++c) {
+      const double delta = rt.rt[c] == 1 ? 1.0 : 0.0;
       re[(long long)c * nw + warp] = delta + (r[c] * caux);
       im[(long long)c * nw + warp] = a[c] * caux;
     }
@@ -66,10 +75,10 @@ __global__ void __launch_bounds__(256) k_spectrum(const double* __restrict__ E, 
 }
 
 // imagrenorm per component + real(spinf*x) output, eps(nw,2,6)
-__global__ void k_renorm_out(const double* E, const double* om, const double* re, double* im, int nw, int renorm,
-                             double spinf, float* eps) {
+__global__ void k_renorm_out(const double* E, const double* om, const double* re, double* im, int nw, int ncomp,
+                             int renorm, double spinf, float* eps) {
   const int c = threadIdx.x;
-  if (c >= 6) return;
+  if (c >= ncomp) return;
   double* ic = im + (long long)c * nw;
   if (renorm) {
     const double aux = E[0] - (double)0.15f;
@@ -95,23 +104,36 @@ __global__ void k_renorm_out(const double* E, const double* om, const double* re
 
 }  // namespace
 
-int launch_spectrum(wtbg_ctx* ctx, int n, const double* d_e, const double* d_f, const int* ngrid, double vcell3d,
-                    double ebse0, double ebsef, double numbse, double sme, int renorm, double spinf, double* d_om,
-                    float* d_eps) {
+int launch_spectrum(wtbg_ctx* ctx, int n, int ncomp, const double* d_e, const double* d_f, const int* rtype,
+                    const int* ngrid, double vcell3d, double ebse0, double ebsef, double numbse, double sme,
+                    int renorm, double spinf, double* d_om, float* d_eps) {
   const int nw = (int)numbse;
-  ENSURE(ctx->sp_out, (size_t)12 * nw * 8 + 64);
+  ENSURE(ctx->sp_out, (size_t)2 * kMaxComp * nw * 8 + 64);
   double* re = ctx->sp_out.as<double>();
-  double* im = re + 6 * (size_t)nw;
-  double* eta = im + 6 * (size_t)nw;
+  double* im = re + (size_t)ncomp * nw;
+  double* eta = im + (size_t)ncomp * nw;
+  SpecRtype rt{};
+  for (int c = 0; c < ncomp; ++c) rt.rt[c] = rtype[c];
   const double baux = (double)(float)(ngrid[0] * ngrid[1] * ngrid[2]) * vcell3d;
   const double caux = (double)180.90f / (baux * 1.0);
-  k_avgsme<<<1, 32, 0, ctx->stream>>>(d_e, n, sme, eta);
+  k_avgsme<<<1, 32, 0, ctx->stream>>>(d_e, n, sme, eta); WTBG_COUNT(ctx, 1);
   CKL("k_avgsme");
   const int threads = 256;
   const int blocks = (nw * 32 + threads - 1) / threads;
-  k_spectrum<<<blocks, threads, 0, ctx->stream>>>(d_e, d_f, n, eta, ebse0, ebsef, numbse, nw, caux, d_om, re, im);
+  switch (ncomp) {
+#define WTBG_SPEC_CASE(K)                                                                                      \
+  case K:                                                                                                      \
+    k_spectrum<K><<<blocks, threads, 0, ctx->stream>>>(d_e, d_f, n, eta, ebse0, ebsef, numbse, nw, caux, rt,   \
+                                                       d_om, re, im);                                          \
+    break;
+    WTBG_SPEC_CASE(1) WTBG_SPEC_CASE(2) WTBG_SPEC_CASE(3) WTBG_SPEC_CASE(4)
+    WTBG_SPEC_CASE(5) WTBG_SPEC_CASE(6) WTBG_SPEC_CASE(7) WTBG_SPEC_CASE(8)
+#undef WTBG_SPEC_CASE
+    default: return set_err(ctx, WTBG_ERR_ARG, "spectrum: ncomp must be 1..8");
+  }
+  WTBG_COUNT(ctx, 1);
   CKL("k_spectrum");
-  k_renorm_out<<<1, 32, 0, ctx->stream>>>(d_e, d_om, re, im, nw, renorm, spinf, d_eps);
+  k_renorm_out<<<1, 32, 0, ctx->stream>>>(d_e, d_om, re, im, nw, ncomp, renorm, spinf, d_eps); WTBG_COUNT(ctx, 1);
   CKL("k_renorm_out");
   return 0;
 }

@@ -330,10 +330,10 @@ int run_tridiagonal_solve(wtbg_ctx* ctx, int dtfull, int cpol, bool vectors) {
   ENSURE(ctx->tmp2, (size_t)n * 8 + 64);
   double* e2 = ctx->tmp2.as<double>();
   if (n > 1) {
-    k_e2<<<(int)((n + 255) / 256), 256, 0, s>>>(ctx->e.as<double>(), n, e2);
+    k_e2<<<(int)((n + 255) / 256), 256, 0, s>>>(ctx->e.as<double>(), n, e2); WTBG_COUNT(ctx, 1);
     CKL("k_e2");
   }
-  k_bisect<<<(int)((n + 127) / 128), 128, 0, s>>>(ctx->d.as<double>(), e2, n, lo, hi, pivmin, ctx->lam.as<double>());
+  k_bisect<<<(int)((n + 127) / 128), 128, 0, s>>>(ctx->d.as<double>(), e2, n, lo, hi, pivmin, ctx->lam.as<double>()); WTBG_COUNT(ctx, 1);
   CKL("k_bisect");
   ctx->lam_host.resize(n);
   CK(cudaMemcpyAsync(ctx->lam_host.data(), ctx->lam.as<double>(), n * 8, cudaMemcpyDeviceToHost, s));
@@ -392,7 +392,7 @@ int run_tridiagonal_solve(wtbg_ctx* ctx, int dtfull, int cpol, bool vectors) {
     a.m1 = m1;
     a.M = (int)M;
     const int cnt = (int)(m1 - m0);
-    k_inviter<<<(cnt + 127) / 128, 128, 0, s>>>(a);
+    k_inviter<<<(cnt + 127) / 128, 128, 0, s>>>(a); WTBG_COUNT(ctx, 1);
     CKL("k_inviter");
     m0 = m1;
   }
@@ -438,11 +438,11 @@ int run_eigvecs(wtbg_ctx* ctx, int n0, int n1, double2* d_out) {
     a.zsel = ctx->zsel.as<double>();
     a.zs0 = n0 - 1;
     a.zs1 = n1 - 1;
-    k_inviter<<<(int)((M + 127) / 128), 128, 0, s>>>(a);
+    k_inviter<<<(int)((M + 127) / 128), 128, 0, s>>>(a); WTBG_COUNT(ctx, 1);
     CKL("k_inviter(eigvecs)");
   }
   const long long cnt = (long long)nvec * n;
-  k_real_to_complex<<<(int)((cnt + 255) / 256), 256, 0, s>>>(ctx->zsel.as<double>(), d_out, cnt);
+  k_real_to_complex<<<(int)((cnt + 255) / 256), 256, 0, s>>>(ctx->zsel.as<double>(), d_out, cnt); WTBG_COUNT(ctx, 1);
   CKL("k_real_to_complex");
   const int nparts_max = (int)((n + BT_RB - 1) / BT_RB) + 1;
   ENSURE(ctx->tmp, (size_t)nparts_max * PB * (PB + 64) * 16 + PB * 64 * 16 + 1024);
@@ -457,12 +457,12 @@ int run_eigvecs(wtbg_ctx* ctx, int n0, int n1, double2* d_out) {
     const int jb = (int)std::min<long long>(PB, n - 1 - j0);
     const int nrows = (int)(n - j0 - 1);
     const int nparts = (nrows + BT_RB - 1) / BT_RB;
-    k_bt_gram<<<nparts, BT_RB, shb, s>>>(ctx->H.as<double2>(), n, j0, jb, d_out, nvec, part);
-    k_bt_tmat<<<1, 256, 0, s>>>(part, nparts, jb, nvec, ctx->tau.as<double2>(), j0, Y);
-    k_bt_apply<<<(nrows + 255) / 256, 256, 0, s>>>(ctx->H.as<double2>(), n, j0, jb, d_out, nvec, Y);
+    k_bt_gram<<<nparts, BT_RB, shb, s>>>(ctx->H.as<double2>(), n, j0, jb, d_out, nvec, part); WTBG_COUNT(ctx, 1);
+    k_bt_tmat<<<1, 256, 0, s>>>(part, nparts, jb, nvec, ctx->tau.as<double2>(), j0, Y); WTBG_COUNT(ctx, 1);
+    k_bt_apply<<<(nrows + 255) / 256, 256, 0, s>>>(ctx->H.as<double2>(), n, j0, jb, d_out, nvec, Y); WTBG_COUNT(ctx, 1);
   }
   CKL("back-transform");
-  k_gauge_last<<<nvec, 256, 0, s>>>(d_out, n, nvec);
+  k_gauge_last<<<nvec, 256, 0, s>>>(d_out, n, nvec); WTBG_COUNT(ctx, 1);
   CKL("k_gauge_last");
   return 0;
 }

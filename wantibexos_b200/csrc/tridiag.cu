@@ -27,14 +27,6 @@ constexpr int NB = WTBG_PANEL;       // 32
 constexpr int RB = 256;              // rows per block of the column kernels
 constexpr int NG = 5;                // h vectors carried through (x, y, z, sp, sm)
 
-struct ColScal {
-  double2 tau;
-  double2 scal;
-  double2 alpha2;
-  double beta;
-  int trivial;
-};
-
 __device__ __forceinline__ double2 warp_sum2(double2 v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -49,14 +41,49 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// (1) column update + partial |x|^2 for rows >= i+2
-__global__ void __launch_bounds__(RB) k_colupd(double2* A, long long N, const double2* Wp, int j0, int p, int i,
-                                               double* part) {
+__device__ __forceinline__ double2 vload(const double2* p) {
+  const volatile double* q = reinterpret_cast<const volatile double*>(p);
+  return make_double2(q[0], q[1]);
+}
+
+// Per-column state shared by the column kernels (device memory).  Reductions across
+// blocks use the "last block finishes" pattern: every block writes its partial, fences,
+// and takes a ticket; the block that takes the last ticket reduces and resets the counter.
+struct ColState {
+  double2 tau;
+  double2 scal;
+  double2 alpha2;   // w(prev) += alpha2 * v(prev): applied by the next column kernel
+  double beta;
+  int trivial;
+  unsigned int cntA, cntC, cntE;
+  double2 z[2 * NB + NG];   // z1 = W^H v (p values), z2 = V^H v (p values), s = v^T g (5)
+};
+
+__device__ __forceinline__ bool last_block(unsigned int* cnt) {
+  __shared__ bool s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int t = atomicAdd(cnt, 1u);
+    s_last = (t == gridDim.x * gridDim.y - 1);
+  }
+  __syncthreads();
+  if (s_last) __threadfence();
+  return s_last;
+}
+
+// (A) apply the previous column's w correction, update column i with the panel's pending
+//     rank-2 terms, |x|^2 partials; the last block computes the reflector (ZLARFG).
+__global__ void __launch_bounds__(RB) k_colA(double2* A, long long N, double2* Wp, int j0, int p, int i, double* part,
+                                             ColState* st, double* d, double* e, double2* tau_out) {
   __shared__ double2 wrow[NB], vrow[NB];
   __shared__ double red[RB / 32];
   const int tid = threadIdx.x;
+  const double2 alpha2 = (p > 0) ? st->alpha2 : make_double2(0, 0);
   if (tid < p) {
-    wrow[tid] = Wp[i + (long long)tid * N];
+    double2 wv = Wp[i + (long long)tid * N];
+    if (tid == p - 1) wv = cadd(wv, alpha2);   // v(prev)(i) = 1
+    wrow[tid] = wv;
     vrow[tid] = A[i + (long long)(j0 + tid) * N];
   }
   __syncthreads();
@@ -65,10 +92,14 @@ __global__ void __launch_bounds__(RB) k_colupd(double2* A, long long N, const do
   if (r < N) {
     double2 a = A[r + (long long)i * N];
     if (p > 0) {
+      // finish w of the previous column for this row
+      const double2 vprev = A[r + (long long)(i - 1) * N];
+      const double2 wlast = cadd(Wp[r + (long long)(p - 1) * N], cmul(alpha2, vprev));
+      Wp[r + (long long)(p - 1) * N] = wlast;
       double2 s1 = make_double2(0, 0), s2 = make_double2(0, 0);
       for (int q = 0; q < p; ++q) {
         const double2 vq = A[r + (long long)(j0 + q) * N];
-        const double2 wq = Wp[r + (long long)q * N];
+        const double2 wq = (q == p - 1) ? wlast : Wp[r + (long long)q * N];
         s1 = cadd(s1, cmul(vq, cconj(wrow[q])));
         s2 = cadd(s2, cmul(wq, cconj(vrow[q])));
       }
@@ -86,206 +117,229 @@ __global__ void __launch_bounds__(RB) k_colupd(double2* A, long long N, const do
     for (int k = 0; k < RB / 32; ++k) s += red[k];
     part[blockIdx.x] = s;
   }
-}
-
-// (2) reflector scalars (ZLARFG)
-__global__ void k_reflector(const double2* A, long long N, int i, const double* part, int nparts, double* d,
-                            double* e, double2* tau_out, ColScal* sc) {
-  __shared__ double red[32];
-  const int tid = threadIdx.x;
+  if (!last_block(&st->cntA)) return;
+  // reflector scalars
   double s = 0.0;
-  for (int k = tid; k < nparts; k += blockDim.x) s += part[k];
+  for (int k = tid; k < (int)gridDim.x; k += RB) s += ((volatile double*)part)[k];
   s = warp_sum(s);
+  __syncthreads();
   if ((tid & 31) == 0) red[tid >> 5] = s;
   __syncthreads();
   if (tid == 0) {
     double xn2 = 0.0;
-    for (int k = 0; k < (int)(blockDim.x / 32); ++k) xn2 += red[k];
-    const double2 alpha = A[(i + 1) + (long long)i * N];
-    ColScal c;
-    c.alpha2 = make_double2(0, 0);
+    for (int k = 0; k < RB / 32; ++k) xn2 += red[k];
+    const double2 alpha = vload(A + (i + 1) + (long long)i * N);
     if (xn2 == 0.0 && alpha.y == 0.0) {
-      c.tau = make_double2(0, 0);
-      c.scal = make_double2(0, 0);
-      c.beta = alpha.x;
-      c.trivial = 1;
+      st->tau = make_double2(0, 0);
+      st->scal = make_double2(0, 0);
+      st->beta = alpha.x;
+      st->trivial = 1;
     } else {
       const double beta = -copysign(sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2), alpha.x);
-      c.tau = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
-      // scal = 1 / (alpha - beta)
+      st->tau = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
       const double2 den = make_double2(alpha.x - beta, alpha.y);
       const double dd = den.x * den.x + den.y * den.y;
-      c.scal = make_double2(den.x / dd, -den.y / dd);
-      c.beta = beta;
-      c.trivial = 0;
+      st->scal = make_double2(den.x / dd, -den.y / dd);
+      st->beta = beta;
+      st->trivial = 0;
     }
-    *sc = c;
-    e[i] = c.beta;
-    d[i] = A[i + (long long)i * N].x;
-    tau_out[i] = c.tau;
+    e[i] = st->beta;
+    d[i] = vload(A + i + (long long)i * N).x;
+    tau_out[i] = st->tau;
+    st->cntA = 0;
   }
 }
 
-// (2b) scale v in place, v(i+1)=1; partial dots z1 = W^H v, z2 = V^H v, s = v^T g
-__global__ void __launch_bounds__(RB) k_scale_dots(double2* A, long long N, const double2* Wp, int j0, int p, int i,
-                                                   const ColScal* sc, const double2* g, double2* part) {
-  __shared__ double2 red[RB / 32][2 * NB + NG];
+// (C) scale v in place (v(i+1) = 1); partial dots z1 = W^H v, z2 = V^H v, s = v^T g.  One
+//     warp per dot product over the block's rows; the last block reduces into st->z.
+__global__ void __launch_bounds__(RB) k_colC(double2* A, long long N, const double2* Wp, int j0, int p, int i,
+                                             ColState* st, const double2* g, double2* part) {
+  __shared__ double2 vs[RB];
+  __shared__ double2 red[2 * NB + NG];
   const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-  const long long r = (long long)i + 1 + (long long)blockIdx.x * RB + tid;
-  const ColScal c = *sc;
+  const long long rbase = (long long)i + 1 + (long long)blockIdx.x * RB;
+  const long long r = rbase + tid;
+  const double2 scal = st->scal;
+  const int trivial = st->trivial;
   double2 v = make_double2(0, 0);
   if (r < N) {
     if (r == i + 1) v = make_double2(1.0, 0.0);
-    else v = c.trivial ? make_double2(0, 0) : cmul(A[r + (long long)i * N], c.scal);
+    else v = trivial ? make_double2(0, 0) : cmul(A[r + (long long)i * N], scal);
     A[r + (long long)i * N] = v;
   }
+  vs[tid] = v;
+  __syncthreads();
   const int nval = 2 * p + NG;
-  for (int q = 0; q < nval; ++q) {
+  const int nrow = (int)((N - rbase) < RB ? (N - rbase) : RB);
+  for (int q = wp; q < nval; q += RB / 32) {
     double2 t = make_double2(0, 0);
-    if (r < N) {
-      if (q < p) t = cmulc(Wp[r + (long long)q * N], v);
-      else if (q < 2 * p) t = cmulc(A[r + (long long)(j0 + q - p) * N], v);
-      else t = cmul(v, g[(long long)(q - 2 * p) * N + r]);
+    for (int k = lane; k < nrow; k += 32) {
+      const long long rr = rbase + k;
+      if (q < p) t = cadd(t, cmulc(Wp[rr + (long long)q * N], vs[k]));
+      else if (q < 2 * p) t = cadd(t, cmulc(A[rr + (long long)(j0 + q - p) * N], vs[k]));
+      else t = cadd(t, cmul(vs[k], g[(long long)(q - 2 * p) * N + rr]));
     }
     t = warp_sum2(t);
-    if (lane == 0) red[wp][q] = t;
+    if (lane == 0) red[q] = t;
   }
   __syncthreads();
+  for (int q = tid; q < nval; q += RB) part[(long long)blockIdx.x * (2 * NB + NG) + q] = red[q];
+  if (!last_block(&st->cntC)) return;
   for (int q = tid; q < nval; q += RB) {
     double2 s = make_double2(0, 0);
-    for (int k = 0; k < RB / 32; ++k) s = cadd(s, red[k][q]);
-    part[(long long)blockIdx.x * (2 * NB + NG) + q] = s;
+    for (int k = 0; k < (int)gridDim.x; ++k) {
+      s = cadd(s, vload(part + (long long)k * (2 * NB + NG) + q));
+    }
+    st->z[q] = s;
   }
+  __syncthreads();
+  if (tid == 0) st->cntC = 0;
 }
 
-// (3) y = A22 v over the lower-triangular 64x64 tiles of rows/cols [i+1, N).
-// Tile (I, J), I >= J: slot[I][J] += A_IJ x_J (for y_I); slot[J][I] = A_IJ^H x_I (for y_J).
-__global__ void __launch_bounds__(256) k_hemv(const double2* __restrict__ A, long long N, int i, int nblk,
-                                              double2* __restrict__ slots) {
-  __shared__ double2 xI[TB], xJ[TB];
-  __shared__ double2 rowp[8][TB];
-  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+// (D) y = A22 v, A22 = rows/cols [i+1, N) of the lower-stored Hermitian matrix.
+// One CTA streams a chunk of up to HS 64x64 tiles down one block-column J: the row sums
+// A_IJ x_J go to slot[I][J] per tile; the column sums A_IJ^H x_I stay in registers across
+// the chunk and go to slot[J][I0] (I0 = first tile of the chunk, zeros in the rest of the
+// chunk's slots), so that y_a = sum_b slot[a][b] over b in the trailing block range.
+constexpr int HS = 8;
+
+__global__ void __launch_bounds__(256, 2) k_hemv(const double2* __restrict__ A, long long N, int i, int nblk,
+                                                 double2* __restrict__ slots) {
+  __shared__ double2 xJs[TB];
+  __shared__ double2 rowp[2][8][TB];
+  __shared__ double2 diagrow[TB];
+  __shared__ double2 colp[TB];
   const int b0 = (i + 1) / TB;
-  const int nt = nblk - b0;
-  const long long ntiles = (long long)nt * (nt + 1) / 2;
+  const int J = b0 + blockIdx.x;
+  const int I0 = J + blockIdx.y * HS;
+  if (I0 >= nblk) return;
+  const int I1 = min(I0 + HS, nblk);
+  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   const long long lo = (long long)i + 1;
   const double2* xcol = A + (long long)i * N;
-  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    int bi = (int)floor((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-    while ((long long)(bi + 1) * (bi + 2) / 2 <= t) ++bi;
-    while ((long long)bi * (bi + 1) / 2 > t) --bi;
-    const int bj = (int)(t - (long long)bi * (bi + 1) / 2);
-    const int I = b0 + bi, J = b0 + bj;
-    const long long R0 = (long long)I * TB, C0 = (long long)J * TB;
-    __syncthreads();
-    if (tid < TB) {
-      const long long r = R0 + tid;
-      xI[tid] = (r >= lo && r < N) ? xcol[r] : make_double2(0, 0);
-    } else if (tid < 2 * TB) {
-      const long long cc = C0 + tid - TB;
-      xJ[tid - TB] = (cc >= lo && cc < N) ? xcol[cc] : make_double2(0, 0);
-    }
-    __syncthreads();
+  const long long C0 = (long long)J * TB;
+  if (tid < TB) {
+    const long long c = C0 + tid;
+    xJs[tid] = (c >= lo && c < N) ? xcol[c] : make_double2(0, 0);
+  }
+  __syncthreads();
+  double2 cacc[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) cacc[m] = make_double2(0, 0);
+  bool cvalid[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const long long c = C0 + wp + 8 * m;
+    cvalid[m] = (c >= lo && c < N);
+  }
+  for (int I = I0; I < I1; ++I) {
+    const int buf = (I - I0) & 1;
+    const long long R0 = (long long)I * TB;
+    const long long ra = R0 + lane, rb = ra + 32;
     const bool diag = (I == J);
-    double2 rp0 = make_double2(0, 0), rp1 = make_double2(0, 0);
-    double2 cp[8];
-    const long long ra = R0 + lane, rb = R0 + lane + 32;
     const bool va = (ra >= lo && ra < N), vb = (rb >= lo && rb < N);
+    const double2 xa = va ? xcol[ra] : make_double2(0, 0);
+    const double2 xb = vb ? xcol[rb] : make_double2(0, 0);
+    double2 rp0 = make_double2(0, 0), rp1 = make_double2(0, 0);
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      const int cl = wp + 8 * m;
-      const long long cc = C0 + cl;
-      cp[m] = make_double2(0, 0);
-      const bool vc = (cc >= lo && cc < N);
-      if (!vc) continue;
-      const double2* colp = A + cc * N;
-      const double2 xj = xJ[cl];
-      if (va && (!diag || lane >= cl)) {
-        double2 a = colp[ra];
-        if (diag && lane == cl) a.y = 0.0;
-        rp0 = cadd(rp0, cmul(a, xj));
-        if (!(diag && lane == cl)) cp[m] = cadd(cp[m], cmulc(a, xI[lane]));
+    for (int h = 0; h < 2; ++h) {
+      double2 a0[4], a1[4];
+#pragma unroll
+      for (int mm = 0; mm < 4; ++mm) {
+        const int m = h * 4 + mm;
+        const int cl = wp + 8 * m;
+        const double2* colp_ = A + (C0 + cl) * N;
+        const bool ok0 = cvalid[m] && va && (!diag || lane >= cl);
+        const bool ok1 = cvalid[m] && vb && (!diag || lane + 32 >= cl);
+        a0[mm] = ok0 ? colp_[ra] : make_double2(0, 0);
+        a1[mm] = ok1 ? colp_[rb] : make_double2(0, 0);
       }
-      if (vb && (!diag || lane + 32 >= cl)) {
-        double2 a = colp[rb];
-        if (diag && lane + 32 == cl) a.y = 0.0;
-        rp1 = cadd(rp1, cmul(a, xj));
-        if (!(diag && lane + 32 == cl)) cp[m] = cadd(cp[m], cmulc(a, xI[lane + 32]));
+#pragma unroll
+      for (int mm = 0; mm < 4; ++mm) {
+        const int m = h * 4 + mm;
+        const int cl = wp + 8 * m;
+        const double2 xj = xJs[cl];
+        double2 e0 = a0[mm], e1 = a1[mm];
+        const bool d0 = diag && (lane == cl), d1 = diag && (lane + 32 == cl);
+        if (d0) e0.y = 0.0;
+        if (d1) e1.y = 0.0;
+        rp0 = cadd(rp0, cmul(e0, xj));
+        rp1 = cadd(rp1, cmul(e1, xj));
+        if (!d0) cacc[m] = cadd(cacc[m], cmulc(e0, xa));
+        if (!d1) cacc[m] = cadd(cacc[m], cmulc(e1, xb));
       }
     }
-    rowp[wp][lane] = rp0;
-    rowp[wp][lane + 32] = rp1;
-    // column partials: reduce over the 32 lanes for each of this warp's 8 columns
-    double2 mycol = make_double2(0, 0);
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      double2 s = warp_sum2(cp[m]);
-      if (lane == m) mycol = s;
-    }
+    rowp[buf][wp][lane] = rp0;
+    rowp[buf][wp][lane + 32] = rp1;
     __syncthreads();
-    double2* sIJ = slots + ((long long)I * nblk + J) * TB;
-    double2* sJI = slots + ((long long)J * nblk + I) * TB;
     if (tid < TB) {
       double2 s = make_double2(0, 0);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) s = cadd(s, rowp[k][tid]);
-      if (!diag) sIJ[tid] = s;
-      else rowp[0][tid] = s;   // combined below
+      for (int k = 0; k < 8; ++k) s = cadd(s, rowp[buf][k][tid]);
+      if (diag) diagrow[tid] = s;
+      else slots[((long long)I * nblk + J) * TB + tid] = s;
     }
-    __syncthreads();
-    if (lane < 8) {
-      const int cl = wp + 8 * lane;   // column owned by (warp wp, m = lane)
-      if (!diag) sJI[cl] = mycol;
-      else rowp[1][cl] = mycol;
-    }
-    __syncthreads();
-    if (diag && tid < TB) sIJ[tid] = cadd(rowp[0][tid], rowp[1][tid]);
   }
+  // column sums of the chunk
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const double2 s = warp_sum2(cacc[m]);
+    if (lane == m) colp[wp + 8 * m] = s;
+  }
+  __syncthreads();
+  if (tid < TB) {
+    double2 v = colp[tid];
+    if (I0 == J) v = cadd(v, diagrow[tid]);
+    slots[((long long)J * nblk + I0) * TB + tid] = v;
+  }
+  for (int I = I0 + 1; I < I1; ++I)
+    if (tid < TB) slots[((long long)J * nblk + I) * TB + tid] = make_double2(0, 0);
 }
 
-// (4) y rows from slots; w = tau*(y - V z1 - W z2); g update; partial w^H v
-__global__ void __launch_bounds__(256) k_hemv_finish(double2* A, long long N, double2* Wp, int j0, int p, int i, int nblk,
-                                                     const double2* slots, const double2* partC, int nC,
-                                                     const ColScal* sc, double2* g, double2* partE) {
-  __shared__ double2 zz[2 * NB + NG];
+// (E) y rows from the slots; w = tau (y - V z1 - W z2); g <- g - tau conj(v) s; partial
+//     w^H v.  The last block computes alpha2 = -tau/2 w^H v for the next column kernel.
+__global__ void __launch_bounds__(256) k_colE(const double2* A, long long N, double2* Wp, int j0, int p, int i, int nblk,
+                                              const double2* slots, ColState* st, double2* g, double2* part) {
   __shared__ double2 acc4[4][TB];
+  __shared__ double2 tq4[4][TB];
+  __shared__ double2 zz[2 * NB + NG];
   __shared__ double2 red[8];
   const int tid = threadIdx.x;
   const int nval = 2 * p + NG;
-  for (int q = tid; q < nval; q += blockDim.x) {
-    double2 s = make_double2(0, 0);
-    for (int k = 0; k < nC; ++k) s = cadd(s, partC[(long long)k * (2 * NB + NG) + q]);
-    zz[q] = s;
-  }
+  for (int q = tid; q < nval; q += blockDim.x) zz[q] = st->z[q];
+  const double2 tau = st->tau;
   const int b0 = (i + 1) / TB;
-  const int a = b0 + blockIdx.x;   // block-row
-  const int e = tid & (TB - 1), part = tid >> 6;
+  const int a = b0 + blockIdx.x;
+  const int el = tid & (TB - 1), grp = tid >> 6;
   double2 s = make_double2(0, 0);
-  for (int b = b0 + part; b < nblk; b += 4) s = cadd(s, slots[((long long)a * nblk + b) * TB + e]);
-  acc4[part][e] = s;
+  for (int b = b0 + grp; b < nblk; b += 4) s = cadd(s, slots[((long long)a * nblk + b) * TB + el]);
+  acc4[grp][el] = s;
   __syncthreads();
-  const ColScal c = *sc;
+  const long long r = (long long)a * TB + el;
+  const bool rv = (r >= (long long)i + 1 && r < N);
+  // V z1 + W z2 for this row, the q range split over the 4 thread groups
+  double2 t = make_double2(0, 0);
+  if (rv) {
+    for (int q = grp; q < p; q += 4) {
+      t = cadd(t, cmul(A[r + (long long)(j0 + q) * N], zz[q]));
+      t = cadd(t, cmul(Wp[r + (long long)q * N], zz[p + q]));
+    }
+  }
+  tq4[grp][el] = t;
+  __syncthreads();
   double2 dot = make_double2(0, 0);
-  if (tid < TB) {
-    const long long r = (long long)a * TB + tid;
-    if (r >= (long long)i + 1 && r < N) {
-      double2 y = cadd(cadd(acc4[0][tid], acc4[1][tid]), cadd(acc4[2][tid], acc4[3][tid]));
-      double2 t1 = make_double2(0, 0), t2 = make_double2(0, 0);
-      for (int q = 0; q < p; ++q) {
-        t1 = cadd(t1, cmul(A[r + (long long)(j0 + q) * N], zz[q]));
-        t2 = cadd(t2, cmul(Wp[r + (long long)q * N], zz[p + q]));
-      }
-      const double2 w = cmul(c.tau, csub(csub(y, t1), t2));
-      Wp[r + (long long)p * N] = w;
-      const double2 v = A[r + (long long)i * N];
-      dot = cmulc(w, v);
-      // g <- g - tau conj(v) (v^T g)
-      const double2 tv = cmul(c.tau, cconj(v));
+  if (tid < TB && rv) {
+    const double2 y = cadd(cadd(acc4[0][tid], acc4[1][tid]), cadd(acc4[2][tid], acc4[3][tid]));
+    const double2 vz = cadd(cadd(tq4[0][tid], tq4[1][tid]), cadd(tq4[2][tid], tq4[3][tid]));
+    const double2 w = cmul(tau, csub(y, vz));
+    Wp[r + (long long)p * N] = w;
+    const double2 v = A[r + (long long)i * N];
+    dot = cmulc(w, v);
+    const double2 tv = cmul(tau, cconj(v));
 #pragma unroll
-      for (int al = 0; al < NG; ++al) {
-        const double2 sa = zz[2 * p + al];
-        g[(long long)al * N + r] = csub(g[(long long)al * N + r], cmul(tv, sa));
-      }
+    for (int al = 0; al < NG; ++al) {
+      const double2 sa = zz[2 * p + al];
+      g[(long long)al * N + r] = csub(g[(long long)al * N + r], cmul(tv, sa));
     }
   }
   if (tid < 64) {
@@ -293,26 +347,23 @@ __global__ void __launch_bounds__(256) k_hemv_finish(double2* A, long long N, do
     if ((tid & 31) == 0) red[tid >> 5] = dot;
   }
   __syncthreads();
-  if (tid == 0) partE[blockIdx.x] = cadd(red[0], red[1]);
+  if (tid == 0) part[blockIdx.x] = cadd(red[0], red[1]);
+  if (!last_block(&st->cntE)) return;
+  if (tid == 0) {
+    double2 sum = make_double2(0, 0);
+    for (int k = 0; k < (int)gridDim.x; ++k) sum = cadd(sum, vload(part + k));
+    st->alpha2 = cscale(cmul(tau, sum), -0.5);
+    st->cntE = 0;
+  }
 }
 
-// (4b) w += alpha2 v with alpha2 = -tau/2 (w^H v)
-__global__ void __launch_bounds__(RB) k_wfix(const double2* A, long long N, double2* Wp, int p, int i,
-                                             const double2* partE, int nE, const ColScal* sc) {
-  __shared__ double2 s_alpha;
-  const int tid = threadIdx.x;
-  if (tid == 0) {
-    double2 s = make_double2(0, 0);
-    for (int k = 0; k < nE; ++k) s = cadd(s, partE[k]);
-    const ColScal c = *sc;
-    s_alpha = cscale(cmul(c.tau, s), -0.5);
-  }
-  __syncthreads();
-  const long long r = (long long)i + 1 + (long long)blockIdx.x * RB + tid;
-  if (r < N) {
-    const double2 v = A[r + (long long)i * N];
-    Wp[r + (long long)p * N] = cadd(Wp[r + (long long)p * N], cmul(s_alpha, v));
-  }
+// w(last column of the panel) += alpha2 v, rows [k0, N), before the trailing update
+__global__ void __launch_bounds__(RB) k_wfix_last(const double2* A, long long N, double2* Wp, int p, int i, long long k0,
+                                                  const ColState* st) {
+  const long long r = k0 + (long long)blockIdx.x * RB + threadIdx.x;
+  if (r >= N) return;
+  const double2 alpha2 = st->alpha2;
+  Wp[r + (long long)p * N] = cadd(Wp[r + (long long)p * N], cmul(alpha2, A[r + (long long)i * N]));
 }
 
 // Trailing update A22 -= V W^H + W V^H on the lower triangle with FP64 mma.sync.
@@ -417,7 +468,7 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
   ENSURE(ctx->Wp, (size_t)N * 16 * NB);
   ENSURE(ctx->slots, (size_t)nblk * nblk * TB * 16);
   ENSURE(ctx->part, (size_t)maxRB * (2 * NB + NG) * 16 + (size_t)maxRB * 16 + (size_t)(nblk + 1) * 16 + 4096);
-  ENSURE(ctx->scal, sizeof(ColScal) + 64);
+  ENSURE(ctx->scal, sizeof(ColState) + 64);
   double2* A = ctx->H.as<double2>();
   double2* Wp = ctx->Wp.as<double2>();
   double* d = ctx->d.as<double>();
@@ -429,46 +480,62 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
   double* partA = reinterpret_cast<double*>(pb);
   double2* partC = reinterpret_cast<double2*>(pb + (size_t)maxRB * 16);
   double2* partE = partC + (size_t)maxRB * (2 * NB + NG);
-  ColScal* sc = ctx->scal.as<ColScal>();
+  ColState* st = ctx->scal.as<ColState>();
   cudaStream_t s = ctx->stream;
+  CK(cudaMemsetAsync(st, 0, sizeof(ColState), s));
 
   if (ctx->have_velocity) {
-    k_copy_g<<<(int)((N * NG + 255) / 256), 256, 0, s>>>(ctx->h.as<double2>(), g, N * NG);
+    k_copy_g<<<(int)((N * NG + 255) / 256), 256, 0, s>>>(ctx->h.as<double2>(), g, N * NG); WTBG_COUNT(ctx, 1);
   } else {
     CK(cudaMemsetAsync(g, 0, (size_t)N * 16 * NG, s));
   }
   CKL("k_copy_g");
-  int num_sms = 148;
-  cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  const bool prof = ctx->profiling != 0;
+  if (prof) {
+    if (int r = ensure_events(ctx, 2 * (size_t)N)) return r;
+  }
 
   for (long long j0 = 0; j0 < N - 1; j0 += NB) {
     const int jb = (int)((N - 1 - j0) < NB ? (N - 1 - j0) : NB);
     for (int p = 0; p < jb; ++p) {
       const int i = (int)(j0 + p);
       const int nA = (int)((N - i + RB - 1) / RB);
-      k_colupd<<<nA, RB, 0, s>>>(A, N, Wp, (int)j0, p, i, partA);
-      k_reflector<<<1, 256, 0, s>>>(A, N, i, partA, nA, d, e, tau, sc);
+      k_colA<<<nA, RB, 0, s>>>(A, N, Wp, (int)j0, p, i, partA, st, d, e, tau); WTBG_COUNT(ctx, 1);
       const int nC = (int)((N - i - 1 + RB - 1) / RB);
-      k_scale_dots<<<nC, RB, 0, s>>>(A, N, Wp, (int)j0, p, i, sc, g, partC);
+      k_colC<<<nC, RB, 0, s>>>(A, N, Wp, (int)j0, p, i, st, g, partC); WTBG_COUNT(ctx, 1);
       const int b0 = (i + 1) / TB;
-      const long long nt = nblk - b0;
-      const long long ntiles = nt * (nt + 1) / 2;
-      const int grid = (int)(ntiles < (long long)num_sms * 8 ? ntiles : (long long)num_sms * 8);
-      k_hemv<<<grid, 256, 0, s>>>(A, N, i, nblk, slots);
-      const int nE = nblk - b0;
-      k_hemv_finish<<<nE, 256, 0, s>>>(A, N, Wp, (int)j0, p, i, nblk, slots, partC, nC, sc, g, partE);
-      k_wfix<<<nC, RB, 0, s>>>(A, N, Wp, p, i, partE, nE, sc);
+      const int nt = nblk - b0;
+      if (prof) cudaEventRecord(ctx->evpool[2 * i], s);
+      k_hemv<<<dim3(nt, (nt + HS - 1) / HS), 256, 0, s>>>(A, N, i, nblk, slots); WTBG_COUNT(ctx, 1);
+      if (prof) cudaEventRecord(ctx->evpool[2 * i + 1], s);
+      k_colE<<<nt, 256, 0, s>>>(A, N, Wp, (int)j0, p, i, nblk, slots, st, g, partE); WTBG_COUNT(ctx, 1);
     }
     CKL("tridiagonal panel");
     const long long k0 = j0 + jb;
     if (k0 < N) {
+      const int il = (int)(j0 + jb - 1);
+      k_wfix_last<<<(int)((N - k0 + RB - 1) / RB), RB, 0, s>>>(A, N, Wp, jb - 1, il, k0, st); WTBG_COUNT(ctx, 1);
       const long long T = (N - k0 + TB - 1) / TB;
       const long long ntile = T * (T + 1) / 2;
-      k_her2k<<<(unsigned)ntile, 256, 0, s>>>(A, N, Wp, (int)j0, jb, (int)k0);
+      k_her2k<<<(unsigned)ntile, 256, 0, s>>>(A, N, Wp, (int)j0, jb, (int)k0); WTBG_COUNT(ctx, 1);
       CKL("k_her2k");
     }
   }
-  k_last_diag<<<1, 1, 0, s>>>(A, N, d);
+  k_last_diag<<<1, 1, 0, s>>>(A, N, d); WTBG_COUNT(ctx, 1);
   CKL("k_last_diag");
+  if (prof) {
+    CK(cudaEventSynchronize(ctx->evpool[2 * (N - 2) + 1]));
+    double ms = 0.0, bytes = 0.0;
+    for (long long i = 0; i < N - 1; ++i) {
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, ctx->evpool[2 * i], ctx->evpool[2 * i + 1]));
+      ms += t;
+      const double np = (double)(N - i - 1);
+      bytes += np * (np + 1.0) * 0.5 * 16.0;   // lower triangle of the trailing matrix
+    }
+    ctx->stats.hemv_ms += ms;
+    ctx->stats.hemv_bytes += bytes;
+    ctx->stats.hemv_launches += N - 1;
+  }
   return 0;
 }

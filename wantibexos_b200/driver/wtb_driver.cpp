@@ -1,0 +1,1185 @@
+// Host driver of the BSE exciton + optics path: the C++ counterpart of the reference's
+// Fortran driver layer for BSE=T / BSE_BND=T / SPEC=T runs.  It keeps the reference's input
+// grammar (stdin deck, params file) and writes the same output files, and calls the GPU
+// through the C-ABI of libwtbgpu.so (include/wtbgpu.h).
+//
+// Reference structure mirrored here:
+//   wtb_main.f90:60-357          program main (deck, params header, mesh, tool dispatch)
+//   module_input_read.f90:235-816 input_read / param_out (log.dat)
+//   module_input_read.f90:32-176  hamiltonian_input_read (params file, incl. SP merge)
+//   bse_solver-tool-diel.f90      bsesolver  -> log_bse-diel.dat, sp_optics*.dat, tm_coef*.dat,
+//                                               bse_opt_diel*.dat, exc_wf_n.dat
+//   bse_kpath-tool.f90            bsebnds    -> bands_bse.dat, log_bse_kpath.dat, KLABELS-BSE.dat
+//   bse_diel-tool(-pol).f90       bsedielraw(pol) -> bse_diel_*.dat / bse_diel-pol_*.dat
+//   sp_diel-tool(-pol).f90        spdielraw(pol)  -> sp_diel_*.dat / sp_diel-pol_*.dat
+//   diel-pp-*.f90, diel-pp-subs   bseoptprop(pol), spoptprop(pol) -> refractive index, ...
+//   exciton_lifetime.f90          lifetime(pol) -> exciton_lifetime(-pol).dat
+// Fortran list-directed output is compiler-specific; numeric parity (not byte parity) is the
+// contract, and every number is printed with enough digits to be read back exactly.
+#include <algorithm>
+#include <array>
+#include <cctype>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/wtbgpu.h"
+#include "../../include/wtb_driver.h"
+
+namespace {
+
+// ------------------------------------------------------------------------------ errors
+struct Stop : std::runtime_error {
+  explicit Stop(const std::string& m) : std::runtime_error(m) {}
+};
+
+void gpu_check(wtbg_ctx* ctx, int st, const char* where) {
+  if (st != 0) {
+    std::string m = std::string(where) + ": " + wtbg_error_string(st) + " (" + wtbg_last_error(ctx) + ")";
+    throw Stop(m);
+  }
+}
+
+// ------------------------------------------------------------------------------ deck
+struct Deck {
+  int nthreads = 1;
+  int ngrid[3] = {1, 1, 1};
+  double rk = 0.0;
+  int nc = 1, nv = 1;
+  double numdos = 6001, ebse0 = 0.0, ebsef = 3.0, numbse = 6001;
+  double sme = (double)0.08f, cshift = (double)0.01f, exc = 0.0;
+  double mshift[3] = {0, 0, 0};
+  double ktol = (double)0.001f;
+  std::string outputfolder = "./", calcparms = "./", meshtype = "MKH", coultype = "V3D";
+  std::string orbw = "non declared file", kpaths = "non declared file", kpathsbse = "non declared file";
+  std::string params;
+  std::string sysdim = "3D", dft = "V", ta = "FA", ses = "AM15G";
+  bool bandscalc = false, doscalc = false, bse = false, bsepol = false, bsekpath = false, spdiel = false;
+  bool spdielpol = false, sppolbz = false, spec = false, berryk = false, berrybz = false, pponly = false;
+  bool bsewf = false, tmcoef = false, dtfull = false, cpol = false, bset = false, bsetbnd = false;
+  bool pce = false, renorm = true;
+  int excwf0 = 1, excwff = 2;
+  double ediel[3] = {1, 1, 1};
+  double ez = 1.0, w = 0.0, lc = 1.0, r0 = 1.0;
+  double st = 0, phavg = 0, temp = 0;
+  double ctemp = (double)298.15f, tmax = (double)5e-6f, eg = 0, egd = 0, egs = 0, ebgs = 0;
+};
+
+// one record split into list-directed character items (quotes keep blanks)
+std::vector<std::string> items_of(const std::string& line) {
+  std::vector<std::string> out;
+  size_t i = 0, n = line.size();
+  while (i < n) {
+    char c = line[i];
+    if (c == ' ' || c == '\t' || c == ',' || c == '\r') {
+      ++i;
+      continue;
+    }
+    if (c == '"' || c == '\'') {
+      size_t j = line.find(c, i + 1);
+      if (j == std::string::npos) j = n;
+      out.push_back(line.substr(i + 1, j - i - 1));
+      i = j + 1;
+      continue;
+    }
+    size_t j = i;
+    while (j < n && line[j] != ' ' && line[j] != '\t' && line[j] != ',' && line[j] != '\r') ++j;
+    out.push_back(line.substr(i, j - i));
+    i = j;
+  }
+  return out;
+}
+
+double num(const std::string& s) {
+  std::string t = s;
+  for (char& c : t)
+    if (c == 'd' || c == 'D') c = 'e';
+  char* end = nullptr;
+  double v = strtod(t.c_str(), &end);
+  if (end == t.c_str()) throw Stop("bad number in deck: " + s);
+  return v;
+}
+
+bool logical(const std::string& s) {
+  size_t i = 0;
+  while (i < s.size() && s[i] == '.') ++i;
+  if (i >= s.size()) throw Stop("bad logical in deck");
+  char c = (char)toupper(s[i]);
+  if (c == 'T') return true;
+  if (c == 'F') return false;
+  throw Stop("bad logical in deck: " + s);
+}
+
+// input_read (module_input_read.f90:235-663): each READ takes two items "a b" starting on a
+// fresh record; unknown keys are ignored.
+Deck parse_deck(const std::string& text) {
+  Deck d;
+  std::vector<std::vector<std::string>> recs;
+  {
+    std::istringstream is(text);
+    std::string line;
+    while (std::getline(is, line)) recs.push_back(items_of(line));
+  }
+  std::vector<std::pair<std::string, std::string>> pairs;
+  size_t r = 0;
+  while (r < recs.size()) {
+    while (r < recs.size() && recs[r].empty()) ++r;
+    if (r >= recs.size()) break;
+    if (recs[r].size() >= 2) {
+      pairs.emplace_back(recs[r][0], recs[r][1]);
+      ++r;
+      continue;
+    }
+    std::string a = recs[r][0];
+    ++r;
+    while (r < recs.size() && recs[r].empty()) ++r;
+    if (r >= recs.size()) break;
+    pairs.emplace_back(a, recs[r][0]);
+    ++r;
+  }
+  auto trunc = [](const std::string& s, size_t n) { return s.substr(0, std::min(n, s.size())); };
+  for (auto& p : pairs) {
+    const std::string& a = p.first;
+    const std::string& b = p.second;
+    if (a == "RNMD=") d.renorm = logical(b);
+    else if (a == "PCE=") d.pce = logical(b);
+    else if (a == "SES=") d.ses = trunc(b, 6);
+    else if (a == "CTEMP=") d.ctemp = num(b);
+    else if (a == "THMAX=") d.tmax = num(b);
+    else if (a == "EG=") d.eg = num(b);
+    else if (a == "EGD=") d.egd = num(b);
+    else if (a == "EGS=") d.egs = num(b);
+    else if (a == "EBGS=") d.ebgs = num(b);
+    else if (a == "TA=") d.ta = trunc(b, 2);
+    else if (a == "BSET=") d.bset = logical(b);
+    else if (a == "BSET_BND=") d.bsetbnd = logical(b);
+    else if (a == "TEMP=") d.temp = num(b);
+    else if (a == "PHAVG=") d.phavg = num(b);
+    else if (a == "ST=") d.st = num(b);
+    else if (a == "DFT=") d.dft = trunc(b, 1);
+    else if (a == "CSHIFT=") d.cshift = num(b);
+    else if (a == "DTDIAG=") d.dtfull = logical(b);
+    else if (a == "CPOL=") d.cpol = logical(b);
+    else if (a == "SYSDIM=") d.sysdim = trunc(b, 5);
+    else if (a == "R_0=") d.r0 = num(b);
+    else if (a == "LC=") d.lc = num(b);
+    else if (a == "EDIEL_Z=") d.ez = num(b);
+    else if (a == "W_COUL=") d.w = num(b);
+    else if (a == "TMCOEF=") d.tmcoef = logical(b);
+    else if (a == "EXC_WF_F=") d.excwff = (int)num(b);
+    else if (a == "EXC_WF_I=") d.excwf0 = (int)num(b);
+    else if (a == "BSE_WF=") d.bsewf = logical(b);
+    else if (a == "PP_ONLY=") d.pponly = logical(b);
+    else if (a == "BERRY_BZ=") d.berrybz = logical(b);
+    else if (a == "BERRY=") d.berryk = logical(b);
+    else if (a == "SPEC=") d.spec = logical(b);
+    else if (a == "OPT_BZ=") d.sppolbz = logical(b);
+    else if (a == "DIEL=") d.spdiel = logical(b);
+    else if (a == "BSE_BND=") d.bsekpath = logical(b);
+    else if (a == "BSE=") d.bse = logical(b);
+    else if (a == "DOS=") d.doscalc = logical(b);
+    else if (a == "BANDS=") d.bandscalc = logical(b);
+    else if (a == "RK=") d.rk = num(b);
+    else if (a == "COULOMB_POT=") d.coultype = trunc(b, 5);
+    else if (a == "MESH_TYPE=") d.meshtype = trunc(b, 70);
+    else if (a == "OUTPUT=") d.outputfolder = trunc(b, 70);
+    else if (a == "CALC_DATA=") d.calcparms = trunc(b, 70);
+    else if (a == "NGX=") d.ngrid[0] = (int)num(b);
+    else if (a == "NGY=") d.ngrid[1] = (int)num(b);
+    else if (a == "NGZ=") d.ngrid[2] = (int)num(b);
+    else if (a == "NBANDSC=") d.nc = (int)num(b);
+    else if (a == "NBANDSV=") d.nv = (int)num(b);
+    else if (a == "NEDOS=") d.numdos = num(b);
+    else if (a == "ENSPECI=") d.ebse0 = num(b);
+    else if (a == "ENSPECF=") d.ebsef = num(b);
+    else if (a == "NESPEC=") d.numbse = num(b);
+    else if (a == "SIGMA=") d.sme = num(b);
+    else if (a == "KTOL=") d.ktol = num(b);
+    else if (a == "PARAMS_FILE=") d.params = trunc(b, 70);
+    else if (a == "KPATH_FILE=") d.kpaths = trunc(b, 70);
+    else if (a == "KPATH_BSE=") d.kpathsbse = trunc(b, 70);
+    else if (a == "ORB_W=") d.orbw = trunc(b, 70);
+    else if (a == "EDIEL_T=") d.ediel[0] = num(b);
+    else if (a == "EDIEL=") d.ediel[1] = num(b);
+    else if (a == "EDIEL_B=") d.ediel[2] = num(b);
+    else if (a == "EXC_CORR=") d.exc = num(b);
+    else if (a == "NTHREADS=") d.nthreads = (int)num(b);
+    else if (a == "SHIFT_1=") d.mshift[0] = num(b);
+    else if (a == "SHIFT_2=") d.mshift[1] = num(b);
+    else if (a == "SHIFT_3=") d.mshift[2] = num(b);
+  }
+  return d;
+}
+
+// ------------------------------------------------------------------------------ params
+struct Model {
+  std::string systype;
+  double scs = 0, efermi = 0;
+  double rlat[3][3] = {{0}};
+  int w = 0, nvec = 0;
+  std::vector<int> rvec;       // (nvec,3) column-major
+  std::vector<int> deg;        // (nvec)
+  std::vector<double> hre, him;  // (nvec,w,w) column-major
+};
+
+struct Reader {
+  std::vector<std::string> lines;
+  size_t pos = 0;
+  explicit Reader(const std::string& path) {
+    std::ifstream f(path);
+    if (!f) throw Stop("Error opening wannier90 hr input file");
+    std::string l;
+    while (std::getline(f, l)) lines.push_back(l);
+  }
+  std::vector<std::string> rec() {
+    while (pos < lines.size()) {
+      auto it = items_of(lines[pos++]);
+      if (!it.empty()) return it;
+    }
+    throw Stop("params file ended early");
+  }
+};
+
+// hamiltonian_input_read (module_input_read.f90:32-176)
+Model read_params(const std::string& path) {
+  Reader rd(path);
+  Model m;
+  m.systype = rd.rec()[0].substr(0, 4);
+  m.scs = num(rd.rec()[0]);
+  m.efermi = num(rd.rec()[0]);
+  for (int i = 0; i < 3; ++i) {
+    auto t = rd.rec();
+    if (t.size() < 3) throw Stop("bad lattice line in params file");
+    for (int c = 0; c < 3; ++c) m.rlat[i][c] = num(t[c]);
+  }
+  struct Block {
+    int w, nvec;
+    std::vector<int> deg, rvec;
+    std::vector<double> hre, him;
+  };
+  auto block = [&]() {
+    Block b;
+    rd.rec();  // header
+    b.w = (int)num(rd.rec()[0]);
+    b.nvec = (int)num(rd.rec()[0]);
+    while ((int)b.deg.size() < b.nvec)
+      for (auto& t : rd.rec()) b.deg.push_back((int)num(t));
+    b.deg.resize(b.nvec);
+    b.rvec.assign(3 * (size_t)b.nvec, 0);
+    b.hre.assign((size_t)b.nvec * b.w * b.w, 0.0);
+    b.him.assign((size_t)b.nvec * b.w * b.w, 0.0);
+    for (int i = 0; i < b.nvec; ++i)
+      for (int n = 0; n < b.w; ++n)
+        for (int mm = 0; mm < b.w; ++mm) {
+          auto t = rd.rec();
+          if (t.size() < 7) throw Stop("bad hopping row in params file");
+          for (int c = 0; c < 3; ++c) b.rvec[i + (size_t)b.nvec * c] = (int)num(t[c]);
+          const size_t idx = (size_t)i + (size_t)b.nvec * ((size_t)mm + (size_t)b.w * n);
+          b.hre[idx] = num(t[5]);
+          b.him[idx] = num(t[6]);
+        }
+    return b;
+  };
+  std::string st = m.systype;
+  while (!st.empty() && st.back() == ' ') st.pop_back();
+  if (st == "SP") {
+    Block u = block(), dn = block();
+    m.w = u.w + dn.w;
+    m.nvec = u.nvec + dn.nvec;
+    m.deg = u.deg;
+    m.deg.insert(m.deg.end(), dn.deg.begin(), dn.deg.end());
+    m.rvec.assign(3 * (size_t)m.nvec, 0);
+    m.hre.assign((size_t)m.nvec * m.w * m.w, 0.0);
+    m.him.assign((size_t)m.nvec * m.w * m.w, 0.0);
+    for (int i = 0; i < m.nvec; ++i) {
+      const bool up = i < u.nvec;
+      const Block& b = up ? u : dn;
+      const int ib = up ? i : i - u.nvec, off = up ? 0 : u.w;
+      for (int c = 0; c < 3; ++c) m.rvec[i + (size_t)m.nvec * c] = b.rvec[ib + (size_t)b.nvec * c];
+      for (int n = 0; n < b.w; ++n)
+        for (int mm = 0; mm < b.w; ++mm) {
+          const size_t s = (size_t)ib + (size_t)b.nvec * ((size_t)mm + (size_t)b.w * n);
+          const size_t d = (size_t)i + (size_t)m.nvec * ((size_t)(mm + off) + (size_t)m.w * (n + off));
+          m.hre[d] = b.hre[s];
+          m.him[d] = b.him[s];
+        }
+    }
+  } else {
+    Block b = block();
+    m.w = b.w;
+    m.nvec = b.nvec;
+    m.deg = b.deg;
+    m.rvec = b.rvec;
+    m.hre = b.hre;
+    m.him = b.him;
+  }
+  return m;
+}
+
+// ------------------------------------------------------------------------------ lattice
+const double kPi32 = (double)3.14159274101257324219f;   // acos(-1.) in real(4)
+
+void cross(const double* a, const double* b, double* o) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// recvec (mhkpack_subs.f90:409-432)
+void recvec(const double r[3][3], double b[3][3]) {
+  double v23[3], v31[3], v12[3];
+  cross(r[1], r[2], v23);
+  cross(r[2], r[0], v31);
+  cross(r[0], r[1], v12);
+  const double vol = fabs(r[0][0] * v23[0] + r[0][1] * v23[1] + r[0][2] * v23[2]);
+  const double s = (2.0 * kPi32) / vol;
+  for (int c = 0; c < 3; ++c) {
+    b[0][c] = s * v23[c];
+    b[1][c] = s * v31[c];
+    b[2][c] = s * v12[c];
+  }
+}
+
+double vcell2d(const double r[3][3]) {
+  double v[3];
+  cross(r[0], r[1], v);
+  return sqrt((v[0] * v[0]) + (v[1] * v[1]) + (v[2] * v[2]));
+}
+
+double vcell3d(const double r[3][3]) {
+  double v[3];
+  cross(r[0], r[1], v);
+  return fabs(v[0] * r[2][0] + v[1] * r[2][1] + v[2] * r[2][2]);
+}
+
+// monhkhorst_pack / monhkhorst_packq (mhkpack_subs.f90:305-407); kpt (nk,3) column-major
+std::vector<double> kmesh(const int n[3], const double shift[3], const double r[3][3], const double* q) {
+  double b[3][3];
+  recvec(r, b);
+  double ks[3];
+  for (int c = 0; c < 3; ++c) ks[c] = b[0][c] * shift[0] + b[1][c] * shift[1] + b[2][c] * shift[2];
+  const int nk = n[0] * n[1] * n[2];
+  std::vector<double> k(3 * (size_t)nk);
+  int cnt = 0;
+  for (int i = 0; i < n[0]; ++i)
+    for (int j = 0; j < n[1]; ++j)
+      for (int l = 0; l < n[2]; ++l) {
+        for (int c = 0; c < 3; ++c) {
+          double v;
+          if (q)
+            v = q[c] + (b[0][c] / (double)n[0]) * (double)i + (b[1][c] / (double)n[1]) * (double)j +
+                (b[2][c] / (double)n[2]) * (double)l + ks[c];
+          else
+            v = (b[0][c] / (double)n[0]) * (double)i + (b[1][c] / (double)n[1]) * (double)j +
+                (b[2][c] / (double)n[2]) * (double)l + ks[c];
+          k[cnt + (size_t)nk * c] = v;
+        }
+        ++cnt;
+      }
+  return k;
+}
+
+// rkmesh / rkmesh2D (mhkpack_subs.f90:2-52)
+void rkmesh(double rk, const double r[3][3], int ng[3], bool twod) {
+  double b[3][3];
+  recvec(r, b);
+  for (int i = 0; i < 3; ++i) {
+    const double vs = sqrt(b[i][0] * b[i][0] + b[i][1] * b[i][1] + b[i][2] * b[i][2]) / (2 * kPi32);
+    ng[i] = (int)std::max(1.0, (rk * vs) + 0.5);
+  }
+  if (twod) ng[2] = 1;
+}
+
+// ------------------------------------------------------------------------------ formats
+std::string F(double x, int w, int d) {
+  char buf[64];
+  snprintf(buf, sizeof buf, "%*.*f", w, d, x);
+  std::string s(buf);
+  if ((int)s.size() > w) return std::string(w, '*');
+  if (s.find("nan") != std::string::npos || s.find("inf") != std::string::npos) {
+    std::string t = std::isnan(x) ? "NaN" : (x > 0 ? "Infinity" : "-Infinity");
+    return std::string(std::max(0, w - (int)t.size()), ' ') + t;
+  }
+  return s;
+}
+
+// Ew.d with the 0.dddd mantissa of Fortran output
+std::string E(double x, int w, int d) {
+  if (std::isnan(x) || std::isinf(x)) {
+    std::string t = std::isnan(x) ? "NaN" : (x > 0 ? "Infinity" : "-Infinity");
+    return std::string(std::max(0, w - (int)t.size()), ' ') + t;
+  }
+  std::string body;
+  if (x == 0.0) {
+    body = "0." + std::string(d, '0') + "E+00";
+  } else {
+    // format |x| with d significant digits, then shift the decimal point
+    char buf[64];
+    snprintf(buf, sizeof buf, "%.*e", d - 1, fabs(x));
+    // buf = m.mmmE+xx  -> 0.mmmm E(xx+1)
+    std::string s(buf);
+    const size_t epos = s.find('e');
+    std::string mant = s.substr(0, epos);
+    int ex = atoi(s.c_str() + epos + 1) + 1;
+    mant.erase(std::remove(mant.begin(), mant.end(), '.'), mant.end());
+    char eb[16];
+    if (std::abs(ex) < 100) snprintf(eb, sizeof eb, "E%c%02d", ex < 0 ? '-' : '+', std::abs(ex));
+    else snprintf(eb, sizeof eb, "%c%03d", ex < 0 ? '-' : '+', std::abs(ex));
+    body = (x < 0 ? "-0." : "0.") + mant + eb;
+  }
+  if ((int)body.size() > w) return std::string(w, '*');
+  return std::string(w - body.size(), ' ') + body;
+}
+
+std::string I(long long v, int w) {
+  char buf[64];
+  snprintf(buf, sizeof buf, "%*lld", w, v);
+  return buf;
+}
+
+std::string LD(double x) {   // list-directed real(8)
+  char buf[64];
+  snprintf(buf, sizeof buf, " %24.16E", x);
+  return buf;
+}
+std::string LS(float x) {    // list-directed real(4)
+  char buf[64];
+  snprintf(buf, sizeof buf, " %15.8E", (double)x);
+  return buf;
+}
+std::string LI(long long v) { return I(v, 12); }
+
+std::string join_path(const std::string& folder, const std::string& name) { return folder + name; }
+
+struct Out {
+  FILE* f = nullptr;
+  std::string path;
+  Out(const std::string& p, const char* errmsg) : path(p) {
+    f = fopen(p.c_str(), "w");
+    if (!f) throw Stop(errmsg);
+  }
+  ~Out() {
+    if (f) fclose(f);
+  }
+  void line(const std::string& s) { fprintf(f, "%s\n", s.c_str()); }
+  void flush() { fflush(f); }
+};
+
+std::string stamp(const char* what) {
+  time_t t = time(nullptr);
+  struct tm lt;
+  localtime_r(&t, &lt);
+  char buf[160];
+  snprintf(buf, sizeof buf, " %s  day%12d%12d hours%12d min%12d seg", what, lt.tm_mday, lt.tm_hour, lt.tm_min,
+           lt.tm_sec);
+  return buf;
+}
+
+int coul_code(const std::string& s0) {
+  std::string s = s0;
+  while (!s.empty() && s.back() == ' ') s.pop_back();
+  if (s == "V2DK") return WTBG_V2DK;
+  if (s == "V3D") return WTBG_V3D;
+  if (s == "V3DL") return WTBG_V3DL;
+  if (s == "V2DT") return WTBG_V2DT;
+  if (s == "V2DT2") return WTBG_V2DT2;
+  if (s == "V2DOH") return WTBG_V2DOH;
+  if (s == "V2DRK") return WTBG_V2DRK;
+  if (s == "V1DT") return WTBG_V1DT;
+  if (s == "V0DT") return WTBG_V0DT;
+  throw Stop("Wrong Coulomb Potential");
+}
+
+wtbg_coulomb coulomb_of(const Deck& d) {
+  wtbg_coulomb p{};
+  p.coultype = coul_code(d.coultype);
+  for (int i = 0; i < 3; ++i) {
+    p.ngrid[i] = d.ngrid[i];
+    p.ediel[i] = d.ediel[i];
+  }
+  p.ktol = d.ktol;
+  p.lc = d.lc;
+  p.ez = d.ez;
+  p.w = d.w;
+  p.r0 = d.r0;
+  return p;
+}
+
+void upload_model(wtbg_ctx* ctx, const Model& m) {
+  double rl[9];
+  for (int i = 0; i < 3; ++i)
+    for (int c = 0; c < 3; ++c) rl[i + 3 * c] = m.rlat[i][c];
+  gpu_check(ctx, wtbg_set_model(ctx, m.w, m.nvec, m.hre.data(), m.him.data(), m.rvec.data(), m.deg.data(), rl,
+                                m.efermi, m.scs),
+            "wtbg_set_model");
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// ------------------------------------------------------------------------------ log.dat
+void param_out(Out& o, const Deck& d) {
+  auto L = [&](const std::string& s) { o.line(s); };
+  auto pad = [](const std::string& s, size_t n) {
+    std::string t = s.substr(0, std::min(n, s.size()));
+    return t + std::string(n - t.size(), ' ');
+  };
+  auto f84 = [](double x) { return F(x, 8, 4); };
+  auto l1 = [](bool b) { return std::string(b ? "T" : "F"); };
+  L("NTHREADS= " + std::to_string(d.nthreads));
+  L("SYSDIM= " + pad(d.sysdim, 2));
+  L("DFT= " + pad(d.dft, 1));
+  L("");
+  L(" INPUT/OUTPUT FILES");
+  L("");
+  L("OUTPUT= " + pad(d.outputfolder, 70));
+  L("CALC_DATA= " + pad(d.calcparms, 70));
+  L("PARAMS_FILE= " + pad(d.params, 70));
+  L("KPATH_FILE= " + pad(d.kpaths, 70));
+  L("KPATH_BSE= " + pad(d.kpathsbse, 70));
+  L("ORB_W= " + pad(d.orbw, 70));
+  L("");
+  L(" CONTROL");
+  L("");
+  L("BANDS= " + l1(d.bandscalc));
+  L("DOS= " + l1(d.doscalc));
+  L("BSE= " + l1(d.bse));
+  L("BSET= " + l1(d.bset));
+  L("BSE_BND= " + l1(d.bsekpath));
+  L("BSET_BND= " + l1(d.bsetbnd));
+  L("DIEL= " + l1(d.spdiel));
+  L("OPT_BZ= " + l1(d.sppolbz));
+  L("SPEC= " + l1(d.spec));
+  L("BERRY_BZ= " + l1(d.berrybz));
+  L("BERRY= " + l1(d.berryk));
+  L("PP_ONLY= " + l1(d.pponly));
+  L("BSE_WF= " + l1(d.bsewf));
+  L("TMCOEF= " + l1(d.tmcoef));
+  L("DTDIAG= " + l1(d.dtfull));
+  L("CPOL= " + l1(d.cpol));
+  L("PCE= " + l1(d.pce));
+  L("");
+  L(" K-MESH");
+  L("");
+  L("NGX= " + std::to_string(d.ngrid[0]));
+  L("NGY= " + std::to_string(d.ngrid[1]));
+  L("NGZ= " + std::to_string(d.ngrid[2]));
+  L("SHIFT_1= " + f84(d.mshift[0]));
+  L("SHIFT_2= " + f84(d.mshift[1]));
+  L("SHIFT_3= " + f84(d.mshift[2]));
+  L("");
+  L(" DOS");
+  L("");
+  L("NEDOS= " + std::to_string((long long)d.numdos));
+  L("SIGMA= " + f84(d.sme));
+  L("");
+  L(" BSE/OPTICAL PROPERTIES");
+  L("");
+  L("NBANDSC= " + std::to_string(d.nc));
+  L("NBANDSV= " + std::to_string(d.nv));
+  L("ENSPECI= " + f84(d.ebse0));
+  L("ENSPECF= " + f84(d.ebsef));
+  L("NESPEC= " + std::to_string((long long)d.numbse));
+  L("KTOL= " + f84(d.ktol));
+  L("EXC_WF_I= " + std::to_string(d.excwf0));
+  L("EXC_WF_F= " + std::to_string(d.excwff));
+  L("COULOMB_POT= " + pad(d.coultype, 5));
+  L("CSHIFT= " + f84(d.cshift));
+  L("RNMD= " + l1(d.renorm));
+  L("");
+  L(" PARAMETERS FOR COULOMB POTENTIALS");
+  L("");
+  L("EDIEL_Z= " + f84(d.ez));
+  L("W_COUL= " + f84(d.w));
+  L("LC= " + f84(d.lc));
+  L("R_0= " + f84(d.r0));
+  L("EDIEL_T= " + f84(d.ediel[0]));
+  L("EDIEL_B= " + f84(d.ediel[2]));
+  L("EDIEL= " + f84(d.ediel[1]));
+  L("");
+  L(" PARAMETERS FOR BSE with Temperature Effects");
+  L("");
+  L("TA= " + pad(d.ta, 2));
+  L("ST= " + f84(d.st));
+  L("PHAVG= " + f84(d.phavg));
+  L("TEMP= " + f84(d.temp));
+  L("");
+  L(" PARAMETERS FOR PCE");
+  L("");
+  L("SES= " + pad(d.ses, 6));
+  L("CTEMP= " + f84(d.ctemp));
+  L("THMAX= " + E(d.tmax, 15, 4));
+  L("EG= " + f84(d.eg));
+  L("EGD= " + f84(d.egd));
+  L("EGS= " + f84(d.egs));
+  L("EBGS= " + f84(d.ebgs));
+  L("");
+  L("");
+  o.flush();
+}
+
+// ------------------------------------------------------------------------------ bsesolver
+void bsesolver(wtbg_ctx* ctx, const Deck& d, const Model& m, Timings* tm) {
+  const std::string of = d.outputfolder;
+  Out log(join_path(of, "log_bse-diel.dat"), "Error opening log_bse-diel output file");
+  Out f301(join_path(of, "bse_opt_diel.dat"), "Error opening bse_opt_diel output file");
+  Out f302(join_path(of, "bse_opt_diel-pol.dat"), "Error opening output file");
+  Out f401(join_path(of, "sp_optics.dat"), "Error opening bse_opt_diel-pol output file");
+  FILE* f402 = nullptr;
+  FILE* f404 = nullptr;
+  if (d.tmcoef) {
+    f402 = fopen(join_path(of, "tm_coef.dat").c_str(), "w");
+    f404 = fopen(join_path(of, "tm_coef-pol.dat").c_str(), "w");
+    if (!f402 || !f404) throw Stop("Error opening tm_coef output file");
+  }
+  Out f403(join_path(of, "sp_optics-pol.dat"), "Error opening sp_optics-pol output file");
+  double t0 = now_s();
+  upload_model(ctx, m);
+  f301.line(" #  exciton energy  xx  yy  zz xy  xz  yz");
+  f302.line(" #  exciton energy  xx  yy  zz sp  sm");
+  const int nk = d.ngrid[0] * d.ngrid[1] * d.ngrid[2];
+  const long long N = (long long)nk * d.nc * d.nv;
+  log.line("");
+  log.line("");
+  log.line("");
+  log.line(" threads:" + LI(d.nthreads));
+  log.line("");
+  log.line(" grid:" + LI(d.ngrid[0]) + LI(d.ngrid[1]) + LI(d.ngrid[2]));
+  log.line("");
+  log.line("  ktol-coulomb:" + E(d.ktol, 15, 4));
+  log.line("");
+  log.line(" kmesh shift:" + F(d.mshift[0], 15, 4) + F(d.mshift[1], 15, 4) + F(d.mshift[2], 15, 4));
+  log.line("");
+  log.line(" conduction bands, nc:" + LI(d.nc) + "   valence bands, nv:" + LI(d.nv));
+  log.line("");
+  log.line("");
+  log.line(stamp("begin"));
+  log.line("");
+  log.flush();
+  std::vector<double> kpt = kmesh(d.ngrid, d.mshift, m.rlat, nullptr);
+  const int nb = d.nc + d.nv;
+  std::vector<double> eigv((size_t)nk * nb);
+  std::vector<int> nocpk(nk);
+  double egap = 0;
+  gpu_check(ctx, wtbg_bands(ctx, nk, kpt.data(), d.nv, d.nc, eigv.data(), nullptr, nocpk.data(), &egap), "wtbg_bands");
+  double t1 = now_s();
+  if (tm) tm->bands = t1 - t0;
+  log.line(" direct gap:" + LD(egap));
+  log.line(" eigenvalues and eigenvectors calculated");
+  log.line(" quantum numbers for exciton basis set finished");
+  log.flush();
+  // single-particle optics (bse_solver-tool-diel.f90:338-423)
+  std::vector<double> hr(2 * 5 * (size_t)N);
+  gpu_check(ctx, wtbg_velocity(ctx, d.cshift, hr.data()), "wtbg_velocity");
+  std::vector<float> vr(15 * (size_t)N);
+  gpu_check(ctx, wtbg_sp_table(ctx, vr.data()), "wtbg_sp_table");
+  f401.line(" #  energy  xx  yy  zz  xy  xz  yz");
+  f403.line(" #  energy  xx  yy  zz  sp  sm");
+  if (d.tmcoef) {
+    fprintf(f402, " number of kpoints:%12d\n number of conduction states%12d\n number of valence states%12d\n", nk,
+            d.nc, d.nv);
+    fprintf(f402, " #  kx  ky  kz  nocp  nc  nv  energy  xx  yy  zz  xy  xz  yz\n");
+    fprintf(f404, " number of kpoints:%12d\n number of conduction states%12d\n number of valence states%12d\n", nk,
+            d.nc, d.nv);
+    fprintf(f404, " #  kx  ky  kz  nocp  nc  nv  energy  xx  yy  zz  sp  sm\n");
+  }
+  auto col = [&](long long i, int c) { return (double)vr[i + (size_t)N * c]; };
+  auto i100 = [](double v) {   // I10.0: a zero value prints as blanks
+    long long k = (long long)v;
+    return k == 0 ? std::string(10, ' ') : I(k, 10);
+  };
+  {
+    std::string b401, b403, b402, b404;
+    b401.reserve(N * 106);
+    b403.reserve(N * 91);
+    for (long long i = 0; i < N; ++i) {
+      b401 += F(col(i, 6), 15, 4) + F(col(i, 7), 15, 4) + F(col(i, 8), 15, 4) + F(col(i, 9), 15, 4) +
+              F(col(i, 10), 15, 4) + F(col(i, 11), 15, 4) + F(col(i, 12), 15, 4) + "\n";
+      b403 += F(col(i, 6), 15, 4) + F(col(i, 7), 15, 4) + F(col(i, 8), 15, 4) + F(col(i, 9), 15, 4) +
+              F(col(i, 13), 15, 4) + F(col(i, 14), 15, 4) + "\n";
+      if (d.tmcoef) {
+        std::string head = F(col(i, 0), 10, 4) + F(col(i, 1), 10, 4) + F(col(i, 2), 10, 4) + i100(col(i, 3)) +
+                           i100(col(i, 4)) + i100(col(i, 5)) + F(col(i, 6), 10, 4) + F(col(i, 7), 10, 4) +
+                           F(col(i, 8), 10, 4) + F(col(i, 9), 10, 4);
+        b402 += head + F(col(i, 10), 10, 4) + F(col(i, 11), 10, 4) + F(col(i, 12), 10, 4) + "\n";
+        b404 += head + F(col(i, 13), 10, 4) + F(col(i, 14), 10, 4) + "\n";
+      }
+    }
+    fputs(b401.c_str(), f401.f);
+    fputs(b403.c_str(), f403.f);
+    if (d.tmcoef) {
+      fputs(b402.c_str(), f402);
+      fputs(b404.c_str(), f404);
+    }
+  }
+  log.line(" single particle optics finished");
+  log.flush();
+  double t2 = now_s();
+  if (tm) tm->sp = t2 - t1;
+  wtbg_coulomb p = coulomb_of(d);
+  gpu_check(ctx, wtbg_bse_build(ctx, &p), "wtbg_bse_build");
+  log.line(" exciton Hamiltonian matrix finished");
+  log.flush();
+  double t3 = now_s();
+  if (tm) tm->build = t3 - t2;
+  std::vector<double> W(N), act(8 * (size_t)N);
+  gpu_check(ctx, wtbg_bse_solve(ctx, d.dtfull, d.cpol, W.data(), act.data()), "wtbg_bse_solve");
+  double t4 = now_s();
+  if (tm) tm->solve = t4 - t3;
+  if (d.bsewf) {
+    const int a0 = std::max(1, d.excwf0), a1 = std::min<long long>(d.excwff, N);
+    if (a1 >= a0) {
+      std::vector<double> A(2 * (size_t)N * (a1 - a0 + 1));
+      gpu_check(ctx, wtbg_bse_eigvecs(ctx, a0, a1, A.data()), "wtbg_bse_eigvecs");
+      for (int n = a0; n <= a1; ++n) {
+        // excwf2 (bse_subs.f90:534-576)
+        Out o(join_path(of, "exc_wf_" + std::to_string(n) + ".dat"), "Error opening wf BSE output file");
+        o.line(" # excitonic state" + LI(n));
+        o.line(" # exciton energy:" + LD(W[n - 1]));
+        o.line(" # number occupied states" + LI(nocpk[0]) + "(not valid for metallic systems)");
+        o.line(" # Number of conduction states" + LI(d.nc));
+        o.line(" # Number of valence states" + LI(d.nv));
+        o.line(" # Number of kpoints" + LI(nk));
+        o.line(" # nocpk kx ky kz nc nv re_wf imag_wf");
+        std::string buf;
+        const double* an = A.data() + 2 * (size_t)N * (n - a0);
+        for (long long i = 0; i < N; ++i) {
+          const int k = (int)(i / (d.nc * d.nv)), c = (int)((i % (d.nc * d.nv)) / d.nv) + d.nv + 1,
+                    v = (int)(i % d.nv) + 1;
+          buf += I(nocpk[k], 12) + F(kpt[k], 15, 4) + F(kpt[k + (size_t)nk], 15, 4) + F(kpt[k + 2 * (size_t)nk], 15, 4) +
+                 I(nocpk[k] + c - d.nv, 12) + I(nocpk[k] - d.nv + v, 12) + E(an[2 * i], 15, 4) +
+                 E(an[2 * i + 1], 15, 4) + "\n";
+        }
+        fputs(buf.c_str(), o.f);
+      }
+    }
+  }
+  log.line(" exciton Hamiltonian diagonalized");
+  log.line(" exciton ground state" + LD(W[0]));
+  const char* comps[] = {"xx tensor component", "yy tensor component", "zz tensor component"};
+  for (auto c : comps) log.line(std::string(" ") + c);
+  if (d.dtfull) {
+    log.line(" xy tensor component");
+    log.line(" xz tensor component");
+    log.line(" yz tensor component");
+  } else {
+    log.line(" xy tensor component set to 0");
+    log.line(" xz tensor component set to 0");
+    log.line(" yz tensor component set to 0");
+  }
+  log.line(d.cpol ? " sp polarization" : " sp polarization set to 0");
+  log.line(d.cpol ? " sm polarization" : " sm polarization set to 0");
+  log.line(" optics finished");
+  log.flush();
+  {
+    std::string b301, b302;
+    b301.reserve(N * 106);
+    for (long long i = 0; i < N; ++i) {
+      b301 += F(W[i], 15, 4);
+      for (int c = 0; c < 6; ++c) b301 += F(act[i + (size_t)N * c], 15, 4);
+      b301 += "\n";
+      if (d.cpol) {
+        b302 += F(W[i], 15, 4) + F(act[i], 15, 4) + F(act[i + (size_t)N], 15, 4) + F(act[i + 2 * (size_t)N], 15, 4) +
+                F(act[i + 6 * (size_t)N], 15, 4) + F(act[i + 7 * (size_t)N], 15, 4) + "\n";
+      }
+    }
+    fputs(b301.c_str(), f301.f);
+    fputs(b302.c_str(), f302.f);
+  }
+  log.line("");
+  log.line(stamp("end"));
+  log.line("");
+  if (f402) fclose(f402);
+  if (f404) fclose(f404);
+  if (tm) tm->write_opt = now_s() - t4;
+}
+
+// ------------------------------------------------------------------------------ bsebnds
+void bsebnds(wtbg_ctx* ctx, const Deck& d, const Model& m) {
+  const std::string of = d.outputfolder;
+  std::ifstream kf(d.kpathsbse);
+  if (!kf) throw Stop("Error opening bse-kpath input file");
+  Out log(join_path(of, "log_bse_kpath.dat"), "Error opening log_bse_kpath output file");
+  Out f400(join_path(of, "bands_bse.dat"), "Error opening bands_bse output file");
+  upload_model(ctx, m);
+  std::vector<std::string> kl;
+  {
+    std::string l;
+    while (std::getline(kf, l))
+      if (!items_of(l).empty()) kl.push_back(l);
+  }
+  if (kl.size() < 2) throw Stop("bad bse-kpath file");
+  const int nks = (int)num(items_of(kl[0])[0]);
+  const int npts = (int)num(items_of(kl[1])[0]);
+  if ((int)kl.size() < 2 + nks) throw Stop("bad bse-kpath file");
+  std::vector<std::array<double, 3>> ks(nks);
+  for (int i = 0; i < nks; ++i) {
+    auto t = items_of(kl[2 + i]);
+    for (int c = 0; c < 3; ++c) ks[i][c] = num(t[c]);
+  }
+  // kpathbse (mhkpack_subs.f90:132-208): the fraction (i-1.)/(npts-1.) is real(4)
+  double b[3][3];
+  recvec(m.rlat, b);
+  std::vector<std::array<double, 3>> kx(nks);
+  for (int i = 0; i < nks; ++i)
+    for (int c = 0; c < 3; ++c) kx[i][c] = ks[i][0] * b[0][c] + ks[i][1] * b[1][c] + ks[i][2] * b[2][c];
+  const int half = nks / 2;
+  std::vector<double> kdis(half);
+  double tot = 0.0;
+  for (int i = 0; i < half; ++i) {
+    const double dx = kx[2 * i + 1][0] - kx[2 * i][0], dy = kx[2 * i + 1][1] - kx[2 * i][1],
+                 dz = kx[2 * i + 1][2] - kx[2 * i][2];
+    kdis[i] = sqrt(dx * dx + dy * dy + dz * dz);
+    tot += kdis[i];
+  }
+  for (auto& v : kdis) v = v / tot;
+  const int nq = half * npts;
+  std::vector<std::array<double, 4>> qp(nq);
+  {
+    Out kl_out(join_path(of, "KLABELS-BSE.dat"), "Error opening KLABELS-BSE output file");
+    double acc = 0.0;
+    kl_out.line(LS(0.0f));
+    for (int j = 0; j < half; ++j) {
+      for (int i = 0; i < npts; ++i) {
+        const double t = (double)((float)i / (float)(npts - 1));
+        auto& q = qp[(size_t)j * npts + i];
+        q[0] = acc + kdis[j] * t;
+        for (int c = 0; c < 3; ++c) q[1 + c] = kx[2 * j][c] + (kx[2 * j + 1][c] - kx[2 * j][c]) * t;
+      }
+      acc += kdis[j];
+      kl_out.line(LS((float)acc));
+    }
+  }
+  log.line(" threads:" + LI(d.nthreads));
+  log.line("");
+  log.line(" grid:" + LI(d.ngrid[0]) + LI(d.ngrid[1]) + LI(d.ngrid[2]));
+  log.line("");
+  log.line(" ktol-coulomb:" + LD(d.ktol));
+  log.line("");
+  log.line(" kmesh shift:" + LD(d.mshift[0]) + LD(d.mshift[1]) + LD(d.mshift[2]));
+  log.line("");
+  log.line(" conduction bands, nc:" + LI(d.nc) + "   valence bands, nv:" + LI(d.nv));
+  log.line("");
+  log.line(" number of kpoints in the path:   " + LI(nq));
+  log.line("");
+  log.line("");
+  log.line(stamp("begin"));
+  log.line("");
+  log.flush();
+  const int nk = d.ngrid[0] * d.ngrid[1] * d.ngrid[2];
+  const long long N = (long long)nk * d.nc * d.nv;
+  std::vector<double> kpt = kmesh(d.ngrid, d.mshift, m.rlat, nullptr);
+  gpu_check(ctx, wtbg_bands(ctx, nk, kpt.data(), d.nv, d.nc, nullptr, nullptr, nullptr, nullptr), "wtbg_bands");
+  log.line(" quantum numbers for exciton basis set finished");
+  log.flush();
+  wtbg_coulomb p = coulomb_of(d);
+  std::vector<double> exk((size_t)N * nq);
+  for (int iq = 0; iq < nq; ++iq) {
+    const double q3[3] = {qp[iq][1], qp[iq][2], qp[iq][3]};
+    std::vector<double> kq = kmesh(d.ngrid, d.mshift, m.rlat, q3);
+    double q4[4] = {qp[iq][0], qp[iq][1], qp[iq][2], qp[iq][3]};
+    gpu_check(ctx, wtbg_bse_q_eigenvalues(ctx, nk, kq.data(), q4, &p, exk.data() + (size_t)N * iq),
+              "wtbg_bse_q_eigenvalues");
+    log.line(" progress:" + LI(iq + 1) + " /" + LI(nq));
+    log.flush();
+  }
+  std::string buf;
+  for (long long i2 = 0; i2 < N; ++i2) {
+    for (int iq = 0; iq < nq; ++iq) buf += LS((float)qp[iq][0]) + LD(exk[i2 + (size_t)N * iq]) + "\n";
+    buf += "\n";
+  }
+  fputs(buf.c_str(), f400.f);
+  log.line("");
+  log.line(stamp("end"));
+  log.line("");
+}
+
+// ------------------------------------------------------------------------------ spectra
+struct Table {
+  std::vector<double> E;
+  std::vector<double> Fv;   // (n, ncomp) column-major
+  int n = 0, ncomp = 0;
+};
+
+// read_back of a (7F15.4)/(6F15.4) file written above (header line + n rows)
+Table read_table(const std::string& path, int n, int ncol, const char* errmsg) {
+  FILE* f = fopen(path.c_str(), "r");
+  if (!f) throw Stop(errmsg);
+  Table t;
+  t.n = n;
+  t.ncomp = ncol - 1;
+  t.E.resize(n);
+  t.Fv.resize((size_t)n * t.ncomp);
+  char* line = nullptr;
+  size_t cap = 0;
+  if (getline(&line, &cap, f) < 0) throw Stop(std::string(errmsg) + " (empty)");
+  for (int i = 0; i < n; ++i) {
+    if (getline(&line, &cap, f) < 0) throw Stop(std::string(errmsg) + " (short)");
+    char* p = line;
+    for (int c = 0; c < ncol; ++c) {
+      char* end = nullptr;
+      const double v = strtod(p, &end);
+      if (end == p) throw Stop(std::string(errmsg) + " (bad row)");
+      p = end;
+      if (c == 0) t.E[i] = v;
+      else t.Fv[i + (size_t)n * (c - 1)] = v;
+    }
+  }
+  free(line);
+  fclose(f);
+  return t;
+}
+
+struct Spec {
+  std::vector<double> om;
+  std::vector<float> eps;   // (nw, 2, ncomp)
+  int nw = 0, ncomp = 0;
+  float re(int j, int c) const { return eps[j + (size_t)nw * (0 + 2 * c)]; }
+  float im(int j, int c) const { return eps[j + (size_t)nw * (1 + 2 * c)]; }
+};
+
+Spec run_spectrum(wtbg_ctx* ctx, const Deck& d, const Model& m, const Table& t, const std::vector<int>& rtype) {
+  Spec s;
+  s.nw = (int)d.numbse;
+  s.ncomp = t.ncomp;
+  s.om.resize(s.nw);
+  s.eps.resize((size_t)s.nw * 2 * t.ncomp);
+  std::string st = m.systype;
+  while (!st.empty() && st.back() == ' ') st.pop_back();
+  const double spinf = (st == "NP") ? 2.0 : 1.0;
+  gpu_check(ctx, wtbg_spectrum(ctx, t.n, t.ncomp, t.E.data(), t.Fv.data(), rtype.data(), d.ngrid, vcell3d(m.rlat),
+                               d.ebse0, d.ebsef, d.numbse, d.cshift, d.renorm, spinf, s.om.data(), s.eps.data()),
+            "wtbg_spectrum");
+  return s;
+}
+
+void write_diel(const std::string& path, const Spec& s, int c) {
+  Out o(path, ("Error opening " + path).c_str());
+  o.line(" #  energy  real  imag");
+  std::string buf;
+  for (int j = 0; j < s.nw; ++j) buf += LD(s.om[j]) + LS(s.re(j, c)) + LS(s.im(j, c)) + "\n";
+  fputs(buf.c_str(), o.f);
+}
+
+// diel-pp-subs.f90:1-73
+void optprops(double e1, double e2, double efoton, double out[5]) {
+  const double aux = sqrt((e1 * e1) + (e2 * e2));
+  const double refr = sqrt((aux + e1) / 2.0);
+  const double ext = sqrt((aux - e1) / 2.0);
+  const double a1 = (refr - 1.0) * (refr - 1.0), a2 = (refr + 1.0) * (refr + 1.0), a3 = ext * ext;
+  const double refl = (a1 + a3) / (a2 + a3);
+  const double hc = (double)19.746E-06f;
+  const double absc = ((double)sqrtf(2.0f) * efoton) * (1.0 / hc) * sqrt(aux - e1);
+  const double eloss = e2 / ((e1 * e1) + (e2 * e2));
+  out[0] = refr;
+  out[1] = ext;
+  out[2] = refl;
+  out[3] = absc;
+  out[4] = eloss;
+}
+
+// bseoptprop / spoptprop (and -pol): reads the diel files back as written, then 5 files
+void optprop_files(const std::string& of, const std::string& prefix, const std::vector<std::string>& dielnames,
+                   const std::vector<int>& outorder, const std::string& suffix, int nw) {
+  const int nc = (int)dielnames.size();
+  std::vector<std::vector<double>> re(nc, std::vector<double>(nw)), im(nc, std::vector<double>(nw));
+  std::vector<double> energy(nw);
+  for (int c = 0; c < nc; ++c) {
+    FILE* f = fopen((of + dielnames[c]).c_str(), "r");
+    if (!f) throw Stop("Error opening " + dielnames[c] + " input file");
+    char* line = nullptr;
+    size_t cap = 0;
+    if (getline(&line, &cap, f) < 0) throw Stop("empty " + dielnames[c]);
+    for (int i = 0; i < nw; ++i) {
+      if (getline(&line, &cap, f) < 0) throw Stop("short " + dielnames[c]);
+      char* p = line;
+      char* end;
+      const double e = strtod(p, &end);
+      p = end;
+      re[c][i] = strtod(p, &end);
+      p = end;
+      im[c][i] = strtod(p, &end);
+      if (c == 0) energy[i] = e;
+    }
+    free(line);
+    fclose(f);
+  }
+  const char* names[5] = {"refractive_index", "extinction_coef", "reflectibility", "absorption_coef", "en_loss_func"};
+  std::string header = " #  energy";
+  for (int k : outorder) {
+    std::string nm = dielnames[k];
+    nm = nm.substr(nm.rfind('_') + 1);
+    nm = nm.substr(0, nm.find('.'));
+    header += "  " + nm;
+  }
+  for (int q = 0; q < 5; ++q) {
+    Out o(of + prefix + names[q] + suffix + ".dat", "Error opening output file");
+    o.line(header);
+    std::string buf;
+    for (int i = 0; i < nw; ++i) {
+      buf += F(energy[i], 15, 4);
+      for (int k : outorder) {
+        double v[5];
+        optprops(re[k][i], im[k][i], energy[i], v);
+        buf += F(v[q], 15, 4);
+      }
+      buf += "\n";
+    }
+    fputs(buf.c_str(), o.f);
+  }
+}
+
+// exclft (bse_subs.f90:472-530)
+double exclft(const std::string& sysdim0, const int ng[3], const double r[3][3], double fosc, double enexc) {
+  std::string s = sysdim0;
+  while (!s.empty() && s.back() == ' ') s.pop_back();
+  const double cfe = (double)7.297E-3f, lspd = (double)299.792E16f, hbar = (double)6.582E-16f;
+  const double nkt = (double)(ng[0] * ng[1] * ng[2]);
+  if (s == "3D") {
+    const double aux1 = (4.0 * cfe) * (enexc * enexc * enexc);
+    const double aux2 = fosc / nkt;
+    const double aux3 = 3.0 * (lspd * lspd) * (hbar * hbar * hbar);
+    return 1.0 / ((aux1 * aux2) / aux3);
+  }
+  if (s == "2D") {
+    const double aux1 = nkt * vcell2d(r) * hbar;
+    const double aux2 = (8.0 * kPi32 * cfe * enexc) * fosc;
+    return aux1 / aux2;
+  }
+  if (s == "1D") {
+    const double aux2 = (2.0 * kPi32 * cfe * enexc * enexc) * fosc;
+    const double aux1 = nkt * r[0][0] * hbar * hbar * lspd;
+    return aux1 / aux2;
+  }
+  throw Stop("Wrong System dimension");
+}
+
+void lifetime_file(const std::string& of, const Deck& d, const Model& m, const Table& t, bool pol) {
+  Out o(of + (pol ? "exciton_lifetime-pol.dat" : "exciton_lifetime.dat"), "Error opening exciton_lifetime output file");
+  o.line(pol ? " #energy(eV) sum-lft(s)  x-lft(s) y-lft(s) z-lft(s) sp-lft(s) sm-lft(s)"
+             : " #energy(eV) sum-lft(s)  x-lft(s) y-lft(s) z-lft(s)");
+  std::string buf;
+  const int ncol = pol ? 5 : 3;
+  for (int i = 0; i < t.n; ++i) {
+    const double e = t.E[i];
+    auto f = [&](int c) { return t.Fv[i + (size_t)t.n * c]; };
+    buf += F(e, 15, 4) + E(exclft(d.sysdim, d.ngrid, m.rlat, f(0) + f(1) + f(2), e), 15, 4);
+    for (int c = 0; c < ncol; ++c) buf += E(exclft(d.sysdim, d.ngrid, m.rlat, f(c), e), 15, 4);
+    buf += "\n";
+  }
+  fputs(buf.c_str(), o.f);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------ entry
+extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* errbuf, int errlen) {
+  wtbg_ctx* ctx = nullptr;
+  auto fail = [&](const std::string& m) {
+    if (errbuf && errlen > 0) {
+      snprintf(errbuf, (size_t)errlen, "%s", m.c_str());
+    }
+    if (ctx) wtbg_destroy(ctx);
+    return 1;
+  };
+  try {
+    const double t0 = now_s();
+    if (tm) *tm = Timings{};
+    Deck d = parse_deck(deck_text ? deck_text : "");
+    // params header + mesh (wtb_main.f90:77-104)
+    Model m;
+    if (d.bse || d.bsekpath || d.spec || d.spdiel) m = read_params(d.params);
+    if (d.meshtype.rfind("RK3D", 0) == 0) rkmesh(d.rk, m.rlat, d.ngrid, false);
+    else if (d.meshtype.rfind("RK2D", 0) == 0) rkmesh(d.rk, m.rlat, d.ngrid, true);
+    Out log(d.calcparms + "log.dat", "Error opening log output file ");
+    param_out(log, d);
+    log.line("");
+    log.line(stamp("Begin"));
+    log.line("");
+    log.flush();
+    if (d.bset || d.bsetbnd) throw Stop("temperature BSE (BSET/BSET_BND) is not part of this build");
+    int st = wtbg_create(&ctx, device);
+    if (st != 0) return fail(std::string("wtbg_create: ") + wtbg_error_string(st));
+    if (!d.pponly) {
+      if (d.bse) {
+        bsesolver(ctx, d, m, tm);
+        log.line(" BSE and Single particle dielectric calculation finished");
+        log.flush();
+      }
+      if (d.bsekpath) {
+        bsebnds(ctx, d, m);
+        log.line(" BSE exciton band structure finished");
+        log.flush();
+      }
+    }
+    const double t1 = now_s();
+    const int nk = d.ngrid[0] * d.ngrid[1] * d.ngrid[2];
+    const int N = nk * d.nc * d.nv;
+    const std::string of = d.outputfolder;
+    if (d.spec && d.bse) {
+      // bsedielraw / bseoptprop / lifetime (wtb_main.f90:257-300)
+      Table t = read_table(of + "bse_opt_diel.dat", N, 7, "Error opening bse_opt_diel input file");
+      Spec s = run_spectrum(ctx, d, m, t, {1, 1, 1, 0, 0, 0});
+      const char* nm[6] = {"xx", "yy", "zz", "xy", "xz", "yz"};
+      for (int c = 0; c < 6; ++c) write_diel(of + "bse_diel_" + nm[c] + ".dat", s, c);
+      if (tm) tm->spectrum = now_s() - t1;
+      optprop_files(of, "bse_", {"bse_diel_xx.dat", "bse_diel_yy.dat", "bse_diel_zz.dat", "bse_diel_xy.dat",
+                                 "bse_diel_xz.dat", "bse_diel_yz.dat"}, {0, 1, 2, 3, 4, 5}, "", s.nw);
+      lifetime_file(of, d, m, t, false);
+      log.line(" BSE dielectric properties calculated");
+      log.flush();
+      if (d.cpol) {
+        Table tp = read_table(of + "bse_opt_diel-pol.dat", N, 6, "Error opening bse_opt_diel-pol input file");
+        Spec sp = run_spectrum(ctx, d, m, tp, {1, 1, 1, 1, 1});
+        const char* pn[5] = {"x", "y", "z", "sp", "sm"};
+        for (int c = 0; c < 5; ++c) write_diel(of + "bse_diel-pol_" + pn[c] + ".dat", sp, c);
+        optprop_files(of, "bse_", {"bse_diel-pol_x.dat", "bse_diel-pol_y.dat", "bse_diel-pol_z.dat",
+                                   "bse_diel-pol_sp.dat", "bse_diel-pol_sm.dat"}, {0, 1, 2, 3, 4}, "-pol", sp.nw);
+        lifetime_file(of, d, m, tp, true);
+        log.line(" BSE absorption spectrum with light polarization calculated");
+        log.flush();
+      }
+    }
+    if (d.spec && (d.spdiel || d.bse)) {
+      // spdielraw / spoptprop (wtb_main.f90:304-313)
+      Table t = read_table(of + "sp_optics.dat", N, 7, "Error opening sp_optics input file");
+      Spec s = run_spectrum(ctx, d, m, t, {1, 1, 1, 0, 0, 0});
+      const char* nm[6] = {"xx", "yy", "zz", "xy", "xz", "yz"};
+      for (int c = 0; c < 6; ++c) write_diel(of + "sp_diel_" + nm[c] + ".dat", s, c);
+      optprop_files(of, "sp_", {"sp_diel_xx.dat", "sp_diel_yy.dat", "sp_diel_zz.dat", "sp_diel_xy.dat",
+                                "sp_diel_xz.dat", "sp_diel_yz.dat"}, {0, 1, 2, 3, 4, 5}, "", s.nw);
+      log.line(" Single particle dielectric properties calculated");
+      log.flush();
+    }
+    if (d.spec && (d.cpol || d.bse)) {
+      // spdielrawpol / spoptproppol (wtb_main.f90:317-326)
+      Table t = read_table(of + "sp_optics-pol.dat", N, 6, "Error opening sp_optics-pol input file");
+      Spec s = run_spectrum(ctx, d, m, t, {1, 1, 1, 1, 1});
+      const char* pn[5] = {"x", "y", "z", "sp", "sm"};
+      for (int c = 0; c < 5; ++c) write_diel(of + "sp_diel-pol_" + pn[c] + ".dat", s, c);
+      optprop_files(of, "sp_", {"sp_diel-pol_x.dat", "sp_diel-pol_y.dat", "sp_diel-pol_z.dat", "sp_diel-pol_sp.dat",
+                                "sp_diel-pol_sm.dat"}, {0, 1, 2, 3, 4}, "-pol", s.nw);
+      log.line(" Single particle absorption spectrum with light polarization calculated");
+      log.flush();
+    }
+    log.line("");
+    log.line(stamp("End"));
+    log.line("");
+    if (tm) tm->total = now_s() - t0;
+    wtbg_destroy(ctx);
+    ctx = nullptr;
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e.what());
+  }
+}

@@ -21,6 +21,12 @@ distance max(|i|,|j|,|i-j|) <= n_shell (37/61/91 cells for 3/4/5 shells); deg=1;
 H(R) for one of each +-R pair is complex Gaussian * 0.2*exp(-|R|/a) eV with
 H(-R)=H(R)^dagger; H(0) has onsite energies on the diagonal and a Hermitian
 Gaussian*0.2 off-diagonal part.  E_F=0, scs=0, systype NP.
+
+For w > 8 every random coupling (hoppings and the H(0) off-diagonal) is additionally
+scaled by sqrt(8/w): the band width of a random w x w coupling grows like sqrt(w), and
+with the bare 0.2 eV scale the valence and conduction groups of a w=24 model overlap at
+any seed.  The normalisation keeps every material at the band width of the w=8 model,
+so that the gap check (nocp = w/2 at every k, gap > 0) can be met.
 """
 from __future__ import annotations
 
@@ -77,8 +83,12 @@ def hex_rlat(a: float = A_LAT, c: float = C_VAC) -> np.ndarray:
 
 
 def make_hex_model(w: int, n_shell: int, onsite_lo: tuple, onsite_hi: tuple,
-                   seed: int, hop_scale: float = 0.2, h0_scale: float = 0.2) -> TBModel:
+                   seed: int, hop_scale: Optional[float] = None,
+                   h0_scale: Optional[float] = None) -> TBModel:
     """Generate one synthetic model (no gap check; see :func:`make_gapped_model`)."""
+    norm = math.sqrt(8.0 / w) if w > 8 else 1.0
+    hop_scale = 0.2 * norm if hop_scale is None else hop_scale
+    h0_scale = 0.2 * norm if h0_scale is None else h0_scale
     rng = np.random.Generator(np.random.PCG64(seed))
     rlat = hex_rlat()
     rvec = hex_cells(n_shell)

@@ -22,13 +22,20 @@ COULOMB_TYPES = {"V2DK": 1, "V3D": 2, "V3DL": 3, "V2DT": 4, "V2DT2": 5, "V2DOH":
 EXPORTS = ["wtbg_create", "wtbg_destroy", "wtbg_error_string", "wtbg_last_error",
            "wtbg_last_device_ms", "wtbg_set_model", "wtbg_bands", "wtbg_velocity",
            "wtbg_sp_table", "wtbg_bse_build", "wtbg_bse_get_matrix", "wtbg_bse_solve",
-           "wtbg_bse_eigvecs", "wtbg_spectrum", "wtbg_bse_q_eigenvalues"]
+           "wtbg_bse_eigvecs", "wtbg_spectrum", "wtbg_bse_q_eigenvalues", "wtbg_set_profiling",
+           "wtbg_get_stats", "wtbg_reset_stats"]
 
 
 class WtbgError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"wtbg status {status}: {message}")
         self.status = status
+
+
+class Stats(C.Structure):
+    _fields_ = [("launches", C.c_longlong), ("hemv_launches", C.c_longlong), ("hemv_ms", C.c_double),
+                ("hemv_bytes", C.c_double), ("build_launches", C.c_longlong), ("build_ms", C.c_double),
+                ("build_bytes", C.c_double)]
 
 
 class Coulomb(C.Structure):
@@ -66,9 +73,12 @@ def load_library(path: str = LIB_PATH):
         "wtbg_bse_get_matrix": (C.c_int, [P, dp]),
         "wtbg_bse_solve": (C.c_int, [P, C.c_int, C.c_int, dp, dp]),
         "wtbg_bse_eigvecs": (C.c_int, [P, C.c_int, C.c_int, dp]),
-        "wtbg_spectrum": (C.c_int, [P, C.c_int, dp, dp, ip, C.c_double, C.c_double, C.c_double,
+        "wtbg_spectrum": (C.c_int, [P, C.c_int, C.c_int, dp, dp, ip, ip, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, C.c_int, C.c_double, dp, fp]),
         "wtbg_bse_q_eigenvalues": (C.c_int, [P, C.c_int, dp, dp, C.POINTER(Coulomb), dp]),
+        "wtbg_set_profiling": (C.c_int, [P, C.c_int]),
+        "wtbg_get_stats": (C.c_int, [P, C.POINTER(Stats)]),
+        "wtbg_reset_stats": (C.c_int, [P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -147,6 +157,17 @@ class Context:
     def last_ms(self) -> float:
         return float(self.lib.wtbg_last_device_ms(self.h))
 
+    def set_profiling(self, on: bool) -> None:
+        self._check(self.lib.wtbg_set_profiling(self.h, int(bool(on))))
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(self.lib.wtbg_get_stats(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    def reset_stats(self) -> None:
+        self._check(self.lib.wtbg_reset_stats(self.h))
+
     # ---------------------------------------------------------------- stages
     def set_model(self, model) -> None:
         # (nvec, w, w) arrays in Fortran order = hopmatrices(iR, m, n)
@@ -203,17 +224,22 @@ class Context:
         self._check(self.lib.wtbg_bse_eigvecs(self.h, n0, n1, A.ctypes.data_as(C.POINTER(C.c_double))))
         return A
 
-    def spectrum(self, E, F, ngrid, vcell3d, ebse0, ebsef, numbse, sme, renorm, spinf):
+    def spectrum(self, E, F, ngrid, vcell3d, ebse0, ebsef, numbse, sme, renorm, spinf, rtype=None):
+        """optdiel over the photon grid for every column of F (n, ncomp); returns
+        (omega (nw,), eps (nw, 2, ncomp) float32)."""
         E = _f64(E)
         F = _f64(F)
-        n = E.shape[0]
+        n, ncomp = F.shape
+        if rtype is None:
+            rtype = [1, 1, 1, 0, 0, 0][:ncomp] if ncomp == 6 else [1] * ncomp
+        rt = np.array(rtype, dtype=np.int32)
         nw = int(numbse)
         ng = np.array(ngrid, dtype=np.int32)
         om = np.zeros(nw)
-        eps = np.zeros((nw, 2, 6), dtype=np.float32, order="F")
-        self._check(self.lib.wtbg_spectrum(self.h, n, _dp(E), _dp(F), _ip(ng), float(vcell3d), float(ebse0),
-                                           float(ebsef), float(numbse), float(sme), int(bool(renorm)),
-                                           float(spinf), _dp(om), _fp(eps)))
+        eps = np.zeros((nw, 2, ncomp), dtype=np.float32, order="F")
+        self._check(self.lib.wtbg_spectrum(self.h, n, ncomp, _dp(E), _dp(F), _ip(rt), _ip(ng), float(vcell3d),
+                                           float(ebse0), float(ebsef), float(numbse), float(sme),
+                                           int(bool(renorm)), float(spinf), _dp(om), _fp(eps)))
         return om, eps
 
     def bse_q_eigenvalues(self, kptq, q4, coul: Coulomb):
