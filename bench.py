@@ -48,6 +48,11 @@ WORKLOADS = {
                desc="config 5 size: w=16, 61 cells, 60x60x1 mesh, nv=nc=2, N=14400, V2DRK r0=35"),
     "c1": dict(model="c1", n=12, nv=2, nc=2, r0=40.0, cshift=0.05, ebsef=5.0, nespec=1001,
                desc="config 1: w=8, 37 cells, 12x12x1 mesh, nv=nc=2, N=576, V2DRK r0=40, eps 0-5 eV x1001"),
+    # smaller meshes of the config-2 model, for profiling captures
+    "c2s": dict(model="c2", n=12, nv=4, nc=4, r0=30.0, cshift=0.03, ebsef=6.0, nespec=2001,
+                desc="config-2 model on a 12x12x1 mesh, nv=nc=4, N=2304"),
+    "c2m": dict(model="c2", n=24, nv=4, nc=4, r0=30.0, cshift=0.03, ebsef=6.0, nespec=2001,
+                desc="config-2 model on a 24x24x1 mesh, nv=nc=4, N=9216"),
 }
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -271,6 +276,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=os.environ.get("WTB_BENCH_WORKLOAD", "c2"), choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--device-only", action="store_true",
+                    help="only the device-resident steps (no e2e run, no CPU baseline): profiling captures")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
 
@@ -334,6 +341,10 @@ def main():
     per_step = [sum(s.values()) for s in steps]
     t_dev = float(np.mean(per_step))
     ctx.close()
+    if args.device_only:
+        print(json.dumps({"metric": metric, "value": t_dev, "unit": unit, "stages_s": steps[-1],
+                          "config": cfg, "device_only": True}))
+        return
     # e2e through the deck-level C entry (host buffers, files)
     workdir = tempfile.mkdtemp(prefix="wtb_bench_")
     synth.write_params(model, os.path.join(workdir, "tb_synthetic.dat"))
