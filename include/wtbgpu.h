@@ -137,6 +137,26 @@ int wtbg_spectrum(wtbg_ctx* ctx, int n, int ncomp, const double* ebse, const dou
                   double ebsef, double numbse, double sme, int renorm, double spinf,
                   double* omega, float* eps);
 
+/* Allocation-free variant of wtbg_spectrum (no counterpart in the reference).
+ * For hosts that cannot let a library allocate device memory: applications that hand out
+ * all device memory from their own pool or a fixed arena, and services that must not call
+ * cudaMalloc/cudaFree during a run because those calls can synchronise the whole device and
+ * can fail with out-of-memory part-way through.  The caller owns every buffer:
+ * d_ebse (n), d_fosc (n,ncomp), d_omega (nw) and d_eps (nw,2,ncomp) are DEVICE pointers on
+ * the current device; rtype (ncomp) and ngrid (3) are host arrays; stream is a cudaStream_t
+ * (NULL = default stream).  The kernels' scratch is a fixed static device array of
+ * 2*8*8192+32 doubles (about 1 MB) that every GPU loading this library keeps until exit, so
+ * nw = int(numbse) must be <= 8192 and ncomp <= 8; larger sizes return WTBG_ERR_UNSUPPORTED
+ * with a message in errbuf.  The first call on a device looks up the scratch address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All calls share the
+ * scratch: calls whose work overlaps on the GPU (different streams or host threads without
+ * ordering) race.  Nothing in the scratch has to start at zero.  The call is asynchronous on
+ * `stream`; no memory is allocated or freed. */
+int wtbg_spectrum_noalloc(int n, int ncomp, const double* d_ebse, const double* d_fosc,
+                          const int* rtype, const int* ngrid, double vcell3d, double ebse0,
+                          double ebsef, double numbse, double sme, int renorm, double spinf,
+                          double* d_omega, float* d_eps, void* stream, char* errbuf, int errlen);
+
 /* ---- exciton band structure: one centre-of-mass Q of bsebnds
  *      (bse_kpath-tool.f90:246-435; matrizelbsekq = bse_subs_kpath.f90:1-208).
  *      Uses the k-mesh bands of the last wtbg_bands call; kptq (nk,3) is the k+Q mesh

@@ -10,6 +10,9 @@
 //   the next grid point (clamped at 0), and every value is written as real(spinf * x).
 // One warp per photon energy reduces over the excitons with shuffles; the six tensor
 // components share the two divisions of each (w, n) term.
+#include <cstdio>
+#include <mutex>
+
 #include "common.cuh"
 
 namespace {
@@ -136,4 +139,86 @@ int launch_spectrum(wtbg_ctx* ctx, int n, int ncomp, const double* d_e, const do
   k_renorm_out<<<1, 32, 0, ctx->stream>>>(d_e, d_om, re, im, nw, ncomp, renorm, spinf, d_eps); WTBG_COUNT(ctx, 1);
   CKL("k_renorm_out");
   return 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free entry point.  The scratch of the three spectrum kernels (Re/Im sums per
+// component and photon energy, and eta) lives in this fixed file-scope device array instead
+// of context buffers, so the call performs no device allocation.  Host code must not use
+// the symbol itself as an address: the device address is looked up once per device with
+// cudaGetSymbolAddress while that device is current.
+namespace {
+constexpr int kNoAllocMaxNw = 8192;
+constexpr int kNoAllocMaxComp = 8;
+constexpr size_t kNoAllocScratch = 2 * (size_t)kNoAllocMaxComp * kNoAllocMaxNw + 32;
+constexpr int kMaxDevices = 64;
+
+double* g_noalloc_ptr[kMaxDevices] = {nullptr};
+std::mutex g_noalloc_mu;
+
+int noalloc_fail(char* errbuf, int errlen, int code, const char* msg) {
+  if (errbuf && errlen > 0) snprintf(errbuf, (size_t)errlen, "%s", msg);
+  return code;
+}
+}  // namespace
+
+static __device__ __align__(256) double g_spectrum_scratch[kNoAllocScratch];
+
+extern "C" int wtbg_spectrum_noalloc(int n, int ncomp, const double* d_ebse, const double* d_fosc, const int* rtype,
+                                     const int* ngrid, double vcell3d, double ebse0, double ebsef, double numbse,
+                                     double sme, int renorm, double spinf, double* d_omega, float* d_eps,
+                                     void* stream, char* errbuf, int errlen) {
+  if (!d_ebse || !d_fosc || !rtype || !ngrid || !d_omega || !d_eps)
+    return noalloc_fail(errbuf, errlen, WTBG_ERR_ARG, "spectrum_noalloc: null pointer");
+  const int nw = (int)numbse;
+  if (n <= 0 || nw < 2 || ncomp < 1)
+    return noalloc_fail(errbuf, errlen, WTBG_ERR_ARG, "spectrum_noalloc: bad sizes");
+  if (nw > kNoAllocMaxNw || ncomp > kNoAllocMaxComp)
+    return noalloc_fail(errbuf, errlen, WTBG_ERR_UNSUPPORTED,
+                        "spectrum_noalloc: NESPEC above 8192 or more than 8 components exceeds the fixed scratch");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return noalloc_fail(errbuf, errlen, WTBG_ERR_CUDA, "spectrum_noalloc: no current device");
+  }
+  double* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_spectrum_scratch);
+      if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return noalloc_fail(errbuf, errlen, WTBG_ERR_CUDA, "spectrum_noalloc: cudaGetSymbolAddress failed");
+      }
+      g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* re = scratch;
+  double* im = re + (size_t)ncomp * nw;
+  double* eta = im + (size_t)ncomp * nw;
+  SpecRtype rt{};
+  for (int c = 0; c < ncomp; ++c) rt.rt[c] = rtype[c];
+  const double baux = (double)(float)(ngrid[0] * ngrid[1] * ngrid[2]) * vcell3d;
+  const double caux = (double)180.90f / (baux * 1.0);
+  k_avgsme<<<1, 32, 0, s>>>(d_ebse, n, sme, eta);
+  const int threads = 256;
+  const int blocks = (nw * 32 + threads - 1) / threads;
+  switch (ncomp) {
+#define WTBG_SPEC_CASE(K)                                                                                    \
+  case K:                                                                                                    \
+    k_spectrum<K><<<blocks, threads, 0, s>>>(d_ebse, d_fosc, n, eta, ebse0, ebsef, numbse, nw, caux, rt,     \
+                                             d_omega, re, im);                                               \
+    break;
+    WTBG_SPEC_CASE(1) WTBG_SPEC_CASE(2) WTBG_SPEC_CASE(3) WTBG_SPEC_CASE(4)
+    WTBG_SPEC_CASE(5) WTBG_SPEC_CASE(6) WTBG_SPEC_CASE(7) WTBG_SPEC_CASE(8)
+#undef WTBG_SPEC_CASE
+    default: break;
+  }
+  k_renorm_out<<<1, 32, 0, s>>>(d_ebse, d_omega, re, im, nw, ncomp, renorm, spinf, d_eps);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return noalloc_fail(errbuf, errlen, WTBG_ERR_CUDA, cudaGetErrorString(e));
+  return WTBG_OK;
 }

@@ -23,7 +23,7 @@ EXPORTS = ["wtbg_create", "wtbg_destroy", "wtbg_error_string", "wtbg_last_error"
            "wtbg_last_device_ms", "wtbg_set_model", "wtbg_bands", "wtbg_velocity",
            "wtbg_sp_table", "wtbg_bse_build", "wtbg_bse_get_matrix", "wtbg_bse_solve",
            "wtbg_bse_eigvecs", "wtbg_spectrum", "wtbg_bse_q_eigenvalues", "wtbg_set_profiling",
-           "wtbg_get_stats", "wtbg_reset_stats"]
+           "wtbg_get_stats", "wtbg_reset_stats", "wtbg_spectrum_noalloc"]
 
 
 class WtbgError(RuntimeError):
@@ -79,6 +79,10 @@ def load_library(path: str = LIB_PATH):
         "wtbg_set_profiling": (C.c_int, [P, C.c_int]),
         "wtbg_get_stats": (C.c_int, [P, C.POINTER(Stats)]),
         "wtbg_reset_stats": (C.c_int, [P]),
+        "wtbg_spectrum_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, ip, ip, C.c_double,
+                                            C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                            C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p,
+                                            C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
