@@ -124,6 +124,33 @@ int wtbg_bse_solve(wtbg_ctx* ctx, int dtfull, int cpol, double* W, double* act);
  * normalised with its last component real and >= 0. */
 int wtbg_bse_eigvecs(wtbg_ctx* ctx, int n0, int n1, double* A);
 
+/* ---- fast form: the nev lowest (largest = 0) or highest (largest = 1) eigenpairs of the
+ *      built BSE matrix by block Davidson in FP64 (no counterpart in the reference: it
+ *      replaces the dense ZHEEV when only the lowest excitons are needed; its oracle is the
+ *      dense solve).  nb = block size (multiple of 8, nev <= nb <= 40); X0 (N,nb) complex
+ *      optional initial block (NULL: unit vectors at the smallest / largest diagonal
+ *      entries); convergence when every residual |H x - theta x| of the nev wanted states
+ *      is below tol (eV) or after max_iter iterations.  Outputs W (nev), act (nev,8) as in
+ *      wtbg_bse_solve (requires wtbg_velocity; may be NULL), X (N,nev) complex eigenvectors
+ *      (may be NULL), iterations used and the largest final residual.  The BSE matrix is
+ *      kept, so the call can be repeated (e.g. lowest and highest states). */
+int wtbg_bse_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, double tol,
+                      const double* X0, int dtfull, int cpol, double* W, double* act, double* X,
+                      int* iters, double* maxres);
+
+/* ---- fast form of the BSE spectrum: eps(omega) of bsedielraw (and bsedielrawpol) from the
+ *      Haydock recursion on the built BSE matrix, nsteps Lanczos steps per chain closed by a
+ *      square-root terminator (no counterpart in the reference; oracle = dense solve +
+ *      optdiel).  Because the reference's oscillator has no conjugate on the exciton vector,
+ *      sum_n f_n/(z - E_n) = u^H (z - H)^-1 u with u = conj(h).  The broadening follows
+ *      avgsme: eta = sme + 10 (emax - e1) / N, with e1, emax the lowest and highest exciton
+ *      energies (wtbg_bse_davidson gives both); imagrenorm uses e1.  eps (nw,2,8) as real(4):
+ *      components xx, yy, zz, xy, xz, yz, sp, sm (xy/xz/yz only if dtfull, sp/sm only if cpol,
+ *      else zero).  Requires wtbg_velocity and wtbg_bse_build; keeps the matrix. */
+int wtbg_bse_spectrum_fast(wtbg_ctx* ctx, int nsteps, int dtfull, int cpol, double e1, double emax,
+                           const int* ngrid, double vcell3d, double ebse0, double ebsef, double numbse,
+                           double sme, int renorm, double spinf, double* omega, float* eps);
+
 /* ---- spectrum: replaces the omega loop of bsedielraw with optdiel, avgsme and
  *      imagrenorm (bse_diel-tool.f90:137-210; optics.f90:160-390), and the same loop of
  *      bsedielrawpol, spdielraw and spdielrawpol (bse_diel-tool-pol.f90, sp_diel-tool.f90,

@@ -1,0 +1,76 @@
+"""Fast form: block Davidson for the lowest / highest excitons against the dense FP64 solve."""
+import numpy as np
+import pytest
+
+from oracle import wtb_oracle as O
+from oracle.deck import parse_deck
+from wantibexos_b200 import synth, wtbgpu
+
+pytestmark = pytest.mark.gpu
+
+
+def setup(ctx, n=12):
+    m = synth.config_model("c1")
+    deck = parse_deck(f"NGX= {n}\nNGY= {n}\nNGZ= 1\nNBANDSV= 2\nNBANDSC= 2\nCOULOMB_POT= V2DRK\nR_0= 40\n"
+                      "CSHIFT= 0.05\nKTOL= 0.001\n")
+    kpts = O.monkhorst_pack(n, n, 1, [0, 0, 0], m.rlat)
+    ctx.set_model(m)
+    ctx.bands(kpts, 2, 2, want_vectors=False)
+    ctx.velocity(0.05, want=False)
+    c = wtbgpu.coulomb_params("V2DRK", [n, n, 1], deck["ktol"], deck["ediel"], deck["lc"], deck["ez"], deck["w"],
+                              deck["r0"])
+    ctx.bse_build(c)
+    return c
+
+
+def test_davidson_lowest_and_highest_match_dense(gpu_ctx):
+    c = setup(gpu_ctx)
+    W, act, X, it, res = gpu_ctx.bse_davidson(16, nb=24, tol=1e-7, dtfull=True, want_vectors=True)
+    Wt, _, _, it2, res2 = gpu_ctx.bse_davidson(4, nb=8, largest=True, tol=1e-7, want_act=False)
+    Wd, actd = gpu_ctx.bse_solve(True, False)
+    assert res < 1e-7 and res2 < 1e-7
+    assert np.abs(W - Wd[:16]).max() < 1e-9
+    assert np.abs(Wt - Wd[::-1][:4]).max() < 1e-9
+    scale = np.abs(actd[:16, :3]).max()
+    assert np.abs(act[:, :3] - actd[:16, :3]).max() < 1e-4 * scale
+    # orthonormal eigenvectors
+    G = X.conj().T @ X
+    assert np.abs(G - np.eye(16)).max() < 1e-10
+
+
+def test_davidson_warm_start_converges_faster(gpu_ctx):
+    setup(gpu_ctx)
+    W, _, X, it_cold, _ = gpu_ctx.bse_davidson(8, nb=16, tol=1e-8, want_act=False, want_vectors=True)
+    rng = np.random.default_rng(0)
+    X0 = np.zeros((gpu_ctx.N, 16), dtype=np.complex128)
+    X0[:, :8] = X + 1e-3 * (rng.standard_normal(X.shape) + 1j * rng.standard_normal(X.shape))
+    X0[:, 8:] = rng.standard_normal((gpu_ctx.N, 8))
+    W2, _, _, it_warm, _ = gpu_ctx.bse_davidson(8, nb=16, tol=1e-8, X0=X0, want_act=False)
+    assert np.abs(W2 - W).max() < 1e-10
+    assert it_warm < it_cold
+
+
+@pytest.mark.parametrize("dtfull,cpol", [(False, False), (True, True)])
+def test_haydock_spectrum_matches_dense(gpu_ctx, dtfull, cpol):
+    """Fast-form eps(omega) (Haydock) against optdiel over all excitons of the dense solve
+    (unrounded oscillators, same eta and renormalisation)."""
+    setup(gpu_ctx)
+    m = synth.config_model("c1")
+    lo = gpu_ctx.bse_davidson(1, nb=8, tol=1e-8, want_act=False)[0][0]
+    hi = gpu_ctx.bse_davidson(1, nb=8, largest=True, tol=1e-8, want_act=False)[0][0]
+    vc = O.vcell3d(m.rlat)
+    om, eps = gpu_ctx.bse_spectrum_fast(200, lo, hi, [12, 12, 1], vc, 0.0, 5.0, 501.0, 0.05, True, 2.0,
+                                        dtfull=dtfull, cpol=cpol)
+    W, act = gpu_ctx.bse_solve(dtfull, cpol)
+    cols = [0, 1, 2, 3, 4, 5, 6, 7]
+    for o in cols:
+        if (3 <= o <= 5 and not dtfull) or (o >= 6 and not cpol):
+            assert np.all(eps[:, :, o] == 0)
+            continue
+        rtype = 0 if 3 <= o <= 5 else 1
+        re, im = O.optdiel_grid(rtype, vc, [12, 12, 1], om, W, act[:, o], 0.05)
+        d = O.bsedielraw("NP", m.rlat, [12, 12, 1], W, np.column_stack([act[:, o]] * 6), 0.0, 5.0, 501.0, 0.05, True)
+        want = d["xx" if rtype == 1 else "xy"]
+        scale = np.abs(want[:, 1:]).max()
+        assert np.abs(eps[:, 0, o] - want[:, 1]).max() <= 2e-5 * scale, o
+        assert np.abs(eps[:, 1, o] - want[:, 2]).max() <= 2e-5 * scale, o

@@ -362,6 +362,111 @@ int wtbg_bse_solve(wtbg_ctx* ctx, int dtfull, int cpol, double* W, double* act) 
   return WTBG_OK;
 }
 
+int wtbg_bse_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, double tol, const double* X0,
+                      int dtfull, int cpol, double* W, double* act, double* X, int* iters, double* maxres) {
+  if (!ctx || !W) return WTBG_ERR_ARG;
+  if (!ctx->have_matrix) return set_err(ctx, WTBG_ERR_STATE, "bse_davidson: call wtbg_bse_build first");
+  if (act && !ctx->have_velocity) return set_err(ctx, WTBG_ERR_STATE, "bse_davidson: call wtbg_velocity first");
+  if (nev < 1 || nev > ctx->N || nb > ctx->N || max_iter < 1 || !(tol > 0))
+    return set_err(ctx, WTBG_ERR_ARG, "bse_davidson: bad arguments");
+  if (int r = set_device(ctx)) return r;
+  const long long N = ctx->N;
+  Timer t(ctx);
+  double2* dX0 = nullptr;
+  if (X0) {
+    ENSURE(ctx->zsel, (size_t)N * nb * 16);
+    dX0 = ctx->zsel.as<double2>();
+    CK(cudaMemcpyAsync(dX0, X0, (size_t)N * nb * 16, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  double2* dX = nullptr;
+  if (X) {
+    ENSURE(ctx->yv, (size_t)N * nev * 16);
+    dX = ctx->yv.as<double2>();
+  }
+  std::vector<double> w, ac;
+  int it = 0;
+  double mr = 0.0;
+  if (int r = run_davidson(ctx, nev, nb, largest, max_iter, tol, dX0, dtfull, cpol, w, ac, dX, &it, &mr)) return r;
+  if (int r = t.stop()) return r;
+  memcpy(W, w.data(), (size_t)nev * 8);
+  if (act) memcpy(act, ac.data(), (size_t)nev * 8 * 8);
+  if (X) CK(cudaMemcpy(X, dX, (size_t)N * nev * 16, cudaMemcpyDeviceToHost));
+  if (iters) *iters = it;
+  if (maxres) *maxres = mr;
+  if (mr >= tol) return set_err(ctx, WTBG_ERR_NOCONV, "bse_davidson: residual above tolerance after max_iter");
+  return WTBG_OK;
+}
+
+int wtbg_bse_spectrum_fast(wtbg_ctx* ctx, int nsteps, int dtfull, int cpol, double e1, double emax, const int* ngrid,
+                           double vcell3d, double ebse0, double ebsef, double numbse, double sme, int renorm,
+                           double spinf, double* omega, float* eps) {
+  if (!ctx || !ngrid || !omega || !eps) return WTBG_ERR_ARG;
+  if (!ctx->have_matrix) return set_err(ctx, WTBG_ERR_STATE, "bse_spectrum_fast: call wtbg_bse_build first");
+  if (!ctx->have_velocity) return set_err(ctx, WTBG_ERR_STATE, "bse_spectrum_fast: call wtbg_velocity first");
+  const int nw = (int)numbse;
+  if (nsteps < 2 || nw < 2) return set_err(ctx, WTBG_ERR_ARG, "bse_spectrum_fast: bad sizes");
+  if (int r = set_device(ctx)) return r;
+  // chains: x, y, z [, x+y, x-y, x+z, x-z, y+z, y-z] [, sp, sm]
+  std::vector<int> codes = {0, 1, 2};
+  if (dtfull)
+    for (int k = 5; k <= 10; ++k) codes.push_back(k);
+  const int isp = (int)codes.size();
+  if (cpol) {
+    codes.push_back(3);
+    codes.push_back(4);
+  }
+  // outputs (kind, chain): 8 components, absent ones point at chain 0 with kind 2 (zero)
+  std::vector<int> oc(16);
+  auto put = [&](int o, int kind, int ch) {
+    oc[2 * o] = kind;
+    oc[2 * o + 1] = ch;
+  };
+  put(0, 0, 0);
+  put(1, 0, 1);
+  put(2, 0, 2);
+  if (dtfull) {
+    put(3, 1, 3);
+    put(4, 1, 5);
+    put(5, 1, 7);
+  } else {
+    put(3, 1, 0);
+    put(4, 1, 0);
+    put(5, 1, 0);
+  }
+  if (cpol) {
+    put(6, 0, isp);
+    put(7, 0, isp + 1);
+  } else {
+    put(6, 1, 0);
+    put(7, 1, 0);
+  }
+  const long long N = ctx->N;
+  const double eta = sme + 10.0 * ((emax - e1) / (double)N);
+  Timer t(ctx);
+  std::vector<double> al, be, n2;
+  if (int r = run_haydock(ctx, nsteps, (int)codes.size(), codes.data(), al, be, n2)) return r;
+  ENSURE(ctx->sp_om, (size_t)nw * 8 + (size_t)nw * 16 * 4 + 64);
+  double* dom = ctx->sp_om.as<double>();
+  float* deps = reinterpret_cast<float*>(dom + nw);
+  if (int r = run_haydock_spectrum(ctx, nsteps, (int)codes.size(), al.data(), be.data(), n2.data(), 8, oc.data(), ngrid,
+                                   vcell3d, ebse0, ebsef, numbse, eta, e1, renorm, spinf, dom, deps))
+    return r;
+  CK(cudaMemcpyAsync(omega, dom, (size_t)nw * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(eps, deps, (size_t)nw * 16 * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  if (int r = t.stop()) return r;
+  // components that were not requested (kind 1 on chain 0 with chain 0 - chain 1 is not zero):
+  // zero them explicitly
+  for (int o = 3; o < 8; ++o) {
+    const bool want = (o < 6) ? dtfull : cpol;
+    if (!want)
+      for (int j = 0; j < nw; ++j) {
+        eps[(size_t)j + (size_t)nw * (0 + 2 * o)] = 0.0f;
+        eps[(size_t)j + (size_t)nw * (1 + 2 * o)] = 0.0f;
+      }
+  }
+  return WTBG_OK;
+}
+
 int wtbg_bse_eigvecs(wtbg_ctx* ctx, int n0, int n1, double* A) {
   if (!ctx || !A) return WTBG_ERR_ARG;
   if (!ctx->have_solution || ctx->csize_host.empty())

@@ -139,6 +139,13 @@ int launch_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p, const double* q4);
 int run_tridiagonalise(wtbg_ctx* ctx);
 int run_tridiagonal_solve(wtbg_ctx* ctx, int dtfull, int cpol, bool vectors);
 int run_eigvecs(wtbg_ctx* ctx, int n0, int n1, double2* d_out);
+int run_haydock(wtbg_ctx* ctx, int K, int ncomp, const int* codes, std::vector<double>& alpha, std::vector<double>& beta,
+                std::vector<double>& norm2);
+int run_haydock_spectrum(wtbg_ctx* ctx, int K, int nchain, const double* alpha, const double* beta, const double* norm2,
+                         int nout, const int* ocode, const int* ngrid, double vcell3d, double ebse0, double ebsef,
+                         double numbse, double eta, double e1, int renorm, double spinf, double* d_om, float* d_eps);
+int run_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, double tol, const double2* dX0, int dtfull,
+                 int cpol, std::vector<double>& W, std::vector<double>& act, double2* dXout, int* iters, double* maxres);
 int launch_spectrum(wtbg_ctx* ctx, int n, int ncomp, const double* d_e, const double* d_f, const int* rtype,
                     const int* ngrid, double vcell3d, double ebse0, double ebsef, double numbse, double sme,
                     int renorm, double spinf, double* d_om, float* d_eps);

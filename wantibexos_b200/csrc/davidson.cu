@@ -1,0 +1,1031 @@
+// Block Davidson on the built BSE matrix: the lowest (or highest) exciton states without a
+// dense solve.  This is the fast form of the path (no reference counterpart; its oracle is
+// the dense FP64 solve).  All arithmetic is FP64; the matrix is the lower-stored Hermitian
+// N x N array written by k_bse_build and is not modified.
+//
+// Iteration (basis V = [X T], nb + nb columns):
+//   R = H X - X diag(theta),  T = R / (diag(H) - theta)   (Davidson preconditioner)
+//   T <- T - X (X^H T) (twice), T <- T chol(T^H T)^-1 (twice: CholQR2)
+//   M = V^H (H V)  (2nb x 2nb),  (theta, Y) = eig(M) by one-CTA Jacobi,  X = V Y, HX = HV Y
+// Oscillator strengths of the converged states: f_n = |sum_j X_jn h_j|^2 (dielbsev,
+// bse_subs.f90:336-378, no conjugate on the eigenvector).
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include <cub/cub.cuh>
+
+#include "common.cuh"
+
+namespace {
+
+constexpr int TB = 64;        // tile edge
+constexpr int JCH = 8;        // column chunks of the Hermitian product (partials)
+constexpr int NG = 5;
+constexpr int kMaxRR = 80;    // largest Rayleigh-Ritz size (two 80x80 complex matrices fit in one CTA)
+
+// Y[part][N][m] partial of H X over the block-columns of chunk blockIdx.y; H lower-stored.
+// Thread layout: 256 threads = 32 row pairs x 8 vector groups; each thread owns rows
+// (r, r+32) and MV vectors.
+template <int MV>
+__global__ void __launch_bounds__(256) k_hemm(const double2* __restrict__ A, long long N, const double2* __restrict__ X,
+                                              int ldx, double2* __restrict__ Yp) {
+  constexpr int M = 8 * MV;
+  extern __shared__ __align__(16) unsigned char hsm[];
+  double2 (*tile)[TB + 1] = reinterpret_cast<double2 (*)[TB + 1]>(hsm);                      // tile[c][r]
+  double2 (*xs)[M + 1] = reinterpret_cast<double2 (*)[M + 1]>(hsm + sizeof(double2) * TB * (TB + 1));  // xs[c][v]
+  const int I = blockIdx.x;
+  const int nblk = (int)((N + TB - 1) / TB);
+  const int tid = threadIdx.x;
+  const int r = tid & 31, vg = tid >> 5;
+  double2 acc[2][MV];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int v = 0; v < MV; ++v) acc[a][v] = make_double2(0, 0);
+  const int jper = (nblk + JCH - 1) / JCH;
+  const int J0 = blockIdx.y * jper, J1 = min(nblk, J0 + jper);
+  const long long R0 = (long long)I * TB;
+  for (int J = J0; J < J1; ++J) {
+    const long long C0 = (long long)J * TB;
+    __syncthreads();
+    // load H(I,J): J < I from the lower tile (rows I, cols J); J > I from the conj
+    // transpose of the lower tile (rows J, cols I); J == I from the lower part of the
+    // diagonal tile, mirrored.
+    for (int it = tid; it < TB * TB; it += 256) {
+      const int a = it & (TB - 1), b = it >> 6;   // a fastest: coalesced global reads
+      double2 v = make_double2(0, 0);
+      if (J < I) {
+        const long long rr = R0 + a, cc = C0 + b;
+        if (rr < N && cc < N) v = A[rr + cc * N];
+        tile[b][a] = v;                 // H(R0+a, C0+b)
+      } else if (J > I) {
+        const long long rr = C0 + a, cc = R0 + b;   // lower element (C0+a, R0+b)
+        if (rr < N && cc < N) v = cconj(A[rr + cc * N]);
+        tile[a][b] = v;                 // H(R0+b, C0+a) = conj(L(C0+a, R0+b))
+      } else {
+        const long long rr = R0 + a, cc = C0 + b;
+        if (rr < N && cc < N) {
+          if (a > b) {
+            v = A[rr + cc * N];
+            tile[b][a] = v;
+            tile[a][b] = cconj(v);
+          } else if (a == b) {
+            v = A[rr + cc * N];
+            tile[a][a] = make_double2(v.x, 0.0);
+          }
+        } else {
+          tile[b][a] = make_double2(0, 0);
+          tile[a][b] = make_double2(0, 0);
+        }
+      }
+    }
+    for (int it = tid; it < TB * M; it += 256) {
+      const int c = it % TB, v = it / TB;
+      const long long rr = C0 + c;
+      xs[c][v] = (rr < N) ? X[rr + (long long)v * ldx] : make_double2(0, 0);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int c = 0; c < TB; ++c) {
+      const double2 h0 = tile[c][r], h1 = tile[c][r + 32];
+#pragma unroll
+      for (int v = 0; v < MV; ++v) {
+        const double2 x = xs[c][vg * MV + v];
+        acc[0][v] = cadd(acc[0][v], cmul(h0, x));
+        acc[1][v] = cadd(acc[1][v], cmul(h1, x));
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+    const long long rr = R0 + r + 32 * a;
+    if (rr >= N) continue;
+#pragma unroll
+    for (int v = 0; v < MV; ++v)
+      Yp[((long long)blockIdx.y * M + vg * MV + v) * N + rr] = acc[a][v];
+  }
+}
+
+// Y = H X reading every lower tile once (for narrow blocks, M = 8*MV <= 16): a CTA streams a
+// chunk of up to LHS tiles down block-column J.  Row products L_IJ X_J go to slot[I][J];
+// column products L_IJ^H X_I accumulate in registers over the chunk and go to slot[J][I0]
+// (zeros for the other tiles of the chunk; added into slot[J][J] for the chunk holding the
+// diagonal tile), so that Y_a = sum_b slot[a][b].  Slot layout [a][b][v][64].
+constexpr int LHS = 8;
+template <int MV>
+__global__ void __launch_bounds__(256) k_hemm_lower(const double2* __restrict__ A, long long N, const double2* __restrict__ X,
+                                                    int ldx, int nblk, double2* __restrict__ slots) {
+  constexpr int M = 8 * MV;
+  extern __shared__ __align__(16) unsigned char hsm[];
+  double2 (*tile)[TB + 1] = reinterpret_cast<double2 (*)[TB + 1]>(hsm);   // tile[c][r] = H(R0+r, C0+c)
+  double2 (*xJ)[M + 1] = reinterpret_cast<double2 (*)[M + 1]>(hsm + sizeof(double2) * TB * (TB + 1));
+  double2 (*xI)[M + 1] = xJ + TB;
+  const int J = blockIdx.x;
+  const int I0 = J + blockIdx.y * LHS;
+  if (I0 >= nblk) return;
+  const int I1 = min(I0 + LHS, nblk);
+  const int tid = threadIdx.x, r = tid & 31, vg = tid >> 5;
+  const long long C0 = (long long)J * TB;
+  for (int it = tid; it < TB * M; it += 256) {
+    const int c = it % TB, v = it / TB;
+    xJ[c][v] = (C0 + c < N) ? X[C0 + c + (long long)v * ldx] : make_double2(0, 0);
+  }
+  double2 cacc[2][MV];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int v = 0; v < MV; ++v) cacc[a][v] = make_double2(0, 0);
+  for (int I = I0; I < I1; ++I) {
+    const long long R0 = (long long)I * TB;
+    const bool diag = (I == J);
+    __syncthreads();
+    for (int it = tid; it < TB * TB; it += 256) {
+      const int a = it & (TB - 1), b = it >> 6;
+      const long long rr = R0 + a, cc = C0 + b;
+      if (!diag) {
+        tile[b][a] = (rr < N && cc < N) ? A[rr + cc * N] : make_double2(0, 0);
+      } else if (rr < N && cc < N) {
+        if (a > b) {
+          const double2 v = A[rr + cc * N];
+          tile[b][a] = v;
+          tile[a][b] = cconj(v);
+        } else if (a == b) {
+          tile[a][a] = make_double2(A[rr + cc * N].x, 0.0);
+        }
+      } else {
+        tile[b][a] = make_double2(0, 0);
+        tile[a][b] = make_double2(0, 0);
+      }
+    }
+    for (int it = tid; it < TB * M; it += 256) {
+      const int c = it % TB, v = it / TB;
+      xI[c][v] = (R0 + c < N) ? X[R0 + c + (long long)v * ldx] : make_double2(0, 0);
+    }
+    __syncthreads();
+    // row products
+    double2 acc[2][MV];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int v = 0; v < MV; ++v) acc[a][v] = make_double2(0, 0);
+#pragma unroll 4
+    for (int c = 0; c < TB; ++c) {
+      const double2 h0 = tile[c][r], h1 = tile[c][r + 32];
+#pragma unroll
+      for (int v = 0; v < MV; ++v) {
+        const double2 x = xJ[c][vg * MV + v];
+        acc[0][v] = cadd(acc[0][v], cmul(h0, x));
+        acc[1][v] = cadd(acc[1][v], cmul(h1, x));
+      }
+    }
+    double2* sl = slots + ((long long)I * nblk + J) * M * TB;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int v = 0; v < MV; ++v) sl[(long long)(vg * MV + v) * TB + r + 32 * a] = acc[a][v];
+    // column products (the diagonal tile is complete in its row products)
+    if (!diag) {
+#pragma unroll 4
+      for (int rr = 0; rr < TB; ++rr) {
+        const double2 h0 = tile[r][rr], h1 = tile[r + 32][rr];   // L(R0+rr, C0+c), c = r, r+32
+#pragma unroll
+        for (int v = 0; v < MV; ++v) {
+          const double2 x = xI[rr][vg * MV + v];
+          cacc[0][v] = cadd(cacc[0][v], cmulc(h0, x));
+          cacc[1][v] = cadd(cacc[1][v], cmulc(h1, x));
+        }
+      }
+    }
+  }
+  double2* sl = slots + ((long long)J * nblk + I0) * M * TB;
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int v = 0; v < MV; ++v) {
+      double2* p = sl + (long long)(vg * MV + v) * TB + r + 32 * a;
+      *p = (I0 == J) ? cadd(*p, cacc[a][v]) : cacc[a][v];
+    }
+  for (int I = I0 + 1; I < I1; ++I) {
+    double2* z = slots + ((long long)J * nblk + I) * M * TB;
+    for (int it = tid; it < M * TB; it += 256) z[it] = make_double2(0, 0);
+  }
+}
+
+__global__ void k_sum_slots(const double2* slots, long long N, int nblk, int m, double2* Y, int ldy) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nblk * TB * m) return;
+  const int row = (int)(i % TB);
+  const int v = (int)((i / TB) % m);
+  const int a = (int)(i / ((long long)TB * m));
+  const long long gr = (long long)a * TB + row;
+  if (gr >= N) return;
+  double2 s = make_double2(0, 0);
+  for (int b = 0; b < nblk; ++b) s = cadd(s, slots[(((long long)a * nblk + b) * m + v) * TB + row]);
+  Y[gr + (long long)v * ldy] = s;
+}
+
+// Y(:, v) = sum over chunks of the partials
+__global__ void k_sum_parts(const double2* Yp, long long N, int m, double2* Y, int ldy) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= N * m) return;
+  const long long row = i % N, v = i / N;
+  double2 s = make_double2(0, 0);
+  for (int p = 0; p < JCH; ++p) s = cadd(s, Yp[((long long)p * m + v) * N + row]);
+  Y[row + v * ldy] = s;
+}
+
+// C (p x q) = A^H B, A (N x p, lda), B (N x q, ldb): per-block partials [blk][p*q]; rows are
+// staged 32 at a time in shared memory and every thread accumulates its outputs in registers.
+constexpr int GR = 16;
+constexpr int GMAXO = 25;   // outputs per thread: p*q <= 256*25 = 6400 (80 x 80)
+__global__ void __launch_bounds__(256) k_gram(const double2* A, int lda, int p, const double2* B, int ldb, int q,
+                                              long long N, double2* part) {
+  __shared__ double2 as[GR][kMaxRR + 1], bsm[GR][kMaxRR + 1];
+  const int tid = threadIdx.x;
+  const long long rows_per = (N + gridDim.x - 1) / gridDim.x;
+  const long long r0 = (long long)blockIdx.x * rows_per, r1 = min(N, r0 + rows_per);
+  const int pq = p * q;
+  double2 acc[GMAXO];
+#pragma unroll
+  for (int j = 0; j < GMAXO; ++j) acc[j] = make_double2(0, 0);
+  for (long long c0 = r0; c0 < r1; c0 += GR) {
+    __syncthreads();
+    for (int it = tid; it < GR * p; it += 256) {
+      const int rr = it % GR, a = it / GR;
+      as[rr][a] = (c0 + rr < r1) ? A[c0 + rr + (long long)a * lda] : make_double2(0, 0);
+    }
+    for (int it = tid; it < GR * q; it += 256) {
+      const int rr = it % GR, b = it / GR;
+      bsm[rr][b] = (c0 + rr < r1) ? B[c0 + rr + (long long)b * ldb] : make_double2(0, 0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < GMAXO; ++j) {
+      const int o = tid + 256 * j;
+      if (o >= pq) break;
+      const int a = o % p, b = o / p;
+      double2 sacc = acc[j];
+      for (int rr = 0; rr < GR; ++rr) sacc = cadd(sacc, cmulc(as[rr][a], bsm[rr][b]));
+      acc[j] = sacc;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < GMAXO; ++j) {
+    const int o = tid + 256 * j;
+    if (o < pq) part[(long long)blockIdx.x * pq + o] = acc[j];
+  }
+}
+
+__global__ void k_gram_sum(const double2* part, int nparts, int pq, double2* C) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= pq) return;
+  double2 s = make_double2(0, 0);
+  for (int k = 0; k < nparts; ++k) s = cadd(s, part[(long long)k * pq + i]);
+  C[i] = s;
+}
+
+// C (N x q, ldc) = A (N x p, lda) * B (p x q, column-major, ldb = p), or C -= A * B
+template <bool SUB>
+__global__ void k_tall_gemm(const double2* A, int lda, int p, const double2* B, int q, long long N, double2* Cm, int ldc) {
+  extern __shared__ double2 bs[];
+  for (int i = threadIdx.x; i < p * q; i += blockDim.x) bs[i] = B[i];
+  __syncthreads();
+  const long long rr = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (rr >= N) return;
+  for (int b0 = 0; b0 < q; b0 += 8) {
+    double2 s[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s[k] = make_double2(0, 0);
+    const int nb = min(8, q - b0);
+    for (int a = 0; a < p; ++a) {
+      const double2 x = A[rr + (long long)a * lda];
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (k < nb) s[k] = cadd(s[k], cmul(x, bs[a + (b0 + k) * p]));
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (k >= nb) break;
+      double2* cp = Cm + rr + (long long)(b0 + k) * ldc;
+      *cp = SUB ? csub(*cp, s[k]) : s[k];
+    }
+  }
+}
+
+// G (q x q Hermitian PD, q <= 64) -> Rinv (upper triangular) with G = R^H R.  A column with a
+// non-positive pivot gets a zero row in R^-1 (its vector is dropped).  One CTA.
+__global__ void __launch_bounds__(128) k_chol_inv(const double2* G, int q, double2* Rinv, int* bad) {
+  extern __shared__ double2 csm[];
+  const int ld = q + 1;
+  double2* Rm = csm;              // R(a, b) at Rm[a * ld + b]
+  double2* Rim = csm + q * ld;    // Rinv(a, b) at Rim[a * ld + b]
+#define R(a, b) Rm[(a) * ld + (b)]
+#define Ri(a, b) Rim[(a) * ld + (b)]
+  __shared__ double s_d;
+  const int tid = threadIdx.x;
+  for (int it = tid; it < q * q; it += blockDim.x) {
+    const int a = it % q, b = it / q;
+    R(a, b) = make_double2(0, 0);
+    Ri(a, b) = make_double2(0, 0);
+  }
+  __syncthreads();
+  int nbad = 0;
+  for (int j = 0; j < q; ++j) {
+    if (tid == 0) {
+      double d = G[j + j * q].x;
+      for (int k = 0; k < j; ++k) d -= R(k, j).x * R(k, j).x + R(k, j).y * R(k, j).y;
+      const double scale = fabs(G[j + j * q].x) + 1e-300;
+      s_d = (d > 1e-28 * scale) ? sqrt(d) : 0.0;
+      R(j, j) = make_double2(s_d, 0.0);
+    }
+    __syncthreads();
+    const double rjj = s_d;
+    if (rjj == 0.0) {
+      ++nbad;
+      __syncthreads();
+      continue;
+    }
+    for (int i = j + 1 + tid; i < q; i += blockDim.x) {
+      double2 t = G[j + i * q];
+      for (int k = 0; k < j; ++k) t = csub(t, cmulc(R(k, j), R(k, i)));
+      R(j, i) = cscale(t, 1.0 / rjj);
+    }
+    __syncthreads();
+  }
+  // columns of R^-1 in parallel: R Ri(:, j) = e_j
+  for (int j = tid; j < q; j += blockDim.x) {
+    if (R(j, j).x == 0.0) continue;
+    Ri(j, j) = make_double2(1.0 / R(j, j).x, 0.0);
+    for (int i = j - 1; i >= 0; --i) {
+      if (R(i, i).x == 0.0) continue;
+      double2 sacc = make_double2(0, 0);
+      for (int k = i + 1; k <= j; ++k) sacc = cadd(sacc, cmul(R(i, k), Ri(k, j)));
+      Ri(i, j) = cscale(sacc, -1.0 / R(i, i).x);
+    }
+  }
+  __syncthreads();
+  for (int it = tid; it < q * q; it += blockDim.x) {
+    const int a = it % q, b = it / q;
+    Rinv[it] = Ri(a, b);
+  }
+  if (tid == 0) *bad = nbad;
+#undef R
+#undef Ri
+}
+
+// One-CTA cyclic Jacobi of a Hermitian n x n matrix M (column-major, n <= kMaxRR is checked by
+// the host): eigenvalues ascending (or descending), eigenvectors as columns of Y (n x n).
+struct RRot {
+  int p, q, active, pad;
+  double cs, sn, ex, ey, ap, aq;
+};
+
+__global__ void __launch_bounds__(1024) k_rr_jacobi(const double2* Min, int n, int descending, double* theta,
+                                                    double2* Yout, int* status) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const int m2 = n + (n & 1), npair = m2 / 2;
+  double2* Am = reinterpret_cast<double2*>(smem);
+  double2* V = Am + n * n;
+  RRot* rot = reinterpret_cast<RRot*>(V + n * n);
+  double* lam = reinterpret_cast<double*>(rot + npair);
+  int* perm = reinterpret_cast<int*>(lam + n + 1);
+  __shared__ int s_rot;
+  __shared__ double s_tol;
+  double fro = 0.0;
+  for (int it = tid; it < n * n; it += bs) {
+    const int a = it % n, b = it / n;
+    double2 v = Min[it];
+    if (a == b) v.y = 0.0;
+    if (a < b) v = cconj(Min[b + a * n]);   // Hermitian from the lower triangle
+    Am[it] = v;
+    V[it] = make_double2(a == b ? 1.0 : 0.0, 0.0);
+    fro += v.x * v.x + v.y * v.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) fro += __shfl_xor_sync(0xffffffffu, fro, o);
+  __shared__ double red[32];
+  if ((tid & 31) == 0) red[tid >> 5] = fro;
+  __syncthreads();
+  if (tid == 0) {
+    double s = 0;
+    for (int k = 0; k < bs / 32; ++k) s += red[k];
+    s_tol = DBL_EPSILON * 1e-2 * sqrt(s);
+  }
+  int converged = 0;
+  for (int sweep = 0; sweep < 60 && !converged; ++sweep) {
+    if (tid == 0) s_rot = 0;
+    __syncthreads();
+    for (int rr = 0; rr < m2 - 1; ++rr) {
+      if (tid < npair) {
+        const int t = tid;
+        int p = (t == 0) ? (m2 - 1) : ((rr + t - 1) % (m2 - 1));
+        int q = (rr + (m2 - 1 - t) - 1) % (m2 - 1);
+        if (p > q) { const int x = p; p = q; q = x; }
+        RRot ro;
+        ro.p = p;
+        ro.q = q;
+        ro.active = 0;
+        if (q < n) {
+          const double aa = Am[p + p * n].x, bb = Am[q + q * n].x;
+          const double2 c = Am[p + q * n];
+          const double ac = hypot(c.x, c.y);
+          const double thr = fmax(0.5 * DBL_EPSILON * sqrt(fabs(aa * bb)), s_tol);
+          if (ac > thr && ac > 0.0) {
+            const double zeta = (bb - aa) / (2.0 * ac);
+            const double tt = (fabs(zeta) > 1e150) ? 0.5 / zeta
+                                                   : (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+            const double cs = 1.0 / sqrt(1.0 + tt * tt);
+            ro.cs = cs;
+            ro.sn = tt * cs;
+            ro.ex = c.x / ac;
+            ro.ey = c.y / ac;
+            ro.ap = aa - tt * ac;
+            ro.aq = bb + tt * ac;
+            ro.active = 1;
+            s_rot = 1;
+          }
+        }
+        rot[t] = ro;
+      }
+      __syncthreads();
+      for (int it = tid; it < npair * n; it += bs) {
+        const RRot& ro = rot[it / n];
+        if (!ro.active) continue;
+        const int col = it % n;
+        const double2 e = make_double2(ro.ex, ro.ey);
+        const double2 rp = Am[ro.p + col * n], rq = Am[ro.q + col * n];
+        Am[ro.p + col * n] = csub(cscale(rp, ro.cs), cscale(cmul(e, rq), ro.sn));
+        Am[ro.q + col * n] = cadd(cscale(cmulc(e, rp), ro.sn), cscale(rq, ro.cs));
+      }
+      __syncthreads();
+      for (int it = tid; it < npair * n; it += bs) {
+        const RRot& ro = rot[it / n];
+        if (!ro.active) continue;
+        const int row = it % n;
+        const double2 e = make_double2(ro.ex, ro.ey);
+        double2 cp = Am[row + ro.p * n], cq = Am[row + ro.q * n];
+        Am[row + ro.p * n] = csub(cscale(cp, ro.cs), cscale(cmulc(e, cq), ro.sn));
+        Am[row + ro.q * n] = cadd(cscale(cmul(e, cp), ro.sn), cscale(cq, ro.cs));
+        cp = V[row + ro.p * n];
+        cq = V[row + ro.q * n];
+        V[row + ro.p * n] = csub(cscale(cp, ro.cs), cscale(cmulc(e, cq), ro.sn));
+        V[row + ro.q * n] = cadd(cscale(cmul(e, cp), ro.sn), cscale(cq, ro.cs));
+      }
+      __syncthreads();
+    }
+    converged = (s_rot == 0);
+    __syncthreads();
+  }
+  if (tid < n) lam[tid] = Am[tid + tid * n].x;
+  __syncthreads();
+  if (tid < n) {
+    const double lj = lam[tid];
+    int rank = 0;
+    for (int i = 0; i < n; ++i) {
+      const double li = lam[i];
+      const bool before = descending ? (li > lj || (li == lj && i < tid)) : (li < lj || (li == lj && i < tid));
+      rank += before ? 1 : 0;
+    }
+    perm[rank] = tid;
+  }
+  __syncthreads();
+  if (tid < n) theta[tid] = lam[perm[tid]];
+  for (int it = tid; it < n * n; it += bs) {
+    const int row = it % n, col = it / n;
+    Yout[it] = V[row + perm[col] * n];
+  }
+  if (tid == 0) *status = converged ? 0 : 1;
+}
+
+
+// One-CTA Hermitian eigensolver for the Rayleigh-Ritz matrix (n <= kMaxRR): Householder
+// reduction to real tridiagonal form in shared memory (ZHETRD-style lower reflectors),
+// Sturm bisection for the nb wanted eigenvalues (lowest, or highest when descending), inverse
+// iteration with partial pivoting for their vectors (clusters re-orthogonalised in sequence
+// by one thread), and the back-transform y = H_0 ... H_{n-2} z, one thread per vector.
+__global__ void __launch_bounds__(256) k_rr_tridiag(const double2* Min, int n, int nb, int descending, double* theta,
+                                                    double2* Yout, int* status) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double2* A = reinterpret_cast<double2*>(smem);          // n x n, column-major
+  double2* vv = A + n * n;                                  // reflector scratch (n)
+  double2* pp = vv + n;                                     // n
+  double2* taus = pp + n;                                   // n
+  double* dd = reinterpret_cast<double*>(taus + n);         // n
+  double* ee = dd + n;                                      // n
+  double* lam = ee + n;                                     // nb
+  double* Z = lam + kMaxRR;                                 // n x nb (column-major)
+  __shared__ double red[8];
+  __shared__ double2 redc[8];
+  __shared__ double2 s_tau, s_scal, s_a2;
+  __shared__ int s_triv;
+  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5, bs = blockDim.x;
+  for (int it = tid; it < n * n; it += bs) {
+    const int a = it % n, b = it / n;
+    double2 v = Min[it];
+    if (a == b) v.y = 0.0;
+    if (a < b) v = cconj(Min[b + a * n]);
+    A[it] = v;
+  }
+  __syncthreads();
+  for (int j = 0; j < n - 1; ++j) {
+    const int m = n - j - 1;   // length of x = A[j+1:, j]
+    // |x(2:)|^2
+    double s = 0.0;
+    for (int i = 1 + tid; i < m; i += bs) {
+      const double2 x = A[(j + 1 + i) + j * n];
+      s += x.x * x.x + x.y * x.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[wp] = s;
+    __syncthreads();
+    if (tid == 0) {
+      double xn2 = 0;
+      for (int k = 0; k < bs / 32; ++k) xn2 += red[k];
+      const double2 al = A[(j + 1) + j * n];
+      if (xn2 == 0.0 && al.y == 0.0) {
+        s_triv = 1;
+        s_tau = make_double2(0, 0);
+        ee[j] = al.x;
+      } else {
+        s_triv = 0;
+        const double beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xn2), al.x);
+        s_tau = make_double2((beta - al.x) / beta, -al.y / beta);
+        const double2 den = make_double2(al.x - beta, al.y);
+        const double dn = den.x * den.x + den.y * den.y;
+        s_scal = make_double2(den.x / dn, -den.y / dn);
+        ee[j] = beta;
+      }
+      dd[j] = A[j + j * n].x;
+      taus[j] = s_tau;
+    }
+    __syncthreads();
+    const int triv = s_triv;
+    const double2 tau = s_tau;
+    for (int i = tid; i < m; i += bs) {
+      double2 v = (i == 0) ? make_double2(1, 0) : (triv ? make_double2(0, 0) : cmul(A[(j + 1 + i) + j * n], s_scal));
+      vv[i] = v;
+      A[(j + 1 + i) + j * n] = v;   // keep v for the back-transform
+    }
+    __syncthreads();
+    if (triv) continue;
+    // p = tau * A22 v
+    for (int i = tid; i < m; i += bs) {
+      double2 acc = make_double2(0, 0);
+      for (int k = 0; k < m; ++k) acc = cadd(acc, cmul(A[(j + 1 + i) + (j + 1 + k) * n], vv[k]));
+      pp[i] = cmul(tau, acc);
+    }
+    __syncthreads();
+    // alpha2 = -tau/2 (p^H v)
+    double2 t = make_double2(0, 0);
+    for (int i = tid; i < m; i += bs) t = cadd(t, cmulc(pp[i], vv[i]));
+    for (int o = 16; o > 0; o >>= 1) {
+      t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
+      t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
+    }
+    if (lane == 0) redc[wp] = t;
+    __syncthreads();
+    if (tid == 0) {
+      double2 sum = make_double2(0, 0);
+      for (int k = 0; k < bs / 32; ++k) sum = cadd(sum, redc[k]);
+      s_a2 = cscale(cmul(tau, sum), -0.5);
+    }
+    __syncthreads();
+    const double2 a2 = s_a2;
+    for (int i = tid; i < m; i += bs) pp[i] = cadd(pp[i], cmul(a2, vv[i]));   // w
+    __syncthreads();
+    // A22 -= v w^H + w v^H
+    for (int it = tid; it < m * m; it += bs) {
+      const int r = it % m, c = it / m;
+      double2 x = A[(j + 1 + r) + (j + 1 + c) * n];
+      x = csub(x, cadd(cmul(vv[r], cconj(pp[c])), cmul(pp[r], cconj(vv[c]))));
+      A[(j + 1 + r) + (j + 1 + c) * n] = x;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) dd[n - 1] = A[(n - 1) + (n - 1) * n].x;
+  __syncthreads();
+  // bisection for the wanted eigenvalues
+  __shared__ double s_lo, s_hi, s_tn;
+  if (tid == 0) {
+    double lo = dd[0], hi = dd[0];
+    for (int i = 0; i < n; ++i) {
+      const double r = (i > 0 ? fabs(ee[i - 1]) : 0.0) + (i < n - 1 ? fabs(ee[i]) : 0.0);
+      lo = fmin(lo, dd[i] - r);
+      hi = fmax(hi, dd[i] + r);
+    }
+    s_tn = fmax(fabs(lo), fabs(hi));
+    const double pad = 4.0 * DBL_EPSILON * s_tn + 1e-300;
+    s_lo = lo - pad;
+    s_hi = hi + pad;
+  }
+  __syncthreads();
+  const double pivmin = DBL_MIN * 4.0;
+  if (tid < nb) {
+    const int mi = descending ? (n - 1 - tid) : tid;
+    double a = s_lo, b = s_hi;
+    for (int it = 0; it < 200; ++it) {
+      const double mid = 0.5 * (a + b);
+      if (!(mid > a && mid < b)) break;
+      int cnt = 0;
+      double q = dd[0] - mid;
+      if (fabs(q) < pivmin) q = -pivmin;
+      cnt += (q < 0);
+      for (int i = 1; i < n; ++i) {
+        q = (dd[i] - mid) - ee[i - 1] * ee[i - 1] / q;
+        if (fabs(q) < pivmin) q = -pivmin;
+        cnt += (q < 0);
+      }
+      if (cnt <= mi) a = mid;
+      else b = mid;
+    }
+    lam[tid] = 0.5 * (a + b);
+  }
+  __syncthreads();
+  // inverse iteration; clusters (gap <= 1e-7 |T|) handled in order by their first thread
+  if (tid < nb) {
+    const double ctol = 1e-7 * fmax(1e-3, s_tn);
+    const bool leader = (tid == 0) || fabs(lam[tid] - lam[tid - 1]) > ctol;
+    if (leader) {
+      int cs = 1;
+      while (tid + cs < nb && fabs(lam[tid + cs] - lam[tid + cs - 1]) <= ctol) ++cs;
+      const double pert = DBL_EPSILON * fmax(s_tn, 1e-300);
+      double u1[kMaxRR], u2[kMaxRR], u3[kMaxRR];
+      for (int sidx = 0; sidx < cs; ++sidx) {
+        const int col = tid + sidx;
+        double* x = Z + (long long)col * n;
+        const double lm = lam[col];
+        for (int k = 0; k < n; ++k) x[k] = 1.0 + 0.1 * (double)((k * 7 + col * 13) % 17) / 17.0;
+        double sc = 1.0;
+        for (int itr = 0; itr < 3; ++itr) {
+          double diag = dd[0] - lm, sup = (n > 1) ? ee[0] : 0.0, cur = x[0] * sc;
+          for (int k = 0; k < n - 1; ++k) {
+            const double sub = ee[k], nd = dd[k + 1] - lm, nsup = (k + 1 < n - 1) ? ee[k + 1] : 0.0;
+            const double nxt = x[k + 1] * sc;
+            if (fabs(diag) >= fabs(sub)) {
+              if (fabs(diag) < pert) diag = copysign(pert, diag);
+              const double mult = sub / diag;
+              u1[k] = diag; u2[k] = sup; u3[k] = 0.0; x[k] = cur;
+              cur = nxt - mult * cur;
+              diag = nd - mult * sup;
+              sup = nsup;
+            } else {
+              const double mult = diag / sub;
+              u1[k] = sub; u2[k] = nd; u3[k] = nsup; x[k] = nxt;
+              cur = cur - mult * nxt;
+              diag = sup - mult * nd;
+              sup = -mult * nsup;
+            }
+          }
+          if (fabs(diag) < pert) diag = copysign(pert, diag);
+          double x2 = 0.0, x1 = cur / diag, nrm = x1 * x1;
+          x[n - 1] = x1;
+          for (int k = n - 2; k >= 0; --k) {
+            const double xk = (x[k] - u2[k] * x1 - u3[k] * x2) / u1[k];
+            x[k] = xk;
+            nrm += xk * xk;
+            x2 = x1;
+            x1 = xk;
+          }
+          sc = 1.0 / sqrt(nrm);
+          for (int k = 0; k < n; ++k) x[k] *= sc;
+          sc = 1.0;
+          for (int t2 = 0; t2 < sidx; ++t2) {
+            const double* y = Z + (long long)(tid + t2) * n;
+            double dot = 0.0;
+            for (int k = 0; k < n; ++k) dot += x[k] * y[k];
+            for (int k = 0; k < n; ++k) x[k] -= dot * y[k];
+          }
+          if (sidx > 0) {
+            double n2 = 0.0;
+            for (int k = 0; k < n; ++k) n2 += x[k] * x[k];
+            const double s2 = 1.0 / sqrt(n2);
+            for (int k = 0; k < n; ++k) x[k] *= s2;
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // back-transform: y = H_0 (H_1 (... H_{n-2} z)), v_j stored in A[j+1:, j]
+  if (tid < nb) {
+    double2* y = Yout + (long long)tid * n;
+    for (int k = 0; k < n; ++k) y[k] = make_double2(Z[(long long)tid * n + k], 0.0);
+    for (int j = n - 2; j >= 0; --j) {
+      const double2 tau = taus[j];
+      if (tau.x == 0.0 && tau.y == 0.0) continue;
+      double2 dot = make_double2(0, 0);
+      for (int k = j + 1; k < n; ++k) dot = cadd(dot, cmulc(A[k + j * n], y[k]));
+      const double2 f = cmul(tau, dot);
+      for (int k = j + 1; k < n; ++k) y[k] = csub(y[k], cmul(A[k + j * n], f));
+    }
+    theta[tid] = lam[tid];
+  }
+  if (tid == 0) *status = 0;
+}
+
+__global__ void k_diag(const double2* A, long long N, double* D) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < N) D[i] = A[i + i * N].x;
+}
+
+__global__ void k_unit_block(const int* idx, int nb, long long N, double2* X, int ldx) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= N * nb) return;
+  const long long row = i % N;
+  const int v = (int)(i / N);
+  X[row + (long long)v * ldx] = make_double2(row == idx[v] ? 1.0 : 0.0, 0.0);
+}
+
+// R = HX - X diag(theta); T = R / (D - theta) (guarded); per-column |R|^2 partials
+__global__ void __launch_bounds__(256) k_resid_precond(const double2* X, const double2* HX, int ldx, int nb,
+                                                       const double* theta, const double* D, long long N, double2* T,
+                                                       int ldt, double* rpart) {
+  __shared__ double red[8][64];
+  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  const long long rr = blockIdx.x * (long long)blockDim.x + tid;
+  for (int v = 0; v < nb; ++v) {
+    double n2 = 0.0;
+    if (rr < N) {
+      const double th = theta[v];
+      const double2 r = csub(HX[rr + (long long)v * ldx], cscale(X[rr + (long long)v * ldx], th));
+      n2 = r.x * r.x + r.y * r.y;
+      double den = D[rr] - th;
+      if (fabs(den) < 0.05) den = copysign(0.05, den);   // clamp of the Davidson preconditioner (eV)
+      T[rr + (long long)v * ldt] = cscale(r, 1.0 / den);
+    }
+    for (int o = 16; o > 0; o >>= 1) n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+    if (lane == 0) red[wp][v] = n2;
+  }
+  __syncthreads();
+  if (tid < nb) {
+    double s = 0;
+    for (int k = 0; k < 8; ++k) s += red[k][tid];
+    rpart[(long long)blockIdx.x * 64 + tid] = s;
+  }
+}
+
+// oscillators of the nev converged vectors: s_al = sum_j X_jn h_al(j) (no conjugate)
+__global__ void __launch_bounds__(256) k_osc_part(const double2* X, int ldx, int nev, const double2* h, long long N,
+                                                  double2* part) {
+  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  const long long rows_per = (N + gridDim.x - 1) / gridDim.x;
+  const long long r0 = (long long)blockIdx.x * rows_per, r1 = min(N, r0 + rows_per);
+  for (int pq = wp; pq < nev * NG; pq += 8) {
+    const int n = pq % nev, al = pq / nev;
+    double2 s = make_double2(0, 0);
+    for (long long rr = r0 + lane; rr < r1; rr += 32) s = cadd(s, cmul(X[rr + (long long)n * ldx], h[al * N + rr]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+      s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+    }
+    if (lane == 0) part[(long long)blockIdx.x * nev * NG + pq] = s;
+  }
+}
+
+__global__ void k_osc_final(const double2* part, int nparts, int nev, int dtfull, int cpol, double* act) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nev) return;
+  double2 s[NG];
+  for (int al = 0; al < NG; ++al) {
+    double2 t = make_double2(0, 0);
+    for (int k = 0; k < nparts; ++k) t = cadd(t, part[(long long)k * nev * NG + al * nev + n]);
+    s[al] = t;
+  }
+  act[0 * nev + n] = s[0].x * s[0].x + s[0].y * s[0].y;
+  act[1 * nev + n] = s[1].x * s[1].x + s[1].y * s[1].y;
+  act[2 * nev + n] = s[2].x * s[2].x + s[2].y * s[2].y;
+  act[3 * nev + n] = dtfull ? s[0].x * s[1].x + s[0].y * s[1].y : 0.0;
+  act[4 * nev + n] = dtfull ? s[0].x * s[2].x + s[0].y * s[2].y : 0.0;
+  act[5 * nev + n] = dtfull ? s[1].x * s[2].x + s[1].y * s[2].y : 0.0;
+  act[6 * nev + n] = cpol ? s[3].x * s[3].x + s[3].y * s[3].y : 0.0;
+  act[7 * nev + n] = cpol ? s[4].x * s[4].x + s[4].y * s[4].y : 0.0;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+struct DavWork {
+  double2 *V, *HV, *Xn, *HXn, *Yp, *small, *part;
+  double *D, *theta, *rpart;
+  int* istat;
+};
+
+static int hemm(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y, int ldy, double2* Yp) {
+  const long long N = ctx->N;
+  const int nblk = (int)((N + TB - 1) / TB);
+  dim3 grid(nblk, JCH);
+  const size_t sm = sizeof(double2) * TB * (TB + 1) + sizeof(double2) * TB * (m + 1);
+  switch (m / 8) {
+#define WTBG_HEMM_CASE(MV)                                                                       \
+  case MV:                                                                                       \
+    CK(cudaFuncSetAttribute(k_hemm<MV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)); \
+    k_hemm<MV><<<grid, 256, sm, ctx->stream>>>(ctx->H.as<double2>(), N, X, ldx, Yp);            \
+    break;
+    WTBG_HEMM_CASE(1) WTBG_HEMM_CASE(2) WTBG_HEMM_CASE(3) WTBG_HEMM_CASE(4) WTBG_HEMM_CASE(5)
+#undef WTBG_HEMM_CASE
+    default: return set_err(ctx, WTBG_ERR_UNSUPPORTED, "davidson: block size must be 8, 16, 24, 32 or 40");
+  }
+  if (m % 8) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "davidson: block size must be a multiple of 8");
+  WTBG_COUNT(ctx, 1);
+  const long long tot = N * m;
+  k_sum_parts<<<(int)((tot + 255) / 256), 256, 0, ctx->stream>>>(Yp, N, m, Y, ldy); WTBG_COUNT(ctx, 1);
+  CKL("hemm");
+  return 0;
+}
+
+static int gram(wtbg_ctx* ctx, const double2* A, int lda, int p, const double2* B, int ldb, int q, double2* C,
+                double2* part) {
+  const long long N = ctx->N;
+  if (p > kMaxRR || q > kMaxRR || p * q > 256 * GMAXO) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "davidson: gram too large");
+  const int nparts = (int)std::min<long long>(148, (N + 63) / 64);
+  k_gram<<<nparts, 256, 0, ctx->stream>>>(A, lda, p, B, ldb, q, N, part); WTBG_COUNT(ctx, 1);
+  k_gram_sum<<<(p * q + 255) / 256, 256, 0, ctx->stream>>>(part, nparts, p * q, C); WTBG_COUNT(ctx, 1);
+  CKL("gram");
+  return 0;
+}
+
+static int tall(wtbg_ctx* ctx, const double2* A, int lda, int p, const double2* B, int q, double2* Cm, int ldc,
+                bool sub) {
+  const long long N = ctx->N;
+  const size_t sh = (size_t)p * q * 16;
+  if (sh > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "davidson: small matrix too large");
+  if (sub) {
+    CK(cudaFuncSetAttribute(k_tall_gemm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+    k_tall_gemm<true><<<(int)((N + 127) / 128), 128, sh, ctx->stream>>>(A, lda, p, B, q, N, Cm, ldc);
+  } else {
+    CK(cudaFuncSetAttribute(k_tall_gemm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
+    k_tall_gemm<false><<<(int)((N + 127) / 128), 128, sh, ctx->stream>>>(A, lda, p, B, q, N, Cm, ldc);
+  }
+  WTBG_COUNT(ctx, 1);
+  CKL("tall");
+  return 0;
+}
+
+// orthonormalise the q columns of T (ld N) in place: T <- T R^-1, twice (CholQR2)
+static int cholqr2(wtbg_ctx* ctx, double2* T, int q, double2* tmp, DavWork& w) {
+  const long long N = ctx->N;
+  for (int pass = 0; pass < 2; ++pass) {
+    if (int r = gram(ctx, T, (int)N, q, T, (int)N, q, w.small, w.part)) return r;
+    const size_t csm = (size_t)2 * q * (q + 1) * 16;
+    CK(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+    k_chol_inv<<<1, 128, csm, ctx->stream>>>(w.small, q, w.small + 64 * 64, w.istat); WTBG_COUNT(ctx, 1);
+    CKL("chol");
+    if (int r = tall(ctx, T, (int)N, q, w.small + 64 * 64, q, tmp, (int)N, false)) return r;
+    CK(cudaMemcpyAsync(T, tmp, (size_t)N * q * 16, cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  return 0;
+}
+
+int run_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, double tol, const double2* dX0, int dtfull,
+                 int cpol, std::vector<double>& W, std::vector<double>& act, double2* dXout, int* iters, double* maxres) {
+  const long long N = ctx->N;
+  if (nb < nev || nb % 8 != 0 || nb > 40 || 2 * nb > kMaxRR)
+    return set_err(ctx, WTBG_ERR_ARG, "davidson: block size must be a multiple of 8, >= nev and <= 40");
+  const int n2 = 2 * nb;
+  // workspace
+  const size_t vbytes = (size_t)N * n2 * 16;
+  ENSURE(ctx->ws, 2 * vbytes + 2 * (size_t)N * nb * 16 + (size_t)JCH * N * nb * 16 + 4096);
+  char* base = ctx->ws.as<char>();
+  DavWork w;
+  w.V = reinterpret_cast<double2*>(base);
+  w.HV = w.V + (size_t)N * n2;
+  w.Xn = w.HV + (size_t)N * n2;
+  w.HXn = w.Xn + (size_t)N * nb;
+  w.Yp = w.HXn + (size_t)N * nb;
+  ENSURE(ctx->tmp, (size_t)N * 8 + (size_t)kMaxRR * kMaxRR * 16 * 3 + 4096 * 16 + 300 * 64 * 64 * 16 + (size_t)N * 4 * 2 + 65536);
+  char* tb = ctx->tmp.as<char>();
+  w.D = reinterpret_cast<double*>(tb);
+  w.small = reinterpret_cast<double2*>(tb + (size_t)N * 8);                     // M, Y, ...
+  w.theta = reinterpret_cast<double*>(w.small + 3 * kMaxRR * kMaxRR);
+  w.rpart = w.theta + kMaxRR;
+  w.part = reinterpret_cast<double2*>(w.rpart + 4096);
+  w.istat = reinterpret_cast<int*>(w.part + 300 * 64 * 64);
+  int* d_idx = w.istat + 16;
+  cudaStream_t s = ctx->stream;
+  const int th = 256;
+  k_diag<<<(int)((N + th - 1) / th), th, 0, s>>>(ctx->H.as<double2>(), N, w.D); WTBG_COUNT(ctx, 1);
+  CKL("k_diag");
+  double2* X = w.V;          // first nb columns of V
+  double2* T = w.V + (size_t)N * nb;
+  double2* HX = w.HV;
+  double2* HT = w.HV + (size_t)N * nb;
+  // initial block
+  if (dX0) {
+    CK(cudaMemcpyAsync(X, dX0, (size_t)N * nb * 16, cudaMemcpyDeviceToDevice, s));
+  } else {
+    // unit vectors at the nb smallest (largest) diagonal entries
+    std::vector<double> Dh(N);
+    CK(cudaMemcpyAsync(Dh.data(), w.D, N * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    std::vector<int> idx(N);
+    for (long long i = 0; i < N; ++i) idx[i] = (int)i;
+    if (largest)
+      std::partial_sort(idx.begin(), idx.begin() + nb, idx.end(), [&](int a, int b) { return Dh[a] > Dh[b] || (Dh[a] == Dh[b] && a < b); });
+    else
+      std::partial_sort(idx.begin(), idx.begin() + nb, idx.end(), [&](int a, int b) { return Dh[a] < Dh[b] || (Dh[a] == Dh[b] && a < b); });
+    CK(cudaMemcpyAsync(d_idx, idx.data(), nb * 4, cudaMemcpyHostToDevice, s));
+    k_unit_block<<<(int)((N * nb + th - 1) / th), th, 0, s>>>(d_idx, nb, N, X, (int)N); WTBG_COUNT(ctx, 1);
+    CKL("k_unit_block");
+  }
+  if (int r = cholqr2(ctx, X, nb, w.Xn, w)) return r;
+  if (int r = hemm(ctx, X, (int)N, nb, HX, (int)N, w.Yp)) return r;
+  // first Rayleigh-Ritz on X alone
+  const size_t rrsm = (size_t)2 * kMaxRR * kMaxRR * 16 + (size_t)(kMaxRR / 2 + 1) * sizeof(RRot) + (kMaxRR + 2) * 8 +
+                      (kMaxRR + 2) * 4 + 64;
+  CK(cudaFuncSetAttribute(k_rr_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rrsm));
+  CK(cudaFuncSetAttribute(k_rr_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rrsm));
+  double2* Mm = w.small;
+  double2* Y = w.small + kMaxRR * kMaxRR;
+  auto rr = [&](const double2* Vb, const double2* HVb, int n) -> int {
+    if (int r = gram(ctx, Vb, (int)N, n, HVb, (int)N, n, Mm, w.part)) return r;
+    const size_t sm = (size_t)n * n * 16 + (size_t)3 * n * 16 + (size_t)2 * n * 8 + (size_t)kMaxRR * 8 +
+                      (size_t)n * nb * 8 + 64;
+    k_rr_tridiag<<<1, 256, sm, s>>>(Mm, n, nb, largest, w.theta, Y, w.istat + 1); WTBG_COUNT(ctx, 1);
+    CKL("k_rr_tridiag");
+    // X = V Y(:, :nb), HX = HV Y(:, :nb)
+    if (int r = tall(ctx, Vb, (int)N, n, Y, nb, w.Xn, (int)N, false)) return r;
+    if (int r = tall(ctx, HVb, (int)N, n, Y, nb, w.HXn, (int)N, false)) return r;
+    CK(cudaMemcpyAsync(X, w.Xn, (size_t)N * nb * 16, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(HX, w.HXn, (size_t)N * nb * 16, cudaMemcpyDeviceToDevice, s));
+    return 0;
+  };
+  if (int r = rr(X, HX, nb)) return r;
+  std::vector<double> res(nb), thh(nb);
+  const int nrb = (int)((N + th - 1) / th);
+  ENSURE(ctx->tmp2, (size_t)nrb * 64 * 8 + 64);
+  double* rp = ctx->tmp2.as<double>();
+  int it = 0;
+  double worst = 0.0;
+  for (; it < max_iter; ++it) {
+    k_resid_precond<<<nrb, th, 0, s>>>(X, HX, (int)N, nb, w.theta, w.D, N, T, (int)N, rp); WTBG_COUNT(ctx, 1);
+    CKL("k_resid_precond");
+    std::vector<double> rph((size_t)nrb * 64);
+    CK(cudaMemcpyAsync(rph.data(), rp, rph.size() * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(thh.data(), w.theta, nb * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    worst = 0.0;
+    for (int v = 0; v < nb; ++v) {
+      double ss = 0;
+      for (int b = 0; b < nrb; ++b) ss += rph[(size_t)b * 64 + v];
+      res[v] = sqrt(ss);
+      if (v < nev) worst = std::max(worst, res[v]);
+    }
+    if (worst < tol) break;
+    // T <- T - X (X^H T), twice; orthonormalise
+    for (int pass = 0; pass < 2; ++pass) {
+      if (int r = gram(ctx, X, (int)N, nb, T, (int)N, nb, w.small + 2 * kMaxRR * kMaxRR, w.part)) return r;
+      if (int r = tall(ctx, X, (int)N, nb, w.small + 2 * kMaxRR * kMaxRR, nb, T, (int)N, true)) return r;
+    }
+    if (int r = cholqr2(ctx, T, nb, w.Xn, w)) return r;
+    if (int r = hemm(ctx, T, (int)N, nb, HT, (int)N, w.Yp)) return r;
+    if (int r = rr(w.V, w.HV, n2)) return r;
+  }
+  if (iters) *iters = it;
+  if (maxres) *maxres = worst;
+  W.assign(thh.begin(), thh.begin() + nev);
+  // oscillators
+  act.assign((size_t)nev * 8, 0.0);
+  if (ctx->have_velocity) {
+    const int nparts = (int)std::min<long long>(296, (N + 255) / 256);
+    k_osc_part<<<nparts, 256, 0, s>>>(X, (int)N, nev, ctx->h.as<double2>(), N, w.part); WTBG_COUNT(ctx, 1);
+    double* dact = w.rpart;
+    k_osc_final<<<(nev + 63) / 64, 64, 0, s>>>(w.part, nparts, nev, dtfull, cpol, dact); WTBG_COUNT(ctx, 1);
+    CKL("oscillators");
+    CK(cudaMemcpyAsync(act.data(), dact, (size_t)nev * 8 * 8, cudaMemcpyDeviceToHost, s));
+  }
+  if (dXout) CK(cudaMemcpyAsync(dXout, X, (size_t)N * nev * 16, cudaMemcpyDeviceToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int run_hemm_public(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y, int ldy, double2* Yp) {
+  return hemm(ctx, X, ldx, m, Y, ldy, Yp);
+}
+
+// Y = H X for a narrow block (m = 8 or 16), reading the lower triangle once
+int run_hemm_narrow(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y, int ldy) {
+  const long long N = ctx->N;
+  const int nblk = (int)((N + TB - 1) / TB);
+  ENSURE(ctx->slots, (size_t)nblk * nblk * TB * m * 16);
+  double2* slots = ctx->slots.as<double2>();
+  const size_t sm = sizeof(double2) * TB * (TB + 1) + 2 * sizeof(double2) * TB * (m + 1);
+  dim3 grid(nblk, (nblk + LHS - 1) / LHS);
+  if (m == 8) {
+    CK(cudaFuncSetAttribute(k_hemm_lower<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_hemm_lower<1><<<grid, 256, sm, ctx->stream>>>(ctx->H.as<double2>(), N, X, ldx, nblk, slots);
+  } else if (m == 16) {
+    CK(cudaFuncSetAttribute(k_hemm_lower<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_hemm_lower<2><<<grid, 256, sm, ctx->stream>>>(ctx->H.as<double2>(), N, X, ldx, nblk, slots);
+  } else {
+    return set_err(ctx, WTBG_ERR_UNSUPPORTED, "hemm_narrow: m must be 8 or 16");
+  }
+  WTBG_COUNT(ctx, 1);
+  const long long tot = (long long)nblk * TB * m;
+  k_sum_slots<<<(int)((tot + 255) / 256), 256, 0, ctx->stream>>>(slots, N, nblk, m, Y, ldy); WTBG_COUNT(ctx, 1);
+  CKL("hemm_narrow");
+  return 0;
+}

@@ -23,7 +23,8 @@ EXPORTS = ["wtbg_create", "wtbg_destroy", "wtbg_error_string", "wtbg_last_error"
            "wtbg_last_device_ms", "wtbg_set_model", "wtbg_bands", "wtbg_velocity",
            "wtbg_sp_table", "wtbg_bse_build", "wtbg_bse_get_matrix", "wtbg_bse_solve",
            "wtbg_bse_eigvecs", "wtbg_spectrum", "wtbg_bse_q_eigenvalues", "wtbg_set_profiling",
-           "wtbg_get_stats", "wtbg_reset_stats", "wtbg_spectrum_noalloc"]
+           "wtbg_get_stats", "wtbg_reset_stats", "wtbg_spectrum_noalloc", "wtbg_bse_davidson",
+           "wtbg_bse_spectrum_fast"]
 
 
 class WtbgError(RuntimeError):
@@ -79,6 +80,11 @@ def load_library(path: str = LIB_PATH):
         "wtbg_set_profiling": (C.c_int, [P, C.c_int]),
         "wtbg_get_stats": (C.c_int, [P, C.POINTER(Stats)]),
         "wtbg_reset_stats": (C.c_int, [P]),
+        "wtbg_bse_davidson": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, dp, C.c_int, C.c_int,
+                                        dp, dp, dp, ip, dp]),
+        "wtbg_bse_spectrum_fast": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, ip, C.c_double,
+                                             C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
+                                             dp, fp]),
         "wtbg_spectrum_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, ip, ip, C.c_double,
                                             C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                                             C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p,
@@ -222,6 +228,40 @@ class Context:
         act = np.zeros((self.N, 8), order="F") if want_act else None
         self._check(self.lib.wtbg_bse_solve(self.h, int(dtfull), int(cpol), _dp(W), _dp(act)))
         return W, act
+
+    def bse_davidson(self, nev: int, nb: int = 40, largest: bool = False, max_iter: int = 200, tol: float = 1e-6,
+                     X0=None, dtfull: bool = False, cpol: bool = False, want_act: bool = True,
+                     want_vectors: bool = False, check: bool = True):
+        """Block Davidson for the nev lowest (or highest) states; returns (W, act, X, iters, maxres)."""
+        W = np.zeros(nev)
+        act = np.zeros((nev, 8), order="F") if want_act else None
+        X = np.zeros((self.N, nev), dtype=np.complex128, order="F") if want_vectors else None
+        x0 = None
+        if X0 is not None:
+            x0 = np.asfortranarray(np.asarray(X0, dtype=np.complex128))
+        it = C.c_int(0)
+        mr = C.c_double(0.0)
+        st = self.lib.wtbg_bse_davidson(self.h, nev, nb, int(bool(largest)), max_iter, float(tol),
+                                        x0.ctypes.data_as(C.POINTER(C.c_double)) if x0 is not None else None,
+                                        int(dtfull), int(cpol), _dp(W), _dp(act),
+                                        X.ctypes.data_as(C.POINTER(C.c_double)) if X is not None else None,
+                                        C.byref(it), C.byref(mr))
+        if check or st not in (0, -4):
+            self._check(st)
+        return W, act, X, it.value, mr.value
+
+    def bse_spectrum_fast(self, nsteps, e1, emax, ngrid, vcell3d, ebse0, ebsef, numbse, sme, renorm, spinf,
+                          dtfull=False, cpol=False):
+        """Haydock spectrum; returns (omega (nw,), eps (nw, 2, 8) float32)."""
+        nw = int(numbse)
+        ng = np.array(ngrid, dtype=np.int32)
+        om = np.zeros(nw)
+        eps = np.zeros((nw, 2, 8), dtype=np.float32, order="F")
+        self._check(self.lib.wtbg_bse_spectrum_fast(self.h, int(nsteps), int(dtfull), int(cpol), float(e1), float(emax),
+                                                    _ip(ng), float(vcell3d), float(ebse0), float(ebsef),
+                                                    float(numbse), float(sme), int(bool(renorm)), float(spinf),
+                                                    _dp(om), _fp(eps)))
+        return om, eps
 
     def bse_eigvecs(self, n0: int, n1: int):
         A = np.zeros((self.N, n1 - n0 + 1), dtype=np.complex128, order="F")
