@@ -268,7 +268,41 @@ def cpu_baseline(wl, model, budget_s=30.0):
 
 
 # ----------------------------------------------------------------------------- main
+def ncu_launch_summary(path: str) -> str:
+    """Per-kernel launches, total device time and share from an ncu CSV launch list
+    (``ncu --metrics gpu__time_duration.sum --csv --log-file path``)."""
+    import csv
+    import collections
+    scale = {"nsecond": 1e-6, "ns": 1e-6, "usecond": 1e-3, "us": 1e-3, "msecond": 1.0, "ms": 1.0, "second": 1e3, "s": 1e3}
+    agg = collections.OrderedDict()
+    hdr = None
+    with open(path, newline="") as f:
+        for r in csv.reader(f):
+            if r and r[0] == "ID":
+                hdr = r
+                continue
+            if hdr is None or len(r) != len(hdr):
+                continue
+            d = dict(zip(hdr, r))
+            if d.get("Metric Name") != "gpu__time_duration.sum":
+                continue
+            name = d["Kernel Name"].split("(")[0].replace("void ", "").replace("<unnamed>::", "")
+            ms = float(d["Metric Value"].replace(",", "")) * scale.get(d.get("Metric Unit", "ns"), 1e-6)
+            a = agg.setdefault(name, [0, 0.0])
+            a[0] += 1
+            a[1] += ms
+    tot = sum(a[1] for a in agg.values())
+    lines = [f"{'kernel':48s} {'launches':>9s} {'total ms':>11s} {'avg us':>10s} {'share':>7s}"]
+    for name, (n, t) in sorted(agg.items(), key=lambda x: -x[1][1]):
+        lines.append(f"{name[:48]:48s} {n:9d} {t:11.3f} {1e3 * t / n:10.1f} {100 * t / max(tot, 1e-30):6.2f}%")
+    lines.append(f"{'total':48s} {sum(a[0] for a in agg.values()):9d} {tot:11.3f}")
+    return "\n".join(lines)
+
+
 def main():
+    if len(sys.argv) == 3 and sys.argv[1] == "--ncu-summary":
+        print(ncu_launch_summary(sys.argv[2]))
+        return
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1)

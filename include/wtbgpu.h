@@ -138,6 +138,57 @@ int wtbg_bse_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter,
                       const double* X0, int dtfull, int cpol, double* W, double* act, double* X,
                       int* iters, double* maxres);
 
+/* ---- product used by the fast form (wtbg_bse_davidson, wtbg_bse_spectrum_fast, wtbg_bse_apply).
+ *      mode 0: FP64 on CUDA cores (the lower triangle of H read once per product).
+ *      mode 1: split-BF16 tensor-core product: the off-diagonal part of H is stored once per
+ *      build as bf16 hi + lo planes of Re H and Im H (8 bytes per element, row-major), the
+ *      vectors likewise, three bf16 products per pair accumulate in FP32, and the diagonal
+ *      (band-energy differences) is applied in FP64; relative error ~1e-5 of |H_offdiag x|.
+ *      No counterpart in the reference (its solver is ZHEEV on the full FP64 matrix). */
+int wtbg_set_fast_product(wtbg_ctx* ctx, int mode);
+
+/* ---- Y = H X for m vectors with the product selected by wtbg_set_fast_product; X, Y are
+ *      complex(8) N x m column-major (interleaved re, im).  Requires wtbg_bse_build; keeps the
+ *      matrix.  No counterpart in the reference. */
+int wtbg_bse_apply(wtbg_ctx* ctx, int m, const double* X, double* Y);
+
+/* ---- learned warm start for wtbg_bse_davidson (no counterpart in the reference).
+ *      A per-transition MLP (3 layers, width 512, SiLU, BF16 weights with an FP32 master copy,
+ *      FP32 accumulation on the tensor cores) maps band-edge data of each basis state
+ *      (k, c, v) -- BSE diagonal, velocity matrix elements, k position, band indices -- and
+ *      the sweep globals glob = {qx, qy, qz, r0, eps_env} to 5 complex coefficients per
+ *      state; the 32-vector block is X[i,s] = sum_c coef * carrier_c[i] with carriers
+ *      1, hx/|h|, hy/|h|, conj(hx)/|h|, conj(hy)/|h|.  Samples are the current basis of ctx
+ *      (after wtbg_bands, wtbg_velocity and a build) plus the 32 lowest eigenvectors of the
+ *      plain dense FP64 solve (A: N x 32 complex(8), column-major).  Training minimises
+ *      ||X - A A^H X||^2 + 0.25 ||X^H X - I||^2 per sample with Adam (hand-written forward,
+ *      backward and update kernels).  The network is bound to ctx (device, stream). */
+typedef struct wtbg_net wtbg_net;
+int wtbg_net_create(wtbg_ctx* ctx, wtbg_net** net, unsigned long long seed);
+int wtbg_net_destroy(wtbg_net* net);
+long long wtbg_net_num_params(void);   /* flat fp32: W1[512][32] b1[512] W2[512][512] b2 W3[320][512] b3[320] */
+int wtbg_net_get_params(wtbg_net* net, float* p);
+int wtbg_net_set_params(wtbg_net* net, const float* p);
+/* features F (N x 32 row-major, as rounded to bf16) and carriers CAR (5 x N complex(4)) of the
+ * current basis; either may be NULL */
+int wtbg_net_features(wtbg_net* net, const double* glob, float* F, float* CAR);
+int wtbg_net_add_sample(wtbg_net* net, const double* glob, const double* A);
+int wtbg_net_num_samples(wtbg_net* net);
+/* epochs over samples [first, first+count) (count <= 0: all from first), mini-batches of
+ * `batch` samples; loss_hist[epochs] gets the mean training loss per epoch (may be NULL) */
+int wtbg_net_train(wtbg_net* net, int epochs, int batch, float lr, int first, int count, float* loss_hist);
+int wtbg_net_eval_loss(wtbg_net* net, int first, int count, float* loss);
+/* predicted block for the current basis of the bound context: X0 (N x 32 complex(8)) */
+int wtbg_net_predict(wtbg_net* net, const double* glob, double* X0);
+/* one forward + backward on explicit inputs (gradient check): F (nsamp*rows x 32, fp32),
+ * CAR (5 x nsamp*rows complex(4)), A (32 x nsamp*rows complex(4), each sample's rows
+ * orthonormal); loss and the flat gradient (layout of wtbg_net_get_params). rows % 8 == 0. */
+int wtbg_net_loss_grad(wtbg_net* net, int nsamp, long long rows, const float* F, const float* CAR, const float* A,
+                       float* loss, float* grad);
+/* C (M x N, row-major, fp32) = A (M x K) B (N x K)^T with A, B rounded to bf16 and FP32
+ * accumulation: the tcgen05 GEMM the network kernels use, exposed for checks. K % 8 == 0. */
+int wtbg_gemm_bf16(wtbg_ctx* ctx, int M, int N, int K, const float* A, const float* B, float* C);
+
 /* ---- fast form of the BSE spectrum: eps(omega) of bsedielraw (and bsedielrawpol) from the
  *      Haydock recursion on the built BSE matrix, nsteps Lanczos steps per chain closed by a
  *      square-root terminator (no counterpart in the reference; oracle = dense solve +

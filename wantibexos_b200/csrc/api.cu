@@ -42,30 +42,10 @@ int ensure(wtbg_ctx* c, DevBuf& b, size_t bytes) {
 
 namespace {
 
-struct Timer {
-  wtbg_ctx* c;
-  explicit Timer(wtbg_ctx* ctx) : c(ctx) { cudaEventRecord(c->ev0, c->stream); }
-  int stop() {
-    cudaEventRecord(c->ev1, c->stream);
-    cudaError_t e = cudaEventSynchronize(c->ev1);
-    if (e != cudaSuccess) return cuda_fail(c, e, "stream");
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-    c->last_ms = ms;
-    return 0;
-  }
-};
-
 void free_buf(DevBuf& b) {
   if (b.p) cudaFree(b.p);
   b.p = nullptr;
   b.bytes = 0;
-}
-
-int set_device(wtbg_ctx* ctx) {
-  cudaError_t e = cudaSetDevice(ctx->device);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
-  return 0;
 }
 
 }  // namespace
@@ -206,6 +186,7 @@ int wtbg_set_model(wtbg_ctx* ctx, int w, int nvec, const double* hre, const doub
   CK(cudaMemcpyAsync(ctx->isR0.p, is0.data(), is0.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->have_bands = ctx->have_velocity = ctx->have_matrix = ctx->have_solution = false;
+  ctx->fast_ready = false;
   return WTBG_OK;
 }
 
@@ -249,6 +230,7 @@ int wtbg_bands(wtbg_ctx* ctx, int nk, const double* kpt, int nv, int nc, double*
   if (int r = check_kstat(ctx, nk)) return r;
   ctx->have_bands = true;
   ctx->have_velocity = ctx->have_matrix = ctx->have_solution = false;
+  ctx->fast_ready = false;
   std::vector<double> e((size_t)nk * nb);
   CK(cudaMemcpyAsync(e.data(), ctx->eig.p, e.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
   std::vector<int> no(nk);
@@ -321,6 +303,7 @@ int wtbg_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p) {
   if (int r = launch_bse_build(ctx, p, nullptr)) return r;
   if (int r = t.stop()) return r;
   ctx->have_matrix = true;
+  ctx->fast_ready = false;
   ctx->have_solution = false;
   return WTBG_OK;
 }
@@ -354,6 +337,7 @@ int wtbg_bse_solve(wtbg_ctx* ctx, int dtfull, int cpol, double* W, double* act) 
   Timer t(ctx);
   if (int r = run_tridiagonalise(ctx)) return r;
   ctx->have_matrix = false;   // overwritten by the reflectors
+  ctx->fast_ready = false;
   if (int r = run_tridiagonal_solve(ctx, dtfull, cpol, act != nullptr)) return r;
   if (int r = t.stop()) return r;
   ctx->have_solution = true;
@@ -387,6 +371,8 @@ int wtbg_bse_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter,
   int it = 0;
   double mr = 0.0;
   if (int r = run_davidson(ctx, nev, nb, largest, max_iter, tol, dX0, dtfull, cpol, w, ac, dX, &it, &mr)) return r;
+  if (ctx->fast_mode)
+    if (int r = fast_check(ctx)) return r;
   if (int r = t.stop()) return r;
   memcpy(W, w.data(), (size_t)nev * 8);
   if (act) memcpy(act, ac.data(), (size_t)nev * 8 * 8);
@@ -394,6 +380,37 @@ int wtbg_bse_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter,
   if (iters) *iters = it;
   if (maxres) *maxres = mr;
   if (mr >= tol) return set_err(ctx, WTBG_ERR_NOCONV, "bse_davidson: residual above tolerance after max_iter");
+  return WTBG_OK;
+}
+
+int wtbg_set_fast_product(wtbg_ctx* ctx, int mode) {
+  if (!ctx || mode < 0 || mode > 1) return WTBG_ERR_ARG;
+  ctx->fast_mode = mode;
+  return WTBG_OK;
+}
+
+int wtbg_bse_apply(wtbg_ctx* ctx, int m, const double* X, double* Y) {
+  if (!ctx || !X || !Y || m < 1) return WTBG_ERR_ARG;
+  if (!ctx->have_matrix) return set_err(ctx, WTBG_ERR_STATE, "bse_apply: call wtbg_bse_build first");
+  if (int r = set_device(ctx)) return r;
+  const long long N = ctx->N;
+  const int mp = (m + 7) / 8 * 8;
+  Timer t(ctx);
+  ENSURE(ctx->tmp, (size_t)N * mp * 16);
+  ENSURE(ctx->tmp2, (size_t)N * mp * 16);
+  double2* dX = ctx->tmp.as<double2>();
+  double2* dY = ctx->tmp2.as<double2>();
+  CK(cudaMemsetAsync(dX, 0, (size_t)N * mp * 16, ctx->stream));
+  CK(cudaMemcpyAsync(dX, X, (size_t)N * m * 16, cudaMemcpyHostToDevice, ctx->stream));
+  if (ctx->fast_mode) {
+    if (int r = run_fastprod(ctx, dX, (int)N, m, dY, (int)N)) return r;
+    if (int r = fast_check(ctx)) return r;
+  } else {
+    for (int c = 0; c < mp; c += 8)
+      if (int r = run_hemm_narrow(ctx, dX + (long long)c * N, (int)N, 8, dY + (long long)c * N, (int)N)) return r;
+  }
+  if (int r = t.stop()) return r;
+  CK(cudaMemcpy(Y, dY, (size_t)N * m * 16, cudaMemcpyDeviceToHost));
   return WTBG_OK;
 }
 
@@ -445,6 +462,8 @@ int wtbg_bse_spectrum_fast(wtbg_ctx* ctx, int nsteps, int dtfull, int cpol, doub
   Timer t(ctx);
   std::vector<double> al, be, n2;
   if (int r = run_haydock(ctx, nsteps, (int)codes.size(), codes.data(), al, be, n2)) return r;
+  if (ctx->fast_mode)
+    if (int r = fast_check(ctx)) return r;
   ENSURE(ctx->sp_om, (size_t)nw * 8 + (size_t)nw * 16 * 4 + 64);
   double* dom = ctx->sp_om.as<double>();
   float* deps = reinterpret_cast<float*>(dom + nw);
@@ -542,6 +561,7 @@ int wtbg_bse_q_eigenvalues(wtbg_ctx* ctx, int nk, const double* kptq, const doub
   if ((r = run_tridiagonal_solve(ctx, 0, 0, false))) return r;
   if ((r = t.stop())) return r;
   ctx->have_matrix = false;
+  ctx->fast_ready = false;
   ctx->have_solution = false;
   memcpy(W, ctx->lam_host.data(), (size_t)N * 8);
   return WTBG_OK;

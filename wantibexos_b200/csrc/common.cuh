@@ -79,6 +79,15 @@ struct wtbg_ctx {
   DevBuf tmp, tmp2, istat;
 
   // counters
+  // fast form: split-BF16 planes of the kernel matrix for the tensor-core product
+  int fast_mode = 0;
+  bool fast_ready = false;
+  long long fast_ld = 0;
+  int fast_mp = 0;
+  DevBuf fA, fB, fY, fD, fErr;
+  alignas(64) unsigned char tmA[128];   // CUtensorMap of the H planes
+  alignas(64) unsigned char tmB[128];   // CUtensorMap of the X planes (current padded width)
+
   wtbg_stats stats{};
   int profiling = 0;
   std::vector<cudaEvent_t> evpool;   // event pairs for per-launch timing when profiling
@@ -144,6 +153,33 @@ int run_haydock(wtbg_ctx* ctx, int K, int ncomp, const int* codes, std::vector<d
 int run_haydock_spectrum(wtbg_ctx* ctx, int K, int nchain, const double* alpha, const double* beta, const double* norm2,
                          int nout, const int* ocode, const int* ngrid, double vcell3d, double ebse0, double ebsef,
                          double numbse, double eta, double e1, int renorm, double spinf, double* d_om, float* d_eps);
+// CUDA-event timing of one C-ABI call on the context's stream (sets last_ms)
+struct Timer {
+  wtbg_ctx* c;
+  explicit Timer(wtbg_ctx* ctx) : c(ctx) { cudaEventRecord(c->ev0, c->stream); }
+  int stop() {
+    cudaEventRecord(c->ev1, c->stream);
+    cudaError_t e = cudaEventSynchronize(c->ev1);
+    if (e != cudaSuccess) return cuda_fail(c, e, "stream");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->last_ms = ms;
+    return 0;
+  }
+};
+
+
+inline int set_device(wtbg_ctx* ctx) {
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  return 0;
+}
+
+
+int run_fast_setup(wtbg_ctx* ctx);
+int run_fastprod(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y, int ldy);
+int run_hemm_narrow(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y, int ldy);
+int fast_check(wtbg_ctx* ctx);
 int run_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, double tol, const double2* dX0, int dtfull,
                  int cpol, std::vector<double>& W, std::vector<double>& act, double2* dXout, int* iters, double* maxres);
 int launch_spectrum(wtbg_ctx* ctx, int n, int ncomp, const double* d_e, const double* d_f, const int* rtype,

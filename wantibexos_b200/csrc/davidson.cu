@@ -6,7 +6,7 @@
 // Iteration (basis V = [X T], nb + nb columns):
 //   R = H X - X diag(theta),  T = R / (diag(H) - theta)   (Davidson preconditioner)
 //   T <- T - X (X^H T) (twice), T <- T chol(T^H T)^-1 (twice: CholQR2)
-//   M = V^H (H V)  (2nb x 2nb),  (theta, Y) = eig(M) by one-CTA Jacobi,  X = V Y, HX = HV Y
+//   M = V^H (H V)  (2nb x 2nb),  (theta, Y) = eig(M) by a one-CTA tridiagonal eigensolver,  X = V Y, HX = HV Y
 // Oscillator strengths of the converged states: f_n = |sum_j X_jn h_j|^2 (dielbsev,
 // bse_subs.f90:336-378, no conjugate on the eigenvector).
 #include <algorithm>
@@ -237,20 +237,22 @@ __global__ void k_sum_parts(const double2* Yp, long long N, int m, double2* Y, i
   Y[row + v * ldy] = s;
 }
 
-// C (p x q) = A^H B, A (N x p, lda), B (N x q, ldb): per-block partials [blk][p*q]; rows are
-// staged 32 at a time in shared memory and every thread accumulates its outputs in registers.
+// C (p x q) = A^H B, A (N x p, lda), B (N x q, ldb): per-block partials [blk][p*q]. Rows are
+// staged GR at a time in shared memory; the 16 x 16 threads each own a register tile of
+// outputs (a = tx + 16 i, b = ty + 16 j), so every staged value feeds up to 5 products.
 constexpr int GR = 16;
-constexpr int GMAXO = 25;   // outputs per thread: p*q <= 256*25 = 6400 (80 x 80)
+constexpr int GT = 5;   // register tile: p, q <= 16 * GT = 80
 __global__ void __launch_bounds__(256) k_gram(const double2* A, int lda, int p, const double2* B, int ldb, int q,
                                               long long N, double2* part) {
   __shared__ double2 as[GR][kMaxRR + 1], bsm[GR][kMaxRR + 1];
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const long long rows_per = (N + gridDim.x - 1) / gridDim.x;
   const long long r0 = (long long)blockIdx.x * rows_per, r1 = min(N, r0 + rows_per);
-  const int pq = p * q;
-  double2 acc[GMAXO];
+  double2 acc[GT][GT];
 #pragma unroll
-  for (int j = 0; j < GMAXO; ++j) acc[j] = make_double2(0, 0);
+  for (int i = 0; i < GT; ++i)
+#pragma unroll
+    for (int j = 0; j < GT; ++j) acc[i][j] = make_double2(0, 0);
   for (long long c0 = r0; c0 < r1; c0 += GR) {
     __syncthreads();
     for (int it = tid; it < GR * p; it += 256) {
@@ -262,266 +264,187 @@ __global__ void __launch_bounds__(256) k_gram(const double2* A, int lda, int p, 
       bsm[rr][b] = (c0 + rr < r1) ? B[c0 + rr + (long long)b * ldb] : make_double2(0, 0);
     }
     __syncthreads();
+#pragma unroll 2
+    for (int rr = 0; rr < GR; ++rr) {
+      double2 av[GT], bv[GT];
 #pragma unroll
-    for (int j = 0; j < GMAXO; ++j) {
-      const int o = tid + 256 * j;
-      if (o >= pq) break;
-      const int a = o % p, b = o / p;
-      double2 sacc = acc[j];
-      for (int rr = 0; rr < GR; ++rr) sacc = cadd(sacc, cmulc(as[rr][a], bsm[rr][b]));
-      acc[j] = sacc;
+      for (int i = 0; i < GT; ++i) av[i] = (tx + 16 * i < p) ? as[rr][tx + 16 * i] : make_double2(0, 0);
+#pragma unroll
+      for (int j = 0; j < GT; ++j) bv[j] = (ty + 16 * j < q) ? bsm[rr][ty + 16 * j] : make_double2(0, 0);
+#pragma unroll
+      for (int i = 0; i < GT; ++i)
+#pragma unroll
+        for (int j = 0; j < GT; ++j) acc[i][j] = cadd(acc[i][j], cmulc(av[i], bv[j]));
     }
   }
+  const int pq = p * q;
 #pragma unroll
-  for (int j = 0; j < GMAXO; ++j) {
-    const int o = tid + 256 * j;
-    if (o < pq) part[(long long)blockIdx.x * pq + o] = acc[j];
+  for (int i = 0; i < GT; ++i)
+#pragma unroll
+    for (int j = 0; j < GT; ++j) {
+      const int a = tx + 16 * i, b = ty + 16 * j;
+      if (a < p && b < q) part[(long long)blockIdx.x * pq + a + b * p] = acc[i][j];
+    }
+}
+
+// C[i] = sum over blocks of part[blk][i]: 32 outputs x 8 block groups per CTA
+__global__ void k_gram_sum(const double2* part, int nparts, int pq, double2* C) {
+  __shared__ double2 red[8][33];
+  const int x = threadIdx.x & 31, y = threadIdx.x >> 5;
+  const int i = blockIdx.x * 32 + x;
+  double2 s = make_double2(0, 0);
+  if (i < pq)
+    for (int k = y; k < nparts; k += 8) s = cadd(s, part[(long long)k * pq + i]);
+  red[y][x] = s;
+  __syncthreads();
+  if (y == 0 && i < pq) {
+    for (int k = 1; k < 8; ++k) s = cadd(s, red[k][x]);
+    C[i] = s;
   }
 }
 
-__global__ void k_gram_sum(const double2* part, int nparts, int pq, double2* C) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= pq) return;
-  double2 s = make_double2(0, 0);
-  for (int k = 0; k < nparts; ++k) s = cadd(s, part[(long long)k * pq + i]);
-  C[i] = s;
-}
-
-// C (N x q, ldc) = A (N x p, lda) * B (p x q, column-major, ldb = p), or C -= A * B
+// C (N x q, ldc) = A (N x p, lda) * B (p x q, column-major, ldb = p), or C -= A * B.
+// Grid (rows / 256, q / 8): every thread owns one row and eight output columns.
 template <bool SUB>
-__global__ void k_tall_gemm(const double2* A, int lda, int p, const double2* B, int q, long long N, double2* Cm, int ldc) {
-  extern __shared__ double2 bs[];
-  for (int i = threadIdx.x; i < p * q; i += blockDim.x) bs[i] = B[i];
+__global__ void __launch_bounds__(256) k_tall_gemm(const double2* A, int lda, int p, const double2* B, int q,
+                                                   long long N, double2* Cm, int ldc) {
+  __shared__ double2 bs[kMaxRR * 8];
+  const int b0 = blockIdx.y * 8;
+  const int nb = min(8, q - b0);
+  for (int i = threadIdx.x; i < p * 8; i += blockDim.x) {
+    const int a = i % p, k = i / p;
+    bs[a * 8 + k] = (k < nb) ? B[a + (b0 + k) * p] : make_double2(0, 0);
+  }
   __syncthreads();
   const long long rr = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (rr >= N) return;
-  for (int b0 = 0; b0 < q; b0 += 8) {
-    double2 s[8];
+  double2 s[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) s[k] = make_double2(0, 0);
-    const int nb = min(8, q - b0);
-    for (int a = 0; a < p; ++a) {
-      const double2 x = A[rr + (long long)a * lda];
+  for (int k = 0; k < 8; ++k) s[k] = make_double2(0, 0);
+#pragma unroll 4
+  for (int a = 0; a < p; ++a) {
+    const double2 x = A[rr + (long long)a * lda];
 #pragma unroll
-      for (int k = 0; k < 8; ++k)
-        if (k < nb) s[k] = cadd(s[k], cmul(x, bs[a + (b0 + k) * p]));
-    }
+    for (int k = 0; k < 8; ++k) s[k] = cadd(s[k], cmul(x, bs[a * 8 + k]));
+  }
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      if (k >= nb) break;
-      double2* cp = Cm + rr + (long long)(b0 + k) * ldc;
-      *cp = SUB ? csub(*cp, s[k]) : s[k];
-    }
+  for (int k = 0; k < 8; ++k) {
+    if (k >= nb) break;
+    double2* cp = Cm + rr + (long long)(b0 + k) * ldc;
+    *cp = SUB ? csub(*cp, s[k]) : s[k];
   }
 }
 
-// G (q x q Hermitian PD, q <= 64) -> Rinv (upper triangular) with G = R^H R.  A column with a
-// non-positive pivot gets a zero row in R^-1 (its vector is dropped).  One CTA.
-__global__ void __launch_bounds__(128) k_chol_inv(const double2* G, int q, double2* Rinv, int* bad) {
+// G (q x q Hermitian PD, q <= 64) -> Rinv (upper triangular, column-major) with G = R^H R,
+// R = L^H from a right-looking Cholesky G = L L^H in shared memory; L^-1 by row-wise forward
+// substitution with all columns in parallel, Rinv = (L^-1)^H. A non-positive pivot gets a zero
+// row in Rinv (its vector is dropped). One CTA.
+__global__ void __launch_bounds__(512) k_chol_inv(const double2* G, int q, double2* Rinv, int* bad) {
   extern __shared__ double2 csm[];
   const int ld = q + 1;
-  double2* Rm = csm;              // R(a, b) at Rm[a * ld + b]
-  double2* Rim = csm + q * ld;    // Rinv(a, b) at Rim[a * ld + b]
-#define R(a, b) Rm[(a) * ld + (b)]
-#define Ri(a, b) Rim[(a) * ld + (b)]
-  __shared__ double s_d;
-  const int tid = threadIdx.x;
-  for (int it = tid; it < q * q; it += blockDim.x) {
-    const int a = it % q, b = it / q;
-    R(a, b) = make_double2(0, 0);
-    Ri(a, b) = make_double2(0, 0);
-  }
-  __syncthreads();
-  int nbad = 0;
-  for (int j = 0; j < q; ++j) {
-    if (tid == 0) {
-      double d = G[j + j * q].x;
-      for (int k = 0; k < j; ++k) d -= R(k, j).x * R(k, j).x + R(k, j).y * R(k, j).y;
-      const double scale = fabs(G[j + j * q].x) + 1e-300;
-      s_d = (d > 1e-28 * scale) ? sqrt(d) : 0.0;
-      R(j, j) = make_double2(s_d, 0.0);
-    }
-    __syncthreads();
-    const double rjj = s_d;
-    if (rjj == 0.0) {
-      ++nbad;
-      __syncthreads();
-      continue;
-    }
-    for (int i = j + 1 + tid; i < q; i += blockDim.x) {
-      double2 t = G[j + i * q];
-      for (int k = 0; k < j; ++k) t = csub(t, cmulc(R(k, j), R(k, i)));
-      R(j, i) = cscale(t, 1.0 / rjj);
-    }
-    __syncthreads();
-  }
-  // columns of R^-1 in parallel: R Ri(:, j) = e_j
-  for (int j = tid; j < q; j += blockDim.x) {
-    if (R(j, j).x == 0.0) continue;
-    Ri(j, j) = make_double2(1.0 / R(j, j).x, 0.0);
-    for (int i = j - 1; i >= 0; --i) {
-      if (R(i, i).x == 0.0) continue;
-      double2 sacc = make_double2(0, 0);
-      for (int k = i + 1; k <= j; ++k) sacc = cadd(sacc, cmul(R(i, k), Ri(k, j)));
-      Ri(i, j) = cscale(sacc, -1.0 / R(i, i).x);
-    }
-  }
-  __syncthreads();
-  for (int it = tid; it < q * q; it += blockDim.x) {
-    const int a = it % q, b = it / q;
-    Rinv[it] = Ri(a, b);
-  }
-  if (tid == 0) *bad = nbad;
-#undef R
-#undef Ri
-}
-
-// One-CTA cyclic Jacobi of a Hermitian n x n matrix M (column-major, n <= kMaxRR is checked by
-// the host): eigenvalues ascending (or descending), eigenvectors as columns of Y (n x n).
-struct RRot {
-  int p, q, active, pad;
-  double cs, sn, ex, ey, ap, aq;
-};
-
-__global__ void __launch_bounds__(1024) k_rr_jacobi(const double2* Min, int n, int descending, double* theta,
-                                                    double2* Yout, int* status) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  double2* Lm = csm;             // L(i, k) at Lm[i + k * ld] (lower)
+  double2* Xm = csm + q * ld;    // X = L^-1 (lower), X(i, j) at Xm[i + j * ld]
+  __shared__ double s_piv[64];
   const int tid = threadIdx.x, bs = blockDim.x;
-  const int m2 = n + (n & 1), npair = m2 / 2;
-  double2* Am = reinterpret_cast<double2*>(smem);
-  double2* V = Am + n * n;
-  RRot* rot = reinterpret_cast<RRot*>(V + n * n);
-  double* lam = reinterpret_cast<double*>(rot + npair);
-  int* perm = reinterpret_cast<int*>(lam + n + 1);
-  __shared__ int s_rot;
-  __shared__ double s_tol;
-  double fro = 0.0;
-  for (int it = tid; it < n * n; it += bs) {
-    const int a = it % n, b = it / n;
-    double2 v = Min[it];
-    if (a == b) v.y = 0.0;
-    if (a < b) v = cconj(Min[b + a * n]);   // Hermitian from the lower triangle
-    Am[it] = v;
-    V[it] = make_double2(a == b ? 1.0 : 0.0, 0.0);
-    fro += v.x * v.x + v.y * v.y;
+  for (int it = tid; it < q * q; it += bs) {
+    const int i = it % q, k = it / q;
+    Lm[i + k * ld] = (i >= k) ? G[i + k * q] : make_double2(0, 0);
+    Xm[i + k * ld] = make_double2(0, 0);
   }
-  for (int o = 16; o > 0; o >>= 1) fro += __shfl_xor_sync(0xffffffffu, fro, o);
-  __shared__ double red[32];
-  if ((tid & 31) == 0) red[tid >> 5] = fro;
   __syncthreads();
+  for (int j = 0; j < q; ++j) {
+    const double gjj = Lm[j + j * ld].x;
+    const double scale = fabs(G[j + j * q].x) + 1e-300;
+    const double rjj = (gjj > 1e-28 * scale) ? sqrt(gjj) : 0.0;
+    __syncthreads();
+    if (tid == 0) {
+      s_piv[j] = rjj;
+      Lm[j + j * ld] = make_double2(rjj, 0.0);
+    }
+    const double inv = rjj > 0.0 ? 1.0 / rjj : 0.0;
+    for (int i = j + 1 + tid; i < q; i += bs) Lm[i + j * ld] = cscale(Lm[i + j * ld], inv);
+    __syncthreads();
+    // trailing update of the lower part: L(i, k) -= L(i, j) conj(L(k, j)), i >= k > j
+    const int m = q - j - 1;
+    for (int it = tid; it < m * m; it += bs) {
+      const int i = j + 1 + it % m, k = j + 1 + it / m;
+      if (i >= k) Lm[i + k * ld] = csub(Lm[i + k * ld], cmul(Lm[i + j * ld], cconj(Lm[k + j * ld])));
+    }
+    __syncthreads();
+  }
+  // X = L^-1: row i from rows < i, all columns j <= i in parallel
+  for (int i = 0; i < q; ++i) {
+    const double lii = s_piv[i];
+    for (int j = tid; j <= i; j += bs) {
+      double2 sacc = (i == j) ? make_double2(1.0, 0.0) : make_double2(0, 0);
+      for (int k = j; k < i; ++k) sacc = csub(sacc, cmul(Lm[i + k * ld], Xm[k + j * ld]));
+      Xm[i + j * ld] = (lii > 0.0) ? cscale(sacc, 1.0 / lii) : make_double2(0, 0);
+    }
+    __syncthreads();
+  }
+  // Rinv = X^H: Rinv(a, b) = conj(X(b, a)), upper triangular
+  for (int it = tid; it < q * q; it += bs) {
+    const int a = it % q, b = it / q;
+    Rinv[it] = (a <= b) ? cconj(Xm[b + a * ld]) : make_double2(0, 0);
+  }
   if (tid == 0) {
-    double s = 0;
-    for (int k = 0; k < bs / 32; ++k) s += red[k];
-    s_tol = DBL_EPSILON * 1e-2 * sqrt(s);
+    int nbad = 0;
+    for (int j = 0; j < q; ++j) nbad += (s_piv[j] == 0.0);
+    *bad = nbad;
   }
-  int converged = 0;
-  for (int sweep = 0; sweep < 60 && !converged; ++sweep) {
-    if (tid == 0) s_rot = 0;
-    __syncthreads();
-    for (int rr = 0; rr < m2 - 1; ++rr) {
-      if (tid < npair) {
-        const int t = tid;
-        int p = (t == 0) ? (m2 - 1) : ((rr + t - 1) % (m2 - 1));
-        int q = (rr + (m2 - 1 - t) - 1) % (m2 - 1);
-        if (p > q) { const int x = p; p = q; q = x; }
-        RRot ro;
-        ro.p = p;
-        ro.q = q;
-        ro.active = 0;
-        if (q < n) {
-          const double aa = Am[p + p * n].x, bb = Am[q + q * n].x;
-          const double2 c = Am[p + q * n];
-          const double ac = hypot(c.x, c.y);
-          const double thr = fmax(0.5 * DBL_EPSILON * sqrt(fabs(aa * bb)), s_tol);
-          if (ac > thr && ac > 0.0) {
-            const double zeta = (bb - aa) / (2.0 * ac);
-            const double tt = (fabs(zeta) > 1e150) ? 0.5 / zeta
-                                                   : (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-            const double cs = 1.0 / sqrt(1.0 + tt * tt);
-            ro.cs = cs;
-            ro.sn = tt * cs;
-            ro.ex = c.x / ac;
-            ro.ey = c.y / ac;
-            ro.ap = aa - tt * ac;
-            ro.aq = bb + tt * ac;
-            ro.active = 1;
-            s_rot = 1;
-          }
-        }
-        rot[t] = ro;
-      }
-      __syncthreads();
-      for (int it = tid; it < npair * n; it += bs) {
-        const RRot& ro = rot[it / n];
-        if (!ro.active) continue;
-        const int col = it % n;
-        const double2 e = make_double2(ro.ex, ro.ey);
-        const double2 rp = Am[ro.p + col * n], rq = Am[ro.q + col * n];
-        Am[ro.p + col * n] = csub(cscale(rp, ro.cs), cscale(cmul(e, rq), ro.sn));
-        Am[ro.q + col * n] = cadd(cscale(cmulc(e, rp), ro.sn), cscale(rq, ro.cs));
-      }
-      __syncthreads();
-      for (int it = tid; it < npair * n; it += bs) {
-        const RRot& ro = rot[it / n];
-        if (!ro.active) continue;
-        const int row = it % n;
-        const double2 e = make_double2(ro.ex, ro.ey);
-        double2 cp = Am[row + ro.p * n], cq = Am[row + ro.q * n];
-        Am[row + ro.p * n] = csub(cscale(cp, ro.cs), cscale(cmulc(e, cq), ro.sn));
-        Am[row + ro.q * n] = cadd(cscale(cmul(e, cp), ro.sn), cscale(cq, ro.cs));
-        cp = V[row + ro.p * n];
-        cq = V[row + ro.q * n];
-        V[row + ro.p * n] = csub(cscale(cp, ro.cs), cscale(cmulc(e, cq), ro.sn));
-        V[row + ro.q * n] = cadd(cscale(cmul(e, cp), ro.sn), cscale(cq, ro.cs));
-      }
-      __syncthreads();
-    }
-    converged = (s_rot == 0);
-    __syncthreads();
-  }
-  if (tid < n) lam[tid] = Am[tid + tid * n].x;
-  __syncthreads();
-  if (tid < n) {
-    const double lj = lam[tid];
-    int rank = 0;
-    for (int i = 0; i < n; ++i) {
-      const double li = lam[i];
-      const bool before = descending ? (li > lj || (li == lj && i < tid)) : (li < lj || (li == lj && i < tid));
-      rank += before ? 1 : 0;
-    }
-    perm[rank] = tid;
-  }
-  __syncthreads();
-  if (tid < n) theta[tid] = lam[perm[tid]];
-  for (int it = tid; it < n * n; it += bs) {
-    const int row = it % n, col = it / n;
-    Yout[it] = V[row + perm[col] * n];
-  }
-  if (tid == 0) *status = converged ? 0 : 1;
 }
 
+// One-CTA Hermitian eigensolver for the Rayleigh-Ritz matrix (n <= kMaxRR, nb wanted pairs):
+//  1. Householder reduction to real tridiagonal form in shared memory (lower reflectors as in
+//     ZHETRD: H = I - tau v v^H, v(1) = 1, beta real), the A22 v product with four threads a row;
+//  2. multisection Sturm bisection: blockDim/nb threads per wanted eigenvalue each evaluate one
+//     point of the current interval, shrinking it (G+1)-fold per round, a fixed number of rounds
+//     down to ~eps |T|;
+//  3. inverse iteration with partial pivoting (3 steps) for the eigenvectors of T, eigenvalues
+//     closer than 1e-7 |T| handled in order by one thread with Gram-Schmidt;
+//  4. back-transform y = H_0 H_1 ... H_{n-2} z, one warp per vector in shared memory.
+constexpr int RR_THREADS = 512;
 
-// One-CTA Hermitian eigensolver for the Rayleigh-Ritz matrix (n <= kMaxRR): Householder
-// reduction to real tridiagonal form in shared memory (ZHETRD-style lower reflectors),
-// Sturm bisection for the nb wanted eigenvalues (lowest, or highest when descending), inverse
-// iteration with partial pivoting for their vectors (clusters re-orthogonalised in sequence
-// by one thread), and the back-transform y = H_0 ... H_{n-2} z, one thread per vector.
-__global__ void __launch_bounds__(256) k_rr_tridiag(const double2* Min, int n, int nb, int descending, double* theta,
-                                                    double2* Yout, int* status) {
+__host__ __device__ constexpr size_t rr_smem_bytes(int n, int nb) {
+  return (size_t)16 * ((size_t)n * n + 3 * n + (size_t)n * nb) + (size_t)8 * (2 * n + 3 * kMaxRR + (size_t)n * nb) +
+         (size_t)4 * RR_THREADS + 64;
+}
+
+__device__ __forceinline__ int sturm_count(const double* dd, const double* ee, int n, double x, double pivmin) {
+  int cnt = 0;
+  double q = dd[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  cnt += (q < 0);
+  for (int i = 1; i < n; ++i) {
+    q = (dd[i] - x) - ee[i - 1] * ee[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    cnt += (q < 0);
+  }
+  return cnt;
+}
+
+__global__ void __launch_bounds__(RR_THREADS) k_rr_tridiag(const double2* Min, int n, int nb, int descending,
+                                                           double* theta, double2* Yout, int* status) {
   extern __shared__ __align__(16) unsigned char smem[];
-  double2* A = reinterpret_cast<double2*>(smem);          // n x n, column-major
-  double2* vv = A + n * n;                                  // reflector scratch (n)
-  double2* pp = vv + n;                                     // n
-  double2* taus = pp + n;                                   // n
-  double* dd = reinterpret_cast<double*>(taus + n);         // n
-  double* ee = dd + n;                                      // n
-  double* lam = ee + n;                                     // nb
-  double* Z = lam + kMaxRR;                                 // n x nb (column-major)
-  __shared__ double red[8];
-  __shared__ double2 redc[8];
+  double2* A = reinterpret_cast<double2*>(smem);   // n x n, column-major; reflectors kept below the diagonal
+  double2* vv = A + n * n;
+  double2* pp = vv + n;
+  double2* taus = pp + n;
+  double2* Ys = taus + n;                           // n x nb back-transformed vectors
+  double* dd = reinterpret_cast<double*>(Ys + n * nb);
+  double* ee = dd + n;
+  double* lam = ee + n;                             // kMaxRR
+  double* blo = lam + kMaxRR;                       // kMaxRR
+  double* bhi = blo + kMaxRR;                       // kMaxRR
+  double* Z = bhi + kMaxRR;                         // n x nb eigenvectors of T
+  int* cnt = reinterpret_cast<int*>(Z + n * nb);    // RR_THREADS
+  __shared__ double red[RR_THREADS / 32];
+  __shared__ double2 redc[RR_THREADS / 32];
   __shared__ double2 s_tau, s_scal, s_a2;
   __shared__ int s_triv;
-  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5, bs = blockDim.x;
+  __shared__ double s_lo, s_hi, s_tn;
+  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  constexpr int bs = RR_THREADS, NW = RR_THREADS / 32;
   for (int it = tid; it < n * n; it += bs) {
     const int a = it % n, b = it / n;
     double2 v = Min[it];
@@ -530,9 +453,9 @@ __global__ void __launch_bounds__(256) k_rr_tridiag(const double2* Min, int n, i
     A[it] = v;
   }
   __syncthreads();
+  // ---- 1. tridiagonal reduction
   for (int j = 0; j < n - 1; ++j) {
-    const int m = n - j - 1;   // length of x = A[j+1:, j]
-    // |x(2:)|^2
+    const int m = n - j - 1;
     double s = 0.0;
     for (int i = 1 + tid; i < m; i += bs) {
       const double2 x = A[(j + 1 + i) + j * n];
@@ -543,7 +466,7 @@ __global__ void __launch_bounds__(256) k_rr_tridiag(const double2* Min, int n, i
     __syncthreads();
     if (tid == 0) {
       double xn2 = 0;
-      for (int k = 0; k < bs / 32; ++k) xn2 += red[k];
+      for (int k = 0; k < NW; ++k) xn2 += red[k];
       const double2 al = A[(j + 1) + j * n];
       if (xn2 == 0.0 && al.y == 0.0) {
         s_triv = 1;
@@ -565,20 +488,27 @@ __global__ void __launch_bounds__(256) k_rr_tridiag(const double2* Min, int n, i
     const int triv = s_triv;
     const double2 tau = s_tau;
     for (int i = tid; i < m; i += bs) {
-      double2 v = (i == 0) ? make_double2(1, 0) : (triv ? make_double2(0, 0) : cmul(A[(j + 1 + i) + j * n], s_scal));
+      const double2 v = (i == 0) ? make_double2(1, 0) : (triv ? make_double2(0, 0) : cmul(A[(j + 1 + i) + j * n], s_scal));
       vv[i] = v;
-      A[(j + 1 + i) + j * n] = v;   // keep v for the back-transform
+      A[(j + 1 + i) + j * n] = v;
     }
     __syncthreads();
     if (triv) continue;
-    // p = tau * A22 v
-    for (int i = tid; i < m; i += bs) {
-      double2 acc = make_double2(0, 0);
-      for (int k = 0; k < m; ++k) acc = cadd(acc, cmul(A[(j + 1 + i) + (j + 1 + k) * n], vv[k]));
-      pp[i] = cmul(tau, acc);
+    // p = tau A22 v: four threads per row
+    {
+      const int part = tid & 3;
+      const unsigned gmask = 0xFu << (lane & ~3);
+      for (int i = tid >> 2; i < m; i += bs / 4) {
+        double2 acc = make_double2(0, 0);
+        for (int k = part; k < m; k += 4) acc = cadd(acc, cmul(A[(j + 1 + i) + (j + 1 + k) * n], vv[k]));
+        acc.x += __shfl_xor_sync(gmask, acc.x, 1);
+        acc.y += __shfl_xor_sync(gmask, acc.y, 1);
+        acc.x += __shfl_xor_sync(gmask, acc.x, 2);
+        acc.y += __shfl_xor_sync(gmask, acc.y, 2);
+        if (part == 0) pp[i] = cmul(tau, acc);
+      }
     }
     __syncthreads();
-    // alpha2 = -tau/2 (p^H v)
     double2 t = make_double2(0, 0);
     for (int i = tid; i < m; i += bs) t = cadd(t, cmulc(pp[i], vv[i]));
     for (int o = 16; o > 0; o >>= 1) {
@@ -589,14 +519,13 @@ __global__ void __launch_bounds__(256) k_rr_tridiag(const double2* Min, int n, i
     __syncthreads();
     if (tid == 0) {
       double2 sum = make_double2(0, 0);
-      for (int k = 0; k < bs / 32; ++k) sum = cadd(sum, redc[k]);
+      for (int k = 0; k < NW; ++k) sum = cadd(sum, redc[k]);
       s_a2 = cscale(cmul(tau, sum), -0.5);
     }
     __syncthreads();
     const double2 a2 = s_a2;
     for (int i = tid; i < m; i += bs) pp[i] = cadd(pp[i], cmul(a2, vv[i]));   // w
     __syncthreads();
-    // A22 -= v w^H + w v^H
     for (int it = tid; it < m * m; it += bs) {
       const int r = it % m, c = it / m;
       double2 x = A[(j + 1 + r) + (j + 1 + c) * n];
@@ -605,16 +534,14 @@ __global__ void __launch_bounds__(256) k_rr_tridiag(const double2* Min, int n, i
     }
     __syncthreads();
   }
-  if (tid == 0) dd[n - 1] = A[(n - 1) + (n - 1) * n].x;
-  __syncthreads();
-  // bisection for the wanted eigenvalues
-  __shared__ double s_lo, s_hi, s_tn;
   if (tid == 0) {
-    double lo = dd[0], hi = dd[0];
+    dd[n - 1] = A[(n - 1) + (n - 1) * n].x;
+    double lo = 0.0, hi = 0.0;
     for (int i = 0; i < n; ++i) {
+      const double dv = (i == n - 1) ? A[(n - 1) + (n - 1) * n].x : dd[i];
       const double r = (i > 0 ? fabs(ee[i - 1]) : 0.0) + (i < n - 1 ? fabs(ee[i]) : 0.0);
-      lo = fmin(lo, dd[i] - r);
-      hi = fmax(hi, dd[i] + r);
+      lo = (i == 0) ? dv - r : fmin(lo, dv - r);
+      hi = (i == 0) ? dv + r : fmax(hi, dv + r);
     }
     s_tn = fmax(fabs(lo), fabs(hi));
     const double pad = 4.0 * DBL_EPSILON * s_tn + 1e-300;
@@ -622,29 +549,51 @@ __global__ void __launch_bounds__(256) k_rr_tridiag(const double2* Min, int n, i
     s_hi = hi + pad;
   }
   __syncthreads();
+  // ---- 2. multisection bisection
   const double pivmin = DBL_MIN * 4.0;
-  if (tid < nb) {
-    const int mi = descending ? (n - 1 - tid) : tid;
-    double a = s_lo, b = s_hi;
-    for (int it = 0; it < 200; ++it) {
-      const double mid = 0.5 * (a + b);
-      if (!(mid > a && mid < b)) break;
-      int cnt = 0;
-      double q = dd[0] - mid;
-      if (fabs(q) < pivmin) q = -pivmin;
-      cnt += (q < 0);
-      for (int i = 1; i < n; ++i) {
-        q = (dd[i] - mid) - ee[i - 1] * ee[i - 1] / q;
-        if (fabs(q) < pivmin) q = -pivmin;
-        cnt += (q < 0);
-      }
-      if (cnt <= mi) a = mid;
-      else b = mid;
+  const int G = max(1, bs / nb);
+  int rounds = 1;
+  {
+    double shrink = 1.0;
+    while (shrink > 0x1p-53 && rounds < 64) {
+      shrink /= (double)(G + 1);
+      ++rounds;
     }
-    lam[tid] = 0.5 * (a + b);
+  }
+  for (int e = tid; e < nb; e += bs) {
+    blo[e] = s_lo;
+    bhi[e] = s_hi;
   }
   __syncthreads();
-  // inverse iteration; clusters (gap <= 1e-7 |T|) handled in order by their first thread
+  for (int rd = 0; rd < rounds; ++rd) {
+    const int e = tid / G, g = tid % G;
+    if (e < nb) {
+      const double lo = blo[e], hi = bhi[e];
+      const double x = lo + (hi - lo) * (double)(g + 1) / (double)(G + 1);
+      cnt[tid] = sturm_count(dd, ee, n, x, pivmin);
+    }
+    __syncthreads();
+    if (e < nb && g == 0) {
+      const int mi = descending ? (n - 1 - e) : e;
+      const double lo = blo[e], hi = bhi[e];
+      double nlo = lo, nhi = hi;
+      for (int gg = 0; gg < G; ++gg) {
+        const double x = lo + (hi - lo) * (double)(gg + 1) / (double)(G + 1);
+        if (cnt[e * G + gg] <= mi) {
+          nlo = x;
+        } else {
+          nhi = x;
+          break;
+        }
+      }
+      blo[e] = nlo;
+      bhi[e] = nhi;
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < nb; e += bs) lam[e] = 0.5 * (blo[e] + bhi[e]);
+  __syncthreads();
+  // ---- 3. inverse iteration
   if (tid < nb) {
     const double ctol = 1e-7 * fmax(1e-3, s_tn);
     const bool leader = (tid == 0) || fabs(lam[tid] - lam[tid - 1]) > ctol;
@@ -655,25 +604,30 @@ __global__ void __launch_bounds__(256) k_rr_tridiag(const double2* Min, int n, i
       double u1[kMaxRR], u2[kMaxRR], u3[kMaxRR];
       for (int sidx = 0; sidx < cs; ++sidx) {
         const int col = tid + sidx;
-        double* x = Z + (long long)col * n;
+        double* x = Z + col * n;
         const double lm = lam[col];
         for (int k = 0; k < n; ++k) x[k] = 1.0 + 0.1 * (double)((k * 7 + col * 13) % 17) / 17.0;
-        double sc = 1.0;
         for (int itr = 0; itr < 3; ++itr) {
-          double diag = dd[0] - lm, sup = (n > 1) ? ee[0] : 0.0, cur = x[0] * sc;
+          double diag = dd[0] - lm, sup = (n > 1) ? ee[0] : 0.0, cur = x[0];
           for (int k = 0; k < n - 1; ++k) {
             const double sub = ee[k], nd = dd[k + 1] - lm, nsup = (k + 1 < n - 1) ? ee[k + 1] : 0.0;
-            const double nxt = x[k + 1] * sc;
+            const double nxt = x[k + 1];
             if (fabs(diag) >= fabs(sub)) {
               if (fabs(diag) < pert) diag = copysign(pert, diag);
               const double mult = sub / diag;
-              u1[k] = diag; u2[k] = sup; u3[k] = 0.0; x[k] = cur;
+              u1[k] = diag;
+              u2[k] = sup;
+              u3[k] = 0.0;
+              x[k] = cur;
               cur = nxt - mult * cur;
               diag = nd - mult * sup;
               sup = nsup;
             } else {
               const double mult = diag / sub;
-              u1[k] = sub; u2[k] = nd; u3[k] = nsup; x[k] = nxt;
+              u1[k] = sub;
+              u2[k] = nd;
+              u3[k] = nsup;
+              x[k] = nxt;
               cur = cur - mult * nxt;
               diag = sup - mult * nd;
               sup = -mult * nsup;
@@ -689,40 +643,46 @@ __global__ void __launch_bounds__(256) k_rr_tridiag(const double2* Min, int n, i
             x2 = x1;
             x1 = xk;
           }
-          sc = 1.0 / sqrt(nrm);
+          double sc = 1.0 / sqrt(nrm);
           for (int k = 0; k < n; ++k) x[k] *= sc;
-          sc = 1.0;
-          for (int t2 = 0; t2 < sidx; ++t2) {
-            const double* y = Z + (long long)(tid + t2) * n;
-            double dot = 0.0;
-            for (int k = 0; k < n; ++k) dot += x[k] * y[k];
-            for (int k = 0; k < n; ++k) x[k] -= dot * y[k];
-          }
           if (sidx > 0) {
+            for (int t2 = 0; t2 < sidx; ++t2) {
+              const double* y = Z + (tid + t2) * n;
+              double dot = 0.0;
+              for (int k = 0; k < n; ++k) dot += x[k] * y[k];
+              for (int k = 0; k < n; ++k) x[k] -= dot * y[k];
+            }
             double n2 = 0.0;
             for (int k = 0; k < n; ++k) n2 += x[k] * x[k];
-            const double s2 = 1.0 / sqrt(n2);
-            for (int k = 0; k < n; ++k) x[k] *= s2;
+            sc = 1.0 / sqrt(n2);
+            for (int k = 0; k < n; ++k) x[k] *= sc;
           }
         }
       }
     }
   }
   __syncthreads();
-  // back-transform: y = H_0 (H_1 (... H_{n-2} z)), v_j stored in A[j+1:, j]
-  if (tid < nb) {
-    double2* y = Yout + (long long)tid * n;
-    for (int k = 0; k < n; ++k) y[k] = make_double2(Z[(long long)tid * n + k], 0.0);
+  // ---- 4. back-transform, one warp per vector
+  for (int c = wp; c < nb; c += NW) {
+    double2* y = Ys + c * n;
+    for (int k = lane; k < n; k += 32) y[k] = make_double2(Z[c * n + k], 0.0);
+    __syncwarp();
     for (int j = n - 2; j >= 0; --j) {
       const double2 tau = taus[j];
       if (tau.x == 0.0 && tau.y == 0.0) continue;
       double2 dot = make_double2(0, 0);
-      for (int k = j + 1; k < n; ++k) dot = cadd(dot, cmulc(A[k + j * n], y[k]));
+      for (int k = j + 1 + lane; k < n; k += 32) dot = cadd(dot, cmulc(A[k + j * n], y[k]));
+      for (int o = 16; o > 0; o >>= 1) {
+        dot.x += __shfl_xor_sync(0xffffffffu, dot.x, o);
+        dot.y += __shfl_xor_sync(0xffffffffu, dot.y, o);
+      }
       const double2 f = cmul(tau, dot);
-      for (int k = j + 1; k < n; ++k) y[k] = csub(y[k], cmul(A[k + j * n], f));
+      for (int k = j + 1 + lane; k < n; k += 32) y[k] = csub(y[k], cmul(A[k + j * n], f));
+      __syncwarp();
     }
-    theta[tid] = lam[tid];
+    for (int k = lane; k < n; k += 32) Yout[(long long)c * n + k] = y[k];
   }
+  if (tid < nb) theta[tid] = lam[tid];
   if (tid == 0) *status = 0;
 }
 
@@ -815,6 +775,7 @@ struct DavWork {
 };
 
 static int hemm(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y, int ldy, double2* Yp) {
+  if (ctx->fast_mode) return run_fastprod(ctx, X, ldx, m, Y, ldy);
   const long long N = ctx->N;
   const int nblk = (int)((N + TB - 1) / TB);
   dim3 grid(nblk, JCH);
@@ -840,10 +801,10 @@ static int hemm(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y, int
 static int gram(wtbg_ctx* ctx, const double2* A, int lda, int p, const double2* B, int ldb, int q, double2* C,
                 double2* part) {
   const long long N = ctx->N;
-  if (p > kMaxRR || q > kMaxRR || p * q > 256 * GMAXO) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "davidson: gram too large");
-  const int nparts = (int)std::min<long long>(148, (N + 63) / 64);
+  if (p > 16 * GT || q > 16 * GT) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "davidson: gram too large");
+  const int nparts = (int)std::min<long long>(296, (N + 63) / 64);
   k_gram<<<nparts, 256, 0, ctx->stream>>>(A, lda, p, B, ldb, q, N, part); WTBG_COUNT(ctx, 1);
-  k_gram_sum<<<(p * q + 255) / 256, 256, 0, ctx->stream>>>(part, nparts, p * q, C); WTBG_COUNT(ctx, 1);
+  k_gram_sum<<<(p * q + 31) / 32, 256, 0, ctx->stream>>>(part, nparts, p * q, C); WTBG_COUNT(ctx, 1);
   CKL("gram");
   return 0;
 }
@@ -851,15 +812,12 @@ static int gram(wtbg_ctx* ctx, const double2* A, int lda, int p, const double2* 
 static int tall(wtbg_ctx* ctx, const double2* A, int lda, int p, const double2* B, int q, double2* Cm, int ldc,
                 bool sub) {
   const long long N = ctx->N;
-  const size_t sh = (size_t)p * q * 16;
-  if (sh > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "davidson: small matrix too large");
-  if (sub) {
-    CK(cudaFuncSetAttribute(k_tall_gemm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-    k_tall_gemm<true><<<(int)((N + 127) / 128), 128, sh, ctx->stream>>>(A, lda, p, B, q, N, Cm, ldc);
-  } else {
-    CK(cudaFuncSetAttribute(k_tall_gemm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh));
-    k_tall_gemm<false><<<(int)((N + 127) / 128), 128, sh, ctx->stream>>>(A, lda, p, B, q, N, Cm, ldc);
-  }
+  if (p > kMaxRR) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "davidson: small matrix too large");
+  const dim3 grid((unsigned)((N + 255) / 256), (unsigned)((q + 7) / 8));
+  if (sub)
+    k_tall_gemm<true><<<grid, 256, 0, ctx->stream>>>(A, lda, p, B, q, N, Cm, ldc);
+  else
+    k_tall_gemm<false><<<grid, 256, 0, ctx->stream>>>(A, lda, p, B, q, N, Cm, ldc);
   WTBG_COUNT(ctx, 1);
   CKL("tall");
   return 0;
@@ -872,7 +830,7 @@ static int cholqr2(wtbg_ctx* ctx, double2* T, int q, double2* tmp, DavWork& w) {
     if (int r = gram(ctx, T, (int)N, q, T, (int)N, q, w.small, w.part)) return r;
     const size_t csm = (size_t)2 * q * (q + 1) * 16;
     CK(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
-    k_chol_inv<<<1, 128, csm, ctx->stream>>>(w.small, q, w.small + 64 * 64, w.istat); WTBG_COUNT(ctx, 1);
+    k_chol_inv<<<1, 512, csm, ctx->stream>>>(w.small, q, w.small + 64 * 64, w.istat); WTBG_COUNT(ctx, 1);
     CKL("chol");
     if (int r = tall(ctx, T, (int)N, q, w.small + 64 * 64, q, tmp, (int)N, false)) return r;
     CK(cudaMemcpyAsync(T, tmp, (size_t)N * q * 16, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -896,14 +854,14 @@ int run_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, doub
   w.Xn = w.HV + (size_t)N * n2;
   w.HXn = w.Xn + (size_t)N * nb;
   w.Yp = w.HXn + (size_t)N * nb;
-  ENSURE(ctx->tmp, (size_t)N * 8 + (size_t)kMaxRR * kMaxRR * 16 * 3 + 4096 * 16 + 300 * 64 * 64 * 16 + (size_t)N * 4 * 2 + 65536);
+  ENSURE(ctx->tmp, (size_t)N * 8 + (size_t)kMaxRR * kMaxRR * 16 * 3 + 4096 * 16 + 300 * kMaxRR * kMaxRR * 16 + (size_t)N * 4 * 2 + 65536);
   char* tb = ctx->tmp.as<char>();
   w.D = reinterpret_cast<double*>(tb);
   w.small = reinterpret_cast<double2*>(tb + (size_t)N * 8);                     // M, Y, ...
   w.theta = reinterpret_cast<double*>(w.small + 3 * kMaxRR * kMaxRR);
   w.rpart = w.theta + kMaxRR;
   w.part = reinterpret_cast<double2*>(w.rpart + 4096);
-  w.istat = reinterpret_cast<int*>(w.part + 300 * 64 * 64);
+  w.istat = reinterpret_cast<int*>(w.part + 300 * kMaxRR * kMaxRR);
   int* d_idx = w.istat + 16;
   cudaStream_t s = ctx->stream;
   const int th = 256;
@@ -934,17 +892,14 @@ int run_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, doub
   if (int r = cholqr2(ctx, X, nb, w.Xn, w)) return r;
   if (int r = hemm(ctx, X, (int)N, nb, HX, (int)N, w.Yp)) return r;
   // first Rayleigh-Ritz on X alone
-  const size_t rrsm = (size_t)2 * kMaxRR * kMaxRR * 16 + (size_t)(kMaxRR / 2 + 1) * sizeof(RRot) + (kMaxRR + 2) * 8 +
-                      (kMaxRR + 2) * 4 + 64;
-  CK(cudaFuncSetAttribute(k_rr_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rrsm));
+  const size_t rrsm = rr_smem_bytes(kMaxRR, kMaxRR / 2);
   CK(cudaFuncSetAttribute(k_rr_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rrsm));
   double2* Mm = w.small;
   double2* Y = w.small + kMaxRR * kMaxRR;
   auto rr = [&](const double2* Vb, const double2* HVb, int n) -> int {
     if (int r = gram(ctx, Vb, (int)N, n, HVb, (int)N, n, Mm, w.part)) return r;
-    const size_t sm = (size_t)n * n * 16 + (size_t)3 * n * 16 + (size_t)2 * n * 8 + (size_t)kMaxRR * 8 +
-                      (size_t)n * nb * 8 + 64;
-    k_rr_tridiag<<<1, 256, sm, s>>>(Mm, n, nb, largest, w.theta, Y, w.istat + 1); WTBG_COUNT(ctx, 1);
+    const size_t sm = rr_smem_bytes(n, nb);
+    k_rr_tridiag<<<1, RR_THREADS, sm, s>>>(Mm, n, nb, largest, w.theta, Y, w.istat + 1); WTBG_COUNT(ctx, 1);
     CKL("k_rr_tridiag");
     // X = V Y(:, :nb), HX = HV Y(:, :nb)
     if (int r = tall(ctx, Vb, (int)N, n, Y, nb, w.Xn, (int)N, false)) return r;
@@ -960,6 +915,17 @@ int run_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, doub
   double* rp = ctx->tmp2.as<double>();
   int it = 0;
   double worst = 0.0;
+  // With the tensor-core product the residual stalls at its rounding level (FP32 accumulation,
+  // ~1e-5 of |H x|): iterate with it down to kFastSwitch (or until it stops improving), then
+  // refresh H X with the FP64 product and finish in FP64.
+  struct FastGuard {
+    wtbg_ctx* c;
+    int saved;
+    ~FastGuard() { c->fast_mode = saved; }
+  } guard{ctx, ctx->fast_mode};
+  constexpr double kFastSwitch = 3e-5;
+  double best = 1e300;
+  int since_best = 0;
   for (; it < max_iter; ++it) {
     k_resid_precond<<<nrb, th, 0, s>>>(X, HX, (int)N, nb, w.theta, w.D, N, T, (int)N, rp); WTBG_COUNT(ctx, 1);
     CKL("k_resid_precond");
@@ -975,6 +941,20 @@ int run_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, doub
       if (v < nev) worst = std::max(worst, res[v]);
     }
     if (worst < tol) break;
+    if (ctx->fast_mode) {
+      if (worst < 0.7 * best) {
+        best = worst;
+        since_best = 0;
+      } else {
+        ++since_best;
+      }
+      if (worst < std::max(kFastSwitch, tol) || since_best >= 8) {
+        ctx->fast_mode = 0;
+        if (int r = hemm(ctx, X, (int)N, nb, HX, (int)N, w.Yp)) return r;
+        if (int r = rr(X, HX, nb)) return r;
+        continue;
+      }
+    }
     // T <- T - X (X^H T), twice; orthonormalise
     for (int pass = 0; pass < 2; ++pass) {
       if (int r = gram(ctx, X, (int)N, nb, T, (int)N, nb, w.small + 2 * kMaxRR * kMaxRR, w.part)) return r;
@@ -1008,6 +988,7 @@ int run_hemm_public(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y,
 
 // Y = H X for a narrow block (m = 8 or 16), reading the lower triangle once
 int run_hemm_narrow(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y, int ldy) {
+  if (ctx->fast_mode) return run_fastprod(ctx, X, ldx, m, Y, ldy);
   const long long N = ctx->N;
   const int nblk = (int)((N + TB - 1) / TB);
   ENSURE(ctx->slots, (size_t)nblk * nblk * TB * m * 16);

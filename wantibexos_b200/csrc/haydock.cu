@@ -203,7 +203,7 @@ __global__ void k_haydock_eps(const double* om, const double* gre, const double*
 
 }  // namespace
 
-int run_hemm_narrow(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y, int ldy);
+
 
 // K Lanczos steps for every chain; alpha/beta (K x ncomp, chain-major) and |u|^2 to the host
 int run_haydock(wtbg_ctx* ctx, int K, int ncomp, const int* codes, std::vector<double>& alpha, std::vector<double>& beta,

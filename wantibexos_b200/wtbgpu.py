@@ -24,7 +24,10 @@ EXPORTS = ["wtbg_create", "wtbg_destroy", "wtbg_error_string", "wtbg_last_error"
            "wtbg_sp_table", "wtbg_bse_build", "wtbg_bse_get_matrix", "wtbg_bse_solve",
            "wtbg_bse_eigvecs", "wtbg_spectrum", "wtbg_bse_q_eigenvalues", "wtbg_set_profiling",
            "wtbg_get_stats", "wtbg_reset_stats", "wtbg_spectrum_noalloc", "wtbg_bse_davidson",
-           "wtbg_bse_spectrum_fast"]
+           "wtbg_bse_spectrum_fast", "wtbg_set_fast_product", "wtbg_bse_apply", "wtbg_net_create",
+           "wtbg_net_destroy", "wtbg_net_num_params", "wtbg_net_get_params", "wtbg_net_set_params",
+           "wtbg_net_features", "wtbg_net_add_sample", "wtbg_net_num_samples", "wtbg_net_train",
+           "wtbg_net_eval_loss", "wtbg_net_predict", "wtbg_net_loss_grad", "wtbg_gemm_bf16"]
 
 
 class WtbgError(RuntimeError):
@@ -85,6 +88,21 @@ def load_library(path: str = LIB_PATH):
         "wtbg_bse_spectrum_fast": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, ip, C.c_double,
                                              C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
                                              dp, fp]),
+        "wtbg_set_fast_product": (C.c_int, [P, C.c_int]),
+        "wtbg_net_create": (C.c_int, [P, C.POINTER(P), C.c_ulonglong]),
+        "wtbg_net_destroy": (C.c_int, [P]),
+        "wtbg_net_num_params": (C.c_longlong, []),
+        "wtbg_net_get_params": (C.c_int, [P, fp]),
+        "wtbg_net_set_params": (C.c_int, [P, fp]),
+        "wtbg_net_features": (C.c_int, [P, dp, fp, fp]),
+        "wtbg_net_add_sample": (C.c_int, [P, dp, dp]),
+        "wtbg_net_num_samples": (C.c_int, [P]),
+        "wtbg_net_train": (C.c_int, [P, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int, fp]),
+        "wtbg_net_eval_loss": (C.c_int, [P, C.c_int, C.c_int, fp]),
+        "wtbg_net_predict": (C.c_int, [P, dp, dp]),
+        "wtbg_net_loss_grad": (C.c_int, [P, C.c_int, C.c_longlong, fp, fp, fp, fp, fp]),
+        "wtbg_bse_apply": (C.c_int, [P, C.c_int, dp, dp]),
+        "wtbg_gemm_bf16": (C.c_int, [P, C.c_int, C.c_int, C.c_int, fp, fp, fp]),
         "wtbg_spectrum_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, ip, ip, C.c_double,
                                             C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                                             C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p,
@@ -263,6 +281,28 @@ class Context:
                                                     _dp(om), _fp(eps)))
         return om, eps
 
+    def set_fast_product(self, mode: int) -> None:
+        """0: FP64 product; 1: split-BF16 tensor-core product (Davidson, Haydock, bse_apply)."""
+        self._check(self.lib.wtbg_set_fast_product(self.h, int(mode)))
+
+    def bse_apply(self, X):
+        """Y = H X with the selected product; X (N, m) complex."""
+        X = np.asfortranarray(np.asarray(X, dtype=np.complex128).reshape(self.N, -1))
+        Y = np.zeros_like(X, order="F")
+        self._check(self.lib.wtbg_bse_apply(self.h, X.shape[1], X.ctypes.data_as(C.POINTER(C.c_double)),
+                                            Y.ctypes.data_as(C.POINTER(C.c_double))))
+        return Y
+
+    def gemm_bf16(self, A, B):
+        """C = A B^T on the tensor cores (bf16 inputs, FP32 accumulation)."""
+        A = np.ascontiguousarray(A, dtype=np.float32)
+        B = np.ascontiguousarray(B, dtype=np.float32)
+        M, K = A.shape
+        N = B.shape[0]
+        Cm = np.zeros((M, N), dtype=np.float32)
+        self._check(self.lib.wtbg_gemm_bf16(self.h, M, N, K, _fp(A), _fp(B), _fp(Cm)))
+        return Cm
+
     def bse_eigvecs(self, n0: int, n1: int):
         A = np.zeros((self.N, n1 - n0 + 1), dtype=np.complex128, order="F")
         self._check(self.lib.wtbg_bse_eigvecs(self.h, n0, n1, A.ctypes.data_as(C.POINTER(C.c_double))))
@@ -292,3 +332,90 @@ class Context:
         W = np.zeros(self.N)
         self._check(self.lib.wtbg_bse_q_eigenvalues(self.h, kq.shape[0], _dp(kq), _dp(q), C.byref(coul), _dp(W)))
         return W
+
+
+class Net:
+    """Learned warm start (wtbg_net_*), bound to a Context's device and stream."""
+
+    NS = 32
+    NF = 32
+    NCAR = 5
+
+    def __init__(self, ctx: Context, seed: int = 0):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.h = C.c_void_p()
+        ctx._check(self.lib.wtbg_net_create(ctx.h, C.byref(self.h), C.c_ulonglong(seed)))
+        self.nparam = int(self.lib.wtbg_net_num_params())
+
+    def close(self):
+        if self.h:
+            self.lib.wtbg_net_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def glob(q, r0, eps):
+        return np.array([q[0], q[1], q[2], r0, eps], dtype=np.float64)
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.nparam, dtype=np.float32)
+        self.ctx._check(self.lib.wtbg_net_get_params(self.h, _fp(p)))
+        return p
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(np.asarray(p, dtype=np.float32))
+        assert p.size == self.nparam
+        self.ctx._check(self.lib.wtbg_net_set_params(self.h, _fp(p)))
+
+    def features(self, glob):
+        N = self.ctx.N
+        F = np.zeros((N, self.NF), dtype=np.float32)
+        CAR = np.zeros((self.NCAR, N), dtype=np.complex64)
+        self.ctx._check(self.lib.wtbg_net_features(self.h, _dp(np.asarray(glob, dtype=np.float64)), _fp(F),
+                                                   CAR.ctypes.data_as(C.POINTER(C.c_float))))
+        return F, CAR
+
+    def add_sample(self, glob, A) -> None:
+        A = np.asfortranarray(np.asarray(A, dtype=np.complex128)[:, :self.NS])
+        assert A.shape == (self.ctx.N, self.NS)
+        self.ctx._check(self.lib.wtbg_net_add_sample(self.h, _dp(np.asarray(glob, dtype=np.float64)),
+                                                     A.ctypes.data_as(C.POINTER(C.c_double))))
+
+    @property
+    def num_samples(self) -> int:
+        return int(self.lib.wtbg_net_num_samples(self.h))
+
+    def train(self, epochs: int, batch: int = 8, lr: float = 1e-3, first: int = 0, count: int = 0):
+        hist = np.zeros(epochs, dtype=np.float32)
+        self.ctx._check(self.lib.wtbg_net_train(self.h, epochs, batch, float(lr), first, count, _fp(hist)))
+        return hist
+
+    def eval_loss(self, first: int, count: int) -> float:
+        v = np.zeros(1, dtype=np.float32)
+        self.ctx._check(self.lib.wtbg_net_eval_loss(self.h, first, count, _fp(v)))
+        return float(v[0])
+
+    def predict(self, glob):
+        X = np.zeros((self.ctx.N, self.NS), dtype=np.complex128, order="F")
+        self.ctx._check(self.lib.wtbg_net_predict(self.h, _dp(np.asarray(glob, dtype=np.float64)),
+                                                  X.ctypes.data_as(C.POINTER(C.c_double))))
+        return X
+
+    def loss_grad(self, F, CAR, A, nsamp: int):
+        """F (M, 32) float32, CAR (5, M) complex64, A (32, M) complex64 with M = nsamp * rows."""
+        F = np.ascontiguousarray(F, dtype=np.float32)
+        CAR = np.ascontiguousarray(CAR, dtype=np.complex64)
+        A = np.ascontiguousarray(A, dtype=np.complex64)
+        M = F.shape[0]
+        loss = np.zeros(1, dtype=np.float32)
+        g = np.zeros(self.nparam, dtype=np.float32)
+        self.ctx._check(self.lib.wtbg_net_loss_grad(self.h, nsamp, M // nsamp, _fp(F),
+                                                    CAR.ctypes.data_as(C.POINTER(C.c_float)),
+                                                    A.ctypes.data_as(C.POINTER(C.c_float)), _fp(loss), _fp(g)))
+        return float(loss[0]), g
