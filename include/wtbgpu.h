@@ -72,6 +72,11 @@ typedef struct wtbg_stats {
   long long build_launches;
   double build_ms;
   double build_bytes;
+  long long fast_launches;   /* tensor-core products (k_fastprod), timed when profiling */
+  double fast_ms;
+  double fast_bytes;         /* algorithmic: 8 N^2 (bf16 hi/lo planes of Re H, Im H) per product */
+  long long dav_fast_iters;  /* Davidson iterations on the tensor-core product (last call) */
+  long long dav_fp64_iters;  /* Davidson iterations on the FP64 product (last call) */
 } wtbg_stats;
 int wtbg_set_profiling(wtbg_ctx* ctx, int on);
 int wtbg_get_stats(const wtbg_ctx* ctx, wtbg_stats* out);
@@ -160,9 +165,10 @@ int wtbg_bse_apply(wtbg_ctx* ctx, int m, const double* X, double* Y);
  *      state; the 32-vector block is X[i,s] = sum_c coef * carrier_c[i] with carriers
  *      1, hx/|h|, hy/|h|, conj(hx)/|h|, conj(hy)/|h|.  Samples are the current basis of ctx
  *      (after wtbg_bands, wtbg_velocity and a build) plus the 32 lowest eigenvectors of the
- *      plain dense FP64 solve (A: N x 32 complex(8), column-major).  Training minimises
- *      ||X - A A^H X||^2 + 0.25 ||X^H X - I||^2 per sample with Adam (hand-written forward,
- *      backward and update kernels).  The network is bound to ctx (device, stream). */
+ *      plain dense FP64 solve (A: N x 32 complex(8), column-major).  Training minimises the
+ *      distance to the nearest orthonormal basis of span(A), min_R ||X - A R||^2 over unitary
+ *      R (the polar factor of A^H X), per sample with Adam (hand-written forward, backward
+ *      and update kernels).  The network is bound to ctx (device, stream). */
 typedef struct wtbg_net wtbg_net;
 int wtbg_net_create(wtbg_ctx* ctx, wtbg_net** net, unsigned long long seed);
 int wtbg_net_destroy(wtbg_net* net);
@@ -234,6 +240,11 @@ int wtbg_spectrum_noalloc(int n, int ncomp, const double* d_ebse, const double* 
                           const int* rtype, const int* ngrid, double vcell3d, double ebse0,
                           double ebsef, double numbse, double sme, int renorm, double spinf,
                           double* d_omega, float* d_eps, void* stream, char* errbuf, int errlen);
+
+/* ---- build the BSE matrix of one centre-of-mass momentum and keep it on the device
+ *      (matrizelbsekq of bse_kpath-tool.f90:246-435 without the solve), for the fast form
+ *      and the learned warm start at Q != 0.  Arguments as wtbg_bse_q_eigenvalues. */
+int wtbg_bse_build_q(wtbg_ctx* ctx, int nk, const double* kptq, const double* q4, const wtbg_coulomb* p);
 
 /* ---- exciton band structure: one centre-of-mass Q of bsebnds
  *      (bse_kpath-tool.f90:246-435; matrizelbsekq = bse_subs_kpath.f90:1-208).

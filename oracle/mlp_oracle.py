@@ -7,7 +7,8 @@ and loss that the GPU kernels of ``wtbg_net_*`` implement, so their gradients ca
                       -> Z2 = H1 W2^T + b2 -> H2 = silu(Z2)     (W2: 512 x 512)
                       -> O  = H2 W3^T + b3                       (W3: 320 x 512)
   X[i, s] = sum_c (O[i, 2(5s+c)] + 1j O[i, 2(5s+c)+1]) * CAR[c, i]         (32 states, 5 carriers)
-  per sample: L = ||X - A A^H X||^2 + mu ||X^H X - I||^2, mu = 0.25, averaged over 32 * nsamp.
+  per sample: L = min over unitary R of ||X - A R||_F^2 = tr(X^H X) - 2 ||A^H X||_* + 32
+  (R = U V^H from the SVD of A^H X), averaged over 32 * nsamp; dL/dX = 2 (X - A R).
 
 ``bf16=True`` rounds what the GPU keeps in bf16 (weights, F, H1, H2, dO, dZ2, dZ1) so the two
 agree to accumulation order; ``bf16=False`` is the exact float64 function, whose gradient is
@@ -19,7 +20,6 @@ import numpy as np
 
 NF, WD, NS, NCAR = 32, 512, 32, 5
 NO = NS * NCAR * 2
-MU = 0.25
 SIZES = [("W1", (WD, NF)), ("b1", (WD,)), ("W2", (WD, WD)), ("b2", (WD,)), ("W3", (NO, WD)), ("b3", (NO,))]
 
 
@@ -82,9 +82,10 @@ def loss_grad(p, F, CAR, A, nsamp, bf16=True):
         sl = slice(s * rows, (s + 1) * rows)
         Xs, As = X[sl], At[sl]
         Pm = As.conj().T @ Xs
-        Gm = Xs.conj().T @ Xs
-        loss += np.real(np.trace(Gm)) - np.sum(np.abs(Pm) ** 2) + MU * np.sum(np.abs(Gm - np.eye(NS)) ** 2)
-        GX[sl] = 2.0 * (Xs - As @ Pm) + 4.0 * MU * Xs @ (Gm - np.eye(NS))
+        U, sv, Vh = np.linalg.svd(Pm)
+        R = U @ Vh
+        loss += np.real(np.vdot(Xs, Xs)) - 2.0 * sv.sum() + NS
+        GX[sl] = 2.0 * (Xs - As @ R)
     loss *= scale
     GX *= scale
     # dO: Re(conj(G) car), -Im(conj(G) car)

@@ -533,9 +533,8 @@ int wtbg_spectrum(wtbg_ctx* ctx, int n, int ncomp, const double* ebse, const dou
   return WTBG_OK;
 }
 
-int wtbg_bse_q_eigenvalues(wtbg_ctx* ctx, int nk, const double* kptq, const double* q4, const wtbg_coulomb* p,
-                           double* W) {
-  if (!ctx || !kptq || !q4 || !p || !W) return WTBG_ERR_ARG;
+int wtbg_bse_build_q(wtbg_ctx* ctx, int nk, const double* kptq, const double* q4, const wtbg_coulomb* p) {
+  if (!ctx || !kptq || !q4 || !p) return WTBG_ERR_ARG;
   if (!ctx->have_bands || nk != ctx->nk) return set_err(ctx, WTBG_ERR_STATE, "bse_q: call wtbg_bands on the k-mesh first");
   if (int r = set_device(ctx)) return r;
   const int nb = ctx->nv + ctx->nc, w = ctx->w;
@@ -553,6 +552,19 @@ int wtbg_bse_q_eigenvalues(wtbg_ctx* ctx, int nk, const double* kptq, const doub
   if (int r = launch_bands(ctx, true)) return r;
   if (int r = check_kstat(ctx, nk)) return r;
   if (int r = launch_bse_build(ctx, p, q4)) return r;
+  if (int r = t.stop()) return r;
+  ctx->have_matrix = true;
+  ctx->fast_ready = false;
+  ctx->have_solution = false;
+  return WTBG_OK;
+}
+
+int wtbg_bse_q_eigenvalues(wtbg_ctx* ctx, int nk, const double* kptq, const double* q4, const wtbg_coulomb* p,
+                           double* W) {
+  if (!ctx || !kptq || !q4 || !p || !W) return WTBG_ERR_ARG;
+  if (int r = wtbg_bse_build_q(ctx, nk, kptq, q4, p)) return r;
+  const long long N = ctx->N;
+  Timer t(ctx);
   const bool hv = ctx->have_velocity;
   ctx->have_velocity = false;   // eigenvalues only: g not needed
   int r = run_tridiagonalise(ctx);

@@ -241,18 +241,19 @@ __global__ void k_sum_parts(const double2* Yp, long long N, int m, double2* Y, i
 // staged GR at a time in shared memory; the 16 x 16 threads each own a register tile of
 // outputs (a = tx + 16 i, b = ty + 16 j), so every staged value feeds up to 5 products.
 constexpr int GR = 16;
-constexpr int GT = 5;   // register tile: p, q <= 16 * GT = 80
+constexpr int GT = 5;   // largest register tile: p, q <= 16 * GT = 80
+template <int T>
 __global__ void __launch_bounds__(256) k_gram(const double2* A, int lda, int p, const double2* B, int ldb, int q,
                                               long long N, double2* part) {
   __shared__ double2 as[GR][kMaxRR + 1], bsm[GR][kMaxRR + 1];
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const long long rows_per = (N + gridDim.x - 1) / gridDim.x;
   const long long r0 = (long long)blockIdx.x * rows_per, r1 = min(N, r0 + rows_per);
-  double2 acc[GT][GT];
+  double2 acc[T][T];
 #pragma unroll
-  for (int i = 0; i < GT; ++i)
+  for (int i = 0; i < T; ++i)
 #pragma unroll
-    for (int j = 0; j < GT; ++j) acc[i][j] = make_double2(0, 0);
+    for (int j = 0; j < T; ++j) acc[i][j] = make_double2(0, 0);
   for (long long c0 = r0; c0 < r1; c0 += GR) {
     __syncthreads();
     for (int it = tid; it < GR * p; it += 256) {
@@ -264,24 +265,29 @@ __global__ void __launch_bounds__(256) k_gram(const double2* A, int lda, int p, 
       bsm[rr][b] = (c0 + rr < r1) ? B[c0 + rr + (long long)b * ldb] : make_double2(0, 0);
     }
     __syncthreads();
-#pragma unroll 2
+#pragma unroll 4
     for (int rr = 0; rr < GR; ++rr) {
-      double2 av[GT], bv[GT];
+      double2 av[T], bv[T];
 #pragma unroll
-      for (int i = 0; i < GT; ++i) av[i] = (tx + 16 * i < p) ? as[rr][tx + 16 * i] : make_double2(0, 0);
+      for (int i = 0; i < T; ++i) av[i] = as[rr][min(tx + 16 * i, kMaxRR)];
 #pragma unroll
-      for (int j = 0; j < GT; ++j) bv[j] = (ty + 16 * j < q) ? bsm[rr][ty + 16 * j] : make_double2(0, 0);
+      for (int j = 0; j < T; ++j) bv[j] = bsm[rr][min(ty + 16 * j, kMaxRR)];
 #pragma unroll
-      for (int i = 0; i < GT; ++i)
+      for (int i = 0; i < T; ++i)
 #pragma unroll
-        for (int j = 0; j < GT; ++j) acc[i][j] = cadd(acc[i][j], cmulc(av[i], bv[j]));
+        for (int j = 0; j < T; ++j) {   // conj(a) b as four FMAs
+          acc[i][j].x = fma(av[i].x, bv[j].x, acc[i][j].x);
+          acc[i][j].x = fma(av[i].y, bv[j].y, acc[i][j].x);
+          acc[i][j].y = fma(av[i].x, bv[j].y, acc[i][j].y);
+          acc[i][j].y = fma(-av[i].y, bv[j].x, acc[i][j].y);
+        }
     }
   }
   const int pq = p * q;
 #pragma unroll
-  for (int i = 0; i < GT; ++i)
+  for (int i = 0; i < T; ++i)
 #pragma unroll
-    for (int j = 0; j < GT; ++j) {
+    for (int j = 0; j < T; ++j) {
       const int a = tx + 16 * i, b = ty + 16 * j;
       if (a < p && b < q) part[(long long)blockIdx.x * pq + a + b * p] = acc[i][j];
     }
@@ -410,17 +416,39 @@ __host__ __device__ constexpr size_t rr_smem_bytes(int n, int nb) {
          (size_t)4 * RR_THREADS + 64;
 }
 
-__device__ __forceinline__ int sturm_count(const double* dd, const double* ee, int n, double x, double pivmin) {
+// Number of eigenvalues of the symmetric tridiagonal (d, e) below x from the sign changes of
+// the leading principal minors p_i = (d_i - x) p_{i-1} - e_{i-1}^2 p_{i-2} (two FMAs a step,
+// no division), rescaled by exact powers of two; a zero minor counts as a sign change.
+__device__ __forceinline__ int sturm_count(const double* dd, const double* ee, int n, double x) {
+  double pm = 0.0, p = 1.0, sgn = 1.0;
   int cnt = 0;
-  double q = dd[0] - x;
-  if (fabs(q) < pivmin) q = -pivmin;
-  cnt += (q < 0);
-  for (int i = 1; i < n; ++i) {
-    q = (dd[i] - x) - ee[i - 1] * ee[i - 1] / q;
-    if (fabs(q) < pivmin) q = -pivmin;
-    cnt += (q < 0);
+  for (int i = 0; i < n; ++i) {
+    const double e2 = (i > 0) ? ee[i - 1] * ee[i - 1] : 0.0;
+    const double pn = fma(dd[i] - x, p, -e2 * pm);
+    pm = p;
+    p = pn;
+    const double ap = fabs(p);
+    if (ap > 0x1p+500) {
+      p *= 0x1p-500;
+      pm *= 0x1p-500;
+    } else if (ap < 0x1p-500 && ap > 0.0) {
+      p *= 0x1p+500;
+      pm *= 0x1p+500;
+    }
+    const double s = (p == 0.0) ? -sgn : (p < 0.0 ? -1.0 : 1.0);
+    cnt += (s != sgn);
+    sgn = s;
+    if (p == 0.0) p = sgn * (fabs(pm) * 0x1p-60 + 0x1p-1000);   // a zero minor: pivot -> sign change
   }
   return cnt;
+}
+
+__device__ __forceinline__ double2 warp_sum2(double2 t) {
+  for (int o = 16; o > 0; o >>= 1) {
+    t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
+    t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
+  }
+  return t;
 }
 
 __global__ void __launch_bounds__(RR_THREADS) k_rr_tridiag(const double2* Min, int n, int nb, int descending,
@@ -464,25 +492,28 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr_tridiag(const double2* Min, i
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) red[wp] = s;
     __syncthreads();
-    if (tid == 0) {
-      double xn2 = 0;
-      for (int k = 0; k < NW; ++k) xn2 += red[k];
-      const double2 al = A[(j + 1) + j * n];
-      if (xn2 == 0.0 && al.y == 0.0) {
-        s_triv = 1;
-        s_tau = make_double2(0, 0);
-        ee[j] = al.x;
-      } else {
-        s_triv = 0;
-        const double beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xn2), al.x);
-        s_tau = make_double2((beta - al.x) / beta, -al.y / beta);
-        const double2 den = make_double2(al.x - beta, al.y);
-        const double dn = den.x * den.x + den.y * den.y;
-        s_scal = make_double2(den.x / dn, -den.y / dn);
-        ee[j] = beta;
+    if (wp == 0) {
+      double xn2 = (lane < NW) ? red[lane] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) xn2 += __shfl_xor_sync(0xffffffffu, xn2, o);
+      if (lane == 0) {
+        const double2 al = A[(j + 1) + j * n];
+        if (xn2 == 0.0 && al.y == 0.0) {
+          s_triv = 1;
+          s_tau = make_double2(0, 0);
+          ee[j] = al.x;
+        } else {
+          s_triv = 0;
+          const double beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xn2), al.x);
+          const double ib = 1.0 / beta;
+          s_tau = make_double2((beta - al.x) * ib, -al.y * ib);
+          const double2 den = make_double2(al.x - beta, al.y);
+          const double idn = 1.0 / (den.x * den.x + den.y * den.y);
+          s_scal = make_double2(den.x * idn, -den.y * idn);
+          ee[j] = beta;
+        }
+        dd[j] = A[j + j * n].x;
+        taus[j] = s_tau;
       }
-      dd[j] = A[j + j * n].x;
-      taus[j] = s_tau;
     }
     __syncthreads();
     const int triv = s_triv;
@@ -494,7 +525,8 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr_tridiag(const double2* Min, i
     }
     __syncthreads();
     if (triv) continue;
-    // p = tau A22 v: four threads per row
+    // p = tau A22 v: four threads per row; the partial p^H v of each row group on the fly
+    double2 t = make_double2(0, 0);
     {
       const int part = tid & 3;
       const unsigned gmask = 0xFu << (lane & ~3);
@@ -505,22 +537,20 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr_tridiag(const double2* Min, i
         acc.y += __shfl_xor_sync(gmask, acc.y, 1);
         acc.x += __shfl_xor_sync(gmask, acc.x, 2);
         acc.y += __shfl_xor_sync(gmask, acc.y, 2);
-        if (part == 0) pp[i] = cmul(tau, acc);
+        const double2 pi = cmul(tau, acc);
+        if (part == 0) {
+          pp[i] = pi;
+          t = cadd(t, cmulc(pi, vv[i]));
+        }
       }
     }
-    __syncthreads();
-    double2 t = make_double2(0, 0);
-    for (int i = tid; i < m; i += bs) t = cadd(t, cmulc(pp[i], vv[i]));
-    for (int o = 16; o > 0; o >>= 1) {
-      t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
-      t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
-    }
+    t = warp_sum2(t);
     if (lane == 0) redc[wp] = t;
     __syncthreads();
-    if (tid == 0) {
-      double2 sum = make_double2(0, 0);
-      for (int k = 0; k < NW; ++k) sum = cadd(sum, redc[k]);
-      s_a2 = cscale(cmul(tau, sum), -0.5);
+    if (wp == 0) {
+      double2 sum = (lane < NW) ? redc[lane] : make_double2(0, 0);
+      sum = warp_sum2(sum);
+      if (lane == 0) s_a2 = cscale(cmul(tau, sum), -0.5);
     }
     __syncthreads();
     const double2 a2 = s_a2;
@@ -538,10 +568,9 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr_tridiag(const double2* Min, i
     dd[n - 1] = A[(n - 1) + (n - 1) * n].x;
     double lo = 0.0, hi = 0.0;
     for (int i = 0; i < n; ++i) {
-      const double dv = (i == n - 1) ? A[(n - 1) + (n - 1) * n].x : dd[i];
       const double r = (i > 0 ? fabs(ee[i - 1]) : 0.0) + (i < n - 1 ? fabs(ee[i]) : 0.0);
-      lo = (i == 0) ? dv - r : fmin(lo, dv - r);
-      hi = (i == 0) ? dv + r : fmax(hi, dv + r);
+      lo = (i == 0) ? dd[i] - r : fmin(lo, dd[i] - r);
+      hi = (i == 0) ? dd[i] + r : fmax(hi, dd[i] + r);
     }
     s_tn = fmax(fabs(lo), fabs(hi));
     const double pad = 4.0 * DBL_EPSILON * s_tn + 1e-300;
@@ -549,17 +578,17 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr_tridiag(const double2* Min, i
     s_hi = hi + pad;
   }
   __syncthreads();
-  // ---- 2. multisection bisection
-  const double pivmin = DBL_MIN * 4.0;
+  // ---- 2. multisection bisection down to ~2^-44 of the Gershgorin width
   const int G = max(1, bs / nb);
   int rounds = 1;
   {
     double shrink = 1.0;
-    while (shrink > 0x1p-53 && rounds < 64) {
+    while (shrink > 0x1p-44 && rounds < 64) {
       shrink /= (double)(G + 1);
       ++rounds;
     }
   }
+  const double ig = 1.0 / (double)(G + 1);
   for (int e = tid; e < nb; e += bs) {
     blo[e] = s_lo;
     bhi[e] = s_hi;
@@ -569,8 +598,8 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr_tridiag(const double2* Min, i
     const int e = tid / G, g = tid % G;
     if (e < nb) {
       const double lo = blo[e], hi = bhi[e];
-      const double x = lo + (hi - lo) * (double)(g + 1) / (double)(G + 1);
-      cnt[tid] = sturm_count(dd, ee, n, x, pivmin);
+      const double x = lo + (hi - lo) * ((double)(g + 1) * ig);
+      cnt[tid] = sturm_count(dd, ee, n, x);
     }
     __syncthreads();
     if (e < nb && g == 0) {
@@ -578,7 +607,7 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr_tridiag(const double2* Min, i
       const double lo = blo[e], hi = bhi[e];
       double nlo = lo, nhi = hi;
       for (int gg = 0; gg < G; ++gg) {
-        const double x = lo + (hi - lo) * (double)(gg + 1) / (double)(G + 1);
+        const double x = lo + (hi - lo) * ((double)(gg + 1) * ig);
         if (cnt[e * G + gg] <= mi) {
           nlo = x;
         } else {
@@ -593,7 +622,8 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr_tridiag(const double2* Min, i
   }
   for (int e = tid; e < nb; e += bs) lam[e] = 0.5 * (blo[e] + bhi[e]);
   __syncthreads();
-  // ---- 3. inverse iteration
+  // ---- 3. inverse iteration: T - lambda I = P L U factored once (partial pivoting), three
+  //         solves; eigenvalues closer than 1e-7 |T| are done in order by their first thread
   if (tid < nb) {
     const double ctol = 1e-7 * fmax(1e-3, s_tn);
     const bool leader = (tid == 0) || fabs(lam[tid] - lam[tid - 1]) > ctol;
@@ -601,43 +631,57 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr_tridiag(const double2* Min, i
       int cs = 1;
       while (tid + cs < nb && fabs(lam[tid + cs] - lam[tid + cs - 1]) <= ctol) ++cs;
       const double pert = DBL_EPSILON * fmax(s_tn, 1e-300);
-      double u1[kMaxRR], u2[kMaxRR], u3[kMaxRR];
+      double r1[kMaxRR], u2[kMaxRR], u3[kMaxRR], ml[kMaxRR];
+      unsigned char sw[kMaxRR];
       for (int sidx = 0; sidx < cs; ++sidx) {
         const int col = tid + sidx;
         double* x = Z + col * n;
         const double lm = lam[col];
+        double diag = dd[0] - lm, sup = (n > 1) ? ee[0] : 0.0;
+        for (int k = 0; k < n - 1; ++k) {
+          const double sub = ee[k], nd = dd[k + 1] - lm, nsup = (k + 1 < n - 1) ? ee[k + 1] : 0.0;
+          if (fabs(diag) >= fabs(sub)) {
+            if (fabs(diag) < pert) diag = copysign(pert, diag);
+            const double rp = 1.0 / diag;
+            const double mult = sub * rp;
+            r1[k] = rp;
+            u2[k] = sup;
+            u3[k] = 0.0;
+            ml[k] = mult;
+            sw[k] = 0;
+            diag = nd - mult * sup;
+            sup = nsup;
+          } else {
+            const double rp = 1.0 / sub;
+            const double mult = diag * rp;
+            r1[k] = rp;
+            u2[k] = nd;
+            u3[k] = nsup;
+            ml[k] = mult;
+            sw[k] = 1;
+            diag = sup - mult * nd;
+            sup = -mult * nsup;
+          }
+        }
+        if (fabs(diag) < pert) diag = copysign(pert, diag);
+        const double rlast = 1.0 / diag;
         for (int k = 0; k < n; ++k) x[k] = 1.0 + 0.1 * (double)((k * 7 + col * 13) % 17) / 17.0;
         for (int itr = 0; itr < 3; ++itr) {
-          double diag = dd[0] - lm, sup = (n > 1) ? ee[0] : 0.0, cur = x[0];
+          double cur = x[0];
           for (int k = 0; k < n - 1; ++k) {
-            const double sub = ee[k], nd = dd[k + 1] - lm, nsup = (k + 1 < n - 1) ? ee[k + 1] : 0.0;
             const double nxt = x[k + 1];
-            if (fabs(diag) >= fabs(sub)) {
-              if (fabs(diag) < pert) diag = copysign(pert, diag);
-              const double mult = sub / diag;
-              u1[k] = diag;
-              u2[k] = sup;
-              u3[k] = 0.0;
-              x[k] = cur;
-              cur = nxt - mult * cur;
-              diag = nd - mult * sup;
-              sup = nsup;
-            } else {
-              const double mult = diag / sub;
-              u1[k] = sub;
-              u2[k] = nd;
-              u3[k] = nsup;
+            if (sw[k]) {
               x[k] = nxt;
-              cur = cur - mult * nxt;
-              diag = sup - mult * nd;
-              sup = -mult * nsup;
+              cur = cur - ml[k] * nxt;
+            } else {
+              x[k] = cur;
+              cur = nxt - ml[k] * cur;
             }
           }
-          if (fabs(diag) < pert) diag = copysign(pert, diag);
-          double x2 = 0.0, x1 = cur / diag, nrm = x1 * x1;
+          double x2 = 0.0, x1 = cur * rlast, nrm = x1 * x1;
           x[n - 1] = x1;
           for (int k = n - 2; k >= 0; --k) {
-            const double xk = (x[k] - u2[k] * x1 - u3[k] * x2) / u1[k];
+            const double xk = (x[k] - u2[k] * x1 - u3[k] * x2) * r1[k];
             x[k] = xk;
             nrm += xk * xk;
             x2 = x1;
@@ -662,25 +706,39 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr_tridiag(const double2* Min, i
     }
   }
   __syncthreads();
-  // ---- 4. back-transform, one warp per vector
-  for (int c = wp; c < nb; c += NW) {
-    double2* y = Ys + c * n;
-    for (int k = lane; k < n; k += 32) y[k] = make_double2(Z[c * n + k], 0.0);
+  // ---- 4. back-transform y = H_0 H_1 ... H_{n-2} z: each warp carries its vectors together
+  {
+    constexpr int VPW = (kMaxRR / 2 + NW - 1) / NW;   // vectors per warp (nb <= kMaxRR / 2)
+    int cols[VPW];
+    int nv = 0;
+    for (int c = wp; c < nb && nv < VPW; c += NW) cols[nv++] = c;
+    for (int q = 0; q < nv; ++q)
+      for (int k = lane; k < n; k += 32) Ys[cols[q] * n + k] = make_double2(Z[cols[q] * n + k], 0.0);
     __syncwarp();
     for (int j = n - 2; j >= 0; --j) {
       const double2 tau = taus[j];
       if (tau.x == 0.0 && tau.y == 0.0) continue;
-      double2 dot = make_double2(0, 0);
-      for (int k = j + 1 + lane; k < n; k += 32) dot = cadd(dot, cmulc(A[k + j * n], y[k]));
-      for (int o = 16; o > 0; o >>= 1) {
-        dot.x += __shfl_xor_sync(0xffffffffu, dot.x, o);
-        dot.y += __shfl_xor_sync(0xffffffffu, dot.y, o);
+      double2 dot[VPW];
+#pragma unroll
+      for (int q = 0; q < VPW; ++q) dot[q] = make_double2(0, 0);
+      for (int k = j + 1 + lane; k < n; k += 32) {
+        const double2 v = A[k + j * n];
+#pragma unroll
+        for (int q = 0; q < VPW; ++q)
+          if (q < nv) dot[q] = cadd(dot[q], cmulc(v, Ys[cols[q] * n + k]));
       }
-      const double2 f = cmul(tau, dot);
-      for (int k = j + 1 + lane; k < n; k += 32) y[k] = csub(y[k], cmul(A[k + j * n], f));
+#pragma unroll
+      for (int q = 0; q < VPW; ++q) dot[q] = warp_sum2(dot[q]);
+      for (int k = j + 1 + lane; k < n; k += 32) {
+        const double2 v = A[k + j * n];
+#pragma unroll
+        for (int q = 0; q < VPW; ++q)
+          if (q < nv) Ys[cols[q] * n + k] = csub(Ys[cols[q] * n + k], cmul(v, cmul(tau, dot[q])));
+      }
       __syncwarp();
     }
-    for (int k = lane; k < n; k += 32) Yout[(long long)c * n + k] = y[k];
+    for (int q = 0; q < nv; ++q)
+      for (int k = lane; k < n; k += 32) Yout[(long long)cols[q] * n + k] = Ys[cols[q] * n + k];
   }
   if (tid < nb) theta[tid] = lam[tid];
   if (tid == 0) *status = 0;
@@ -803,7 +861,18 @@ static int gram(wtbg_ctx* ctx, const double2* A, int lda, int p, const double2* 
   const long long N = ctx->N;
   if (p > 16 * GT || q > 16 * GT) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "davidson: gram too large");
   const int nparts = (int)std::min<long long>(296, (N + 63) / 64);
-  k_gram<<<nparts, 256, 0, ctx->stream>>>(A, lda, p, B, ldb, q, N, part); WTBG_COUNT(ctx, 1);
+  const int t = (std::max(p, q) + 15) / 16;
+  if (t <= 1)
+    k_gram<1><<<nparts, 256, 0, ctx->stream>>>(A, lda, p, B, ldb, q, N, part);
+  else if (t == 2)
+    k_gram<2><<<nparts, 256, 0, ctx->stream>>>(A, lda, p, B, ldb, q, N, part);
+  else if (t == 3)
+    k_gram<3><<<nparts, 256, 0, ctx->stream>>>(A, lda, p, B, ldb, q, N, part);
+  else if (t == 4)
+    k_gram<4><<<nparts, 256, 0, ctx->stream>>>(A, lda, p, B, ldb, q, N, part);
+  else
+    k_gram<5><<<nparts, 256, 0, ctx->stream>>>(A, lda, p, B, ldb, q, N, part);
+  WTBG_COUNT(ctx, 1);
   k_gram_sum<<<(p * q + 31) / 32, 256, 0, ctx->stream>>>(part, nparts, p * q, C); WTBG_COUNT(ctx, 1);
   CKL("gram");
   return 0;
@@ -923,10 +992,13 @@ int run_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, doub
     int saved;
     ~FastGuard() { c->fast_mode = saved; }
   } guard{ctx, ctx->fast_mode};
-  constexpr double kFastSwitch = 3e-5;
+  constexpr double kFastSwitch = 2e-5, kFastStall = 5e-4;
   double best = 1e300;
   int since_best = 0;
+  ctx->stats.dav_fast_iters = 0;
+  ctx->stats.dav_fp64_iters = 0;
   for (; it < max_iter; ++it) {
+    ++(ctx->fast_mode ? ctx->stats.dav_fast_iters : ctx->stats.dav_fp64_iters);
     k_resid_precond<<<nrb, th, 0, s>>>(X, HX, (int)N, nb, w.theta, w.D, N, T, (int)N, rp); WTBG_COUNT(ctx, 1);
     CKL("k_resid_precond");
     std::vector<double> rph((size_t)nrb * 64);
@@ -942,13 +1014,15 @@ int run_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, doub
     }
     if (worst < tol) break;
     if (ctx->fast_mode) {
-      if (worst < 0.7 * best) {
+      // the worst residual of a block is not monotone: stagnation counts only near the
+      // product's rounding level (no halving of the best residual for 10 iterations)
+      if (worst < 0.5 * best) {
         best = worst;
         since_best = 0;
-      } else {
+      } else if (best < kFastStall) {
         ++since_best;
       }
-      if (worst < std::max(kFastSwitch, tol) || since_best >= 8) {
+      if (worst < std::max(kFastSwitch, tol) || since_best >= 10) {
         ctx->fast_mode = 0;
         if (int r = hemm(ctx, X, (int)N, nb, HX, (int)N, w.Yp)) return r;
         if (int r = rr(X, HX, nb)) return r;

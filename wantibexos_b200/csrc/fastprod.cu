@@ -13,8 +13,10 @@
 //
 // Kernel shape: persistent stream-K grid over (128-row tile, 32-wide K block) units; warp 0
 // issues TMA loads (64-byte swizzle) into a 4-stage mbarrier ring, warp 1 issues the MMAs
-// into one of two TMEM accumulators, warps 2..5 drain a finished accumulator (tcgen05.ld)
-// and add it to an FP32 global sum with red.add. Every mbarrier wait is bounded in time; on
+// into one of two TMEM accumulators in chunks of FP_CHUNK K blocks, warps 2..5 drain each
+// finished chunk (tcgen05.ld) into FP64 registers and, at the end of a row tile's K range, add
+// the FP64 sums to global memory with red.add.f64 (short FP32 chains keep the product's
+// rounding near the bf16-split level). Every mbarrier wait is bounded in time; on
 // expiry the CTA raises an error flag, drains its copies and MMAs, frees TMEM and returns.
 #include "common.cuh"
 
@@ -33,7 +35,8 @@ using namespace tc;
 constexpr int FP_BM = 128;          // rows per tile = TMEM lanes
 constexpr int FP_BK = 32;           // K per stage: 64-byte bf16 rows
 constexpr int FP_STAGES = 4;
-constexpr int FP_MAXMP = 64;        // padded vectors per half (2*mp <= 128 TMEM columns)
+constexpr int FP_MAXMP = 48;        // padded vectors per half (2*mp FP64 sums per epilogue thread)
+constexpr int FP_CHUNK = 8;         // K blocks per FP32 TMEM accumulation before the FP64 drain
 constexpr int FP_THREADS = 192;
 constexpr uint32_t FP_TMEM_COLS = 256;   // two accumulators of 128 columns
 constexpr uint32_t FP_A_BYTES = 4u * FP_BM * FP_BK * 2u;
@@ -41,10 +44,11 @@ constexpr uint32_t FP_A_BYTES = 4u * FP_BM * FP_BK * 2u;
 struct FastArgs {
   int N, m, mp, KB;
   long long W;       // units = tiles * KB
-  float* Yacc;       // [2*mp][N]
+  double* Yacc;      // [2*mp][N]
   int* err;
 };
 
+template <int MP>
 __global__ void __launch_bounds__(FP_THREADS, 1)
     k_fastprod(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, FastArgs a) {
   extern __shared__ unsigned char fp_smem[];
@@ -54,7 +58,7 @@ __global__ void __launch_bounds__(FP_THREADS, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t raw = smem_u32(fp_smem);
   const uint32_t base = (raw + 1023u) & ~1023u;
-  const int mp = a.mp;
+  constexpr int mp = MP;
   const uint32_t B_BYTES = 2u * 2u * (uint32_t)mp * FP_BK * 2u;
   const uint32_t STAGE = FP_A_BYTES + B_BYTES;
   const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[FP_STAGES]);
@@ -109,92 +113,112 @@ __global__ void __launch_bounds__(FP_THREADS, 1)
       mbar_wait(full0 + 8 * s, (uint32_t)(last & 1), abort_flag, false);
     }
   } else if (warp == 1 && lane == 0) {
-    // MMA issuer
+    // MMA issuer: each segment (one row tile) is accumulated in chunks of at most FP_CHUNK
+    // K blocks, alternating between the two TMEM accumulators
     const uint32_t idf = idesc_bf16(FP_BM, 2 * mp, false), idh = idesc_bf16(FP_BM, mp, false),
                    idn = idesc_bf16(FP_BM, mp, true);
     long long it = 0, u = u0;
-    int seg = 0;
+    int chunk = 0;
     bool ok = true;
     while (u < u1 && ok) {
-      const int mt = (int)(u / KB);
-      const long long uend = min(u1, (long long)(mt + 1) * KB);
-      const int b = seg & 1;
-      if (seg >= 2 && !mbar_wait(acce0 + 8 * b, (uint32_t)(((seg - 2) >> 1) & 1), abort_flag)) {
-        ok = false;
-        break;
-      }
-      tc_fence_after();
-      const uint32_t dt = tmem + (uint32_t)b * 128u;
-      uint32_t acc = 0;
-      for (; u < uend; ++u, ++it) {
-        const int s = (int)(it % FP_STAGES);
-        const long long r = it / FP_STAGES;
-        if (!mbar_wait(full0 + 8 * s, (uint32_t)(r & 1), abort_flag)) {
+      const long long seg_end = min(u1, (u / KB + 1) * KB);
+      while (u < seg_end && ok) {
+        const long long cend = min(seg_end, u + FP_CHUNK);
+        const int b = chunk & 1;
+        if (chunk >= 2 && !mbar_wait(acce0 + 8 * b, (uint32_t)(((chunk - 2) >> 1) & 1), abort_flag)) {
           ok = false;
           break;
         }
         tc_fence_after();
-        const uint32_t sa = base + (uint32_t)s * STAGE, sb = sa + FP_A_BYTES;
+        const uint32_t dt = tmem + (uint32_t)b * 128u;
+        uint32_t acc = 0;
+        for (; u < cend; ++u, ++it) {
+          const int s = (int)(it % FP_STAGES);
+          const long long r = it / FP_STAGES;
+          if (!mbar_wait(full0 + 8 * s, (uint32_t)(r & 1), abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sa = base + (uint32_t)s * STAGE, sb = sa + FP_A_BYTES;
 #pragma unroll
-        for (int kk = 0; kk < 2; ++kk) {
-          const uint32_t ko = (uint32_t)kk * 32u;
-          const uint64_t arh = sdesc(sa + ko), arl = sdesc(sa + 8192u + ko);
-          const uint64_t aih = sdesc(sa + 16384u + ko), ail = sdesc(sa + 24576u + ko);
-          const uint32_t bh = sb + ko, bl = sb + (uint32_t)(2 * mp) * 64u + ko;
-          const uint64_t bhf = sdesc(bh), blf = sdesc(bl);
-          const uint64_t bhi = sdesc(bh + (uint32_t)mp * 64u), bli = sdesc(bl + (uint32_t)mp * 64u);
-          tc_mma(dt, arh, bhf, idf, acc);
-          acc = 1;
-          tc_mma(dt, arh, blf, idf, 1);
-          tc_mma(dt, arl, bhf, idf, 1);
-          tc_mma(dt, aih, bhi, idn, 1);              // Yr -= Im H Xi
-          tc_mma(dt, aih, bli, idn, 1);
-          tc_mma(dt, ail, bhi, idn, 1);
-          tc_mma(dt + (uint32_t)mp, aih, bhf, idh, 1);   // Yi += Im H Xr
-          tc_mma(dt + (uint32_t)mp, aih, blf, idh, 1);
-          tc_mma(dt + (uint32_t)mp, ail, bhf, idh, 1);
+          for (int kk = 0; kk < 2; ++kk) {
+            const uint32_t ko = (uint32_t)kk * 32u;
+            const uint64_t arh = sdesc(sa + ko), arl = sdesc(sa + 8192u + ko);
+            const uint64_t aih = sdesc(sa + 16384u + ko), ail = sdesc(sa + 24576u + ko);
+            const uint32_t bh = sb + ko, bl = sb + (uint32_t)(2 * mp) * 64u + ko;
+            const uint64_t bhf = sdesc(bh), blf = sdesc(bl);
+            const uint64_t bhi = sdesc(bh + (uint32_t)mp * 64u), bli = sdesc(bl + (uint32_t)mp * 64u);
+            tc_mma(dt, arh, bhf, idf, acc);
+            acc = 1;
+            tc_mma(dt, arh, blf, idf, 1);
+            tc_mma(dt, arl, bhf, idf, 1);
+            tc_mma(dt, aih, bhi, idn, 1);              // Yr -= Im H Xi
+            tc_mma(dt, aih, bli, idn, 1);
+            tc_mma(dt, ail, bhi, idn, 1);
+            tc_mma(dt + (uint32_t)mp, aih, bhf, idh, 1);   // Yi += Im H Xr
+            tc_mma(dt + (uint32_t)mp, aih, blf, idh, 1);
+            tc_mma(dt + (uint32_t)mp, ail, bhf, idh, 1);
+          }
+          tc_commit(empty0 + 8 * s);
         }
-        tc_commit(empty0 + 8 * s);
+        if (!ok) break;
+        tc_commit(accf0 + 8 * b);
+        ++chunk;
       }
-      if (!ok) break;
-      tc_commit(accf0 + 8 * b);
-      ++seg;
     }
     // all MMAs issued by this thread complete before TMEM is released
     tc_commit(done);
     mbar_wait(done, 0, abort_flag, false);
   } else if (warp >= 2) {
-    // epilogue: TMEM lane quarter q belongs to warps with warp % 4 == q
+    // epilogue: TMEM lane quarter q belongs to warps with warp % 4 == q. Every chunk's FP32
+    // partial is added into FP64 registers (one row, 2*mp columns per thread); at the end of
+    // a segment the FP64 sums go to global memory with red.add.f64.
     const int q = warp & 3;
     long long u = u0;
-    int seg = 0;
+    int chunk = 0;
     const int N = a.N, m = a.m;
-    while (u < u1) {
-      const int mt = (int)(u / KB);
-      const long long uend = min(u1, (long long)(mt + 1) * KB);
-      const int b = seg & 1;
-      if (!mbar_wait(accf0 + 8 * b, (uint32_t)((seg >> 1) & 1), abort_flag)) break;
-      tc_fence_after();
-      const int row = mt * FP_BM + q * 32 + lane;
-      const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)b * 128u;
-      for (int c0 = 0; c0 < 2 * mp; c0 += 32) {
-        uint32_t v[32];
-        tc_ld16(ta + (uint32_t)c0, v);
-        if (c0 + 16 < 2 * mp) tc_ld16(ta + (uint32_t)c0 + 16u, v + 16);
-        tc_wait_ld();
-        if (row < N) {
+    double accd[2 * MP];
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int col = c0 + j;
-            if (col < 2 * mp && (col % mp) < m) atomicAdd(a.Yacc + (long long)col * N + row, __uint_as_float(v[j]));
-          }
+    for (int j = 0; j < 2 * MP; ++j) accd[j] = 0.0;
+    bool ok = true;
+    while (u < u1 && ok) {
+      const long long seg_end = min(u1, (u / KB + 1) * KB);
+      const int mt = (int)(u / KB);
+      const int row = mt * FP_BM + q * 32 + lane;
+      while (u < seg_end) {
+        const long long cend = min(seg_end, u + FP_CHUNK);
+        const int b = chunk & 1;
+        if (!mbar_wait(accf0 + 8 * b, (uint32_t)((chunk >> 1) & 1), abort_flag)) {
+          ok = false;
+          break;
         }
+        tc_fence_after();
+        const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)b * 128u;
+#pragma unroll
+        for (int c0 = 0; c0 < 2 * MP; c0 += 32) {
+          uint32_t v[32];
+          tc_ld16(ta + (uint32_t)c0, v);
+          if (c0 + 16 < 2 * MP) tc_ld16(ta + (uint32_t)c0 + 16u, v + 16);
+          tc_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (c0 + j < 2 * MP) accd[c0 + j] += (double)__uint_as_float(v[j]);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acce0 + 8 * b);
+        u = cend;
+        ++chunk;
       }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(acce0 + 8 * b);
-      u = uend;
-      ++seg;
+      if (!ok) break;
+      if (row < N) {
+#pragma unroll
+        for (int j = 0; j < 2 * MP; ++j)
+          if ((j % MP) < m) atomicAdd(a.Yacc + (long long)j * N + row, accd[j]);
+      }
+#pragma unroll
+      for (int j = 0; j < 2 * MP; ++j) accd[j] = 0.0;
     }
   }
   tc_fence_before();
@@ -300,18 +324,18 @@ __global__ void k_split_x(const double2* __restrict__ X, int ldx, int m, int mp,
 }
 
 // Y = Yacc + D X (FP64), and clear Yacc for the next product
-__global__ void k_fast_finish(float* __restrict__ Yacc, const double* __restrict__ D, const double2* __restrict__ X,
+__global__ void k_fast_finish(double* __restrict__ Yacc, const double* __restrict__ D, const double2* __restrict__ X,
                               int ldx, int m, int mp, long long N, double2* __restrict__ Y, int ldy) {
   const long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (row >= N || j >= m) return;
-  float* pr = Yacc + (long long)j * N + row;
-  float* pi = Yacc + (long long)(mp + j) * N + row;
+  double* pr = Yacc + (long long)j * N + row;
+  double* pi = Yacc + (long long)(mp + j) * N + row;
   const double2 x = X[row + (long long)j * ldx];
   const double d = D[row];
-  Y[row + (long long)j * ldy] = make_double2((double)*pr + d * x.x, (double)*pi + d * x.y);
-  *pr = 0.0f;
-  *pi = 0.0f;
+  Y[row + (long long)j * ldy] = make_double2(*pr + d * x.x, *pi + d * x.y);
+  *pr = 0.0;
+  *pi = 0.0;
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -351,10 +375,10 @@ int run_fast_setup(wtbg_ctx* ctx) {
   const long long ld = (N + 63) / 64 * 64;
   if (int r = ensure(ctx, ctx->fA, (size_t)4 * N * ld * 2)) return r;
   if (int r = ensure(ctx, ctx->fB, (size_t)4 * FP_MAXMP * ld * 2)) return r;
-  if (int r = ensure(ctx, ctx->fY, (size_t)2 * FP_MAXMP * N * 4)) return r;
+  if (int r = ensure(ctx, ctx->fY, (size_t)2 * FP_MAXMP * N * 8)) return r;
   if (int r = ensure(ctx, ctx->fD, (size_t)N * 8)) return r;
   if (int r = ensure(ctx, ctx->fErr, 16)) return r;
-  CK(cudaMemsetAsync(ctx->fY.p, 0, (size_t)2 * FP_MAXMP * N * 4, ctx->stream));
+  CK(cudaMemsetAsync(ctx->fY.p, 0, (size_t)2 * FP_MAXMP * N * 8, ctx->stream));
   CK(cudaMemsetAsync(ctx->fErr.p, 0, 16, ctx->stream));
   const int nt = (int)((N + 31) / 32);
   k_split_h<<<dim3(nt, nt), dim3(32, 8), 0, ctx->stream>>>(ctx->H.as<double2>(), N, ld, ctx->fA.as<__nv_bfloat16>(),
@@ -396,23 +420,45 @@ int run_fastprod(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y, in
     a.KB = (int)((N + FP_BK - 1) / FP_BK);
     const long long tiles = (N + FP_BM - 1) / FP_BM;
     a.W = tiles * a.KB;
-    a.Yacc = ctx->fY.as<float>();
+    a.Yacc = ctx->fY.as<double>();
     a.err = ctx->fErr.as<int>();
     const size_t smem = (size_t)FP_STAGES * (FP_A_BYTES + 2u * 2u * mp * FP_BK * 2u) + 1024;
     int dev = 0, nsm = 148;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const int maxsm = (int)(FP_STAGES * (FP_A_BYTES + 2u * 2u * FP_MAXMP * FP_BK * 2u) + 1024);
     if (!attr_done[dev & 63]) {
-      CK(cudaFuncSetAttribute(k_fastprod, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)(FP_STAGES * (FP_A_BYTES + 2u * 2u * FP_MAXMP * FP_BK * 2u) + 1024)));
+      CK(cudaFuncSetAttribute(k_fastprod<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+      CK(cudaFuncSetAttribute(k_fastprod<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+      CK(cudaFuncSetAttribute(k_fastprod<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
       attr_done[dev & 63] = true;
     }
     const int grid = (int)std::min<long long>(nsm, a.W);
-    k_fastprod<<<grid, FP_THREADS, smem, s>>>(*reinterpret_cast<const CUtensorMap*>(ctx->tmA),
-                                              *reinterpret_cast<const CUtensorMap*>(ctx->tmB), a);
+    const bool prof = ctx->profiling != 0;
+    if (prof) {
+      if (int r = ensure_events(ctx, 2)) return r;
+      cudaEventRecord(ctx->evpool[0], s);
+    }
+    const CUtensorMap& ma = *reinterpret_cast<const CUtensorMap*>(ctx->tmA);
+    const CUtensorMap& mb = *reinterpret_cast<const CUtensorMap*>(ctx->tmB);
+    if (mp == 16)
+      k_fastprod<16><<<grid, FP_THREADS, smem, s>>>(ma, mb, a);
+    else if (mp == 32)
+      k_fastprod<32><<<grid, FP_THREADS, smem, s>>>(ma, mb, a);
+    else
+      k_fastprod<48><<<grid, FP_THREADS, smem, s>>>(ma, mb, a);
     WTBG_COUNT(ctx, 1);
     CKL("k_fastprod");
-    k_fast_finish<<<dim3((unsigned)((N + 255) / 256), mm), 256, 0, s>>>(ctx->fY.as<float>(), ctx->fD.as<double>(),
+    if (prof) {
+      cudaEventRecord(ctx->evpool[1], s);
+      CK(cudaEventSynchronize(ctx->evpool[1]));
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, ctx->evpool[0], ctx->evpool[1]));
+      ctx->stats.fast_ms += t;
+      ctx->stats.fast_bytes += 8.0 * (double)N * (double)N;
+      ctx->stats.fast_launches += 1;
+    }
+    k_fast_finish<<<dim3((unsigned)((N + 255) / 256), mm), 256, 0, s>>>(ctx->fY.as<double>(), ctx->fD.as<double>(),
                                                                        X + (long long)j0 * ldx, ldx, mm, mp, N,
                                                                        Y + (long long)j0 * ldy, ldy);
     WTBG_COUNT(ctx, 1);

@@ -10,9 +10,10 @@
 // Network: 3 layers, width 512, SiLU; weights in BF16 (FP32 master copy for Adam), every
 // GEMM on tcgen05 (bf16 inputs, FP32 accumulation in TMEM) through one stream-K kernel that
 // writes C^T with red.add. Loss per sample (targets A = lowest eigenvectors of the plain
-// dense FP64 solve, orthonormal):
-//   L = ||X - A (A^H X)||_F^2 + mu ||X^H X - I||_F^2        (mixing- and phase-invariant)
-// dL/dX = 2 (X - A A^H X) + 4 mu X (X^H X - I); backpropagated by hand-written kernels.
+// dense FP64 solve, orthonormal): the distance to the nearest orthonormal basis of their span,
+//   L = min_R unitary ||X - A R||_F^2 = tr(X^H X) - 2 ||A^H X||_* + 32   (mixing/phase-invariant)
+// with R the polar factor of A^H X (Newton-Schulz); dL/dX = 2 (X - A R), backpropagated by
+// hand-written kernels.
 #include "common.cuh"
 
 #include <algorithm>
@@ -34,7 +35,6 @@ constexpr int WD = 512;     // hidden width
 constexpr int NS = 32;      // states per block
 constexpr int NCAR = 5;     // phase carriers
 constexpr int NO = NS * NCAR * 2;   // 320 outputs
-constexpr float MU = 0.25f;
 
 // ------------------------------------------------------------------ generic tcgen05 GEMM
 // C^T += A B^T: A (M x K) and B (N x K) bf16 row-major (K contiguous), C stored column-major
@@ -381,23 +381,63 @@ __global__ void k_cgram2_sum(const float2* part, int nchunk, float2* PG) {
     sx += v.x;
     sy += v.y;
   }
-  PG[(long long)smp * 2 * NS * NS + i] = make_float2((float)sx, (float)sy);
+  PG[(long long)smp * 3 * NS * NS + i] = make_float2((float)sx, (float)sy);
 }
 
-// loss per sample = tr(G) - ||P||^2 + mu ||G - I||^2 (scaled); one block per sample
+// R = polar factor of P (P = R H, R unitary) by Newton-Schulz, Y <- Y (3I - Y^H Y) / 2 from
+// Y0 = P / ||P||_F; one 1024-thread block per sample, R stored after P and G.
+__global__ void __launch_bounds__(1024) k_polar(float2* PG, int iters) {
+  __shared__ float2 Y[NS][NS + 1], T[NS][NS + 1];
+  __shared__ float red[32];
+  const int smp = blockIdx.x;
+  float2* P = PG + (long long)smp * 3 * NS * NS;
+  float2* R = P + 2 * NS * NS;
+  const int a = threadIdx.x % NS, b = threadIdx.x / NS;
+  const float2 p = P[a + b * NS];
+  float n2 = p.x * p.x + p.y * p.y;
+  for (int o = 16; o > 0; o >>= 1) n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = n2;
+  __syncthreads();
+  float fro = 0.f;
+  for (int k = 0; k < 32; ++k) fro += red[k];
+  fro = sqrtf(fro);
+  Y[a][b] = fro > 0.f ? make_float2(p.x / fro, p.y / fro) : make_float2(a == b ? 1.f : 0.f, 0.f);
+  __syncthreads();
+  for (int it = 0; it < iters; ++it) {
+    float2 g = make_float2(0.f, 0.f);
+    for (int k = 0; k < NS; ++k) {
+      const float2 u = Y[k][a], v = Y[k][b];
+      g.x += u.x * v.x + u.y * v.y;
+      g.y += u.x * v.y - u.y * v.x;
+    }
+    T[a][b] = make_float2((a == b ? 3.f : 0.f) - g.x, -g.y);
+    __syncthreads();
+    float2 y = make_float2(0.f, 0.f);
+    for (int k = 0; k < NS; ++k) {
+      const float2 u = Y[a][k], v = T[k][b];
+      y.x += u.x * v.x - u.y * v.y;
+      y.y += u.x * v.y + u.y * v.x;
+    }
+    __syncthreads();
+    Y[a][b] = make_float2(0.5f * y.x, 0.5f * y.y);
+    __syncthreads();
+  }
+  R[a + b * NS] = Y[a][b];
+}
+
+// loss per sample = ||X - A R||^2 = tr(G) - 2 Re tr(R^H P) + NS (scaled); one block per sample
 __global__ void k_loss(const float2* PG, int nsamp, float scale, float* loss) {
   __shared__ float red[256];
   const int smp = blockIdx.x;
-  const float2* P = PG + (long long)smp * 2 * NS * NS;
+  const float2* P = PG + (long long)smp * 3 * NS * NS;
   const float2* G = P + NS * NS;
+  const float2* R = P + 2 * NS * NS;
   float acc = 0.f;
   for (int i = threadIdx.x; i < NS * NS; i += blockDim.x) {
     const int a = i % NS, b = i / NS;
-    const float2 p = P[i], g = G[i];
-    acc -= p.x * p.x + p.y * p.y;
-    if (a == b) acc += g.x;
-    const float gr = g.x - (a == b ? 1.f : 0.f);
-    acc += MU * (gr * gr + g.y * g.y);
+    const float2 p = P[i], r = R[i];
+    acc -= 2.f * (r.x * p.x + r.y * p.y);
+    if (a == b) acc += G[i].x + 1.f;
   }
   red[threadIdx.x] = acc;
   __syncthreads();
@@ -408,57 +448,58 @@ __global__ void k_loss(const float2* PG, int nsamp, float scale, float* loss) {
   if (threadIdx.x == 0) atomicAdd(loss, red[0] * scale);
 }
 
-// dL/dX -> dO (bf16, [M][NO] and [NO][M]) and db3 (atomics): G_X = 2 (X - A P) + 4 mu X (G - I),
+// dL/dX -> dO (bf16, [M][NO] and [NO][M]) and db3 (atomics): G_X = 2 (X - A R),
 // dO[(s,c) re] = Re(conj(GX) car_c), dO[(s,c) im] = -Im(conj(GX) car_c); all scaled by `scale`.
 __global__ void __launch_bounds__(128) k_dout(const float2* A, const float2* X, const float2* PG, const float2* CAR,
                                               long long M, int rows, float scale, bf16* dO, bf16* dOT, float* db3) {
-  __shared__ float2 Ps[NS * NS], Gs[NS * NS];
+  __shared__ float2 Rs[NS * NS];
   __shared__ float dbs[NO];
   const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  // all rows of this block belong to one sample when rows % blockDim == 0; handle generally
   const long long mfirst = (long long)blockIdx.x * blockDim.x;
   const int smp = (int)(mfirst / rows);
-  const float2* P = PG + (long long)smp * 2 * NS * NS;
-  for (int i = threadIdx.x; i < NS * NS; i += blockDim.x) {
-    Ps[i] = P[i];
-    Gs[i] = P[NS * NS + i];
-  }
+  const float2* R = PG + (long long)smp * 3 * NS * NS + 2 * NS * NS;
+  for (int i = threadIdx.x; i < NS * NS; i += blockDim.x) Rs[i] = R[i];
   for (int i = threadIdx.x; i < NO; i += blockDim.x) dbs[i] = 0.f;
   __syncthreads();
-  const bool act = m < M && (m / rows) == smp;
-  if (act) {
-    float2 x[NS], a[NS];
-    for (int s = 0; s < NS; ++s) {
-      x[s] = X[(long long)s * M + m];
-      a[s] = A[(long long)s * M + m];
+  // a block covers rows of at most two samples (rows >= blockDim): pass 1 handles the second
+  for (int pass = 0; pass < 2; ++pass) {
+    const int sm = smp + pass;
+    const bool act = m < M && (m / rows) == sm;
+    if (pass == 1) {
+      __syncthreads();
+      const long long mlast = min(M, mfirst + (long long)blockDim.x) - 1;
+      if (mlast / rows == smp) break;
+      const float2* R2 = PG + (long long)sm * 3 * NS * NS + 2 * NS * NS;
+      for (int i = threadIdx.x; i < NS * NS; i += blockDim.x) Rs[i] = R2[i];
+      __syncthreads();
     }
-    float2 car[NCAR];
-    for (int c = 0; c < NCAR; ++c) car[c] = CAR[(long long)c * M + m];
-    for (int s = 0; s < NS; ++s) {
-      float2 ap = make_float2(0.f, 0.f), xg = make_float2(0.f, 0.f);
-      for (int t = 0; t < NS; ++t) {
-        const float2 p = Ps[t + s * NS];
-        const float2 g = Gs[t + s * NS];
-        ap.x += a[t].x * p.x - a[t].y * p.y;
-        ap.y += a[t].x * p.y + a[t].y * p.x;
-        const float gr = g.x - (t == s ? 1.f : 0.f);
-        xg.x += x[t].x * gr - x[t].y * g.y;
-        xg.y += x[t].x * g.y + x[t].y * gr;
-      }
-      const float gx = scale * (2.f * (x[s].x - ap.x) + 4.f * MU * xg.x);
-      const float gy = scale * (2.f * (x[s].y - ap.y) + 4.f * MU * xg.y);
-      for (int c = 0; c < NCAR; ++c) {
-        // conj(g) * car
-        const float re = gx * car[c].x + gy * car[c].y;
-        const float im = gx * car[c].y - gy * car[c].x;
-        const int o = (s * NCAR + c) * 2;
-        const bf16 bre = __float2bfloat16(re), bim = __float2bfloat16(-im);
-        dO[m * NO + o] = bre;
-        dO[m * NO + o + 1] = bim;
-        dOT[(long long)o * M + m] = bre;
-        dOT[(long long)(o + 1) * M + m] = bim;
-        atomicAdd(&dbs[o], re);
-        atomicAdd(&dbs[o + 1], -im);
+    if (act) {
+      float2 a[NS];
+      for (int s = 0; s < NS; ++s) a[s] = A[(long long)s * M + m];
+      float2 car[NCAR];
+      for (int c = 0; c < NCAR; ++c) car[c] = CAR[(long long)c * M + m];
+      for (int s = 0; s < NS; ++s) {
+        float2 ar = make_float2(0.f, 0.f);
+        for (int t = 0; t < NS; ++t) {
+          const float2 r = Rs[t + s * NS];
+          ar.x += a[t].x * r.x - a[t].y * r.y;
+          ar.y += a[t].x * r.y + a[t].y * r.x;
+        }
+        const float2 x = X[(long long)s * M + m];
+        const float gx = scale * 2.f * (x.x - ar.x);
+        const float gy = scale * 2.f * (x.y - ar.y);
+        for (int c = 0; c < NCAR; ++c) {
+          const float re = gx * car[c].x + gy * car[c].y;
+          const float im = gx * car[c].y - gy * car[c].x;
+          const int o = (s * NCAR + c) * 2;
+          const bf16 bre = __float2bfloat16(re), bim = __float2bfloat16(-im);
+          dO[m * NO + o] = bre;
+          dO[m * NO + o + 1] = bim;
+          dOT[(long long)o * M + m] = bre;
+          dOT[(long long)(o + 1) * M + m] = bim;
+          atomicAdd(&dbs[o], re);
+          atomicAdd(&dbs[o + 1], -im);
+        }
       }
     }
   }
@@ -688,7 +729,7 @@ size_t work_bytes(long long M) {
   b += (size_t)M * NO * 4;              // OT
   b += (size_t)M * NS * 8 * 2;          // X, Tt
   b += (size_t)M * NCAR * 8;            // CARb
-  b += 64 * 64 * 2 * NS * NS * 8 + 64 * 2 * NS * NS * 8 + 64 * 256;
+  b += 64 * 64 * 2 * NS * NS * 8 + 64 * 3 * NS * NS * 8 + 64 * 256;
   return b;
 }
 
@@ -719,7 +760,7 @@ Work carve(char* p, long long M) {
   w.Tt = (float2*)take((size_t)M * NS * 8);
   w.CARb = (float2*)take((size_t)M * NCAR * 8);
   w.part = (float2*)take((size_t)64 * 64 * 2 * NS * NS * 8);
-  w.PG = (float2*)take((size_t)64 * 2 * NS * NS * 8);
+  w.PG = (float2*)take((size_t)64 * 3 * NS * NS * 8);
   return w;
 }
 
@@ -768,6 +809,8 @@ int loss_backward(wtbg_net* net, Work& w, int nsamp, long long rows, float* loss
   k_cgram2<<<dim3(nchunk, nsamp), 256, 0, s>>>(w.Tt, w.X, M, (int)rows, nchunk, w.part);
   WTBG_COUNT(ctx, 1);
   k_cgram2_sum<<<dim3((2 * NS * NS + 255) / 256, nsamp), 256, 0, s>>>(w.part, nchunk, w.PG);
+  WTBG_COUNT(ctx, 1);
+  k_polar<<<nsamp, 1024, 0, s>>>(w.PG, 40);
   WTBG_COUNT(ctx, 1);
   float* dloss = net->loss.as<float>();
   CK(cudaMemsetAsync(dloss, 0, 4, s));

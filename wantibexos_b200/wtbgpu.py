@@ -27,7 +27,8 @@ EXPORTS = ["wtbg_create", "wtbg_destroy", "wtbg_error_string", "wtbg_last_error"
            "wtbg_bse_spectrum_fast", "wtbg_set_fast_product", "wtbg_bse_apply", "wtbg_net_create",
            "wtbg_net_destroy", "wtbg_net_num_params", "wtbg_net_get_params", "wtbg_net_set_params",
            "wtbg_net_features", "wtbg_net_add_sample", "wtbg_net_num_samples", "wtbg_net_train",
-           "wtbg_net_eval_loss", "wtbg_net_predict", "wtbg_net_loss_grad", "wtbg_gemm_bf16"]
+           "wtbg_net_eval_loss", "wtbg_net_predict", "wtbg_net_loss_grad", "wtbg_gemm_bf16",
+           "wtbg_bse_build_q"]
 
 
 class WtbgError(RuntimeError):
@@ -39,7 +40,8 @@ class WtbgError(RuntimeError):
 class Stats(C.Structure):
     _fields_ = [("launches", C.c_longlong), ("hemv_launches", C.c_longlong), ("hemv_ms", C.c_double),
                 ("hemv_bytes", C.c_double), ("build_launches", C.c_longlong), ("build_ms", C.c_double),
-                ("build_bytes", C.c_double)]
+                ("build_bytes", C.c_double), ("fast_launches", C.c_longlong), ("fast_ms", C.c_double),
+                ("fast_bytes", C.c_double), ("dav_fast_iters", C.c_longlong), ("dav_fp64_iters", C.c_longlong)]
 
 
 class Coulomb(C.Structure):
@@ -102,6 +104,7 @@ def load_library(path: str = LIB_PATH):
         "wtbg_net_predict": (C.c_int, [P, dp, dp]),
         "wtbg_net_loss_grad": (C.c_int, [P, C.c_int, C.c_longlong, fp, fp, fp, fp, fp]),
         "wtbg_bse_apply": (C.c_int, [P, C.c_int, dp, dp]),
+        "wtbg_bse_build_q": (C.c_int, [P, C.c_int, dp, dp, C.POINTER(Coulomb)]),
         "wtbg_gemm_bf16": (C.c_int, [P, C.c_int, C.c_int, C.c_int, fp, fp, fp]),
         "wtbg_spectrum_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, ip, ip, C.c_double,
                                             C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
@@ -325,6 +328,11 @@ class Context:
                                            float(ebse0), float(ebsef), float(numbse), float(sme),
                                            int(bool(renorm)), float(spinf), _dp(om), _fp(eps)))
         return om, eps
+
+    def bse_build_q(self, kptq, q4, coul: Coulomb) -> None:
+        kq = _f64(kptq)
+        q = np.ascontiguousarray(np.asarray(q4, dtype=np.float64))
+        self._check(self.lib.wtbg_bse_build_q(self.h, kq.shape[0], _dp(kq), _dp(q), C.byref(coul)))
 
     def bse_q_eigenvalues(self, kptq, q4, coul: Coulomb):
         kq = _f64(kptq)
