@@ -14,6 +14,11 @@ broadened eps(omega) of the BSE and single-particle spectra.
          tridiagonalisation) timed per launch with CUDA events inside the timed steps
   cpu_baseline  the CPU oracle (numpy restatement of the reference, LAPACK ZHEEV with the
          reference's minimum workspace) on bounded samples of the same workload, scaled
+  fast_form  the same deck's time-to-spectrum by the fast form (block Davidson on the
+         split-BF16 tensor-core product with an FP64 polish to residual 1e-6 eV for the 32
+         lowest excitons, Haydock recursion for eps(omega)), with its error against the plain
+         FP64 step of the same run (lowest-32 energies in meV, eps2 at its peaks) and the
+         roofline of the tensor-core product
 
 Multi-GPU: the dense solve of one deck does not shard; --gpus N runs N independent
 replicas (one per rank) and reports the max over ranks.
@@ -164,8 +169,9 @@ class Clocks:
 
 
 # ----------------------------------------------------------------------------- device step
-def device_step(ctx, model, kpt, wl, c):
-    """One step with the model resident; returns device seconds per stage."""
+def device_step(ctx, model, kpt, wl, c, keep=None):
+    """One step with the model resident; returns device seconds per stage (and, when `keep`
+    is a dict, stores the lowest 32 exciton energies and the BSE eps2_xx there)."""
     t = {}
     ctx.bands(kpt, wl["nv"], wl["nc"], want_vectors=False)
     t["bands"] = ctx.last_ms
@@ -180,13 +186,54 @@ def device_step(ctx, model, kpt, wl, c):
     E = f154(W)
     F = f154(act[:, :6])
     ng = [wl["n"], wl["n"], 1]
-    ctx.spectrum(E, F, ng, vcell3d(model.rlat), 0.0, wl["ebsef"], float(wl["nespec"]), wl["cshift"], True, 2.0)
+    _, eps = ctx.spectrum(E, F, ng, vcell3d(model.rlat), 0.0, wl["ebsef"], float(wl["nespec"]), wl["cshift"], True,
+                          2.0)
     t["spectrum_bse"] = ctx.last_ms
+    if keep is not None:
+        keep["W32"] = W[:32].copy()
+        keep["eps2"] = eps[:, 1, 0].astype(np.float64)
     Es = f154(sp[:, 6].astype(np.float64))
     Fs = f154(sp[:, 7:13].astype(np.float64))
     ctx.spectrum(Es, Fs, ng, vcell3d(model.rlat), 0.0, wl["ebsef"], float(wl["nespec"]), wl["cshift"], True, 2.0)
     t["spectrum_sp"] = ctx.last_ms
     return {k: v / 1e3 for k, v in t.items()}
+
+
+def fast_step(ctx, model, kpt, wl, c):
+    """The fast form of the same step: bands, velocities, build, block Davidson for the 32
+    lowest excitons (tensor-core product, FP64 polish to residual 1e-6 eV), the highest
+    exciton (residual 1e-3 eV, it only sets the broadening rule), and eps(omega) by the Haydock
+    recursion (150 steps). Returns (device seconds per stage, W32, eps2_xx, Davidson stats)."""
+    t = {}
+    ctx.bands(kpt, wl["nv"], wl["nc"], want_vectors=False)
+    t["bands"] = ctx.last_ms
+    ctx.velocity(wl["cshift"], want=False)
+    t["velocity"] = ctx.last_ms
+    ctx.bse_build(c)
+    t["build"] = ctx.last_ms
+    ctx.set_fast_product(1)
+    try:
+        W, _, _, it, res = ctx.bse_davidson(32, nb=40, tol=1e-6, want_act=False)
+        t["davidson"] = ctx.last_ms
+        st = ctx.stats()
+        dav = {"iters": it, "tensor_core_iters": st["dav_fast_iters"], "fp64_iters": st["dav_fp64_iters"],
+               "max_residual_eV": res}
+        top = ctx.bse_davidson(1, nb=8, largest=True, tol=1e-3, want_act=False)[0][0]
+        t["davidson_top"] = ctx.last_ms
+        _, eps = ctx.bse_spectrum_fast(150, W[0], top, [wl["n"], wl["n"], 1], vcell3d(model.rlat), 0.0, wl["ebsef"],
+                                       float(wl["nespec"]), wl["cshift"], True, 2.0)
+        t["haydock"] = ctx.last_ms
+    finally:
+        ctx.set_fast_product(0)
+    return {k: v / 1e3 for k, v in t.items()}, W, eps[:, 1, 0].astype(np.float64), dav
+
+
+def peak_rel_error(ref, x):
+    """max |x - ref| at the local maxima of ref, relative to max |ref|."""
+    pk = np.where((ref[1:-1] > ref[:-2]) & (ref[1:-1] >= ref[2:]))[0] + 1
+    if len(pk) == 0:
+        pk = np.array([int(np.argmax(ref))])
+    return float(np.abs(x[pk] - ref[pk]).max() / np.abs(ref).max())
 
 
 def e2e_run(workdir, wl):
@@ -310,6 +357,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=os.environ.get("WTB_BENCH_WORKLOAD", "c2"), choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", default="both", choices=["both", "plain", "fast"],
+                    help="plain FP64 path (the headline), the fast form, or both (default)")
     ap.add_argument("--device-only", action="store_true",
                     help="only the device-resident steps (no e2e run, no CPU baseline): profiling captures")
     args = ap.parse_args()
@@ -358,7 +407,7 @@ def main():
     ctx.set_model(model)
     kpt = kmesh(wl["n"], model.rlat)
     c = wtbgpu.coulomb_params("V2DRK", [wl["n"], wl["n"], 1], 1e-3, [1, 1, 1], 1.0, 1.0, 0.0, wl["r0"])
-    for _ in range(args.warmup):
+    for _ in range(args.warmup if args.form != "fast" else 0):
         device_step(ctx, model, kpt, wl, c)
     if dist:
         dist.barrier()
@@ -367,17 +416,46 @@ def main():
     ctx.reset_stats()
     ctx.set_profiling(True)
     steps = []
-    for _ in range(args.steps):
-        steps.append(device_step(ctx, model, kpt, wl, c))
+    keep = {}
+    if args.form != "fast":
+        for _ in range(args.steps):
+            steps.append(device_step(ctx, model, kpt, wl, c, keep))
     ctx.set_profiling(False)
     st = ctx.stats()
     ck = clocks.stop()
-    per_step = [sum(s.values()) for s in steps]
+    per_step = [sum(s.values()) for s in steps] or [float("nan")]
     t_dev = float(np.mean(per_step))
+    fast = None
+    if args.form != "plain":
+        # fast form: untimed warm-up steps, then the timed steps with the product timed per launch
+        for _ in range(max(1, args.warmup)):
+            fast_step(ctx, model, kpt, wl, c)
+        ctx.reset_stats()
+        ctx.set_profiling(True)
+        fsteps = []
+        for _ in range(args.steps):
+            fsteps.append(fast_step(ctx, model, kpt, wl, c))
+        ctx.set_profiling(False)
+        fst = ctx.stats()
+        t_fast = float(np.mean([sum(s[0].values()) for s in fsteps]))
+        _, W32, eps2, dav = fsteps[-1]
+        hbm = float(json.load(open(PEAKS_PATH)).get("hbm_gbs", 6650.0)) if os.path.exists(PEAKS_PATH) else 6650.0
+        fgbs = fst["fast_bytes"] / (fst["fast_ms"] / 1e3) / 1e9 if fst["fast_ms"] > 0 else None
+        fast = {"time_to_spectrum_s": t_fast, "stages_s": fsteps[-1][0], "davidson": dav,
+                "gpu_launches": int(fst["launches"] / max(1, args.steps)),
+                "roofline": {"kernel": "split-BF16 tensor-core product Y = H X (k_fastprod)", "bound": "hbm",
+                             "achieved": fgbs, "peak": hbm, "unit": "GB/s", "frac": (fgbs / hbm) if fgbs else None,
+                             "algorithmic_bytes": "8 B x N^2 per product (bf16 hi/lo planes of Re H and Im H)",
+                             "launches": fst["fast_launches"],
+                             "avg_launch_ms": fst["fast_ms"] / max(1, fst["fast_launches"])}}
+        if keep:
+            fast["speedup_vs_plain_fp64"] = t_dev / t_fast
+            fast["dW32_meV"] = float(np.abs(W32 - keep["W32"]).max() * 1e3)
+            fast["eps2_peak_rel_err"] = peak_rel_error(keep["eps2"], eps2)
     ctx.close()
     if args.device_only:
-        print(json.dumps({"metric": metric, "value": t_dev, "unit": unit, "stages_s": steps[-1],
-                          "config": cfg, "device_only": True}))
+        print(json.dumps({"metric": metric, "value": t_dev, "unit": unit, "stages_s": steps[-1] if steps else None,
+                          "fast_form": fast, "config": cfg, "device_only": True}))
         return
     # e2e through the deck-level C entry (host buffers, files)
     workdir = tempfile.mkdtemp(prefix="wtb_bench_")
@@ -425,6 +503,7 @@ def main():
                                       "algorithmic_bytes": "16 B x N(N+1)/2 (lower triangle written once)"}},
         "gpu_launches": int(st["launches"] / max(1, args.steps)),
         "clocks": ck,
+        "fast_form": fast,
     }
     if not args.no_cpu_baseline:
         v, parts, sizes = cpu_baseline(wl, model)
