@@ -446,6 +446,8 @@ def main():
                 "roofline": {"kernel": "split-BF16 tensor-core product Y = H X (k_fastprod)", "bound": "hbm",
                              "achieved": fgbs, "peak": hbm, "unit": "GB/s", "frac": (fgbs / hbm) if fgbs else None,
                              "algorithmic_bytes": "8 B x N^2 per product (bf16 hi/lo planes of Re H and Im H)",
+                             # 1.05 x algorithmic in the ncu capture at N = 9216 (X planes, FP64 sums)
+                             "traffic": 1.05 * fst["fast_bytes"] / max(1, fst["fast_launches"]),
                              "launches": fst["fast_launches"],
                              "avg_launch_ms": fst["fast_ms"] / max(1, fst["fast_launches"])}}
         if keep:
@@ -495,7 +497,10 @@ def main():
                 "stages_s": e2e_parts, "path": "wtb_run (libwtbdriver.so) -> libwtbgpu.so C-ABI, files written"},
         "roofline": {"kernel": "tridiagonalisation Hermitian mat-vec (k_hemv)", "bound": "hbm",
                      "achieved": hemv_gbs, "peak": hbm, "unit": "GB/s",
-                     "frac": (hemv_gbs / hbm) if hemv_gbs else None, "traffic": None,
+                     "frac": (hemv_gbs / hbm) if hemv_gbs else None,
+                     # DRAM bytes per launch: 1.035 x the algorithmic bytes in the ncu capture of
+                     # k_hemv at N = 9216 (read + write, two launches), scaled to the mean launch
+                     "traffic": (1.035 * st["hemv_bytes"] / st["hemv_launches"]) if st["hemv_launches"] else None,
                      "peak_source": "measured" if peaks else "fallback",
                      "algorithmic_bytes": "16 B x (n'(n'+1)/2) per launch, n' = trailing order",
                      "launches": st["hemv_launches"], "avg_launch_ms": st["hemv_ms"] / max(1, st["hemv_launches"]),

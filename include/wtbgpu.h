@@ -143,6 +143,33 @@ int wtbg_bse_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter,
                       const double* X0, int dtfull, int cpol, double* W, double* act, double* X,
                       int* iters, double* maxres);
 
+/* ---- eigsys for every band (hamiltonian_tb.f90:2-137 as the band-structure and DOS tools
+ *      call it: bands-kpath-tool.f90:66-80, tdos-tool.f90:98-120): eig (nk, w) ascending with
+ *      the scissors scs on the states above E_F, vec (nk, w, w) complex(8) = component m of
+ *      band n at k (component 1 real, as ZHEEV('V','L')) or NULL, nocp (nk) or NULL.  Leaves
+ *      the BSE state of the context alone. */
+int wtbg_eigsys(wtbg_ctx* ctx, int nk, const double* kpt, double* eig, double* vec, int* nocp);
+
+/* ---- DOS smearing of the DOS tool (endos, dos_subs.f90:102-152; gaussian,
+ *      general_subs.f90:471-487): out(e, c) = (1/nkpt) sum_i weights(i, c) g(en(e) - etb(i)),
+ *      g(x) = exp(-x^2 / (2 sme^2)) / (sme sqrt(2 pi)) with pi = acos(-1.) in real(4);
+ *      weights (ndim, ncol) column-major, 1 <= ncol <= 4; out (nw, ncol). */
+int wtbg_dos(wtbg_ctx* ctx, long long ndim, const double* etb, const double* weights, int ncol, long long nkpt,
+             int nw, const double* en, double sme, double* out);
+
+/* ---- temperature BSE (BSET=T / BSET_BND=T): with on = 1 every later call uses the
+ *      occupation factor f_i = f_v - f_c (Fermi-Dirac, E_F = 0, kB = 8.617330350E-5 eV/K,
+ *      T = 0 taken as 1E-8 K; fermidisteh, general_subs.f90:607-635) of each basis state:
+ *      the kernel build scales the interaction part of the reference's upper-triangle row i
+ *      by f_i (matrizelbsetemp, bse_subs_temp.f90:2-126; matrizelbsekqtemp :128-337), the
+ *      sp table multiplies the strengths by f_i (bse_solver-tool-diel-temp.f90:416-423), and
+ *      wtbg_bse_solve returns act = Re[(A^T h1) conj(A^T (h2 f))] (dielbseptemp,
+ *      bse_subs_temp.f90:340-395).  The temperature gap correction (TA= VE/BE, gapcortemp /
+ *      gapcortemp2) is a scissors shift the caller adds to scs in wtbg_set_model.  The fast
+ *      form (wtbg_bse_spectrum_fast, oscillators of wtbg_bse_davidson) has no temperature
+ *      form and returns WTBG_ERR_UNSUPPORTED while it is on. */
+int wtbg_set_temperature(wtbg_ctx* ctx, int on, double temp);
+
 /* ---- product used by the fast form (wtbg_bse_davidson, wtbg_bse_spectrum_fast, wtbg_bse_apply).
  *      mode 0: FP64 on CUDA cores (the lower triangle of H read once per product).
  *      mode 1: split-BF16 tensor-core product: the off-diagonal part of H is stored once per

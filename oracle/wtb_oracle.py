@@ -285,21 +285,24 @@ def optsp_all(model, kpts, eigv, vec, nv, nc, sme):
     return h
 
 
-def sp_table(kpts, eigv, nocp, h, nv, nc):
+def sp_table(kpts, eigv, nocp, h, nv, nc, fdeh=None):
     """vecres (N,15) real(4) rows (bse_solver-tool-diel.f90:379-393) sorted by column 7
-    with the stable bubble sort Bubblem (general_subs.f90:405-440)."""
+    with the stable bubble sort Bubblem (general_subs.f90:405-440). With ``fdeh`` the
+    strengths are multiplied by f_v - f_c (bse_solver-tool-diel-temp.f90:416-423)."""
     stt = quantumnumbers2(kpts.shape[0], nc, nv)
     N = stt.shape[0]
     vr = np.zeros((N, 15), dtype=np.float32)
     for i in range(N):
         v, c, k = stt[i, 1] - 1, stt[i, 2] - 1, stt[i, 3] - 1
         hx, hy, hz, hp, hm = h[i]
+        s = [(hx * hx.conjugate()).real, (hy * hy.conjugate()).real,
+             (hz * hz.conjugate()).real, (hx * hy.conjugate()).real,
+             (hx * hz.conjugate()).real, (hy * hz.conjugate()).real,
+             (hp * hp.conjugate()).real, (hm * hm.conjugate()).real]
+        if fdeh is not None:
+            s = [x * fdeh[i] for x in s]
         vr[i] = [kpts[k, 0], kpts[k, 1], kpts[k, 2], nocp[k], nocp[k] - nv + c + 1,
-                 nocp[k] - nv + v + 1, eigv[k, c] - eigv[k, v],
-                 (hx * hx.conjugate()).real, (hy * hy.conjugate()).real,
-                 (hz * hz.conjugate()).real, (hx * hy.conjugate()).real,
-                 (hx * hz.conjugate()).real, (hy * hz.conjugate()).real,
-                 (hp * hp.conjugate()).real, (hm * hm.conjugate()).real]
+                 nocp[k] - nv + v + 1, eigv[k, c] - eigv[k, v]] + s
     order = np.argsort(vr[:, 6], kind="stable")
     return vr[order]
 
@@ -413,7 +416,7 @@ def coulomb(p: CoulombParams, dk):
 
 # ----------------------------------------------------------------------------- BSE
 
-def bse_matrix(p: CoulombParams, kpts, eigv, vec, nv, nc, upper_only=True):
+def bse_matrix(p: CoulombParams, kpts, eigv, vec, nv, nc, upper_only=True, fdeh=None):
     """matrizelbse over j >= i (bse_subs.f90:2-124, loop bse_solver-tool-diel.f90:431-458).
     Off-diagonal: V(k_i - k_j) * <c_i|c_j> * <v_i|v_j> with <a|b> = sum conj(a) b.
     Diagonal: (E_c - E_v) + V(0).  Returns the N x N matrix with the upper triangle set."""
@@ -431,13 +434,19 @@ def bse_matrix(p: CoulombParams, kpts, eigv, vec, nv, nc, upper_only=True):
     H = H.reshape(N, N)
     de = (eigv[:, nv:][:, :, None] - eigv[:, :nv][:, None, :]).reshape(N)
     vdiag = np.repeat(np.diag(V), ncv)
-    H[np.diag_indices(N)] = de + vdiag
+    if fdeh is None:
+        H[np.diag_indices(N)] = de + vdiag
+    else:
+        # matrizelbsetemp (bse_subs_temp.f90:2-126): element (i, j >= i) times f_i, plus dE on i = j
+        H[np.diag_indices(N)] = vdiag
+        H = H * np.asarray(fdeh)[:, None]
+        H[np.diag_indices(N)] += de
     if upper_only:
         H = np.triu(H)
     return H
 
 
-def bse_matrix_q(p: CoulombParams, q4, kpts, energy, vector, energyq, vectorq, nv, nc):
+def bse_matrix_q(p: CoulombParams, q4, kpts, energy, vector, energyq, vectorq, nv, nc, fdeh=None):
     """matrizelbsekq (bse_subs_kpath.f90:1-208) over j >= i: the Q != 0 kernel adds the
     exchange term -V(Q) <c_{k+Q}|v_k> <v_{k'}|c_{k'+Q}> (zero when |Q| == 0, :116)."""
     nk = kpts.shape[0]
@@ -451,7 +460,10 @@ def bse_matrix_q(p: CoulombParams, q4, kpts, energy, vector, energyq, vectorq, n
     H = (V[:, None, None, :, None, None] * Mc[:, :, None, :, :, None]) * Mv[:, None, :, :, None, :]
     H = H.reshape(N, N)
     de = (energyq[:, nv:][:, :, None] - energy[:, :nv][:, None, :]).reshape(N)
-    H[np.diag_indices(N)] = de + np.repeat(np.diag(V), ncv)
+    if fdeh is None:
+        H[np.diag_indices(N)] = de + np.repeat(np.diag(V), ncv)
+    else:
+        H[np.diag_indices(N)] = np.repeat(np.diag(V), ncv)
     modq = math.sqrt(q4[1] ** 2 + q4[2] ** 2 + q4[3] ** 2)
     if modq != 0.0:
         vq = float(coulomb(p, np.array([q4[1], q4[2], q4[3]])))
@@ -461,6 +473,10 @@ def bse_matrix_q(p: CoulombParams, q4, kpts, energy, vector, energyq, vectorq, n
         vcv = np.einsum("kcm,kvm->kcv", cq.conj(), vk).reshape(N)
         vvc = np.einsum("kvm,kcm->kcv", vk.conj(), cq).reshape(N)
         H = H - vq * (vcv[:, None] * vvc[None, :])
+    if fdeh is not None:
+        # matrizelbsekqtemp (bse_subs_temp.f90:128-337): the interaction part times f_i
+        H = H * np.asarray(fdeh)[:, None]
+        H[np.diag_indices(N)] += de
     return np.triu(H)
 
 
@@ -476,23 +492,36 @@ def dielbsep(A, h1, h2):
     return (s1 * s2.conj()).real
 
 
-def bse_solve(p: CoulombParams, kpts, eigv, vec, h, nv, nc, dtfull, cpol, want_vectors=False):
-    """bse_solver-tool-diel.f90:431-602: build, ZHEEV('V','U'), oscillator strengths.
+def dielbseptemp(A, h1, h2, f):
+    """bse_subs_temp.f90:340-395: act(i) = Re[(sum A h1) * conj(sum A h2 f)]."""
+    s1, s2 = A.T @ h1, A.T @ (h2 * f)
+    return (s1 * s2.conj()).real
+
+
+def bse_solve(p: CoulombParams, kpts, eigv, vec, h, nv, nc, dtfull, cpol, want_vectors=False, fdeh=None):
+    """bse_solver-tool-diel.f90:431-602 (bse_solver-tool-diel-temp.f90:470-620 with ``fdeh``):
+    build, ZHEEV('V','U'), oscillator strengths.
     Returns W (N,), act (N, 8) = xx, yy, zz, xy, xz, yz, sp, sm [, A]."""
-    H = bse_matrix(p, kpts, eigv, vec, nv, nc)
+    H = bse_matrix(p, kpts, eigv, vec, nv, nc, fdeh=fdeh)
     W, A = zheev(H, lower=0)
     N = W.shape[0]
     act = np.zeros((N, 8))
-    act[:, 0] = dielbsev(A, h[:, 0])
-    act[:, 1] = dielbsev(A, h[:, 1])
-    act[:, 2] = dielbsev(A, h[:, 2])
+    if fdeh is None:
+        sv = lambda a: dielbsev(A, h[:, a])
+        sp = lambda a, b: dielbsep(A, h[:, a], h[:, b])
+    else:
+        sv = lambda a: dielbseptemp(A, h[:, a], h[:, a], fdeh)
+        sp = lambda a, b: dielbseptemp(A, h[:, a], h[:, b], fdeh)
+    act[:, 0] = sv(0)
+    act[:, 1] = sv(1)
+    act[:, 2] = sv(2)
     if dtfull:
-        act[:, 3] = dielbsep(A, h[:, 0], h[:, 1])
-        act[:, 4] = dielbsep(A, h[:, 0], h[:, 2])
-        act[:, 5] = dielbsep(A, h[:, 1], h[:, 2])
+        act[:, 3] = sp(0, 1)
+        act[:, 4] = sp(0, 2)
+        act[:, 5] = sp(1, 2)
     if cpol:
-        act[:, 6] = dielbsev(A, h[:, 3])
-        act[:, 7] = dielbsev(A, h[:, 4])
+        act[:, 6] = sv(3)
+        act[:, 7] = sv(4)
     if want_vectors:
         return W, act, A
     return W, act
@@ -616,8 +645,61 @@ def exclft(sysdim, ngrid, rlat, fosc, enexc):
 
 # ----------------------------------------------------------------------------- drivers
 
+KB_F32 = float(np.float32(8.617330350e-5))   # kb of general_subs.f90:575 (a real(4) literal)
+
+
+def fermidisteh(ec, ev, temp):
+    """general_subs.f90:607-635: f_v - f_c, E_F = 0; T = 0 is replaced by 1E-8 (real(4))."""
+    t = float(np.float32(1e-8)) if temp == 0.0 else float(temp)
+    beta = 1.0 / (KB_F32 * t)
+    with np.errstate(over="ignore"):
+        fv = 1.0 / (np.exp(np.asarray(ev) * beta) + 1.0)
+        fc = 1.0 / (np.exp(np.asarray(ec) * beta) + 1.0)
+    return fv - fc
+
+
+def gapcortemp(st, phavg, temp):
+    """general_subs.f90:569-586 (Varshni-like form, doi 10.1063/1.104723)."""
+    aux1 = phavg / (2.0 * KB_F32 * temp)
+    return -st * phavg * ((1.0 / math.tanh(aux1)) - 1.0)
+
+
+def gapcortemp2(st, phavg, temp):
+    """general_subs.f90:588-605 (Bose-Einstein form)."""
+    return -((2.0 * st) / (math.exp(phavg / temp) - 1.0))
+
+
+def temperature_shift(deck):
+    """tcor of bse_solver-tool-diel-temp.f90:263-282 (TA= FA / VE / BE)."""
+    ta = deck["ta"].strip()
+    if ta == "VE":
+        return gapcortemp(deck["st"], deck["phavg"], deck["temp"])
+    if ta == "BE":
+        return gapcortemp2(deck["st"], deck["phavg"], deck["temp"])
+    return 0.0
+
+
+def fdeh_states(eigc, eigv, nv, nc, temp):
+    """f_v - f_c of every basis state in quantumnumbers2 order (k outer, c, v inner)."""
+    ec = eigc[:, nv:nv + nc][:, :, None]
+    ev = eigv[:, :nv][:, None, :]
+    return fermidisteh(np.broadcast_to(ec, (eigc.shape[0], nc, nv)),
+                       np.broadcast_to(ev, (eigc.shape[0], nc, nv)), temp).reshape(-1)
+
+
+def with_scs(model, scs):
+    import copy
+    m2 = copy.copy(model)
+    m2.scs = scs
+    return m2
+
+
 def run_bse(model, deck, want_vectors=False):
-    """The numbers of ``bsesolver`` (bse_solver-tool-diel.f90:2-660) for one deck dict."""
+    """The numbers of ``bsesolver`` (bse_solver-tool-diel.f90:2-660) for one deck dict, or of
+    ``bsesolvertemp`` (bse_solver-tool-diel-temp.f90) when BSET=T."""
+    temp = deck.get("bset", False)
+    if temp:
+        model = with_scs(model, model.scs + temperature_shift(deck))
     ngrid = list(deck["ngrid"])
     if deck["meshtype"].strip() == "RK2D":
         ngrid = rkmesh2d(deck["rk"], model.rlat)
@@ -629,16 +711,21 @@ def run_bse(model, deck, want_vectors=False):
     h = optsp_all(model, kpts, eigv, vec, nv, nc, deck["cshift"])
     p = CoulombParams(deck["coultype"], deck["ktol"], deck["ediel"], deck["lc"], deck["ez"],
                       deck["w"], deck["r0"], ngrid, model.rlat)
-    res = bse_solve(p, kpts, eigv, vec, h, nv, nc, deck["dtfull"], deck["cpol"], want_vectors)
+    fdeh = fdeh_states(eigv, eigv, nv, nc, deck["temp"]) if temp else None
+    res = bse_solve(p, kpts, eigv, vec, h, nv, nc, deck["dtfull"], deck["cpol"], want_vectors, fdeh=fdeh)
     out = dict(ngrid=ngrid, kpts=kpts, eigv=eigv, vec=vec, nocp=nocp, egap=egap, h=h,
-               W=res[0], act=res[1])
+               W=res[0], act=res[1], fdeh=fdeh)
     if want_vectors:
         out["A"] = res[2]
     return out
 
 
 def run_bsebnds(model, deck, ks, npts):
-    """The numbers of ``bsebnds`` (bse_kpath-tool.f90:3-479): exk (N, nQ) and the Q path."""
+    """The numbers of ``bsebnds`` (bse_kpath-tool.f90:3-479): exk (N, nQ) and the Q path; of
+    ``bsebndstemp`` (bse_kpath-tool-temp.f90) when BSET_BND=T."""
+    temp = deck.get("bsetbnd", False)
+    if temp:
+        model = with_scs(model, model.scs + temperature_shift(deck))
     ngrid = list(deck["ngrid"])
     if deck["meshtype"].strip() == "RK2D":
         ngrid = rkmesh2d(deck["rk"], model.rlat)
@@ -653,8 +740,97 @@ def run_bsebnds(model, deck, ks, npts):
         q4 = qpath[iq]
         qpt = monkhorst_pack(ngrid[0], ngrid[1], ngrid[2], deck["mshift"], model.rlat, q=q4[1:])
         energyq, vectorq, _, _ = bands(model, qpt, nv, nc)
-        H = bse_matrix_q(p, q4, kpts, energy, vector, energyq, vectorq, nv, nc)
+        fdeh = fdeh_states(energyq, energy, nv, nc, deck["temp"]) if temp else None
+        H = bse_matrix_q(p, q4, kpts, energy, vector, energyq, vectorq, nv, nc, fdeh=fdeh)
         w, info = lapack.zheev(np.asfortranarray(H), compute_v=0, lower=0,
                                lwork=max(2 * H.shape[0] - 1, 1))[0::2]
         exk.append(w)
     return np.array(exk).T, qpath, labels
+
+
+# ----------------------------------------------------------------------------- band and DOS tools
+
+def spin_diag(systype, dft, w):
+    """Diagonal of the Sz operator of spinvl (hamiltonian_tb.f90:281-368) / the up-down split of
+    spincont (dos_subs.f90:37-100): +1 up, -1 down (all +1 for NP in spinvl)."""
+    s = np.ones(w)
+    st = systype.strip()
+    w2 = w // 2
+    if st == "NP":
+        return s
+    if st == "SP" or (st == "SOC" and dft.strip() == "V"):
+        s[w2:] = -1.0
+    else:
+        s[1::2] = -1.0
+    return s
+
+
+def spinvl(wf, dft, systype):
+    return float(np.real(np.vdot(wf, spin_diag(systype, dft, len(wf)) * wf)))
+
+
+def spincont(wf, dft, systype):
+    if systype.strip() == "NP":
+        return 0.0, 0.0
+    s = spin_diag(systype, dft, len(wf))
+    a2 = np.abs(wf) ** 2
+    return float(a2[s > 0].sum()), float(a2[s < 0].sum())
+
+
+def layercont(wf, ow):
+    """dos_subs.f90:154-181."""
+    return float(np.real(np.sum(wf * np.asarray(ow) * wf.conj())))
+
+
+def gaussian(de, sme):
+    """general_subs.f90:471-487 (pi = acos(-1.) in real(4))."""
+    pi = float(np.float32(np.pi))
+    norm = 1.0 / (sme * math.sqrt(2.0 * pi))
+    return norm * np.exp(-1.0 * (de * de) / (2.0 * sme * sme))
+
+
+def bandstool(model, ks, npts, orbw=None, dft="V"):
+    """bands-kpath-tool.f90: rows (band, k) = real(4) of (distance, E, <Sz>, layer weight)."""
+    kp, labels = kpathbse(model.rlat, ks, npts)
+    w = model.w
+    ow = np.ones(w) if orbw is None else np.asarray(orbw)
+    out = np.zeros((w, kp.shape[0], 4), dtype=np.float32)
+    for j in range(kp.shape[0]):
+        e, U, _ = eigsys(model, kp[j, 1:])
+        for i in range(w):
+            out[i, j] = [kp[j, 0], e[i], spinvl(U[i], dft, model.systype), layercont(U[i], ow)]
+    return out, labels
+
+
+def dostool(model, ngrid, mshift, numdos, sme, orbw=None, dft="V"):
+    """tdos-tool.f90: the dos.dat columns (energy, tdos, sumdos, [updos, -dndos,] awdos)."""
+    kpts = monkhorst_pack(ngrid[0], ngrid[1], ngrid[2], mshift, model.rlat)
+    w = model.w
+    ow = np.ones(w) if orbw is None else np.asarray(orbw)
+    res = []
+    e0, e1 = 0.0, 0.0
+    for k in kpts:
+        e, U, _ = eigsys(model, k)
+        e0, e1 = min(e0, e[0]), max(e1, e[-1])
+        for i in range(w):
+            cu, cd = spincont(U[i], dft, model.systype)
+            res.append((e[i], 1.0, cu, cd, layercont(U[i], ow)))
+    res = np.array(res)
+    nw = int(numdos)
+    en = np.array([e0 + ((e1 - e0) * i) / (numdos - 1.0) for i in range(nw)])
+    g = gaussian(en[:, None] - res[None, :, 0], sme)
+    caux = 1.0 / kpts.shape[0]
+    cols = (g @ res[:, 1:]) * caux
+    np_ = model.systype.strip() == "NP"
+    spinf = 2.0 if np_ else 1.0
+    at, up, dn, aw = spinf * cols[:, 0], cols[:, 1], cols[:, 2], spinf * cols[:, 3]
+    dde = (e1 - e0) / (numdos - 1.0)
+    sums = np.zeros(nw)
+    s = 0.0
+    for i in range(nw):
+        sums[i] = s
+        if i > 0:
+            s = s + (dde * (at[i - 1] + at[i]) * 0.5)
+    if np_:
+        return np.column_stack([en, at, sums, aw])
+    return np.column_stack([en, at, sums, up, -dn, aw])

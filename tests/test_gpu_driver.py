@@ -125,3 +125,25 @@ KPATH_BSE= "{tmp_path}/kp.dat"
     assert got.shape == (N * 4, 2)
     assert np.abs(got[:, 1] - exk.reshape(-1)).max() < 1e-9
     assert np.array_equal(got[:4, 0].astype(np.float32), qpath[:, 0].astype(np.float32))
+
+
+def test_temperature_bse_run_files(tmp_path):
+    """BSET=T (bsesolvertemp): bse_opt_diel.dat and sp_optics.dat with the occupation factors
+    and the TA= VE scissors, the temperature line in log_bse-diel.dat, no lifetime files."""
+    m = synth.config_model("c1")
+    synth.write_params(m, str(tmp_path / "tb.dat"))
+    text = deck_for(tmp_path, "TEMP= 4000\nTA= VE\nST= 2.0\nPHAVG= 0.02\n").replace("BSE= T", "BSET= T")
+    run_deck(tmp_path, text)
+    deck = parse_deck(text)
+    ref = O.run_bse(m, deck)
+    got = rows(tmp_path / "bse_opt_diel.dat")
+    want = O.roundtrip_f154(np.column_stack([ref["W"], ref["act"][:, :6]]))
+    d = np.abs(got - want)
+    assert d.max() <= 1.0001e-4 and (d > 0).sum() <= 3
+    sp = O.sp_table(ref["kpts"], ref["eigv"], ref["nocp"], ref["h"], 2, 2, fdeh=ref["fdeh"])
+    got_sp = rows(tmp_path / "sp_optics.dat")
+    assert np.abs(got_sp - O.roundtrip_f154(sp[:, 6:13].astype(np.float64))).max() <= 1.0001e-4
+    log = open(tmp_path / "log_bse-diel.dat").read()
+    assert " temperature" in log
+    assert (tmp_path / "bse_diel_xx.dat").exists() and not (tmp_path / "exciton_lifetime.dat").exists()
+    assert "with temperature, finished" in open(tmp_path / "log.dat").read()

@@ -1,0 +1,89 @@
+"""Tools that share the per-k eigensolver (the next rows after the BSE path): eigsys for every
+band, the DOS smearing kernel, and the deck-level band-structure (BANDS=T) and DOS (DOS=T)
+runs against the CPU oracle."""
+import copy
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import wtb_oracle as O
+from wantibexos_b200 import build as B
+from wantibexos_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def test_eigsys_every_band_matches_oracle(gpu_ctx):
+    m = synth.config_model("c1")
+    kpts = O.monkhorst_pack(5, 5, 1, [0, 0, 0], m.rlat)
+    gpu_ctx.set_model(m)
+    e, v, no = gpu_ctx.eigsys(kpts)
+    for k in range(kpts.shape[0]):
+        er, Ur, nr = O.eigsys(m, kpts[k])
+        assert no[k] == nr
+        assert np.abs(e[k] - er).max() < 1e-8
+        sign = np.sign(v[k, :, 0].real * Ur[:, 0].real)
+        assert np.abs(v[k] - Ur * sign[:, None]).max() < 1e-9
+
+
+def test_dos_kernel_matches_numpy(gpu_ctx):
+    rng = np.random.default_rng(3)
+    etb = rng.uniform(-3, 3, 5000)
+    wts = rng.uniform(0, 1, (5000, 3))
+    en = np.linspace(-3.5, 3.5, 301)
+    gpu_ctx.set_model(synth.config_model("c1"))
+    got = gpu_ctx.dos(etb, wts, 250, en, 0.05)
+    want = (O.gaussian(en[:, None] - etb[None, :], 0.05) @ wts) / 250.0
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+
+
+def _run(tmp_path, text):
+    B.build()
+    r = subprocess.run([B.DRIVER_EXE], input=text.encode(), capture_output=True, cwd=str(tmp_path), timeout=600)
+    assert r.returncode == 0, r.stderr.decode()
+
+
+def _floats(path, skip_hash=True):
+    rows = []
+    for line in open(path).read().splitlines():
+        t = line.split()
+        if not t or (skip_hash and t[0].startswith("#")):
+            continue
+        rows.append([float(x) for x in t])
+    return np.array(rows)
+
+
+@pytest.mark.parametrize("systype", ["NP", "SOC"])
+def test_band_and_dos_runs_match_oracle(tmp_path, systype):
+    m = copy.copy(synth.config_model("c1"))
+    m.systype = systype
+    synth.write_params(m, str(tmp_path / "tb.dat"))
+    ow = np.linspace(0.2, 1.0, m.w)
+    (tmp_path / "orbw.dat").write_text("\n".join(f"{x:.6f}" for x in ow) + "\n")
+    ks = [(0, 0, 0), (0.5, 0, 0), (0.5, 0, 0), (1 / 3, 1 / 3, 0)]
+    (tmp_path / "kpath.dat").write_text("4\n7\n" + "\n".join(f"{a:.10f} {b:.10f} {c:.10f}" for a, b, c in ks) + "\n")
+    text = f"""BANDS= T
+DOS= T
+NGX= 6
+NGY= 6
+NGZ= 1
+NEDOS= 201
+SIGMA= 0.08
+OUTPUT= "{tmp_path}/"
+CALC_DATA= "{tmp_path}/"
+PARAMS_FILE= "{tmp_path}/tb.dat"
+KPATH_FILE= "{tmp_path}/kpath.dat"
+ORB_W= "{tmp_path}/orbw.dat"
+"""
+    _run(tmp_path, text)
+    kin = [tuple(float(x) for x in l.split()) for l in (tmp_path / "kpath.dat").read_text().splitlines()[2:]]
+    want, labels = O.bandstool(m, kin, 7, orbw=[float(f"{x:.6f}") for x in ow])
+    got = _floats(tmp_path / "bands.dat")
+    assert got.shape == (m.w * want.shape[1], 4)
+    assert np.allclose(got, want.reshape(-1, 4), rtol=2e-6, atol=2e-6)
+    assert np.allclose(_floats(tmp_path / "KLABELS.dat").ravel(), np.array(labels, dtype=np.float32), rtol=1e-6)
+    dd = O.dostool(m, [6, 6, 1], [0, 0, 0], 201.0, float(np.float32(0.08)), orbw=[float(f"{x:.6f}") for x in ow])
+    gd = _floats(tmp_path / "dos.dat")
+    assert gd.shape == dd.shape
+    assert np.abs(gd - np.round(dd, 4)).max() <= 1.0001e-4

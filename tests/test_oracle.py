@@ -174,3 +174,30 @@ def test_zheev_min_workspace_gauge():
     assert np.abs(v[-1].imag).max() == 0.0      # 'U': last component real
     w, v = O.zheev(H, lower=1)
     assert np.abs(v[0].imag).max() == 0.0       # 'L': first component real
+
+
+def test_temperature_oracle_reduces_to_plain_at_unit_occupation():
+    """With f = 1 (T -> 0 for a gapped model) the temperature kernel, sp table and
+    oscillators equal the plain ones; at high T they differ."""
+    m = synth.config_model("c1")
+    deck = parse_deck("NGX= 6\nNGY= 6\nNGZ= 1\nNBANDSV= 2\nNBANDSC= 2\nCOULOMB_POT= V2DRK\nR_0= 40\n"
+                      "KTOL= 0.001\nCSHIFT= 0.05\nDTDIAG= T\nCPOL= T\n")
+    kpts = O.monkhorst_pack(6, 6, 1, [0, 0, 0], m.rlat)
+    eigv, vec, nocp, _ = O.bands(m, kpts, 2, 2)
+    f0 = O.fdeh_states(eigv, eigv, 2, 2, 0.0)
+    assert np.all(f0 == 1.0)
+    p = O.CoulombParams("V2DRK", 1e-3, [1, 1, 1], 1, 1, 0, 40, [6, 6, 1], m.rlat)
+    H0 = O.bse_matrix(p, kpts, eigv, vec, 2, 2)
+    H1 = O.bse_matrix(p, kpts, eigv, vec, 2, 2, fdeh=f0)
+    assert np.abs(H0 - H1).max() < 1e-15
+    fT = O.fdeh_states(eigv, eigv, 2, 2, 5000.0)
+    assert fT.min() < 0.95
+    HT = O.bse_matrix(p, kpts, eigv, vec, 2, 2, fdeh=fT)
+    de = np.real(np.diag(H0)) - np.real(np.diag(H0 - np.diag(np.diag(H0))))
+    off = np.triu(H0, 1)
+    assert np.allclose(np.triu(HT, 1), off * fT[:, None])
+    h = O.optsp_all(m, kpts, eigv, vec, 2, 2, 0.05)
+    A = np.linalg.qr(np.random.default_rng(0).standard_normal((h.shape[0], 5)) + 0j)[0]
+    assert np.allclose(O.dielbseptemp(A, h[:, 0], h[:, 1], np.ones(h.shape[0])), O.dielbsep(A, h[:, 0], h[:, 1]))
+    assert abs(O.gapcortemp(2.0, 0.02, 300.0) - (-2.0 * 0.02 * (1.0 / np.tanh(0.02 / (2 * O.KB_F32 * 300.0)) - 1.0))) < 1e-15
+    assert O.gapcortemp2(1.0, 300.0, 300.0) == -(2.0 / (np.exp(1.0) - 1.0))

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwtbgpu.so")
-SOURCES = ["api.cu", "bands.cu", "bse_build.cu", "tridiag.cu", "tdeig.cu", "spectrum.cu", "davidson.cu", "haydock.cu", "fastprod.cu", "learned.cu"]
+SOURCES = ["api.cu", "bands.cu", "bse_build.cu", "tridiag.cu", "tdeig.cu", "spectrum.cu", "davidson.cu", "haydock.cu", "fastprod.cu", "learned.cu", "temperature.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
               "-I" + os.path.join(ROOT, "include")]

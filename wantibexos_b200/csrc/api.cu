@@ -127,7 +127,7 @@ int wtbg_destroy(wtbg_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   DevBuf* bufs[] = {&ctx->HR, &ctx->Rcart, &ctx->Rf32, &ctx->invdeg, &ctx->isR0, &ctx->kpt, &ctx->eig, &ctx->U,
                     &ctx->nocp, &ctx->kstat, &ctx->kptq, &ctx->eigq, &ctx->Uq, &ctx->nocpq, &ctx->h, &ctx->H,
-                    &ctx->d, &ctx->e, &ctx->tau, &ctx->g, &ctx->Wp, &ctx->slots, &ctx->part, &ctx->scal,
+                    &ctx->d, &ctx->e, &ctx->tau, &ctx->g, &ctx->fdeh, &ctx->Wp, &ctx->slots, &ctx->part, &ctx->scal,
                     &ctx->yv, &ctx->lam, &ctx->ws, &ctx->act, &ctx->zsel, &ctx->csz, &ctx->sp_in, &ctx->sp_out,
                     &ctx->sp_om, &ctx->tmp, &ctx->tmp2, &ctx->istat};
   for (DevBuf* b : bufs) free_buf(*b);
@@ -351,6 +351,8 @@ int wtbg_bse_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter,
   if (!ctx || !W) return WTBG_ERR_ARG;
   if (!ctx->have_matrix) return set_err(ctx, WTBG_ERR_STATE, "bse_davidson: call wtbg_bse_build first");
   if (act && !ctx->have_velocity) return set_err(ctx, WTBG_ERR_STATE, "bse_davidson: call wtbg_velocity first");
+  if (act && ctx->temp_on)
+    return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bse_davidson: oscillators with temperature come from wtbg_bse_solve");
   if (nev < 1 || nev > ctx->N || nb > ctx->N || max_iter < 1 || !(tol > 0))
     return set_err(ctx, WTBG_ERR_ARG, "bse_davidson: bad arguments");
   if (int r = set_device(ctx)) return r;
@@ -380,6 +382,84 @@ int wtbg_bse_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter,
   if (iters) *iters = it;
   if (maxres) *maxres = mr;
   if (mr >= tol) return set_err(ctx, WTBG_ERR_NOCONV, "bse_davidson: residual above tolerance after max_iter");
+  return WTBG_OK;
+}
+
+int wtbg_eigsys(wtbg_ctx* ctx, int nk, const double* kpt, double* eig, double* vec, int* nocp) {
+  if (!ctx || nk <= 0 || !kpt || !eig) return WTBG_ERR_ARG;
+  if (ctx->w == 0) return set_err(ctx, WTBG_ERR_STATE, "eigsys: no model");
+  if (int r = set_device(ctx)) return r;
+  const int w = ctx->w;
+  std::vector<double> kp(3 * (size_t)nk);
+  for (int k = 0; k < nk; ++k)
+    for (int c = 0; c < 3; ++c) kp[3 * k + c] = kpt[k + (size_t)nk * c];
+  // scratch only within this call (the BSE state of the context is not touched)
+  const size_t b_kpt = kp.size() * 8, b_eig = (size_t)nk * w * 8, b_int = (size_t)nk * 4;
+  ENSURE(ctx->tmp, b_kpt + b_eig + 2 * b_int + 1024);
+  ENSURE(ctx->ws, (size_t)nk * w * w * 16);
+  char* base = ctx->tmp.as<char>();
+  double* dk = reinterpret_cast<double*>(base);
+  double* de = reinterpret_cast<double*>(base + (b_kpt + 255) / 256 * 256);
+  int* dn = reinterpret_cast<int*>(base + (b_kpt + 255) / 256 * 256 + (b_eig + 255) / 256 * 256);
+  int* ds = dn + nk;
+  Timer t(ctx);
+  CK(cudaMemcpyAsync(dk, kp.data(), b_kpt, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(ds, 0, b_int, ctx->stream));
+  if (int r = launch_eigsys_all(ctx, nk, dk, de, ctx->ws.as<double2>(), dn, ds)) return r;
+  if (int r = t.stop()) return r;
+  std::vector<int> st(nk);
+  CK(cudaMemcpy(st.data(), ds, b_int, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < nk; ++k)
+    if (st[k] == 1) return set_err(ctx, WTBG_ERR_NOCONV, "eigsys: Jacobi did not converge at k-point " + std::to_string(k + 1));
+  std::vector<double> e((size_t)nk * w);
+  CK(cudaMemcpy(e.data(), de, b_eig, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < nk; ++k)
+    for (int b = 0; b < w; ++b) eig[k + (size_t)nk * b] = e[(size_t)k * w + b];
+  if (nocp) CK(cudaMemcpy(nocp, dn, b_int, cudaMemcpyDeviceToHost));
+  if (vec) {
+    std::vector<double2> u((size_t)nk * w * w);
+    CK(cudaMemcpy(u.data(), ctx->ws.p, u.size() * 16, cudaMemcpyDeviceToHost));
+    // vec(k, n, m): k fastest, then band n, then component m (the reference's autovetores per k)
+    for (int k = 0; k < nk; ++k)
+      for (int n = 0; n < w; ++n)
+        for (int m = 0; m < w; ++m) {
+          const double2 v = u[((size_t)k * w + n) * w + m];
+          const size_t o = k + (size_t)nk * (n + (size_t)w * m);
+          vec[2 * o] = v.x;
+          vec[2 * o + 1] = v.y;
+        }
+  }
+  return WTBG_OK;
+}
+
+int wtbg_dos(wtbg_ctx* ctx, long long ndim, const double* etb, const double* weights, int ncol, long long nkpt,
+             int nw, const double* en, double sme, double* out) {
+  if (!ctx || ndim <= 0 || !etb || !weights || !en || !out || nw <= 0 || nkpt <= 0 || !(sme > 0))
+    return WTBG_ERR_ARG;
+  if (ncol < 1 || ncol > 4) return set_err(ctx, WTBG_ERR_ARG, "dos: 1 to 4 weight columns");
+  if (int r = set_device(ctx)) return r;
+  const size_t b_e = (size_t)ndim * 8, b_w = (size_t)ndim * ncol * 8, b_en = (size_t)nw * 8,
+               b_o = (size_t)nw * ncol * 8;
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  ENSURE(ctx->tmp2, up(b_e) + up(b_w) + up(b_en) + up(b_o));
+  char* base = ctx->tmp2.as<char>();
+  double* d_e = reinterpret_cast<double*>(base);
+  double* d_w = reinterpret_cast<double*>(base + up(b_e));
+  double* d_en = reinterpret_cast<double*>(base + up(b_e) + up(b_w));
+  double* d_o = reinterpret_cast<double*>(base + up(b_e) + up(b_w) + up(b_en));
+  Timer t(ctx);
+  CK(cudaMemcpyAsync(d_e, etb, b_e, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(d_w, weights, b_w, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(d_en, en, b_en, cudaMemcpyHostToDevice, ctx->stream));
+  if (int r = launch_dos(ctx, d_e, d_w, ndim, ncol, d_en, nw, sme, nkpt, d_o)) return r;
+  CK(cudaMemcpyAsync(out, d_o, b_o, cudaMemcpyDeviceToHost, ctx->stream));
+  return t.stop();
+}
+
+int wtbg_set_temperature(wtbg_ctx* ctx, int on, double temp) {
+  if (!ctx || on < 0 || on > 1 || !(temp >= 0.0)) return WTBG_ERR_ARG;
+  ctx->temp_on = on;
+  ctx->temp = temp;
   return WTBG_OK;
 }
 
@@ -420,6 +500,7 @@ int wtbg_bse_spectrum_fast(wtbg_ctx* ctx, int nsteps, int dtfull, int cpol, doub
   if (!ctx || !ngrid || !omega || !eps) return WTBG_ERR_ARG;
   if (!ctx->have_matrix) return set_err(ctx, WTBG_ERR_STATE, "bse_spectrum_fast: call wtbg_bse_build first");
   if (!ctx->have_velocity) return set_err(ctx, WTBG_ERR_STATE, "bse_spectrum_fast: call wtbg_velocity first");
+  if (ctx->temp_on) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bse_spectrum_fast: no temperature form");
   const int nw = (int)numbse;
   if (nsteps < 2 || nw < 2) return set_err(ctx, WTBG_ERR_ARG, "bse_spectrum_fast: bad sizes");
   if (int r = set_device(ctx)) return r;

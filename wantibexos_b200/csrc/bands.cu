@@ -56,6 +56,7 @@ struct BandsArgs {
   double2* U;      // [nk][nb][w]
   int* nocp;       // [nk]
   int* kstat;      // [nk]
+  int all;         // 1: every band (eigsys as the band and DOS tools call it), nb = w
 };
 
 __global__ void __launch_bounds__(kBandsThreads) k_bands(BandsArgs a) {
@@ -213,7 +214,7 @@ __global__ void __launch_bounds__(kBandsThreads) k_bands(BandsArgs a) {
         if (lam[perm[i]] > 0.0) { nocp = i; break; }
       }
       int st = s_stat;
-      if (st == 0) {
+      if (st == 0 && !a.all) {
         if (nocp < 0) st = 2;
         else if (a.nv > nocp || a.nc > w - nocp) st = 3;
       }
@@ -223,18 +224,19 @@ __global__ void __launch_bounds__(kBandsThreads) k_bands(BandsArgs a) {
       a.nocp[k] = s_nocp;
     }
     __syncthreads();
-    const int nb = a.nv + a.nc;
+    const int nb = a.all ? w : a.nv + a.nc;
     if (s_stat == 0) {
       const int nocp = s_nocp;
+      const int off = a.all ? 0 : nocp - a.nv;   // all: band sel itself, scissors from nocp on
       for (int it = tid; it < nb * w; it += bs) {
         const int sel = it / w, m = it % w;
-        const int src = perm[nocp - a.nv + sel];
+        const int src = perm[off + sel];
         const double2 v0 = V[src * w];
         const double r = hypot(v0.x, v0.y);
         double2 g = make_double2(1.0, 0.0);
         if (r > 0.0) g = make_double2(v0.x / r, -v0.y / r);
         a.U[((size_t)k * nb + sel) * w + m] = cmul(V[m + src * w], g);
-        if (m == 0) a.eig[(size_t)k * nb + sel] = lam[src] + (sel >= a.nv ? a.scs : 0.0);
+        if (m == 0) a.eig[(size_t)k * nb + sel] = lam[src] + (sel >= (a.all ? nocp : a.nv) ? a.scs : 0.0);
       }
     }
     __syncthreads();
@@ -331,7 +333,7 @@ __global__ void __launch_bounds__(kBandsThreads) k_velocity(VelArgs a) {
 
 // ---------------------------------------------------------------------------------------
 // vecres rows (bse_solver-tool-diel.f90:379-393); key = column 7 (float32 dE)
-__global__ void k_sp_rows(const double* kpt, const double* eig, const int* nocp, const double2* h,
+__global__ void k_sp_rows(const double* kpt, const double* eig, const int* nocp, const double2* h, const double* fdeh,
                           int nk, int nv, int nc, long long N, float* rows, float* key, int* idx) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= N) return;
@@ -346,14 +348,26 @@ __global__ void k_sp_rows(const double* kpt, const double* eig, const int* nocp,
   r[4] = (float)(nocp[k] - nv + (nv + c + 1));
   r[5] = (float)(nocp[k] - nv + (v + 1));
   r[6] = (float)(eig[(size_t)k * nb + nv + c] - eig[(size_t)k * nb + v]);
-  r[7] = (float)(hx.x * hx.x + hx.y * hx.y);
-  r[8] = (float)(hy.x * hy.x + hy.y * hy.y);
-  r[9] = (float)(hz.x * hz.x + hz.y * hz.y);
-  r[10] = (float)(hx.x * hy.x + hx.y * hy.y);
-  r[11] = (float)(hx.x * hz.x + hx.y * hz.y);
-  r[12] = (float)(hy.x * hz.x + hy.y * hz.y);
-  r[13] = (float)(hp.x * hp.x + hp.y * hp.y);
-  r[14] = (float)(hm.x * hm.x + hm.y * hm.y);
+  if (fdeh == nullptr) {
+    r[7] = (float)(hx.x * hx.x + hx.y * hx.y);
+    r[8] = (float)(hy.x * hy.x + hy.y * hy.y);
+    r[9] = (float)(hz.x * hz.x + hz.y * hz.y);
+    r[10] = (float)(hx.x * hy.x + hx.y * hy.y);
+    r[11] = (float)(hx.x * hz.x + hx.y * hz.y);
+    r[12] = (float)(hy.x * hz.x + hy.y * hz.y);
+    r[13] = (float)(hp.x * hp.x + hp.y * hp.y);
+    r[14] = (float)(hm.x * hm.x + hm.y * hm.y);
+  } else {   // temperature: the strengths times f_v - f_c (bse_solver-tool-diel-temp.f90:416-423)
+    const double f = fdeh[i];
+    r[7] = (float)((hx.x * hx.x + hx.y * hx.y) * f);
+    r[8] = (float)((hy.x * hy.x + hy.y * hy.y) * f);
+    r[9] = (float)((hz.x * hz.x + hz.y * hz.y) * f);
+    r[10] = (float)((hx.x * hy.x + hx.y * hy.y) * f);
+    r[11] = (float)((hx.x * hz.x + hx.y * hz.y) * f);
+    r[12] = (float)((hy.x * hz.x + hy.y * hz.y) * f);
+    r[13] = (float)((hp.x * hp.x + hp.y * hp.y) * f);
+    r[14] = (float)((hm.x * hm.x + hm.y * hm.y) * f);
+  }
   key[i] = r[6];
   idx[i] = (int)i;
 }
@@ -399,12 +413,42 @@ int launch_bands(wtbg_ctx* ctx, bool q_mesh) {
     a.nocp = ctx->nocp.as<int>();
   }
   a.kstat = ctx->kstat.as<int>();
+  a.all = 0;
   const size_t smem = bands_smem(w, ctx->nvec);
   if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bands: model too large for shared memory");
   CK(cudaFuncSetAttribute(k_bands, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int grid = ctx->nk;
   k_bands<<<grid, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
   CKL("k_bands");
+  return 0;
+}
+
+// every band of every k (eigsys of the band and DOS tools): eig [nk][w], U [nk][w][w]
+int launch_eigsys_all(wtbg_ctx* ctx, int nk, const double* d_kpt, double* d_eig, double2* d_U, int* d_nocp,
+                      int* d_kstat) {
+  const int w = ctx->w;
+  BandsArgs a;
+  a.HR = ctx->HR.as<double2>();
+  a.Rcart = ctx->Rcart.as<double>();
+  a.invdeg = ctx->invdeg.as<double>();
+  a.nvec = ctx->nvec;
+  a.w = w;
+  a.nk = nk;
+  a.ef32 = (double)(float)ctx->efermi;
+  a.scs = ctx->scs;
+  a.nv = 0;
+  a.nc = w;
+  a.kpt = d_kpt;
+  a.eig = d_eig;
+  a.U = d_U;
+  a.nocp = d_nocp;
+  a.kstat = d_kstat;
+  a.all = 1;
+  const size_t smem = bands_smem(w, ctx->nvec);
+  if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bands: model too large for shared memory");
+  CK(cudaFuncSetAttribute(k_bands, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_bands<<<nk, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
+  CKL("k_bands(all)");
   return 0;
 }
 
@@ -455,8 +499,13 @@ int launch_sp_table(wtbg_ctx* ctx, float* d_out) {
   void* ctmp = reinterpret_cast<void*>(((uintptr_t)(iout + N) + 255) & ~(uintptr_t)255);
   const int th = 256;
   const int gr = (int)((N + th - 1) / th);
+  const double* fd = nullptr;
+  if (ctx->temp_on) {
+    if (int r = ensure_fdeh(ctx, false)) return r;
+    fd = ctx->fdeh.as<double>();
+  }
   k_sp_rows<<<gr, th, 0, ctx->stream>>>(ctx->kpt.as<double>(), ctx->eig.as<double>(), ctx->nocp.as<int>(),
-                                         ctx->h.as<double2>(), ctx->nk, ctx->nv, ctx->nc, N, rows, kin, iin); WTBG_COUNT(ctx, 1);
+                                         ctx->h.as<double2>(), fd, ctx->nk, ctx->nv, ctx->nc, N, rows, kin, iin); WTBG_COUNT(ctx, 1);
   CKL("k_sp_rows");
   // LSD radix sort is stable: equal keys keep their original (quantumnumbers2) order,
   // which is what the strict-greater bubble sort produces.

@@ -36,6 +36,7 @@ struct BuildArgs {
   int exch;
   double vq;
   const double2* vcv;   // [N] <c^{k+Q}|v> per state (exchange only)
+  const double* fdeh;   // [N] occupation factor f_v - f_c (temperature BSE) or nullptr
   double2* H;
   long long N;
   int TK, nbk;
@@ -132,15 +133,25 @@ __global__ void __launch_bounds__(kBuildThreads) k_bse_build(BuildArgs a) {
     const int kc = ci >> 16, cc = (ci >> 8) & 0xff, vv = ci & 0xff;
     const double vk = Vt[kc * TK + kr];
     double2 val;
-    if (I == J) {
-      val = make_double2(dEi + vk, 0.0);
+    if (a.fdeh == nullptr) {
+      if (I == J) {
+        val = make_double2(dEi + vk, 0.0);
+      } else {
+        val = cmul(cscale(Mc_r[(kc * nc + cc) * RC], vk), Mv_r[(kc * nv + vv) * RV]);
+      }
+      if (a.exch) {
+        // vvc_j = conj(<c_j|v_j>) exactly
+        const double2 t2 = cmul(cscale(vcvI, a.vq), cconj(a.vcv[J]));
+        val = csub(val, t2);
+      }
     } else {
-      val = cmul(cscale(Mc_r[(kc * nc + cc) * RC], vk), Mv_r[(kc * nv + vv) * RV]);
-    }
-    if (a.exch) {
-      // vvc_j = conj(<c_j|v_j>) exactly
-      const double2 t2 = cmul(cscale(vcvI, a.vq), cconj(a.vcv[J]));
-      val = csub(val, t2);
+      // temperature: the interaction part of the reference's upper-triangle row J (the
+      // smaller index) is scaled by f_J; the band-energy difference is not
+      double2 inter = (I == J) ? make_double2(vk, 0.0)
+                               : cmul(cscale(Mc_r[(kc * nc + cc) * RC], vk), Mv_r[(kc * nv + vv) * RV]);
+      if (a.exch) inter = csub(inter, cmul(cscale(vcvI, a.vq), cconj(a.vcv[J])));
+      val = cscale(inter, a.fdeh[J]);
+      if (I == J) val.x += dEi;
     }
     Hcol[J * N] = val;
   }
@@ -242,6 +253,11 @@ int launch_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p, const double* q4) {
   a.P = make_coulomb_dev(p, ctx->rlat);
   a.exch = 0;
   a.vq = 0.0;
+  a.fdeh = nullptr;
+  if (ctx->temp_on) {
+    if (int r = ensure_fdeh(ctx, q)) return r;
+    a.fdeh = ctx->fdeh.as<double>();
+  }
   a.vcv = nullptr;
   a.H = ctx->H.as<double2>();
   a.N = ctx->N;

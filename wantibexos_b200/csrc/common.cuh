@@ -79,6 +79,12 @@ struct wtbg_ctx {
   DevBuf tmp, tmp2, istat;
 
   // counters
+  // temperature BSE (BSET / BSET_BND): occupation factor f_v - f_c per basis state
+  int temp_on = 0;
+  double temp = 0.0;     // temperature used in the Fermi factors (0 is replaced as the reference does)
+  DevBuf fdeh;           // [N] double
+  int ng = 5;            // velocity vectors carried through the reduction (10 with temperature)
+
   // fast form: split-BF16 planes of the kernel matrix for the tensor-core product
   int fast_mode = 0;
   bool fast_ready = false;
@@ -176,6 +182,12 @@ inline int set_device(wtbg_ctx* ctx) {
 }
 
 
+int launch_eigsys_all(wtbg_ctx* ctx, int nk, const double* d_kpt, double* d_eig, double2* d_U, int* d_nocp,
+                      int* d_kstat);
+int launch_dos(wtbg_ctx* ctx, const double* d_etb, const double* d_w, long long ndim, int ncol, const double* d_en,
+               int nw, double sme, long long nkpt, double* d_out);
+int ensure_fdeh(wtbg_ctx* ctx, bool q_mesh);
+int fill_g_vectors(wtbg_ctx* ctx, double2* g);
 int run_fast_setup(wtbg_ctx* ctx);
 int run_fastprod(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y, int ldy);
 int run_hemm_narrow(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y, int ldy);

@@ -141,6 +141,47 @@ int launch_spectrum(wtbg_ctx* ctx, int n, int ncomp, const double* d_e, const do
   return 0;
 }
 
+// ---- DOS smearing (endos, subroutines/dos_subs.f90:102-152, with gaussian,
+//      general_subs.f90:471-487): out[e][c] = (1/nkpt) sum_i w_c(i) g(en_e - etb_i),
+//      g(x) = exp(-x^2 / (2 sme^2)) / (sme sqrt(2 pi)), pi = acos(-1.) in real(4).
+namespace {
+__global__ void k_dos(const double* etb, const double* w, long long ndim, int ncol, const double* en, int nw,
+                      double sme, double caux, double* out) {
+  const int e = blockIdx.x;
+  if (e >= nw) return;
+  const double pi32 = (double)3.14159274101257324f;
+  const double norm = 1.0 / (sme * sqrt(2.0 * pi32));
+  const double deno = 2.0 * sme * sme;
+  const double x0 = en[e];
+  __shared__ double red[8][4];
+  double acc[4] = {0, 0, 0, 0};
+  for (long long i = threadIdx.x; i < ndim; i += blockDim.x) {
+    const double dx = x0 - etb[i];
+    const double g = norm * exp(-1.0 * (dx * dx) / deno);
+    for (int c = 0; c < ncol && c < 4; ++c) acc[c] += w[c * ndim + i] * g;
+  }
+  for (int c = 0; c < 4; ++c)
+    for (int o = 16; o > 0; o >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+  if ((threadIdx.x & 31) == 0)
+    for (int c = 0; c < 4; ++c) red[threadIdx.x >> 5][c] = acc[c];
+  __syncthreads();
+  if (threadIdx.x < ncol) {
+    double s = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[k][threadIdx.x];
+    out[(long long)threadIdx.x * nw + e] = s * caux;
+  }
+}
+}  // namespace
+
+int launch_dos(wtbg_ctx* ctx, const double* d_etb, const double* d_w, long long ndim, int ncol, const double* d_en,
+               int nw, double sme, long long nkpt, double* d_out) {
+  if (ncol < 1 || ncol > 4) return set_err(ctx, WTBG_ERR_ARG, "dos: 1 to 4 weight columns");
+  k_dos<<<nw, 256, 0, ctx->stream>>>(d_etb, d_w, ndim, ncol, d_en, nw, sme, 1.0 / (double)nkpt, d_out);
+  WTBG_COUNT(ctx, 1);
+  CKL("k_dos");
+  return 0;
+}
+
 // ---------------------------------------------------------------------------------------
 // Allocation-free entry point.  The scratch of the three spectrum kernels (Re/Im sums per
 // component and photon energy, and eta) lives in this fixed file-scope device array instead

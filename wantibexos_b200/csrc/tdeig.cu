@@ -25,7 +25,7 @@
 
 namespace {
 
-constexpr int NG = 5;
+constexpr int NG = 10;   // largest number of reduced h vectors (5, or 10 with temperature)
 
 __device__ __forceinline__ int sturm_count(const double* __restrict__ d, const double* __restrict__ e2, long long n,
                                            double x, double pivmin) {
@@ -81,7 +81,8 @@ struct InvArgs {
   int M;                // slots in the chunk
   double* ws;           // 4 * n * M
   double pert;          // eps * ||T||: pivot floor
-  const double2* g;     // [5][n]
+  const double2* g;     // [ng][n]: h (x, y, z, sp, sm) [, h * f with temperature]
+  int ng;
   double* act;          // [8][n]
   int dtfull, cpol;
   double* zsel;         // selected vectors (column-major n x nsel) or null
@@ -169,26 +170,33 @@ __global__ void __launch_bounds__(128) k_inviter(InvArgs a) {
 #pragma unroll
     for (int al = 0; al < NG; ++al) sg[al] = make_double2(0, 0);
     const bool keep = (a.zsel != nullptr && mm >= a.zs0 && mm <= a.zs1);
+    const int ng = a.ng;
     for (long long k = 0; k < n; ++k) {
       const double x = X[k * M + jj] * sc;
       X[k * M + jj] = x;
 #pragma unroll
       for (int al = 0; al < NG; ++al) {
-        const double2 gk = a.g[al * n + k];
-        sg[al].x += x * gk.x;
-        sg[al].y += x * gk.y;
+        if (al < ng) {
+          const double2 gk = a.g[al * n + k];
+          sg[al].x += x * gk.x;
+          sg[al].y += x * gk.y;
+        }
       }
       if (keep) a.zsel[(mm - a.zs0) * n + k] = x;
     }
+    // act(a, b) = Re[(z^T g_a) conj(z^T g'_b)], g' = g (dielbsev/dielbsep) or the f-weighted
+    // vectors with temperature (dielbseptemp)
+    const int o = (ng == 10) ? 5 : 0;
+    auto re = [&](int p, int q) { return sg[p].x * sg[o + q].x + sg[p].y * sg[o + q].y; };
     double* act = a.act;
-    act[0 * n + mm] = sg[0].x * sg[0].x + sg[0].y * sg[0].y;
-    act[1 * n + mm] = sg[1].x * sg[1].x + sg[1].y * sg[1].y;
-    act[2 * n + mm] = sg[2].x * sg[2].x + sg[2].y * sg[2].y;
-    act[3 * n + mm] = a.dtfull ? (sg[0].x * sg[1].x + sg[0].y * sg[1].y) : 0.0;
-    act[4 * n + mm] = a.dtfull ? (sg[0].x * sg[2].x + sg[0].y * sg[2].y) : 0.0;
-    act[5 * n + mm] = a.dtfull ? (sg[1].x * sg[2].x + sg[1].y * sg[2].y) : 0.0;
-    act[6 * n + mm] = a.cpol ? (sg[3].x * sg[3].x + sg[3].y * sg[3].y) : 0.0;
-    act[7 * n + mm] = a.cpol ? (sg[4].x * sg[4].x + sg[4].y * sg[4].y) : 0.0;
+    act[0 * n + mm] = re(0, 0);
+    act[1 * n + mm] = re(1, 1);
+    act[2 * n + mm] = re(2, 2);
+    act[3 * n + mm] = a.dtfull ? re(0, 1) : 0.0;
+    act[4 * n + mm] = a.dtfull ? re(0, 2) : 0.0;
+    act[5 * n + mm] = a.dtfull ? re(1, 2) : 0.0;
+    act[6 * n + mm] = a.cpol ? re(3, 3) : 0.0;
+    act[7 * n + mm] = a.cpol ? re(4, 4) : 0.0;
   }
 }
 
@@ -375,6 +383,7 @@ int run_tridiagonal_solve(wtbg_ctx* ctx, int dtfull, int cpol, bool vectors) {
   a.ws = ctx->ws.as<double>();
   a.pert = DBL_EPSILON * std::max(tnorm, DBL_MIN);
   a.g = ctx->g.as<double2>();
+  a.ng = ctx->ng;
   a.act = ctx->act.as<double>();
   a.dtfull = dtfull;
   a.cpol = cpol;
@@ -432,6 +441,7 @@ int run_eigvecs(wtbg_ctx* ctx, int n0, int n1, double2* d_out) {
     a.ws = ctx->ws.as<double>();
     a.pert = DBL_EPSILON * std::max(ctx->tnorm, DBL_MIN);
     a.g = ctx->g.as<double2>();
+    a.ng = ctx->ng;
     a.act = ctx->tmp2.as<double>();
     a.dtfull = 0;
     a.cpol = 0;

@@ -25,7 +25,7 @@ namespace {
 constexpr int TB = WTBG_HEMV_TILE;   // 64
 constexpr int NB = WTBG_PANEL;       // 32
 constexpr int RB = 256;              // rows per block of the column kernels
-constexpr int NG = 5;                // h vectors carried through (x, y, z, sp, sm)
+constexpr int NG = 10;               // h vectors carried through (x, y, z, sp, sm [, each times f])
 
 __device__ __forceinline__ double2 warp_sum2(double2 v) {
 #pragma unroll
@@ -56,7 +56,7 @@ struct ColState {
   double beta;
   int trivial;
   unsigned int cntA, cntC, cntE;
-  double2 z[2 * NB + NG];   // z1 = W^H v (p values), z2 = V^H v (p values), s = v^T g (5)
+  double2 z[2 * NB + NG];   // z1 = W^H v (p values), z2 = V^H v (p values), s = v^T g (ng)
 };
 
 __device__ __forceinline__ bool last_block(unsigned int* cnt) {
@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(RB) k_colA(double2* A, long long N, double2* W
 // (C) scale v in place (v(i+1) = 1); partial dots z1 = W^H v, z2 = V^H v, s = v^T g.  One
 //     warp per dot product over the block's rows; the last block reduces into st->z.
 __global__ void __launch_bounds__(RB) k_colC(double2* A, long long N, const double2* Wp, int j0, int p, int i,
-                                             ColState* st, const double2* g, double2* part) {
+                                             ColState* st, const double2* g, int ng, double2* part) {
   __shared__ double2 vs[RB];
   __shared__ double2 red[2 * NB + NG];
   const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(RB) k_colC(double2* A, long long N, const doub
   }
   vs[tid] = v;
   __syncthreads();
-  const int nval = 2 * p + NG;
+  const int nval = 2 * p + ng;
   const int nrow = (int)((N - rbase) < RB ? (N - rbase) : RB);
   for (int q = wp; q < nval; q += RB / 32) {
     double2 t = make_double2(0, 0);
@@ -299,13 +299,13 @@ __global__ void __launch_bounds__(256, 2) k_hemv(const double2* __restrict__ A, 
 // (E) y rows from the slots; w = tau (y - V z1 - W z2); g <- g - tau conj(v) s; partial
 //     w^H v.  The last block computes alpha2 = -tau/2 w^H v for the next column kernel.
 __global__ void __launch_bounds__(256) k_colE(const double2* A, long long N, double2* Wp, int j0, int p, int i, int nblk,
-                                              const double2* slots, ColState* st, double2* g, double2* part) {
+                                              const double2* slots, ColState* st, double2* g, int ng, double2* part) {
   __shared__ double2 acc4[4][TB];
   __shared__ double2 tq4[4][TB];
   __shared__ double2 zz[2 * NB + NG];
   __shared__ double2 red[8];
   const int tid = threadIdx.x;
-  const int nval = 2 * p + NG;
+  const int nval = 2 * p + ng;
   for (int q = tid; q < nval; q += blockDim.x) zz[q] = st->z[q];
   const double2 tau = st->tau;
   const int b0 = (i + 1) / TB;
@@ -336,8 +336,7 @@ __global__ void __launch_bounds__(256) k_colE(const double2* A, long long N, dou
     const double2 v = A[r + (long long)i * N];
     dot = cmulc(w, v);
     const double2 tv = cmul(tau, cconj(v));
-#pragma unroll
-    for (int al = 0; al < NG; ++al) {
+    for (int al = 0; al < ng; ++al) {
       const double2 sa = zz[2 * p + al];
       g[(long long)al * N + r] = csub(g[(long long)al * N + r], cmul(tv, sa));
     }
@@ -484,10 +483,14 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
   cudaStream_t s = ctx->stream;
   CK(cudaMemsetAsync(st, 0, sizeof(ColState), s));
 
-  if (ctx->have_velocity) {
-    k_copy_g<<<(int)((N * NG + 255) / 256), 256, 0, s>>>(ctx->h.as<double2>(), g, N * NG); WTBG_COUNT(ctx, 1);
+  const int ng = (ctx->have_velocity && ctx->temp_on) ? 10 : 5;
+  ctx->ng = ng;
+  if (ctx->have_velocity && ctx->temp_on) {
+    if (int r = fill_g_vectors(ctx, g)) return r;
+  } else if (ctx->have_velocity) {
+    k_copy_g<<<(int)((N * 5 + 255) / 256), 256, 0, s>>>(ctx->h.as<double2>(), g, N * 5); WTBG_COUNT(ctx, 1);
   } else {
-    CK(cudaMemsetAsync(g, 0, (size_t)N * 16 * NG, s));
+    CK(cudaMemsetAsync(g, 0, (size_t)N * 16 * 5, s));
   }
   CKL("k_copy_g");
   const bool prof = ctx->profiling != 0;
@@ -502,13 +505,13 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
       const int nA = (int)((N - i + RB - 1) / RB);
       k_colA<<<nA, RB, 0, s>>>(A, N, Wp, (int)j0, p, i, partA, st, d, e, tau); WTBG_COUNT(ctx, 1);
       const int nC = (int)((N - i - 1 + RB - 1) / RB);
-      k_colC<<<nC, RB, 0, s>>>(A, N, Wp, (int)j0, p, i, st, g, partC); WTBG_COUNT(ctx, 1);
+      k_colC<<<nC, RB, 0, s>>>(A, N, Wp, (int)j0, p, i, st, g, ng, partC); WTBG_COUNT(ctx, 1);
       const int b0 = (i + 1) / TB;
       const int nt = nblk - b0;
       if (prof) cudaEventRecord(ctx->evpool[2 * i], s);
       k_hemv<<<dim3(nt, (nt + HS - 1) / HS), 256, 0, s>>>(A, N, i, nblk, slots); WTBG_COUNT(ctx, 1);
       if (prof) cudaEventRecord(ctx->evpool[2 * i + 1], s);
-      k_colE<<<nt, 256, 0, s>>>(A, N, Wp, (int)j0, p, i, nblk, slots, st, g, partE); WTBG_COUNT(ctx, 1);
+      k_colE<<<nt, 256, 0, s>>>(A, N, Wp, (int)j0, p, i, nblk, slots, st, g, ng, partE); WTBG_COUNT(ctx, 1);
     }
     CKL("tridiagonal panel");
     const long long k0 = j0 + jb;

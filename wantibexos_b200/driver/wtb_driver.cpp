@@ -221,6 +221,10 @@ Deck parse_deck(const std::string& text) {
 }
 
 // ------------------------------------------------------------------------------ params
+struct double2v {
+  double x, y;
+};
+
 struct Model {
   std::string systype;
   double scs = 0, efermi = 0;
@@ -629,6 +633,29 @@ void param_out(Out& o, const Deck& d) {
 }
 
 // ------------------------------------------------------------------------------ bsesolver
+// Temperature gap correction tcor of bsesolvertemp / bsebndstemp (TA= FA | VE | BE):
+// gapcortemp (general_subs.f90:569-586) and gapcortemp2 (:588-605), kB a real(4) literal.
+double temperature_shift(const Deck& d) {
+  const double kb = (double)8.617330350e-5f;
+  if (d.ta == "VE") {
+    const double aux1 = d.phavg / (2.0 * kb * d.temp);
+    return -d.st * d.phavg * ((1.0 / std::tanh(aux1)) - 1.0);
+  }
+  if (d.ta == "BE") return -((2.0 * d.st) / (std::exp(d.phavg / d.temp) - 1.0));
+  return 0.0;
+}
+
+// The model with the temperature scissors (scs + tcor) and the context's temperature mode.
+void upload_model_temp(wtbg_ctx* ctx, const Model& m, const Deck& d, bool temp) {
+  Model mm = m;
+  if (temp) mm.scs += temperature_shift(d);
+  upload_model(ctx, mm);
+  gpu_check(ctx, wtbg_set_temperature(ctx, temp ? 1 : 0, d.temp), "wtbg_set_temperature");
+}
+
+// bsesolver (bse_solver-tool-diel.f90) and, with d.bset, bsesolvertemp
+// (bse_solver-tool-diel-temp.f90): same files; the temperature run adds the log line, the
+// scissors tcor and the occupation factors.
 void bsesolver(wtbg_ctx* ctx, const Deck& d, const Model& m, Timings* tm) {
   const std::string of = d.outputfolder;
   Out log(join_path(of, "log_bse-diel.dat"), "Error opening log_bse-diel output file");
@@ -644,7 +671,8 @@ void bsesolver(wtbg_ctx* ctx, const Deck& d, const Model& m, Timings* tm) {
   }
   Out f403(join_path(of, "sp_optics-pol.dat"), "Error opening sp_optics-pol output file");
   double t0 = now_s();
-  upload_model(ctx, m);
+  const bool temp = d.bset && !d.bse;
+  upload_model_temp(ctx, m, d, temp);
   f301.line(" #  exciton energy  xx  yy  zz xy  xz  yz");
   f302.line(" #  exciton energy  xx  yy  zz sp  sm");
   const int nk = d.ngrid[0] * d.ngrid[1] * d.ngrid[2];
@@ -654,6 +682,10 @@ void bsesolver(wtbg_ctx* ctx, const Deck& d, const Model& m, Timings* tm) {
   log.line("");
   log.line(" threads:" + LI(d.nthreads));
   log.line("");
+  if (temp) {
+    log.line(" temperature" + LD(d.temp));
+    log.line("");
+  }
   log.line(" grid:" + LI(d.ngrid[0]) + LI(d.ngrid[1]) + LI(d.ngrid[2]));
   log.line("");
   log.line("  ktol-coulomb:" + E(d.ktol, 15, 4));
@@ -811,7 +843,8 @@ void bsebnds(wtbg_ctx* ctx, const Deck& d, const Model& m) {
   if (!kf) throw Stop("Error opening bse-kpath input file");
   Out log(join_path(of, "log_bse_kpath.dat"), "Error opening log_bse_kpath output file");
   Out f400(join_path(of, "bands_bse.dat"), "Error opening bands_bse output file");
-  upload_model(ctx, m);
+  const bool temp = d.bsetbnd && !d.bsekpath;
+  upload_model_temp(ctx, m, d, temp);
   std::vector<std::string> kl;
   {
     std::string l;
@@ -862,6 +895,10 @@ void bsebnds(wtbg_ctx* ctx, const Deck& d, const Model& m) {
   }
   log.line(" threads:" + LI(d.nthreads));
   log.line("");
+  if (temp) {
+    log.line(" temperature" + LD(d.temp));
+    log.line("");
+  }
   log.line(" grid:" + LI(d.ngrid[0]) + LI(d.ngrid[1]) + LI(d.ngrid[2]));
   log.line("");
   log.line(" ktol-coulomb:" + LD(d.ktol));
@@ -902,6 +939,179 @@ void bsebnds(wtbg_ctx* ctx, const Deck& d, const Model& m) {
   log.line("");
   log.line(stamp("end"));
   log.line("");
+}
+
+// ------------------------------------------------------------------------------ band and DOS tools
+// orbital weights of ORB_W= (one value a line), 1.0 each when the file cannot be opened
+std::vector<double> orbital_weights(const Deck& d, int w) {
+  std::vector<double> ow(w, 1.0);
+  std::ifstream f(d.orbw);
+  if (!f) return ow;
+  std::vector<std::string> toks;
+  std::string l;
+  while ((int)toks.size() < w && std::getline(f, l))
+    for (auto& t : items_of(l)) toks.push_back(t);
+  if ((int)toks.size() < w) throw Stop("Error reading orbital weight file");
+  for (int i = 0; i < w; ++i) ow[i] = num(toks[i]);
+  return ow;
+}
+
+// layercont (dos_subs.f90:154-181): sum |wf_i|^2 orbweight_i
+double layercont(const double2v* wf, int w, const std::vector<double>& ow) {
+  double re = 0.0;
+  for (int i = 0; i < w; ++i) re += (wf[i].x * wf[i].x + wf[i].y * wf[i].y) * ow[i];
+  return re;
+}
+
+// spin projection: the diagonal spin operator of spinvl (hamiltonian_tb.f90:281-368) and the
+// up/down split of spincont (dos_subs.f90:37-100); +1 up, -1 down, 0 for NP
+int spin_of(const std::string& systype, const std::string& dft, int i, int w) {
+  const int w2 = w / 2;
+  if (systype.rfind("NP", 0) == 0) return 0;
+  if (systype.rfind("SP", 0) == 0 || (systype.rfind("SOC", 0) == 0 && dft == "V")) return i < w2 ? 1 : -1;
+  return (i % 2 == 0) ? 1 : -1;
+}
+
+// bandstool (bands-kpath-tool.f90): eigsys along the k path of KPATH_FILE=; bands.dat with
+// (k distance, E, <Sz>, layer weight) per band, KLABELS.dat from kpath2 (mhkpack_subs.f90:54-130)
+void bandstool(wtbg_ctx* ctx, const Deck& d, const Model& m) {
+  const std::string of = d.outputfolder;
+  std::ifstream kf(d.kpaths);
+  if (!kf) throw Stop("Error opening kpath input file");
+  Out f300(join_path(of, "bands.dat"), "Error opening bands output file");
+  upload_model(ctx, m);
+  std::vector<std::string> kl;
+  {
+    std::string l;
+    while (std::getline(kf, l))
+      if (!items_of(l).empty()) kl.push_back(l);
+  }
+  if (kl.size() < 2) throw Stop("bad kpath file");
+  const int nks = (int)num(items_of(kl[0])[0]);
+  const int npts = (int)num(items_of(kl[1])[0]);
+  if ((int)kl.size() < 2 + nks) throw Stop("bad kpath file");
+  std::vector<std::array<double, 3>> ks(nks);
+  for (int i = 0; i < nks; ++i) {
+    auto t = items_of(kl[2 + i]);
+    for (int c = 0; c < 3; ++c) ks[i][c] = num(t[c]);
+  }
+  const std::vector<double> ow = orbital_weights(d, m.w);
+  double b[3][3];
+  recvec(m.rlat, b);
+  std::vector<std::array<double, 3>> kx(nks);
+  for (int i = 0; i < nks; ++i)
+    for (int c = 0; c < 3; ++c) kx[i][c] = ks[i][0] * b[0][c] + ks[i][1] * b[1][c] + ks[i][2] * b[2][c];
+  const int half = nks / 2;
+  std::vector<double> kdis(half);
+  double tot = 0.0;
+  for (int i = 0; i < half; ++i) {
+    const double dx = kx[2 * i + 1][0] - kx[2 * i][0], dy = kx[2 * i + 1][1] - kx[2 * i][1],
+                 dz = kx[2 * i + 1][2] - kx[2 * i][2];
+    kdis[i] = sqrt(dx * dx + dy * dy + dz * dz);
+    tot += kdis[i];
+  }
+  for (auto& v : kdis) v = v / tot;
+  const int nk = half * npts;
+  std::vector<double> kp(nk), kc(3 * (size_t)nk);
+  {
+    Out kl_out(join_path(of, "KLABELS.dat"), "Error opening KLABELS output file");
+    double acc = 0.0;
+    kl_out.line(LS(0.0f));
+    for (int j = 0; j < half; ++j) {
+      for (int i = 0; i < npts; ++i) {
+        const double t = (double)((float)i / (float)(npts - 1));
+        const size_t r = (size_t)j * npts + i;
+        kp[r] = acc + kdis[j] * t;
+        for (int c = 0; c < 3; ++c) kc[r + (size_t)nk * c] = kx[2 * j][c] + (kx[2 * j + 1][c] - kx[2 * j][c]) * t;
+      }
+      acc += kdis[j];
+      kl_out.line(LS((float)acc));
+    }
+  }
+  const int w = m.w;
+  std::vector<double> e((size_t)nk * w), vec((size_t)nk * w * w * 2);
+  gpu_check(ctx, wtbg_eigsys(ctx, nk, kc.data(), e.data(), vec.data(), nullptr), "wtbg_eigsys");
+  std::string buf;
+  std::vector<double2v> wf(w);
+  for (int n = 0; n < w; ++n) {
+    buf += " #band" + LI(n + 1) + "\n";
+    for (int k = 0; k < nk; ++k) {
+      double sz = 0.0;
+      for (int c = 0; c < w; ++c) {
+        const size_t o = k + (size_t)nk * (n + (size_t)w * c);
+        wf[c] = {vec[2 * o], vec[2 * o + 1]};
+        sz += (wf[c].x * wf[c].x + wf[c].y * wf[c].y) * (double)spin_of(m.systype, d.dft, c, w);
+      }
+      if (m.systype.rfind("NP", 0) == 0) {
+        sz = 0.0;
+        for (int c = 0; c < w; ++c) sz += wf[c].x * wf[c].x + wf[c].y * wf[c].y;
+      }
+      buf += LS((float)kp[k]) + LS((float)e[k + (size_t)nk * n]) + LS((float)sz) + LS((float)layercont(wf.data(), w, ow)) +
+             "\n";
+    }
+    buf += "\n";
+  }
+  fputs(buf.c_str(), f300.f);
+}
+
+// dostool (tdos-tool.f90): eigsys on the k mesh, Gaussian smearing (endos) of the total,
+// spin-resolved and orbital-weighted DOS on NEDOS points between min(0, E_min) and
+// max(0, E_max); dos.dat (4F15.4) for NP, (6F15.4) otherwise, with the running trapezoid sum
+void dostool(wtbg_ctx* ctx, const Deck& d, const Model& m) {
+  const std::string of = d.outputfolder;
+  Out f300(join_path(of, "dos.dat"), "Error opening dos output file");
+  upload_model(ctx, m);
+  const bool np = m.systype.rfind("NP", 0) == 0;
+  const double spinf = np ? 2.0 : 1.0;
+  f300.line(np ? " #energy tdos sumdos awdos" : " #energy tdos sumdos updos dndos awdos");
+  const std::vector<double> ow = orbital_weights(d, m.w);
+  std::vector<double> kc = kmesh(d.ngrid, d.mshift, m.rlat, nullptr);
+  const int nk = d.ngrid[0] * d.ngrid[1] * d.ngrid[2];
+  const int w = m.w;
+  std::vector<double> e((size_t)nk * w), vec((size_t)nk * w * w * 2);
+  gpu_check(ctx, wtbg_eigsys(ctx, nk, kc.data(), e.data(), vec.data(), nullptr), "wtbg_eigsys");
+  const long long ndim = (long long)nk * w;
+  std::vector<double> etb(ndim), wts((size_t)ndim * 4);
+  double edos0 = 0.0, edosf = 0.0;
+  std::vector<double2v> wf(w);
+  long long cnt = 0;
+  for (int k = 0; k < nk; ++k) {
+    if (e[k] < edos0) edos0 = e[k];
+    if (e[k + (size_t)nk * (w - 1)] > edosf) edosf = e[k + (size_t)nk * (w - 1)];
+    for (int n = 0; n < w; ++n) {
+      double cup = 0.0, cdn = 0.0;
+      for (int c = 0; c < w; ++c) {
+        const size_t o = k + (size_t)nk * (n + (size_t)w * c);
+        wf[c] = {vec[2 * o], vec[2 * o + 1]};
+        const int sp = spin_of(m.systype, d.dft, c, w);
+        const double a2 = wf[c].x * wf[c].x + wf[c].y * wf[c].y;
+        if (sp > 0) cup += a2;
+        if (sp < 0) cdn += a2;
+      }
+      etb[cnt] = e[k + (size_t)nk * n];
+      wts[cnt] = 1.0;
+      wts[ndim + cnt] = cup;
+      wts[2 * ndim + cnt] = cdn;
+      wts[3 * ndim + cnt] = layercont(wf.data(), w, ow);
+      ++cnt;
+    }
+  }
+  const int nw = (int)d.numdos;
+  std::vector<double> en(nw), out((size_t)nw * 4);
+  const double deltaen = (edosf - edos0) / (d.numdos - 1.0);
+  for (int i = 0; i < nw; ++i) en[i] = edos0 + ((edosf - edos0) * (double)i) / (d.numdos - 1.0);
+  gpu_check(ctx, wtbg_dos(ctx, ndim, etb.data(), wts.data(), 4, nk, nw, en.data(), d.sme, out.data()), "wtbg_dos");
+  std::string buf;
+  double sumdos = 0.0;
+  for (int i = 0; i < nw; ++i) {
+    const double at = spinf * out[i], up = out[(size_t)nw + i], dn = out[2 * (size_t)nw + i], aw = spinf * out[3 * (size_t)nw + i];
+    if (np)
+      buf += F(en[i], 15, 4) + F(at, 15, 4) + F(sumdos, 15, 4) + F(aw, 15, 4) + "\n";
+    else
+      buf += F(en[i], 15, 4) + F(at, 15, 4) + F(sumdos, 15, 4) + F(up, 15, 4) + F(-dn, 15, 4) + F(aw, 15, 4) + "\n";
+    if (i > 0) sumdos = sumdos + (deltaen * (spinf * out[i - 1] + at) * 0.5);
+  }
+  fputs(buf.c_str(), f300.f);
 }
 
 // ------------------------------------------------------------------------------ spectra
@@ -1098,7 +1308,8 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
     Deck d = parse_deck(deck_text ? deck_text : "");
     // params header + mesh (wtb_main.f90:77-104)
     Model m;
-    if (d.bse || d.bsekpath || d.spec || d.spdiel) m = read_params(d.params);
+    if (d.bse || d.bset || d.bsekpath || d.bsetbnd || d.spec || d.spdiel || d.bandscalc || d.doscalc)
+      m = read_params(d.params);
     if (d.meshtype.rfind("RK3D", 0) == 0) rkmesh(d.rk, m.rlat, d.ngrid, false);
     else if (d.meshtype.rfind("RK2D", 0) == 0) rkmesh(d.rk, m.rlat, d.ngrid, true);
     Out log(d.calcparms + "log.dat", "Error opening log output file ");
@@ -1107,18 +1318,44 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
     log.line(stamp("Begin"));
     log.line("");
     log.flush();
-    if (d.bset || d.bsetbnd) throw Stop("temperature BSE (BSET/BSET_BND) is not part of this build");
     int st = wtbg_create(&ctx, device);
     if (st != 0) return fail(std::string("wtbg_create: ") + wtbg_error_string(st));
     if (!d.pponly) {
-      if (d.bse) {
+      if (d.bandscalc) {
+        bandstool(ctx, d, m);
+        log.line(" Band Structure finished");
+        log.flush();
+      }
+      if (d.doscalc) {
+        dostool(ctx, d, m);
+        log.line(" DOS finished");
+        log.flush();
+      }
+      // wtb_main.f90:154-202
+      if (d.bse && d.bset) {
+        log.line(" ERROR: Choose BSE=T or BSET=T not both");
+        log.flush();
+        throw Stop("ERROR: Choose BSE=T or BSET=T not both");
+      } else if (d.bse) {
         bsesolver(ctx, d, m, tm);
         log.line(" BSE and Single particle dielectric calculation finished");
         log.flush();
+      } else if (d.bset) {
+        bsesolver(ctx, d, m, tm);
+        log.line(" BSE and Single particle dielectric calculation, with temperature, finished");
+        log.flush();
       }
-      if (d.bsekpath) {
+      if (d.bsekpath && d.bsetbnd) {
+        log.line(" ERROR: Choose BSE_BND=T or BSET_BND=T not both");
+        log.flush();
+        throw Stop("ERROR: Choose BSE_BND=T or BSET_BND=T not both");
+      } else if (d.bsekpath) {
         bsebnds(ctx, d, m);
         log.line(" BSE exciton band structure finished");
+        log.flush();
+      } else if (d.bsetbnd) {
+        bsebnds(ctx, d, m);
+        log.line(" BSE exciton band structure, with temperature, finished");
         log.flush();
       }
     }
@@ -1126,8 +1363,9 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
     const int nk = d.ngrid[0] * d.ngrid[1] * d.ngrid[2];
     const int N = nk * d.nc * d.nv;
     const std::string of = d.outputfolder;
-    if (d.spec && d.bse) {
-      // bsedielraw / bseoptprop / lifetime (wtb_main.f90:257-300)
+    const bool bsex = d.bse || d.bset;
+    if (d.spec && bsex) {
+      // bsedielraw / bseoptprop / lifetime (wtb_main.f90:257-300; no lifetime after BSET)
       Table t = read_table(of + "bse_opt_diel.dat", N, 7, "Error opening bse_opt_diel input file");
       Spec s = run_spectrum(ctx, d, m, t, {1, 1, 1, 0, 0, 0});
       const char* nm[6] = {"xx", "yy", "zz", "xy", "xz", "yz"};
@@ -1135,7 +1373,7 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
       if (tm) tm->spectrum = now_s() - t1;
       optprop_files(of, "bse_", {"bse_diel_xx.dat", "bse_diel_yy.dat", "bse_diel_zz.dat", "bse_diel_xy.dat",
                                  "bse_diel_xz.dat", "bse_diel_yz.dat"}, {0, 1, 2, 3, 4, 5}, "", s.nw);
-      lifetime_file(of, d, m, t, false);
+      if (!d.bset) lifetime_file(of, d, m, t, false);
       log.line(" BSE dielectric properties calculated");
       log.flush();
       if (d.cpol) {
@@ -1145,12 +1383,12 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
         for (int c = 0; c < 5; ++c) write_diel(of + "bse_diel-pol_" + pn[c] + ".dat", sp, c);
         optprop_files(of, "bse_", {"bse_diel-pol_x.dat", "bse_diel-pol_y.dat", "bse_diel-pol_z.dat",
                                    "bse_diel-pol_sp.dat", "bse_diel-pol_sm.dat"}, {0, 1, 2, 3, 4}, "-pol", sp.nw);
-        lifetime_file(of, d, m, tp, true);
+        if (!d.bset) lifetime_file(of, d, m, tp, true);
         log.line(" BSE absorption spectrum with light polarization calculated");
         log.flush();
       }
     }
-    if (d.spec && (d.spdiel || d.bse)) {
+    if (d.spec && (d.spdiel || bsex)) {
       // spdielraw / spoptprop (wtb_main.f90:304-313)
       Table t = read_table(of + "sp_optics.dat", N, 7, "Error opening sp_optics input file");
       Spec s = run_spectrum(ctx, d, m, t, {1, 1, 1, 0, 0, 0});
@@ -1161,7 +1399,7 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
       log.line(" Single particle dielectric properties calculated");
       log.flush();
     }
-    if (d.spec && (d.cpol || d.bse)) {
+    if (d.spec && (d.cpol || bsex)) {
       // spdielrawpol / spoptproppol (wtb_main.f90:317-326)
       Table t = read_table(of + "sp_optics-pol.dat", N, 6, "Error opening sp_optics-pol input file");
       Spec s = run_spectrum(ctx, d, m, t, {1, 1, 1, 1, 1});

@@ -1,0 +1,138 @@
+"""Learned warm start on a parameter sweep: generate, train, evaluate.
+
+Draws `npoints` sweep points (Q, r0, eps_env) from a seed -- Q = (u1 b1 + u2 b2) * qmax with
+u ~ U[0, 1), r0 ~ U[10, 60] Angstrom, eps_env ~ U[1, 5] -- builds the BSE matrix of each (the
+Q != 0 kernel with its exchange term), takes the 32 lowest eigenvectors of the plain dense
+FP64 solve as training targets, trains the network on the first `ntrain` points on the GPU
+and compares, on the held-out rest, the block Davidson started from the network against the
+cold start (unit vectors at the smallest diagonal entries): subspace capture, error of the
+first Rayleigh-Ritz energies, iterations and device time to residual 1e-6 eV, with the dense
+solve as the judge.
+
+  python -m wantibexos_b200.warmstart_sweep --model c4_w16 --n 60 --points 256 --train 192
+
+prints one JSON object (and writes the trained parameters with --save FILE.npy).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import synth, wtbgpu
+
+
+def kmesh(n, rlat):
+    pi32 = float(np.float32(np.pi))
+    a1, a2, a3 = rlat
+    v23, v31 = np.cross(a2, a3), np.cross(a3, a1)
+    vol = abs(a1 @ v23)
+    b1, b2 = (2.0 * pi32) / vol * v23, (2.0 * pi32) / vol * v31
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    k = (b1[None, None, :] / n) * i[..., None] + (b2[None, None, :] / n) * j[..., None]
+    return k.reshape(-1, 3), b1, b2
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--model", default="c4_w16")
+    ap.add_argument("--n", type=int, default=60)
+    ap.add_argument("--nv", type=int, default=2)
+    ap.add_argument("--nc", type=int, default=2)
+    ap.add_argument("--points", type=int, default=256)
+    ap.add_argument("--train", type=int, default=192)
+    ap.add_argument("--qmax", type=float, default=0.05, help="Q range as a fraction of b1, b2")
+    ap.add_argument("--epochs", type=int, default=300)
+    ap.add_argument("--seed", type=int, default=5)
+    ap.add_argument("--eval", type=int, default=0, help="held-out points evaluated (0 = all)")
+    ap.add_argument("--save", default=None)
+    a = ap.parse_args(argv)
+
+    m = synth.config_model(a.model)
+    kpts, b1, b2 = kmesh(a.n, m.rlat)
+    ctx = wtbgpu.Context(0)
+    ctx.set_model(m)
+    ctx.bands(kpts, a.nv, a.nc, want_vectors=False)
+    ctx.velocity(0.03, want=False)
+    rng = np.random.default_rng(a.seed)
+    pts = []
+    for _ in range(a.points):
+        u = rng.uniform(0.0, 1.0, 2)
+        q = (u[0] * b1 + u[1] * b2) * a.qmax
+        pts.append((q, rng.uniform(10.0, 60.0), rng.uniform(1.0, 5.0)))
+
+    def build(q, r0, eps):
+        c = wtbgpu.coulomb_params("V2DRK", [a.n, a.n, 1], 1e-3, [eps] * 3, 1.0, 1.0, 0.0, r0)
+        if np.linalg.norm(q) == 0.0:
+            ctx.bse_build(c)
+        else:
+            ctx.bse_build_q(kpts + q[None, :], [np.linalg.norm(q), q[0], q[1], q[2]], c)
+
+    net = wtbgpu.Net(ctx, seed=a.seed)
+    t0 = time.time()
+    As = []
+    for q, r0, eps in pts:
+        build(q, r0, eps)
+        ctx.bse_solve(False, False)
+        A = ctx.bse_eigvecs(1, 32)
+        As.append(A)
+        build(q, r0, eps)
+        net.add_sample(net.glob(q, r0, eps), A)
+    t_data = time.time() - t0
+    nho = a.points - a.train
+    before = net.eval_loss(a.train, nho)
+    t0 = time.time()
+    hist = []
+    for ep, lr in ((a.epochs // 3, 1e-3), (a.epochs // 3, 3e-4), (a.epochs - 2 * (a.epochs // 3), 1e-4)):
+        hist += list(net.train(ep, batch=8, lr=lr, first=0, count=a.train))
+    t_train = time.time() - t0
+    after = net.eval_loss(a.train, nho)
+    rows = []
+    nev = nho if a.eval <= 0 else min(a.eval, nho)
+    for j in range(nev):
+        q, r0, eps = pts[a.train + j]
+        A = As[a.train + j]
+        build(q, r0, eps)
+        X0 = np.zeros((ctx.N, 40), dtype=np.complex128)
+        X0[:, :32] = net.predict(net.glob(q, r0, eps))
+        t_pred = ctx.last_ms
+        X0[:, 32:] = np.random.default_rng(j).standard_normal((ctx.N, 8))
+        row = {"r0": r0, "eps": eps, "q": float(np.linalg.norm(q)),
+               "capture_learned": float(np.linalg.norm(A.conj().T @ np.linalg.qr(X0[:, :32])[0]) ** 2 / 32)}
+        W1c = ctx.bse_davidson(32, nb=40, tol=1e-12, max_iter=1, want_act=False, check=False)[0]
+        W1w = ctx.bse_davidson(32, nb=40, tol=1e-12, max_iter=1, X0=X0, want_act=False, check=False)[0]
+        for mode in (0, 1):
+            ctx.set_fast_product(mode)
+            Wc, _, _, itc, _ = ctx.bse_davidson(32, nb=40, tol=1e-6, want_act=False)
+            tc = ctx.last_ms
+            Ww, _, _, itw, _ = ctx.bse_davidson(32, nb=40, tol=1e-6, X0=X0, want_act=False)
+            tw = ctx.last_ms + t_pred
+            key = "fp64" if mode == 0 else "fast"
+            row[key] = {"cold_iters": itc, "cold_ms": tc, "learned_iters": itw, "learned_ms": tw}
+        ctx.set_fast_product(0)
+        Wd, _ = ctx.bse_solve(False, False, want_act=False)
+        row["first_rr_err_meV"] = {"cold": float(np.abs(W1c - Wd[:32]).max() * 1e3),
+                                   "learned": float(np.abs(W1w - Wd[:32]).max() * 1e3)}
+        row["final_err_meV"] = float(max(np.abs(Wc - Wd[:32]).max(), np.abs(Ww - Wd[:32]).max()) * 1e3)
+        rows.append(row)
+    summ = {"config": vars(a), "N": ctx.N, "data_s": t_data, "train_s": t_train, "heldout_loss": [before, after],
+            "train_loss_first_last": [hist[0], hist[-1]],
+            "mean_capture_learned": float(np.mean([r["capture_learned"] for r in rows])),
+            "mean_first_rr_err_meV": {k: float(np.mean([r["first_rr_err_meV"][k] for r in rows]))
+                                      for k in ("cold", "learned")},
+            "mean_iters": {f"{m}_{k}": float(np.mean([r[m][f"{k}_iters"] for r in rows]))
+                           for m in ("fp64", "fast") for k in ("cold", "learned")},
+            "mean_ms": {f"{m}_{k}": float(np.mean([r[m][f"{k}_ms"] for r in rows]))
+                        for m in ("fp64", "fast") for k in ("cold", "learned")},
+            "max_final_err_meV": float(max(r["final_err_meV"] for r in rows)), "points": rows}
+    if a.save:
+        np.save(a.save, net.params())
+    print(json.dumps(summ))
+    net.close()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -28,7 +28,7 @@ EXPORTS = ["wtbg_create", "wtbg_destroy", "wtbg_error_string", "wtbg_last_error"
            "wtbg_net_destroy", "wtbg_net_num_params", "wtbg_net_get_params", "wtbg_net_set_params",
            "wtbg_net_features", "wtbg_net_add_sample", "wtbg_net_num_samples", "wtbg_net_train",
            "wtbg_net_eval_loss", "wtbg_net_predict", "wtbg_net_loss_grad", "wtbg_gemm_bf16",
-           "wtbg_bse_build_q"]
+           "wtbg_bse_build_q", "wtbg_set_temperature", "wtbg_eigsys", "wtbg_dos"]
 
 
 class WtbgError(RuntimeError):
@@ -104,6 +104,9 @@ def load_library(path: str = LIB_PATH):
         "wtbg_net_predict": (C.c_int, [P, dp, dp]),
         "wtbg_net_loss_grad": (C.c_int, [P, C.c_int, C.c_longlong, fp, fp, fp, fp, fp]),
         "wtbg_bse_apply": (C.c_int, [P, C.c_int, dp, dp]),
+        "wtbg_set_temperature": (C.c_int, [P, C.c_int, C.c_double]),
+        "wtbg_eigsys": (C.c_int, [P, C.c_int, dp, dp, dp, ip]),
+        "wtbg_dos": (C.c_int, [P, C.c_longlong, dp, dp, C.c_int, C.c_longlong, C.c_int, dp, C.c_double, dp]),
         "wtbg_bse_build_q": (C.c_int, [P, C.c_int, dp, dp, C.POINTER(Coulomb)]),
         "wtbg_gemm_bf16": (C.c_int, [P, C.c_int, C.c_int, C.c_int, fp, fp, fp]),
         "wtbg_spectrum_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, ip, ip, C.c_double,
@@ -283,6 +286,31 @@ class Context:
                                                     float(numbse), float(sme), int(bool(renorm)), float(spinf),
                                                     _dp(om), _fp(eps)))
         return om, eps
+
+    def eigsys(self, kpt, want_vectors: bool = True):
+        """Every band at every k: (eig (nk, w), vec (nk, w, w) or None, nocp (nk,))."""
+        k = _f64(kpt)
+        nk = k.shape[0]
+        e = np.zeros((nk, self.w), order="F")
+        v = np.zeros((nk, self.w, self.w), dtype=np.complex128, order="F") if want_vectors else None
+        no = np.zeros(nk, dtype=np.int32)
+        self._check(self.lib.wtbg_eigsys(self.h, nk, _dp(k), _dp(e),
+                                         v.ctypes.data_as(C.POINTER(C.c_double)) if v is not None else None, _ip(no)))
+        return e, v, no
+
+    def dos(self, etb, weights, nkpt, en, sme):
+        """endos over the energy grid en for each weight column: (nw, ncol)."""
+        etb = _f64(etb)
+        w = _f64(np.asarray(weights).reshape(etb.shape[0], -1))
+        en = _f64(en)
+        out = np.zeros((en.shape[0], w.shape[1]), order="F")
+        self._check(self.lib.wtbg_dos(self.h, etb.shape[0], _dp(etb), _dp(w), w.shape[1], int(nkpt), en.shape[0],
+                                      _dp(en), float(sme), _dp(out)))
+        return out
+
+    def set_temperature(self, on: bool, temp: float = 0.0) -> None:
+        """Temperature BSE (occupation factors f_v - f_c) for the later stages."""
+        self._check(self.lib.wtbg_set_temperature(self.h, int(bool(on)), float(temp)))
 
     def set_fast_product(self, mode: int) -> None:
         """0: FP64 product; 1: split-BF16 tensor-core product (Davidson, Haydock, bse_apply)."""
