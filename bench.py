@@ -236,7 +236,7 @@ def peak_rel_error(ref, x):
     return float(np.abs(x[pk] - ref[pk]).max() / np.abs(ref).max())
 
 
-def e2e_run(workdir, wl):
+def e2e_run(workdir, wl, device=0):
     lib = C.CDLL(wbuild.DRIVER_LIB)
 
     class Timings(C.Structure):
@@ -247,7 +247,7 @@ def e2e_run(workdir, wl):
     tm = Timings()
     err = C.create_string_buffer(1024)
     t0 = time.perf_counter()
-    rc = lib.wtb_run(deck_text(wl, workdir).encode(), 0, C.byref(tm), err, 1024)
+    rc = lib.wtb_run(deck_text(wl, workdir).encode(), device, C.byref(tm), err, 1024)
     t1 = time.perf_counter()
     if rc != 0:
         raise RuntimeError(err.value.decode())
@@ -315,6 +315,15 @@ def cpu_baseline(wl, model, budget_s=30.0):
 
 
 # ----------------------------------------------------------------------------- main
+def max_over_ranks(values, dist):
+    """Element-wise max of per-rank timings over the process group (the whole job ends when
+    its slowest replica ends)."""
+    import torch
+    tt = torch.tensor(list(values), dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return [float(x) for x in tt]
+
+
 def ncu_launch_summary(path: str) -> str:
     """Per-kernel launches, total device time and share from an ncu CSV launch list
     (``ncu --metrics gpu__time_duration.sum --csv --log-file path``)."""
@@ -403,7 +412,7 @@ def main():
         return
 
     wbuild.build()
-    ctx = wtbgpu.Context(0)
+    ctx = wtbgpu.Context(local)   # one replica per GPU (LOCAL_RANK)
     ctx.set_model(model)
     kpt = kmesh(wl["n"], model.rlat)
     c = wtbgpu.coulomb_params("V2DRK", [wl["n"], wl["n"], 1], 1e-3, [1, 1, 1], 1.0, 1.0, 0.0, wl["r0"])
@@ -465,15 +474,12 @@ def main():
     e2e_times = []
     e2e_parts = None
     for _ in range(max(1, min(args.steps, 2))):
-        t, e2e_parts = e2e_run(workdir, wl)
+        t, e2e_parts = e2e_run(workdir, wl, local)
         e2e_times.append(t)
     shutil.rmtree(workdir, ignore_errors=True)
     t_e2e = float(np.mean(e2e_times))
     if dist:
-        import torch
-        tt = torch.tensor([t_dev, t_e2e], dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_dev, t_e2e = float(tt[0]), float(tt[1])
+        t_dev, t_e2e = max_over_ranks([t_dev, t_e2e], dist)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
