@@ -92,10 +92,16 @@ __global__ void __launch_bounds__(256) k_hemm(const double2* __restrict__ A, lon
     for (int c = 0; c < TB; ++c) {
       const double2 h0 = tile[c][r], h1 = tile[c][r + 32];
 #pragma unroll
-      for (int v = 0; v < MV; ++v) {
+      for (int v = 0; v < MV; ++v) {   // acc += h x as four FMAs each
         const double2 x = xs[c][vg * MV + v];
-        acc[0][v] = cadd(acc[0][v], cmul(h0, x));
-        acc[1][v] = cadd(acc[1][v], cmul(h1, x));
+        acc[0][v].x = fma(h0.x, x.x, acc[0][v].x);
+        acc[0][v].x = fma(-h0.y, x.y, acc[0][v].x);
+        acc[0][v].y = fma(h0.x, x.y, acc[0][v].y);
+        acc[0][v].y = fma(h0.y, x.x, acc[0][v].y);
+        acc[1][v].x = fma(h1.x, x.x, acc[1][v].x);
+        acc[1][v].x = fma(-h1.y, x.y, acc[1][v].x);
+        acc[1][v].y = fma(h1.x, x.y, acc[1][v].y);
+        acc[1][v].y = fma(h1.y, x.x, acc[1][v].y);
       }
     }
   }
@@ -744,6 +750,14 @@ __global__ void __launch_bounds__(RR_THREADS) k_rr_tridiag(const double2* Min, i
   if (tid == 0) *status = 0;
 }
 
+// out(:, j) = in(:, idx[j])
+__global__ void k_gather_cols(const double2* in, long long N, const int* idx, double2* out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const int j = blockIdx.y;
+  out[i + (long long)j * N] = in[i + (long long)idx[j] * N];
+}
+
 __global__ void k_diag(const double2* A, long long N, double* D) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i < N) D[i] = A[i + i * N].x;
@@ -993,6 +1007,9 @@ int run_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, doub
     ~FastGuard() { c->fast_mode = saved; }
   } guard{ctx, ctx->fast_mode};
   constexpr double kFastSwitch = 2e-5, kFastStall = 5e-4;
+  double lock_best = 1e300;
+  int lock_stall = 0;
+  bool lock_off = false;
   double best = 1e300;
   int since_best = 0;
   ctx->stats.dav_fast_iters = 0;
@@ -1029,14 +1046,47 @@ int run_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, doub
         continue;
       }
     }
+    // With the FP64 product (compute-bound, cost ~ block width) only the directions of the
+    // largest residuals are expanded: a multiple of 8 covering every unconverged wanted state.
+    // Only near convergence (worst < 1e-4 eV), and while the best residual keeps falling.
+    int m_act = nb;
+    const bool lock_zone = !ctx->fast_mode && worst < 1e-4;
+    if (lock_zone) {
+      if (worst < 0.5 * lock_best) {
+        lock_best = worst;
+        lock_stall = 0;
+      } else if (++lock_stall >= 8) {
+        lock_off = true;
+      }
+    }
+    if (lock_zone && !lock_off) {
+      int nun = 0;
+      for (int v = 0; v < nev; ++v) nun += (res[v] >= tol);
+      m_act = std::min(nb, std::max(16, (nun + 7) / 8 * 8));
+      if (m_act < nb) {
+        std::vector<int> ord(nb);
+        for (int v = 0; v < nb; ++v) ord[v] = v;
+        // unconverged wanted states first, then the rest, each by decreasing residual
+        auto want = [&](int v) { return v < nev && res[v] >= tol; };
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+          if (want(a) != want(b)) return want(a);
+          return res[a] > res[b];
+        });
+        CK(cudaMemcpyAsync(d_idx, ord.data(), m_act * 4, cudaMemcpyHostToDevice, s));
+        k_gather_cols<<<dim3((unsigned)((N + 255) / 256), m_act), 256, 0, s>>>(T, N, d_idx, w.Xn);
+        WTBG_COUNT(ctx, 1);
+        CKL("k_gather_cols");
+        CK(cudaMemcpyAsync(T, w.Xn, (size_t)N * m_act * 16, cudaMemcpyDeviceToDevice, s));
+      }
+    }
     // T <- T - X (X^H T), twice; orthonormalise
     for (int pass = 0; pass < 2; ++pass) {
-      if (int r = gram(ctx, X, (int)N, nb, T, (int)N, nb, w.small + 2 * kMaxRR * kMaxRR, w.part)) return r;
-      if (int r = tall(ctx, X, (int)N, nb, w.small + 2 * kMaxRR * kMaxRR, nb, T, (int)N, true)) return r;
+      if (int r = gram(ctx, X, (int)N, nb, T, (int)N, m_act, w.small + 2 * kMaxRR * kMaxRR, w.part)) return r;
+      if (int r = tall(ctx, X, (int)N, nb, w.small + 2 * kMaxRR * kMaxRR, m_act, T, (int)N, true)) return r;
     }
-    if (int r = cholqr2(ctx, T, nb, w.Xn, w)) return r;
-    if (int r = hemm(ctx, T, (int)N, nb, HT, (int)N, w.Yp)) return r;
-    if (int r = rr(w.V, w.HV, n2)) return r;
+    if (int r = cholqr2(ctx, T, m_act, w.Xn, w)) return r;
+    if (int r = hemm(ctx, T, (int)N, m_act, HT, (int)N, w.Yp)) return r;
+    if (int r = rr(w.V, w.HV, nb + m_act)) return r;
   }
   if (iters) *iters = it;
   if (maxres) *maxres = worst;
