@@ -143,6 +143,15 @@ int wtbg_bse_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter,
                       const double* X0, int dtfull, int cpol, double* W, double* act, double* X,
                       int* iters, double* maxres);
 
+/* ---- bands of several models in one persistent launch (no counterpart in the reference,
+ *      which loops eigsys per k per run): model m is the one set in ctxs[m] (all on one
+ *      device; uneven w, nvec and meshes allowed) and gets exactly the state of
+ *      wtbg_bands(ctxs[m], nk[m], kpt[m], nv[m], nc[m], ...): every (model, k) item runs in one
+ *      kernel that takes items, largest w first, from a global counter.  kpt[m] (nk[m], 3)
+ *      column-major; egap (nmod) or NULL.  Runs on ctxs[0]'s stream. */
+int wtbg_bands_batch(wtbg_ctx* const* ctxs, int nmod, const int* nk, const double* const* kpt, const int* nv,
+                     const int* nc, double* egap);
+
 /* ---- eigsys for every band (hamiltonian_tb.f90:2-137 as the band-structure and DOS tools
  *      call it: bands-kpath-tool.f90:66-80, tdos-tool.f90:98-120): eig (nk, w) ascending with
  *      the scissors scs on the states above E_F, vec (nk, w, w) complex(8) = component m of

@@ -385,6 +385,59 @@ int wtbg_bse_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter,
   return WTBG_OK;
 }
 
+int wtbg_bands_batch(wtbg_ctx* const* ctxs, int nmod, const int* nk, const double* const* kpt, const int* nv,
+                     const int* nc, double* egap) {
+  if (!ctxs || nmod < 1 || !nk || !kpt || !nv || !nc) return WTBG_ERR_ARG;
+  wtbg_ctx* ctx = ctxs[0];
+  if (!ctx) return WTBG_ERR_ARG;
+  for (int m = 0; m < nmod; ++m) {
+    wtbg_ctx* c = ctxs[m];
+    if (!c || c->device != ctx->device) return set_err(ctx, WTBG_ERR_ARG, "bands_batch: contexts must share a device");
+    if (c->w == 0) return set_err(ctx, WTBG_ERR_STATE, "bands_batch: a context has no model");
+    if (nk[m] <= 0 || nv[m] <= 0 || nc[m] <= 0 || !kpt[m] || nv[m] + nc[m] > c->w)
+      return set_err(ctx, WTBG_ERR_ARG, "bands_batch: bad sizes for model " + std::to_string(m));
+  }
+  if (int r = set_device(ctx)) return r;
+  Timer t(ctx);
+  for (int m = 0; m < nmod; ++m) {
+    wtbg_ctx* c = ctxs[m];
+    c->nk = nk[m];
+    c->nv = nv[m];
+    c->nc = nc[m];
+    c->N = (long long)nk[m] * nc[m] * nv[m];
+    const int nb = nv[m] + nc[m];
+    std::vector<double> kp(3 * (size_t)nk[m]);
+    for (int k = 0; k < nk[m]; ++k)
+      for (int a = 0; a < 3; ++a) kp[3 * k + a] = kpt[m][k + (size_t)nk[m] * a];
+    if (int r = ensure(c, c->kpt, kp.size() * 8)) return r;
+    if (int r = ensure(c, c->eig, (size_t)nk[m] * nb * 8)) return r;
+    if (int r = ensure(c, c->U, (size_t)nk[m] * nb * c->w * 16)) return r;
+    if (int r = ensure(c, c->nocp, (size_t)nk[m] * 4)) return r;
+    if (int r = ensure(c, c->kstat, (size_t)nk[m] * 4)) return r;
+    // every upload on the launching stream, so the batch kernel sees them in order
+    CK(cudaMemcpyAsync(c->kpt.p, kp.data(), kp.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  if (int r = launch_bands_batch(ctxs, nmod)) return r;
+  if (int r = t.stop()) return r;
+  for (int m = 0; m < nmod; ++m) {
+    wtbg_ctx* c = ctxs[m];
+    if (int r = check_kstat(c, nk[m])) return set_err(ctx, r, "bands_batch: model " + std::to_string(m) + ": " + c->err);
+    c->have_bands = true;
+    c->have_velocity = c->have_matrix = c->have_solution = false;
+    c->fast_ready = false;
+    if (egap) {
+      const int nb = nv[m] + nc[m];
+      std::vector<double> e((size_t)nk[m] * nb);
+      CK(cudaMemcpy(e.data(), c->eig.p, e.size() * 8, cudaMemcpyDeviceToHost));
+      double gap = 50.0;
+      for (int k = 0; k < nk[m]; ++k) gap = std::min(gap, e[(size_t)k * nb + nv[m]] - e[(size_t)k * nb + nv[m] - 1]);
+      egap[m] = gap;
+    }
+  }
+  return WTBG_OK;
+}
+
 int wtbg_eigsys(wtbg_ctx* ctx, int nk, const double* kpt, double* eig, double* vec, int* nocp) {
   if (!ctx || nk <= 0 || !kpt || !eig) return WTBG_ERR_ARG;
   if (ctx->w == 0) return set_err(ctx, WTBG_ERR_STATE, "eigsys: no model");

@@ -24,6 +24,8 @@
 
 #include "common.cuh"
 
+#include <algorithm>
+
 namespace {
 
 constexpr int kBandsThreads = 256;
@@ -59,8 +61,9 @@ struct BandsArgs {
   int all;         // 1: every band (eigsys as the band and DOS tools call it), nb = w
 };
 
-__global__ void __launch_bounds__(kBandsThreads) k_bands(BandsArgs a) {
-  extern __shared__ __align__(16) unsigned char smem[];
+// One k-point per iteration of the loop k = k0, k0 + kstride, ... (shared-memory work area
+// smem, sized by bands_smem for this model).
+__device__ __forceinline__ void bands_body(const BandsArgs& a, int k0, int kstride, unsigned char* smem) {
   const int w = a.w, nvec = a.nvec, tid = threadIdx.x, bs = blockDim.x;
   const int ww = w * w;
   const int m2 = w + (w & 1);
@@ -76,7 +79,7 @@ __global__ void __launch_bounds__(kBandsThreads) k_bands(BandsArgs a) {
   __shared__ double s_tolabs;
   __shared__ int s_nocp, s_stat;
 
-  for (int k = blockIdx.x; k < a.nk; k += gridDim.x) {
+  for (int k = k0; k < a.nk; k += kstride) {
     const double kx = a.kpt[3 * k], ky = a.kpt[3 * k + 1], kz = a.kpt[3 * k + 2];
     for (int R = tid; R < nvec; R += bs) ph[R] = phase_of(kx, ky, kz, a.Rcart + 3 * R);
     __syncthreads();
@@ -240,6 +243,30 @@ __global__ void __launch_bounds__(kBandsThreads) k_bands(BandsArgs a) {
       }
     }
     __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kBandsThreads) k_bands(BandsArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  bands_body(a, blockIdx.x, gridDim.x, smem);
+}
+
+// Persistent ragged batch: every (model, k) item of several models (different w, nvec and
+// meshes) in one launch. Items are ordered by decreasing w; each CTA takes the next item
+// from a global counter, so the expensive large-w items start first.
+__global__ void __launch_bounds__(kBandsThreads) k_bands_batch(const BandsArgs* mods, const int* item_mod,
+                                                               const int* item_k, int nitems, int* counter) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_item;
+  while (true) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= nitems) break;
+    const BandsArgs a = mods[item_mod[it]];
+    const int k = item_k[it];
+    bands_body(a, k, a.nk, smem);
   }
 }
 
@@ -420,6 +447,79 @@ int launch_bands(wtbg_ctx* ctx, bool q_mesh) {
   int grid = ctx->nk;
   k_bands<<<grid, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
   CKL("k_bands");
+  return 0;
+}
+
+// Bands of several models on one device in one persistent launch (the contexts share a
+// device; the launch goes on the first context's stream). Each context gets its own k-mesh
+// bands exactly as launch_bands would produce them.
+int launch_bands_batch(wtbg_ctx* const* ctxs, int nmod) {
+  wtbg_ctx* c0 = ctxs[0];
+  wtbg_ctx* ctx = c0;   // errors and scratch on the first context
+  std::vector<BandsArgs> mods(nmod);
+  std::vector<std::pair<int, int>> order;   // (w, model)
+  size_t smem = 0;
+  long long nitems = 0;
+  for (int m = 0; m < nmod; ++m) {
+    wtbg_ctx* cm = ctxs[m];
+    BandsArgs& a = mods[m];
+    a.HR = cm->HR.as<double2>();
+    a.Rcart = cm->Rcart.as<double>();
+    a.invdeg = cm->invdeg.as<double>();
+    a.nvec = cm->nvec;
+    a.w = cm->w;
+    a.nk = cm->nk;
+    a.ef32 = (double)(float)cm->efermi;
+    a.scs = cm->scs;
+    a.nv = cm->nv;
+    a.nc = cm->nc;
+    a.kpt = cm->kpt.as<double>();
+    a.eig = cm->eig.as<double>();
+    a.U = cm->U.as<double2>();
+    a.nocp = cm->nocp.as<int>();
+    a.kstat = cm->kstat.as<int>();
+    a.all = 0;
+    smem = std::max(smem, bands_smem(cm->w, cm->nvec));
+    order.push_back({cm->w, m});
+    nitems += cm->nk;
+  }
+  if (smem > 200 * 1024) return set_err(c0, WTBG_ERR_UNSUPPORTED, "bands: model too large for shared memory");
+  std::stable_sort(order.begin(), order.end(), [](const std::pair<int, int>& x, const std::pair<int, int>& y) {
+    return x.first > y.first;
+  });
+  std::vector<int> im, ik;
+  im.reserve(nitems);
+  ik.reserve(nitems);
+  for (auto& o : order)
+    for (int k = 0; k < ctxs[o.second]->nk; ++k) {
+      im.push_back(o.second);
+      ik.push_back(k);
+    }
+  const size_t b_mod = (size_t)nmod * sizeof(BandsArgs), b_it = (size_t)nitems * 4;
+  auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+  ENSURE(c0->tmp, up(b_mod) + 2 * up(b_it) + 256);
+  char* base = c0->tmp.as<char>();
+  BandsArgs* d_mod = reinterpret_cast<BandsArgs*>(base);
+  int* d_im = reinterpret_cast<int*>(base + up(b_mod));
+  int* d_ik = reinterpret_cast<int*>(base + up(b_mod) + up(b_it));
+  int* d_cnt = reinterpret_cast<int*>(base + up(b_mod) + 2 * up(b_it));
+  cudaStream_t s = c0->stream;
+  CK(cudaMemcpyAsync(d_mod, mods.data(), b_mod, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_im, im.data(), b_it, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_ik, ik.data(), b_it, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(d_cnt, 0, 4, s));
+  CK(cudaFuncSetAttribute(k_bands_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, nsm = 148, per = 1;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bands_batch, kBandsThreads, smem));
+  const int grid = (int)std::min<long long>(nitems, (long long)nsm * std::max(1, per));
+  k_bands_batch<<<grid, kBandsThreads, smem, s>>>(d_mod, d_im, d_ik, (int)nitems, d_cnt);
+  WTBG_COUNT(c0, 1);
+  {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c0, e, "k_bands_batch");
+  }
   return 0;
 }
 

@@ -182,6 +182,7 @@ inline int set_device(wtbg_ctx* ctx) {
 }
 
 
+int launch_bands_batch(wtbg_ctx* const* ctxs, int nmod);
 int launch_eigsys_all(wtbg_ctx* ctx, int nk, const double* d_kpt, double* d_eig, double2* d_U, int* d_nocp,
                       int* d_kstat);
 int launch_dos(wtbg_ctx* ctx, const double* d_etb, const double* d_w, long long ndim, int ncol, const double* d_en,

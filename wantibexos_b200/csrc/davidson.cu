@@ -1006,7 +1006,7 @@ int run_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, doub
     int saved;
     ~FastGuard() { c->fast_mode = saved; }
   } guard{ctx, ctx->fast_mode};
-  constexpr double kFastSwitch = 2e-5, kFastStall = 5e-4;
+  constexpr double kFastSwitch = 4e-6, kFastStall = 5e-4;
   double lock_best = 1e300;
   int lock_stall = 0;
   bool lock_off = false;
@@ -1032,14 +1032,14 @@ int run_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, doub
     if (worst < tol) break;
     if (ctx->fast_mode) {
       // the worst residual of a block is not monotone: stagnation counts only near the
-      // product's rounding level (no halving of the best residual for 10 iterations)
+      // product's rounding level (no halving of the best residual for 6 iterations)
       if (worst < 0.5 * best) {
         best = worst;
         since_best = 0;
       } else if (best < kFastStall) {
         ++since_best;
       }
-      if (worst < std::max(kFastSwitch, tol) || since_best >= 10) {
+      if (worst < std::max(kFastSwitch, tol) || since_best >= 6) {
         ctx->fast_mode = 0;
         if (int r = hemm(ctx, X, (int)N, nb, HX, (int)N, w.Yp)) return r;
         if (int r = rr(X, HX, nb)) return r;

@@ -28,7 +28,8 @@ EXPORTS = ["wtbg_create", "wtbg_destroy", "wtbg_error_string", "wtbg_last_error"
            "wtbg_net_destroy", "wtbg_net_num_params", "wtbg_net_get_params", "wtbg_net_set_params",
            "wtbg_net_features", "wtbg_net_add_sample", "wtbg_net_num_samples", "wtbg_net_train",
            "wtbg_net_eval_loss", "wtbg_net_predict", "wtbg_net_loss_grad", "wtbg_gemm_bf16",
-           "wtbg_bse_build_q", "wtbg_set_temperature", "wtbg_eigsys", "wtbg_dos"]
+           "wtbg_bse_build_q", "wtbg_set_temperature", "wtbg_eigsys", "wtbg_dos",
+           "wtbg_bands_batch"]
 
 
 class WtbgError(RuntimeError):
@@ -106,6 +107,7 @@ def load_library(path: str = LIB_PATH):
         "wtbg_bse_apply": (C.c_int, [P, C.c_int, dp, dp]),
         "wtbg_set_temperature": (C.c_int, [P, C.c_int, C.c_double]),
         "wtbg_eigsys": (C.c_int, [P, C.c_int, dp, dp, dp, ip]),
+        "wtbg_bands_batch": (C.c_int, [C.POINTER(P), C.c_int, ip, C.POINTER(dp), ip, ip, dp]),
         "wtbg_dos": (C.c_int, [P, C.c_longlong, dp, dp, C.c_int, C.c_longlong, C.c_int, dp, C.c_double, dp]),
         "wtbg_bse_build_q": (C.c_int, [P, C.c_int, dp, dp, C.POINTER(Coulomb)]),
         "wtbg_gemm_bf16": (C.c_int, [P, C.c_int, C.c_int, C.c_int, fp, fp, fp]),
@@ -368,6 +370,26 @@ class Context:
         W = np.zeros(self.N)
         self._check(self.lib.wtbg_bse_q_eigenvalues(self.h, kq.shape[0], _dp(kq), _dp(q), C.byref(coul), _dp(W)))
         return W
+
+
+def bands_batch(ctxs, kpts, nvs, ncs):
+    """One persistent launch for the k-mesh bands of several contexts (models); returns the
+    direct gap of each. Afterwards each context is as after its own Context.bands call."""
+    P, dp = C.c_void_p, C.POINTER(C.c_double)
+    n = len(ctxs)
+    arr = (P * n)(*[c.h for c in ctxs])
+    ks = [_f64(k) for k in kpts]
+    kp = (dp * n)(*[_dp(k) for k in ks])
+    nk = np.array([k.shape[0] for k in ks], dtype=np.int32)
+    nv = np.array(nvs, dtype=np.int32)
+    nc = np.array(ncs, dtype=np.int32)
+    gap = np.zeros(n)
+    lib = ctxs[0].lib
+    ctxs[0]._check(lib.wtbg_bands_batch(arr, n, _ip(nk), kp, _ip(nv), _ip(nc), _dp(gap)))
+    for c, k, a, b in zip(ctxs, ks, nvs, ncs):
+        c.nk, c.nv, c.nc = k.shape[0], a, b
+        c.N = k.shape[0] * a * b
+    return gap
 
 
 class Net:
