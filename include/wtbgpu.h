@@ -291,6 +291,16 @@ int wtbg_bse_build_q(wtbg_ctx* ctx, int nk, const double* kptq, const double* q4
 int wtbg_bse_q_eigenvalues(wtbg_ctx* ctx, int nk, const double* kptq, const double* q4,
                            const wtbg_coulomb* p, double* W);
 
+/* ---- exciton band structure, all Q of a path in one call (the Q loop of bsebnds,
+ *      bse_kpath-tool.f90:246-435).  kptq holds nq blocks of (nk,3) k+Q meshes, q4 nq rows of
+ *      (distance, qx, qy, qz); W (nq, N) receives each Q's eigenvalues ascending, identical to
+ *      nq calls of wtbg_bse_q_eigenvalues.  With use_graph != 0 the tridiagonalisation (the
+ *      launch-bound part: four launches per column) runs as one captured CUDA graph replayed
+ *      for every Q after the first; the mat-vec chunk is autotuned per (device, N) on the
+ *      first Q.  ms_q (nq, may be NULL) receives the device time of each Q. */
+int wtbg_bse_q_batch(wtbg_ctx* ctx, int nk, int nq, const double* kptq, const double* q4,
+                     const wtbg_coulomb* p, int use_graph, double* W, double* ms_q);
+
 #ifdef __cplusplus
 }
 #endif

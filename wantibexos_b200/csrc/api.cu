@@ -132,6 +132,7 @@ int wtbg_destroy(wtbg_ctx* ctx) {
                     &ctx->sp_om, &ctx->tmp, &ctx->tmp2, &ctx->istat};
   for (DevBuf* b : bufs) free_buf(*b);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
+  if (ctx->tri_exec) cudaGraphExecDestroy(ctx->tri_exec);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   cudaStreamDestroy(ctx->stream);
@@ -711,6 +712,87 @@ int wtbg_bse_q_eigenvalues(wtbg_ctx* ctx, int nk, const double* kptq, const doub
   ctx->have_solution = false;
   memcpy(W, ctx->lam_host.data(), (size_t)N * 8);
   return WTBG_OK;
+}
+
+// Tridiagonalises the current matrix through one captured CUDA graph of the whole
+// column loop. The first call for a given N (or after any work buffer moved) runs eagerly,
+// which also sizes the buffers and autotunes the mat-vec chunk; the next call captures the
+// launch sequence into a graph, and every later call replays it. The graph reads the matrix
+// and writes the tridiagonal through the context's buffers, so it serves every Q of a batch.
+static int tridiagonalise_graph(wtbg_ctx* ctx) {
+  auto signature = [ctx]() {
+    return std::vector<const void*>{ctx->H.p,     ctx->d.p,    ctx->e.p,     ctx->tau.p,  ctx->g.p,
+                                     ctx->Wp.p,    ctx->slots.p, ctx->part.p, ctx->scal.p, ctx->h.p,
+                                     ctx->fdeh.p,  (const void*)(intptr_t)ctx->N,
+                                     (const void*)(intptr_t)ctx->hemv_hs,
+                                     (const void*)(intptr_t)(ctx->have_velocity ? 1 + ctx->temp_on : 0)};
+  };
+  if (ctx->profiling) return run_tridiagonalise(ctx);   // per-launch events need host syncs
+  std::vector<const void*> sig = signature();
+  if (ctx->tri_exec && sig == ctx->tri_sig) {
+    CK(cudaGraphLaunch(ctx->tri_exec, ctx->stream));
+    WTBG_COUNT(ctx, ctx->tri_launches);
+    return 0;
+  }
+  if (ctx->tri_exec) {
+    cudaGraphExecDestroy(ctx->tri_exec);
+    ctx->tri_exec = nullptr;
+  }
+  if (sig != ctx->tri_sig) {
+    if (int r = run_tridiagonalise(ctx)) return r;
+    ctx->tri_sig = signature();
+    return 0;
+  }
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  const long long l0 = ctx->stats.launches;
+  const int r = run_tridiagonalise(ctx);
+  const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &graph);
+  const long long nl = ctx->stats.launches - l0;
+  ctx->stats.launches = l0;
+  if (r) {
+    if (graph) cudaGraphDestroy(graph);
+    return r;
+  }
+  if (ec != cudaSuccess) return cuda_fail(ctx, ec, "cudaStreamEndCapture(tridiagonalise)");
+  const cudaError_t ei = cudaGraphInstantiate(&ctx->tri_exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ei != cudaSuccess) {
+    ctx->tri_exec = nullptr;
+    return cuda_fail(ctx, ei, "cudaGraphInstantiate(tridiagonalise)");
+  }
+  if (signature() != sig) return set_err(ctx, WTBG_ERR_STATE, "tridiagonalise: work buffers moved during capture");
+  ctx->tri_launches = nl;
+  CK(cudaGraphLaunch(ctx->tri_exec, ctx->stream));
+  WTBG_COUNT(ctx, nl);
+  return 0;
+}
+
+int wtbg_bse_q_batch(wtbg_ctx* ctx, int nk, int nq, const double* kptq, const double* q4, const wtbg_coulomb* p,
+                     int use_graph, double* W, double* ms_q) {
+  if (!ctx || !kptq || !q4 || !p || !W || nq < 0) return WTBG_ERR_ARG;
+  if (nq == 0) return WTBG_OK;
+  const bool hv = ctx->have_velocity;
+  int r = 0;
+  for (int iq = 0; iq < nq && !r; ++iq) {
+    if ((r = wtbg_bse_build_q(ctx, nk, kptq + (size_t)iq * nk * 3, q4 + (size_t)iq * 4, p))) break;
+    const double ms_build = ctx->last_ms;
+    const long long N = ctx->N;
+    Timer t(ctx);
+    ctx->have_velocity = false;   // eigenvalues only: g not needed
+    r = use_graph ? tridiagonalise_graph(ctx) : run_tridiagonalise(ctx);
+    ctx->have_velocity = hv;
+    if (r) break;
+    if ((r = run_tridiagonal_solve(ctx, 0, 0, false))) break;
+    if ((r = t.stop())) break;
+    memcpy(W + (size_t)iq * N, ctx->lam_host.data(), (size_t)N * 8);
+    if (ms_q) ms_q[iq] = ms_build + ctx->last_ms;
+  }
+  ctx->have_velocity = hv;
+  ctx->have_matrix = false;
+  ctx->fast_ready = false;
+  ctx->have_solution = false;
+  return r ? r : WTBG_OK;
 }
 
 }  // extern "C"

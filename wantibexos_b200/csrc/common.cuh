@@ -85,6 +85,13 @@ struct wtbg_ctx {
   DevBuf fdeh;           // [N] double
   int ng = 5;            // velocity vectors carried through the reduction (10 with temperature)
 
+  // tridiagonalisation: autotuned mat-vec chunk, and the captured CUDA graph of the whole
+  // reduction for Q batches (valid while N and the work buffers stay the same)
+  int hemv_hs = 0;
+  cudaGraphExec_t tri_exec = nullptr;
+  std::vector<const void*> tri_sig;
+  long long tri_launches = 0;
+
   // fast form: split-BF16 planes of the kernel matrix for the tensor-core product
   int fast_mode = 0;
   bool fast_ready = false;
@@ -187,6 +194,7 @@ int launch_eigsys_all(wtbg_ctx* ctx, int nk, const double* d_kpt, double* d_eig,
                       int* d_kstat);
 int launch_dos(wtbg_ctx* ctx, const double* d_etb, const double* d_w, long long ndim, int ncol, const double* d_en,
                int nw, double sme, long long nkpt, double* d_out);
+int autotune_hemv(wtbg_ctx* ctx, int* hs_out);
 int ensure_fdeh(wtbg_ctx* ctx, bool q_mesh);
 int fill_g_vectors(wtbg_ctx* ctx, double2* g);
 int run_fast_setup(wtbg_ctx* ctx);

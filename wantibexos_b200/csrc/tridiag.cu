@@ -20,6 +20,9 @@
 
 #include "common.cuh"
 
+#include <map>
+#include <mutex>
+
 namespace {
 
 constexpr int TB = WTBG_HEMV_TILE;   // 64
@@ -201,8 +204,8 @@ __global__ void __launch_bounds__(RB) k_colC(double2* A, long long N, const doub
 // A_IJ x_J go to slot[I][J] per tile; the column sums A_IJ^H x_I stay in registers across
 // the chunk and go to slot[J][I0] (I0 = first tile of the chunk, zeros in the rest of the
 // chunk's slots), so that y_a = sum_b slot[a][b] over b in the trailing block range.
-constexpr int HS = 8;
-
+// HS (tiles per CTA chunk) is a template parameter; the autotuner below picks it per (device, N).
+template <int HS>
 __global__ void __launch_bounds__(256, 2) k_hemv(const double2* __restrict__ A, long long N, int i, int nblk,
                                                  double2* __restrict__ slots) {
   __shared__ double2 xJs[TB];
@@ -455,6 +458,67 @@ __global__ void k_copy_g(const double2* h, double2* g, long long n) {
 
 }  // namespace
 
+namespace {
+
+void launch_hemv(int hs, int nt, cudaStream_t s, const double2* A, long long N, int i, int nblk, double2* slots) {
+  if (hs == 4)
+    k_hemv<4><<<dim3(nt, (nt + 3) / 4), 256, 0, s>>>(A, N, i, nblk, slots);
+  else if (hs == 16)
+    k_hemv<16><<<dim3(nt, (nt + 15) / 16), 256, 0, s>>>(A, N, i, nblk, slots);
+  else
+    k_hemv<8><<<dim3(nt, (nt + 7) / 8), 256, 0, s>>>(A, N, i, nblk, slots);
+}
+
+}  // namespace
+
+// Autotuner for the mat-vec chunk (tiles per CTA, 4 / 8 / 16): times each variant on the
+// column N/4 (three launches each, CUDA events; the launches only write the slot partials,
+// which the reduction overwrites) and keeps the fastest per (device, N).
+int autotune_hemv(wtbg_ctx* ctx, int* hs_out) {
+  static std::mutex mu;
+  static std::map<std::pair<int, long long>, int> cache;
+  const long long N = ctx->N;
+  const std::pair<int, long long> key(ctx->device, N);
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      *hs_out = it->second;
+      return 0;
+    }
+  }
+  const int nblk = (int)((N + TB - 1) / TB);
+  *hs_out = 8;
+  if (N < 4 * TB) return 0;
+  ENSURE(ctx->slots, (size_t)nblk * nblk * TB * 16);
+  if (int r = ensure_events(ctx, 2)) return r;
+  const int i = (int)(N / 4);
+  const int nt = nblk - (i + 1) / TB;
+  const int cand[3] = {4, 8, 16};
+  float best = 1e30f;
+  for (int c : cand) {
+    float tot = 0.f;
+    for (int rep = 0; rep < 4; ++rep) {
+      CK(cudaEventRecord(ctx->evpool[0], ctx->stream));
+      launch_hemv(c, nt, ctx->stream, ctx->H.as<double2>(), N, i, nblk, ctx->slots.as<double2>());
+      CK(cudaEventRecord(ctx->evpool[1], ctx->stream));
+      CK(cudaEventSynchronize(ctx->evpool[1]));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ctx->evpool[0], ctx->evpool[1]));
+      if (rep > 0) tot += ms;   // the first launch warms up
+    }
+    WTBG_COUNT(ctx, 4);
+    if (tot < best) {
+      best = tot;
+      *hs_out = c;
+    }
+  }
+  CKL("autotune_hemv");
+  std::lock_guard<std::mutex> g(mu);
+  cache[key] = *hs_out;
+  return 0;
+}
+
 int run_tridiagonalise(wtbg_ctx* ctx) {
   const long long N = ctx->N;
   if (N < 2) return set_err(ctx, WTBG_ERR_ARG, "tridiagonalise: N < 2");
@@ -481,6 +545,15 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
   double2* partE = partC + (size_t)maxRB * (2 * NB + NG);
   ColState* st = ctx->scal.as<ColState>();
   cudaStream_t s = ctx->stream;
+  int hs = 8;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(s, &cap));
+  if (cap == cudaStreamCaptureStatusNone) {
+    if (int r = autotune_hemv(ctx, &hs)) return r;
+  } else {
+    hs = ctx->hemv_hs > 0 ? ctx->hemv_hs : 8;   // chosen before the capture
+  }
+  ctx->hemv_hs = hs;
   CK(cudaMemsetAsync(st, 0, sizeof(ColState), s));
 
   const int ng = (ctx->have_velocity && ctx->temp_on) ? 10 : 5;
@@ -509,7 +582,7 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
       const int b0 = (i + 1) / TB;
       const int nt = nblk - b0;
       if (prof) cudaEventRecord(ctx->evpool[2 * i], s);
-      k_hemv<<<dim3(nt, (nt + HS - 1) / HS), 256, 0, s>>>(A, N, i, nblk, slots); WTBG_COUNT(ctx, 1);
+      launch_hemv(hs, nt, s, A, N, i, nblk, slots); WTBG_COUNT(ctx, 1);
       if (prof) cudaEventRecord(ctx->evpool[2 * i + 1], s);
       k_colE<<<nt, 256, 0, s>>>(A, N, Wp, (int)j0, p, i, nblk, slots, st, g, ng, partE); WTBG_COUNT(ctx, 1);
     }

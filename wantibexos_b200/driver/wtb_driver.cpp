@@ -921,15 +921,19 @@ void bsebnds(wtbg_ctx* ctx, const Deck& d, const Model& m) {
   log.flush();
   wtbg_coulomb p = coulomb_of(d);
   std::vector<double> exk((size_t)N * nq);
+  // every Q in one batch call: the tridiagonalisation is a CUDA graph replayed per Q
+  std::vector<double> kqs, q4s;
+  kqs.reserve((size_t)nq * nk * 3);
   for (int iq = 0; iq < nq; ++iq) {
     const double q3[3] = {qp[iq][1], qp[iq][2], qp[iq][3]};
     std::vector<double> kq = kmesh(d.ngrid, d.mshift, m.rlat, q3);
-    double q4[4] = {qp[iq][0], qp[iq][1], qp[iq][2], qp[iq][3]};
-    gpu_check(ctx, wtbg_bse_q_eigenvalues(ctx, nk, kq.data(), q4, &p, exk.data() + (size_t)N * iq),
-              "wtbg_bse_q_eigenvalues");
-    log.line(" progress:" + LI(iq + 1) + " /" + LI(nq));
-    log.flush();
+    kqs.insert(kqs.end(), kq.begin(), kq.end());
+    for (int c = 0; c < 4; ++c) q4s.push_back(qp[iq][c]);
   }
+  gpu_check(ctx, wtbg_bse_q_batch(ctx, nk, nq, kqs.data(), q4s.data(), &p, 1, exk.data(), nullptr),
+            "wtbg_bse_q_batch");
+  for (int iq = 0; iq < nq; ++iq) log.line(" progress:" + LI(iq + 1) + " /" + LI(nq));
+  log.flush();
   std::string buf;
   for (long long i2 = 0; i2 < N; ++i2) {
     for (int iq = 0; iq < nq; ++iq) buf += LS((float)qp[iq][0]) + LD(exk[i2 + (size_t)N * iq]) + "\n";

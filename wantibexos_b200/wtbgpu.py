@@ -29,7 +29,7 @@ EXPORTS = ["wtbg_create", "wtbg_destroy", "wtbg_error_string", "wtbg_last_error"
            "wtbg_net_features", "wtbg_net_add_sample", "wtbg_net_num_samples", "wtbg_net_train",
            "wtbg_net_eval_loss", "wtbg_net_predict", "wtbg_net_loss_grad", "wtbg_gemm_bf16",
            "wtbg_bse_build_q", "wtbg_set_temperature", "wtbg_eigsys", "wtbg_dos",
-           "wtbg_bands_batch"]
+           "wtbg_bands_batch", "wtbg_bse_q_batch"]
 
 
 class WtbgError(RuntimeError):
@@ -83,6 +83,7 @@ def load_library(path: str = LIB_PATH):
         "wtbg_spectrum": (C.c_int, [P, C.c_int, C.c_int, dp, dp, ip, ip, C.c_double, C.c_double, C.c_double,
                                     C.c_double, C.c_double, C.c_int, C.c_double, dp, fp]),
         "wtbg_bse_q_eigenvalues": (C.c_int, [P, C.c_int, dp, dp, C.POINTER(Coulomb), dp]),
+        "wtbg_bse_q_batch": (C.c_int, [P, C.c_int, C.c_int, dp, dp, C.POINTER(Coulomb), C.c_int, dp, dp]),
         "wtbg_set_profiling": (C.c_int, [P, C.c_int]),
         "wtbg_get_stats": (C.c_int, [P, C.POINTER(Stats)]),
         "wtbg_reset_stats": (C.c_int, [P]),
@@ -370,6 +371,20 @@ class Context:
         W = np.zeros(self.N)
         self._check(self.lib.wtbg_bse_q_eigenvalues(self.h, kq.shape[0], _dp(kq), _dp(q), C.byref(coul), _dp(W)))
         return W
+
+    def bse_q_batch(self, kptqs, q4s, coul: Coulomb, graph: bool = True):
+        """Eigenvalues of the Q kernel for every Q of a path in one call: kptqs is a list of
+        (nk,3) k+Q meshes, q4s (nq,4). Returns (W (nq,N), per-Q device ms)."""
+        blocks = [_f64(k) for k in kptqs]
+        nq = len(blocks)
+        nk = blocks[0].shape[0] if nq else self.nk
+        kq = np.ascontiguousarray(np.concatenate([b.ravel(order="F") for b in blocks])) if nq else np.zeros(3)
+        q = np.ascontiguousarray(np.asarray(q4s, dtype=np.float64).reshape(nq, 4))
+        W = np.zeros((nq, self.N))
+        ms = np.zeros(nq)
+        self._check(self.lib.wtbg_bse_q_batch(self.h, nk, nq, _dp(kq), _dp(q), C.byref(coul), int(graph),
+                                              _dp(W), _dp(ms)))
+        return W, ms
 
 
 def bands_batch(ctxs, kpts, nvs, ncs):
