@@ -27,7 +27,8 @@ namespace {
 
 constexpr int TB = WTBG_HEMV_TILE;   // 64
 constexpr int NB = WTBG_PANEL;       // 32
-constexpr int RB = 256;              // rows per block of the column kernels
+constexpr int RB = 256;              // rows per block of k_wfix_last
+constexpr int RA = 64;               // rows per block of k_colA / k_colC
 constexpr int NG = 10;               // h vectors carried through (x, y, z, sp, sm [, each times f])
 
 __device__ __forceinline__ double2 warp_sum2(double2 v) {
@@ -77,11 +78,14 @@ __device__ __forceinline__ bool last_block(unsigned int* cnt) {
 
 // (A) apply the previous column's w correction, update column i with the panel's pending
 //     rank-2 terms, |x|^2 partials; the last block computes the reflector (ZLARFG).
-__global__ void __launch_bounds__(RB) k_colA(double2* A, long long N, double2* Wp, int j0, int p, int i, double* part,
-                                             ColState* st, double* d, double* e, double2* tau_out) {
+//     RA rows per block; the four 64-thread groups split the panel columns q (mod 4), so that
+//     each thread keeps few loads in flight and the grid covers the SMs at moderate N.
+__global__ void __launch_bounds__(256) k_colA(double2* A, long long N, double2* Wp, int j0, int p, int i, double* part,
+                                              ColState* st, double* d, double* e, double2* tau_out) {
   __shared__ double2 wrow[NB], vrow[NB];
-  __shared__ double red[RB / 32];
-  const int tid = threadIdx.x;
+  __shared__ double2 sacc[4][RA];
+  __shared__ double red[8];
+  const int tid = threadIdx.x, el = tid & (RA - 1), grp = tid >> 6;
   const double2 alpha2 = (p > 0) ? st->alpha2 : make_double2(0, 0);
   if (tid < p) {
     double2 wv = Wp[i + (long long)tid * N];
@@ -90,24 +94,28 @@ __global__ void __launch_bounds__(RB) k_colA(double2* A, long long N, double2* W
     vrow[tid] = A[i + (long long)(j0 + tid) * N];
   }
   __syncthreads();
-  const long long r = (long long)i + (long long)blockIdx.x * RB + tid;
-  double nrm = 0.0;
-  if (r < N) {
-    double2 a = A[r + (long long)i * N];
-    if (p > 0) {
-      // finish w of the previous column for this row
-      const double2 vprev = A[r + (long long)(i - 1) * N];
-      const double2 wlast = cadd(Wp[r + (long long)(p - 1) * N], cmul(alpha2, vprev));
-      Wp[r + (long long)(p - 1) * N] = wlast;
-      double2 s1 = make_double2(0, 0), s2 = make_double2(0, 0);
-      for (int q = 0; q < p; ++q) {
-        const double2 vq = A[r + (long long)(j0 + q) * N];
-        const double2 wq = (q == p - 1) ? wlast : Wp[r + (long long)q * N];
-        s1 = cadd(s1, cmul(vq, cconj(wrow[q])));
-        s2 = cadd(s2, cmul(wq, cconj(vrow[q])));
-      }
-      a = csub(csub(a, s1), s2);
+  const long long r = (long long)i + (long long)blockIdx.x * RA + el;
+  const bool rv = r < N;
+  double2 wlast = make_double2(0, 0);
+  double2 s = make_double2(0, 0);
+  if (rv && p > 0) {
+    // finish w of the previous column for this row
+    const double2 vprev = A[r + (long long)(i - 1) * N];
+    wlast = cadd(Wp[r + (long long)(p - 1) * N], cmul(alpha2, vprev));
+#pragma unroll 4
+    for (int q = grp; q < p; q += 4) {
+      const double2 vq = A[r + (long long)(j0 + q) * N];
+      const double2 wq = (q == p - 1) ? wlast : Wp[r + (long long)q * N];
+      s = cadd(s, cadd(cmul(vq, cconj(wrow[q])), cmul(wq, cconj(vrow[q]))));
     }
+  }
+  sacc[grp][el] = s;
+  __syncthreads();
+  double nrm = 0.0;
+  if (grp == 0 && rv) {
+    if (p > 0) Wp[r + (long long)(p - 1) * N] = wlast;
+    double2 a = A[r + (long long)i * N];
+    a = csub(a, cadd(cadd(sacc[0][el], sacc[1][el]), cadd(sacc[2][el], sacc[3][el])));
     if (r == i) a.y = 0.0;
     A[r + (long long)i * N] = a;
     if (r >= (long long)i + 2) nrm = a.x * a.x + a.y * a.y;
@@ -116,21 +124,21 @@ __global__ void __launch_bounds__(RB) k_colA(double2* A, long long N, double2* W
   if ((tid & 31) == 0) red[tid >> 5] = nrm;
   __syncthreads();
   if (tid == 0) {
-    double s = 0.0;
-    for (int k = 0; k < RB / 32; ++k) s += red[k];
-    part[blockIdx.x] = s;
+    double t = 0.0;
+    for (int k = 0; k < 8; ++k) t += red[k];
+    part[blockIdx.x] = t;
   }
   if (!last_block(&st->cntA)) return;
   // reflector scalars
-  double s = 0.0;
-  for (int k = tid; k < (int)gridDim.x; k += RB) s += ((volatile double*)part)[k];
-  s = warp_sum(s);
+  double t = 0.0;
+  for (int k = tid; k < (int)gridDim.x; k += 256) t += ((volatile double*)part)[k];
+  t = warp_sum(t);
   __syncthreads();
-  if ((tid & 31) == 0) red[tid >> 5] = s;
+  if ((tid & 31) == 0) red[tid >> 5] = t;
   __syncthreads();
   if (tid == 0) {
     double xn2 = 0.0;
-    for (int k = 0; k < RB / 32; ++k) xn2 += red[k];
+    for (int k = 0; k < 8; ++k) xn2 += red[k];
     const double2 alpha = vload(A + (i + 1) + (long long)i * N);
     if (xn2 == 0.0 && alpha.y == 0.0) {
       st->tau = make_double2(0, 0);
@@ -153,47 +161,51 @@ __global__ void __launch_bounds__(RB) k_colA(double2* A, long long N, double2* W
   }
 }
 
-// (C) scale v in place (v(i+1) = 1); partial dots z1 = W^H v, z2 = V^H v, s = v^T g.  One
-//     warp per dot product over the block's rows; the last block reduces into st->z.
-__global__ void __launch_bounds__(RB) k_colC(double2* A, long long N, const double2* Wp, int j0, int p, int i,
-                                             ColState* st, const double2* g, int ng, double2* part) {
-  __shared__ double2 vs[RB];
-  __shared__ double2 red[2 * NB + NG];
+// (C) scale v in place (v(i+1) = 1); partial dots z1 = W^H v, z2 = V^H v, s = v^T g over the
+//     block's RA rows, one warp per dot (two rows per lane); the last block reduces the
+//     partials into st->z, again one warp per dot with the lanes striding over the blocks.
+__global__ void __launch_bounds__(256) k_colC(double2* A, long long N, const double2* Wp, int j0, int p, int i,
+                                              ColState* st, const double2* g, int ng, double2* part) {
+  __shared__ double2 vs[RA];
   const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-  const long long rbase = (long long)i + 1 + (long long)blockIdx.x * RB;
-  const long long r = rbase + tid;
-  const double2 scal = st->scal;
-  const int trivial = st->trivial;
-  double2 v = make_double2(0, 0);
-  if (r < N) {
-    if (r == i + 1) v = make_double2(1.0, 0.0);
-    else v = trivial ? make_double2(0, 0) : cmul(A[r + (long long)i * N], scal);
-    A[r + (long long)i * N] = v;
+  const long long rbase = (long long)i + 1 + (long long)blockIdx.x * RA;
+  if (tid < RA) {
+    const long long r = rbase + tid;
+    double2 v = make_double2(0, 0);
+    if (r < N) {
+      if (r == i + 1) v = make_double2(1.0, 0.0);
+      else v = st->trivial ? make_double2(0, 0) : cmul(A[r + (long long)i * N], st->scal);
+      A[r + (long long)i * N] = v;
+    }
+    vs[tid] = v;
   }
-  vs[tid] = v;
   __syncthreads();
   const int nval = 2 * p + ng;
-  const int nrow = (int)((N - rbase) < RB ? (N - rbase) : RB);
-  for (int q = wp; q < nval; q += RB / 32) {
-    double2 t = make_double2(0, 0);
-    for (int k = lane; k < nrow; k += 32) {
-      const long long rr = rbase + k;
-      if (q < p) t = cadd(t, cmulc(Wp[rr + (long long)q * N], vs[k]));
-      else if (q < 2 * p) t = cadd(t, cmulc(A[rr + (long long)(j0 + q - p) * N], vs[k]));
-      else t = cadd(t, cmul(vs[k], g[(long long)(q - 2 * p) * N + rr]));
+  const long long r0 = rbase + lane, r1 = r0 + 32;
+  const bool ok0 = r0 < N, ok1 = r1 < N;
+  const double2 x0 = vs[lane], x1 = vs[lane + 32];
+  for (int q = wp; q < nval; q += 8) {
+    double2 t;
+    if (q < 2 * p) {
+      const double2* col = (q < p) ? Wp + (long long)q * N : A + (long long)(j0 + q - p) * N;
+      const double2 a0 = ok0 ? col[r0] : make_double2(0, 0);
+      const double2 a1 = ok1 ? col[r1] : make_double2(0, 0);
+      t = cadd(cmulc(a0, x0), cmulc(a1, x1));
+    } else {
+      const double2* col = g + (long long)(q - 2 * p) * N;
+      const double2 a0 = ok0 ? col[r0] : make_double2(0, 0);
+      const double2 a1 = ok1 ? col[r1] : make_double2(0, 0);
+      t = cadd(cmul(x0, a0), cmul(x1, a1));
     }
     t = warp_sum2(t);
-    if (lane == 0) red[q] = t;
+    if (lane == 0) part[(long long)blockIdx.x * (2 * NB + NG) + q] = t;
   }
-  __syncthreads();
-  for (int q = tid; q < nval; q += RB) part[(long long)blockIdx.x * (2 * NB + NG) + q] = red[q];
   if (!last_block(&st->cntC)) return;
-  for (int q = tid; q < nval; q += RB) {
+  for (int q = wp; q < nval; q += 8) {
     double2 s = make_double2(0, 0);
-    for (int k = 0; k < (int)gridDim.x; ++k) {
-      s = cadd(s, vload(part + (long long)k * (2 * NB + NG) + q));
-    }
-    st->z[q] = s;
+    for (int k = lane; k < (int)gridDim.x; k += 32) s = cadd(s, vload(part + (long long)k * (2 * NB + NG) + q));
+    s = warp_sum2(s);
+    if (lane == 0) st->z[q] = s;
   }
   __syncthreads();
   if (tid == 0) st->cntC = 0;
@@ -315,6 +327,7 @@ __global__ void __launch_bounds__(256) k_colE(const double2* A, long long N, dou
   const int a = b0 + blockIdx.x;
   const int el = tid & (TB - 1), grp = tid >> 6;
   double2 s = make_double2(0, 0);
+#pragma unroll 4
   for (int b = b0 + grp; b < nblk; b += 4) s = cadd(s, slots[((long long)a * nblk + b) * TB + el]);
   acc4[grp][el] = s;
   __syncthreads();
@@ -351,10 +364,15 @@ __global__ void __launch_bounds__(256) k_colE(const double2* A, long long N, dou
   __syncthreads();
   if (tid == 0) part[blockIdx.x] = cadd(red[0], red[1]);
   if (!last_block(&st->cntE)) return;
+  double2 sum = make_double2(0, 0);
+  for (int k = tid; k < (int)gridDim.x; k += 256) sum = cadd(sum, vload(part + k));
+  sum = warp_sum2(sum);
+  if ((tid & 31) == 0) red[tid >> 5] = sum;
+  __syncthreads();
   if (tid == 0) {
-    double2 sum = make_double2(0, 0);
-    for (int k = 0; k < (int)gridDim.x; ++k) sum = cadd(sum, vload(part + k));
-    st->alpha2 = cscale(cmul(tau, sum), -0.5);
+    double2 tot = make_double2(0, 0);
+    for (int k = 0; k < 8; ++k) tot = cadd(tot, red[k]);
+    st->alpha2 = cscale(cmul(tau, tot), -0.5);
     st->cntE = 0;
   }
 }
@@ -523,7 +541,7 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
   const long long N = ctx->N;
   if (N < 2) return set_err(ctx, WTBG_ERR_ARG, "tridiagonalise: N < 2");
   const int nblk = (int)((N + TB - 1) / TB);
-  const int maxRB = (int)((N + RB - 1) / RB) + 1;
+  const int maxRB = (int)((N + RA - 1) / RA) + 1;   // blocks of k_colA / k_colC
   ENSURE(ctx->d, (size_t)N * 8);
   ENSURE(ctx->e, (size_t)N * 8);
   ENSURE(ctx->tau, (size_t)N * 16);
@@ -575,10 +593,10 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
     const int jb = (int)((N - 1 - j0) < NB ? (N - 1 - j0) : NB);
     for (int p = 0; p < jb; ++p) {
       const int i = (int)(j0 + p);
-      const int nA = (int)((N - i + RB - 1) / RB);
-      k_colA<<<nA, RB, 0, s>>>(A, N, Wp, (int)j0, p, i, partA, st, d, e, tau); WTBG_COUNT(ctx, 1);
-      const int nC = (int)((N - i - 1 + RB - 1) / RB);
-      k_colC<<<nC, RB, 0, s>>>(A, N, Wp, (int)j0, p, i, st, g, ng, partC); WTBG_COUNT(ctx, 1);
+      const int nA = (int)((N - i + RA - 1) / RA);
+      k_colA<<<nA, 256, 0, s>>>(A, N, Wp, (int)j0, p, i, partA, st, d, e, tau); WTBG_COUNT(ctx, 1);
+      const int nC = (int)((N - i - 1 + RA - 1) / RA);
+      k_colC<<<nC, 256, 0, s>>>(A, N, Wp, (int)j0, p, i, st, g, ng, partC); WTBG_COUNT(ctx, 1);
       const int b0 = (i + 1) / TB;
       const int nt = nblk - b0;
       if (prof) cudaEventRecord(ctx->evpool[2 * i], s);
