@@ -291,6 +291,14 @@ int wtbg_bse_build_q(wtbg_ctx* ctx, int nk, const double* kptq, const double* q4
 int wtbg_bse_q_eigenvalues(wtbg_ctx* ctx, int nk, const double* kptq, const double* q4,
                            const wtbg_coulomb* p, double* W);
 
+/* ---- precision form (mode 1): the Fourier sums H(k) = sum_R e^{ik.R} H(R)/deg(R) of the band
+ *      stage (hamiltonian_tb.f90:73-77) and the band overlaps <c|c'>, <v|v'> of the BSE kernel
+ *      build (bse_subs.f90:2-124) run as 3-term split-BF16 GEMMs on the tensor cores with FP32
+ *      accumulation; the per-k diagonalisation, the q -> 0 cell average, the velocities and the
+ *      tridiagonalisation stay FP64.  mode 0 (default) is the FP64 form.  Switching the form
+ *      discards the context's bands and matrix. */
+int wtbg_set_precision(wtbg_ctx* ctx, int mode);
+
 /* ---- exciton band structure, all Q of a path in one call (the Q loop of bsebnds,
  *      bse_kpath-tool.f90:246-435).  kptq holds nq blocks of (nk,3) k+Q meshes, q4 nq rows of
  *      (distance, qx, qy, qz); W (nq, N) receives each Q's eigenvalues ascending, identical to

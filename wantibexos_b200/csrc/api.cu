@@ -60,6 +60,19 @@ int ensure_events(wtbg_ctx* ctx, size_t n) {
   return 0;
 }
 
+// device flag of the precision-form GEMMs (a pipeline wait that timed out)
+int check_gemm_err(wtbg_ctx* ctx) {
+  if (!ctx->prec || !ctx->pErr.p) return 0;
+  int e = 0;
+  CK(cudaMemcpyAsync(&e, ctx->pErr.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (e) {
+    CK(cudaMemsetAsync(ctx->pErr.p, 0, 4, ctx->stream));
+    return set_err(ctx, WTBG_ERR_CUDA, "precision form: a tensor-core pipeline wait timed out");
+  }
+  return 0;
+}
+
 extern "C" {
 
 int wtbg_set_profiling(wtbg_ctx* ctx, int on) {
@@ -129,7 +142,8 @@ int wtbg_destroy(wtbg_ctx* ctx) {
                     &ctx->nocp, &ctx->kstat, &ctx->kptq, &ctx->eigq, &ctx->Uq, &ctx->nocpq, &ctx->h, &ctx->H,
                     &ctx->d, &ctx->e, &ctx->tau, &ctx->g, &ctx->fdeh, &ctx->Wp, &ctx->slots, &ctx->part, &ctx->scal,
                     &ctx->yv, &ctx->lam, &ctx->ws, &ctx->act, &ctx->zsel, &ctx->csz, &ctx->sp_in, &ctx->sp_out,
-                    &ctx->sp_om, &ctx->tmp, &ctx->tmp2, &ctx->istat};
+                    &ctx->sp_om, &ctx->tmp, &ctx->tmp2, &ctx->istat, &ctx->pOpA, &ctx->pOpB,
+                    &ctx->pHk, &ctx->pOc, &ctx->pOv, &ctx->pErr};
   for (DevBuf* b : bufs) free_buf(*b);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
   if (ctx->tri_exec) cudaGraphExecDestroy(ctx->tri_exec);
@@ -229,6 +243,7 @@ int wtbg_bands(wtbg_ctx* ctx, int nk, const double* kpt, int nv, int nc, double*
   if (int r = launch_bands(ctx, false)) return r;
   if (int r = t.stop()) return r;
   if (int r = check_kstat(ctx, nk)) return r;
+  if (int r = check_gemm_err(ctx)) return r;
   ctx->have_bands = true;
   ctx->have_velocity = ctx->have_matrix = ctx->have_solution = false;
   ctx->fast_ready = false;
@@ -303,6 +318,7 @@ int wtbg_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p) {
   Timer t(ctx);
   if (int r = launch_bse_build(ctx, p, nullptr)) return r;
   if (int r = t.stop()) return r;
+  if (int r = check_gemm_err(ctx)) return r;
   ctx->have_matrix = true;
   ctx->fast_ready = false;
   ctx->have_solution = false;
@@ -517,6 +533,22 @@ int wtbg_set_temperature(wtbg_ctx* ctx, int on, double temp) {
   return WTBG_OK;
 }
 
+int wtbg_set_precision(wtbg_ctx* ctx, int mode) {
+  if (!ctx || mode < 0 || mode > 1) return WTBG_ERR_ARG;
+  if (int r = set_device(ctx)) return r;
+  if (mode == 1) {
+    ENSURE(ctx->pErr, 16);
+    CK(cudaMemsetAsync(ctx->pErr.p, 0, 16, ctx->stream));
+  }
+  if (mode != ctx->prec) {
+    // bands, velocities and matrix of the other form are not reused
+    ctx->have_bands = ctx->have_velocity = ctx->have_matrix = ctx->have_solution = false;
+    ctx->fast_ready = false;
+  }
+  ctx->prec = mode;
+  return WTBG_OK;
+}
+
 int wtbg_set_fast_product(wtbg_ctx* ctx, int mode) {
   if (!ctx || mode < 0 || mode > 1) return WTBG_ERR_ARG;
   ctx->fast_mode = mode;
@@ -686,8 +718,10 @@ int wtbg_bse_build_q(wtbg_ctx* ctx, int nk, const double* kptq, const double* q4
   CK(cudaMemcpyAsync(ctx->kptq.p, kq.data(), kq.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
   if (int r = launch_bands(ctx, true)) return r;
   if (int r = check_kstat(ctx, nk)) return r;
+  if (int r = check_gemm_err(ctx)) return r;
   if (int r = launch_bse_build(ctx, p, q4)) return r;
   if (int r = t.stop()) return r;
+  if (int r = check_gemm_err(ctx)) return r;
   ctx->have_matrix = true;
   ctx->fast_ready = false;
   ctx->have_solution = false;

@@ -59,6 +59,7 @@ struct BandsArgs {
   int* nocp;       // [nk]
   int* kstat;      // [nk]
   int all;         // 1: every band (eigsys as the band and DOS tools call it), nb = w
+  const float* Hk; // precision form: H(k) from the tensor-core Fourier sum, [2 w^2][nk] (Re, Im)
 };
 
 // One k-point per iteration of the loop k = k0, k0 + kstride, ... (shared-memory work area
@@ -88,7 +89,11 @@ __device__ __forceinline__ void bands_body(const BandsArgs& a, int k0, int kstri
     for (int el = tid; el < ww; el += bs) {
       const int m = el % w, n = el / w;
       double2 acc = make_double2(0.0, 0.0);
-      if (m >= n) {
+      if (m >= n && a.Hk) {
+        acc = make_double2((double)a.Hk[(size_t)el * a.nk + k], (double)a.Hk[(size_t)(ww + el) * a.nk + k]);
+        if (m == n) acc = make_double2(acc.x + (-a.ef32), 0.0);
+        fro += (m == n ? 1.0 : 2.0) * (acc.x * acc.x + acc.y * acc.y);
+      } else if (m >= n) {
         const double2* hp = a.HR + el;
         for (int R = 0; R < nvec; ++R) {
           double2 t = cmul(ph[R], hp[(size_t)R * ww]);
@@ -243,6 +248,37 @@ __device__ __forceinline__ void bands_body(const BandsArgs& a, int k0, int kstri
       }
     }
     __syncthreads();
+  }
+}
+
+// Precision form of the Fourier sum H(k) = sum_R e^{i k.R} H(R) / deg(R) as one real GEMM
+// over all k: A rows k = [Re P | Im P] with P(k,R) = phase / deg, B rows (Re out) [Re H | -Im H]
+// and (Im out) [Im H | Re H] per matrix element; segments padded to S (a multiple of 8).
+__global__ void k_hk_opA(const double* kpt, const double* Rcart, const double* invdeg, int nvec, int S,
+                         __nv_bfloat16* A3) {
+  const int k = blockIdx.x;
+  __nv_bfloat16* row = A3 + (size_t)k * 6 * S;
+  for (int R = threadIdx.x; R < S; R += blockDim.x) {
+    double2 p = make_double2(0, 0);
+    if (R < nvec) p = cscale(phase_of(kpt[3 * k], kpt[3 * k + 1], kpt[3 * k + 2], Rcart + 3 * R), invdeg[R]);
+    put_split_row(row, 2 * S, R, p.x, true);
+    put_split_row(row, 2 * S, S + R, p.y, true);
+  }
+}
+
+__global__ void k_hk_opB(const double2* HR, int nvec, int ww, int S, __nv_bfloat16* B3) {
+  const int j = blockIdx.x, el = j % ww;
+  const bool im = j >= ww;
+  __nv_bfloat16* row = B3 + (size_t)j * 6 * S;
+  for (int R = threadIdx.x; R < S; R += blockDim.x) {
+    double x = 0.0, y = 0.0;
+    if (R < nvec) {
+      const double2 h = HR[(size_t)R * ww + el];
+      x = im ? h.y : h.x;
+      y = im ? h.x : -h.y;
+    }
+    put_split_row(row, 2 * S, R, x, false);
+    put_split_row(row, 2 * S, S + R, y, false);
   }
 }
 
@@ -415,6 +451,24 @@ static size_t bands_smem(int w, int nvec) {
          (size_t)(w + (w & 1)) * 4 + 64 * 8;
 }
 
+// H(k) of every k of the mesh by the 3-term split-BF16 tensor-core GEMM (FP32 result
+// [2 w^2][nk] in ctx->pHk)
+static int run_precision_hk(wtbg_ctx* ctx, const double* kpt, int nk) {
+  const int w = ctx->w, ww = w * w, nvec = ctx->nvec;
+  const int S = (nvec + 7) / 8 * 8, K = 6 * S;
+  ENSURE(ctx->pOpA, (size_t)nk * K * 2);
+  ENSURE(ctx->pOpB, (size_t)2 * ww * K * 2);
+  ENSURE(ctx->pHk, (size_t)2 * ww * nk * 4);
+  ENSURE(ctx->pErr, 16);
+  __nv_bfloat16* A3 = ctx->pOpA.as<__nv_bfloat16>();
+  __nv_bfloat16* B3 = ctx->pOpB.as<__nv_bfloat16>();
+  k_hk_opA<<<nk, 128, 0, ctx->stream>>>(kpt, ctx->Rcart.as<double>(), ctx->invdeg.as<double>(), nvec, S, A3);
+  k_hk_opB<<<2 * ww, 128, 0, ctx->stream>>>(ctx->HR.as<double2>(), nvec, ww, S, B3);
+  WTBG_COUNT(ctx, 2);
+  CKL("k_hk_op");
+  return gemm_bf16(ctx, ctx->pErr.as<int>(), A3, K, nk, K, B3, K, 2 * ww, ctx->pHk.as<float>(), nk, true);
+}
+
 int launch_bands(wtbg_ctx* ctx, bool q_mesh) {
   const int w = ctx->w;
   BandsArgs a;
@@ -441,6 +495,11 @@ int launch_bands(wtbg_ctx* ctx, bool q_mesh) {
   }
   a.kstat = ctx->kstat.as<int>();
   a.all = 0;
+  a.Hk = nullptr;
+  if (ctx->prec == 1) {
+    if (int r = run_precision_hk(ctx, a.kpt, ctx->nk)) return r;
+    a.Hk = ctx->pHk.as<float>();
+  }
   const size_t smem = bands_smem(w, ctx->nvec);
   if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bands: model too large for shared memory");
   CK(cudaFuncSetAttribute(k_bands, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -479,6 +538,7 @@ int launch_bands_batch(wtbg_ctx* const* ctxs, int nmod) {
     a.nocp = cm->nocp.as<int>();
     a.kstat = cm->kstat.as<int>();
     a.all = 0;
+    a.Hk = nullptr;   // the batch runs the FP64 form
     smem = std::max(smem, bands_smem(cm->w, cm->nvec));
     order.push_back({cm->w, m});
     nitems += cm->nk;
@@ -544,6 +604,7 @@ int launch_eigsys_all(wtbg_ctx* ctx, int nk, const double* d_kpt, double* d_eig,
   a.nocp = d_nocp;
   a.kstat = d_kstat;
   a.all = 1;
+  a.Hk = nullptr;   // the band and DOS tools run the FP64 form
   const size_t smem = bands_smem(w, ctx->nvec);
   if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bands: model too large for shared memory");
   CK(cudaFuncSetAttribute(k_bands, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -40,6 +40,10 @@ struct BuildArgs {
   double2* H;
   long long N;
   int TK, nbk;
+  // precision form: band overlaps from the tensor-core GEMM, FP32 [2n][n] (Re rows, then Im),
+  // n = nk * nc (conduction) and nk * nv (valence); nullptr for the FP64 form
+  const float* Oc;
+  const float* Ov;
 };
 
 __global__ void __launch_bounds__(kBuildThreads) k_bse_build(BuildArgs a) {
@@ -66,13 +70,13 @@ __global__ void __launch_bounds__(kBuildThreads) k_bse_build(BuildArgs a) {
   double* dE = Vt + TK * TK;           // [TK*ncv]
   int* colinfo = reinterpret_cast<int*>(dE + TK * ncv);  // packed (kc, c', v') per tile column
 
-  for (int it = tid; it < RC * w; it += bs) {
+  for (int it = a.Oc ? RC * w : tid; it < RC * w; it += bs) {
     const int kk = it / (nc * w), rem = it % (nc * w), c = rem / w, m = rem % w;
     const int row = kk * nc + c;
     UcR[row * ws + m] = (kk < nkr) ? a.Uc[((size_t)(kr0 + kk) * nb + nv + c) * w + m] : make_double2(0, 0);
     UcC[row * ws + m] = (kk < nkc) ? a.Uc[((size_t)(kc0 + kk) * nb + nv + c) * w + m] : make_double2(0, 0);
   }
-  for (int it = tid; it < RV * w; it += bs) {
+  for (int it = a.Ov ? RV * w : tid; it < RV * w; it += bs) {
     const int kk = it / (nv * w), rem = it % (nv * w), v = rem / w, m = rem % w;
     const int row = kk * nv + v;
     UvR[row * ws + m] = (kk < nkr) ? a.Uv[((size_t)(kr0 + kk) * nb + v) * w + m] : make_double2(0, 0);
@@ -94,21 +98,40 @@ __global__ void __launch_bounds__(kBuildThreads) k_bse_build(BuildArgs a) {
     colinfo[it] = (kr << 16) | (c << 8) | v;
   }
   __syncthreads();
-  for (int it = tid; it < RC * RC; it += bs) {
-    const int col = it / RC, row = it % RC;
-    const double2* x = UcR + row * ws;
-    const double2* y = UcC + col * ws;
-    double2 acc = make_double2(0, 0);
-    for (int m = 0; m < w; ++m) acc = cadd(acc, cmulc(x[m], y[m]));
-    Mc[it] = acc;
-  }
-  for (int it = tid; it < RV * RV; it += bs) {
-    const int col = it / RV, row = it % RV;
-    const double2* x = UvR + row * ws;
-    const double2* y = UvC + col * ws;
-    double2 acc = make_double2(0, 0);
-    for (int m = 0; m < w; ++m) acc = cadd(acc, cmulc(x[m], y[m]));
-    Mv[it] = acc;
+  if (a.Oc) {
+    // precision form: the overlaps of this tile from the FP32 GEMM results
+    const long long nC = (long long)a.nk * nc, nV = (long long)a.nk * nv;
+    for (int it = tid; it < RC * RC; it += bs) {
+      const int col = it / RC, row = it % RC;
+      const int kr = row / nc, kc = col / nc;
+      const long long i = (long long)kr0 * nc + row, j = (long long)kc0 * nc + col;
+      Mc[it] = (kr < nkr && kc < nkc) ? make_double2((double)a.Oc[j * nC + i], (double)a.Oc[(nC + j) * nC + i])
+                                      : make_double2(0, 0);
+    }
+    for (int it = tid; it < RV * RV; it += bs) {
+      const int col = it / RV, row = it % RV;
+      const int kr = row / nv, kc = col / nv;
+      const long long i = (long long)kr0 * nv + row, j = (long long)kc0 * nv + col;
+      Mv[it] = (kr < nkr && kc < nkc) ? make_double2((double)a.Ov[j * nV + i], (double)a.Ov[(nV + j) * nV + i])
+                                      : make_double2(0, 0);
+    }
+  } else {
+    for (int it = tid; it < RC * RC; it += bs) {
+      const int col = it / RC, row = it % RC;
+      const double2* x = UcR + row * ws;
+      const double2* y = UcC + col * ws;
+      double2 acc = make_double2(0, 0);
+      for (int m = 0; m < w; ++m) acc = cadd(acc, cmulc(x[m], y[m]));
+      Mc[it] = acc;
+    }
+    for (int it = tid; it < RV * RV; it += bs) {
+      const int col = it / RV, row = it % RV;
+      const double2* x = UvR + row * ws;
+      const double2* y = UvC + col * ws;
+      double2 acc = make_double2(0, 0);
+      for (int m = 0; m < w; ++m) acc = cadd(acc, cmulc(x[m], y[m]));
+      Mv[it] = acc;
+    }
   }
   __syncthreads();
 
@@ -229,6 +252,45 @@ CoulombDev make_coulomb_dev(const wtbg_coulomb* p, const double* L) {
   return P;
 }
 
+// Precision form of the band overlaps <a_i|a_j> = sum_m conj(u_im) u_jm over all (k, band)
+// rows of one band block as one real GEMM: A rows [Re u | Im u], B rows (Re out) [Re u | Im u]
+// and (Im out) [Im u | -Re u], 3-term split-BF16 (segments padded to S, a multiple of 8).
+__global__ void k_ovl_ops(const double2* U, int nk, int nb, int off, int cnt, int w, int S, __nv_bfloat16* A3,
+                          __nv_bfloat16* B3) {
+  const long long n = (long long)nk * cnt, i = blockIdx.x;
+  const int k = (int)(i / cnt), b = (int)(i % cnt);
+  __nv_bfloat16* ra = A3 + i * 6 * S;
+  __nv_bfloat16* rr = B3 + i * 6 * S;
+  __nv_bfloat16* ri = B3 + (n + i) * 6 * S;
+  for (int m = threadIdx.x; m < S; m += blockDim.x) {
+    const double2 u = (m < w) ? U[((size_t)k * nb + off + b) * w + m] : make_double2(0, 0);
+    put_split_row(ra, 2 * S, m, u.x, true);
+    put_split_row(ra, 2 * S, S + m, u.y, true);
+    put_split_row(rr, 2 * S, m, u.x, false);
+    put_split_row(rr, 2 * S, S + m, u.y, false);
+    put_split_row(ri, 2 * S, m, u.y, false);
+    put_split_row(ri, 2 * S, S + m, -u.x, false);
+  }
+}
+
+// overlaps of the band block [off, off + cnt) of U on the tensor cores into out ([2n][n] FP32)
+static int run_precision_overlaps(wtbg_ctx* ctx, const double2* U, int off, int cnt, DevBuf& out) {
+  const int nk = ctx->nk, nb = ctx->nv + ctx->nc, w = ctx->w;
+  const long long n = (long long)nk * cnt;
+  const int S = (w + 7) / 8 * 8, K = 6 * S;
+  if (n > 0x7fffffffLL / 2) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "precision form: overlap GEMM too large");
+  ENSURE(ctx->pOpA, (size_t)n * K * 2);
+  ENSURE(ctx->pOpB, (size_t)2 * n * K * 2);
+  ENSURE(out, (size_t)2 * n * n * 4);
+  ENSURE(ctx->pErr, 16);
+  k_ovl_ops<<<(unsigned)n, 64, 0, ctx->stream>>>(U, nk, nb, off, cnt, w, S, ctx->pOpA.as<__nv_bfloat16>(),
+                                                 ctx->pOpB.as<__nv_bfloat16>());
+  WTBG_COUNT(ctx, 1);
+  CKL("k_ovl_ops");
+  return gemm_bf16(ctx, ctx->pErr.as<int>(), ctx->pOpA.as<__nv_bfloat16>(), K, (int)n, K,
+                   ctx->pOpB.as<__nv_bfloat16>(), K, (int)(2 * n), out.as<float>(), n, true);
+}
+
 // Builds the BSE matrix for Q = 0 (q4 == nullptr) or for a centre-of-mass momentum q4.
 int launch_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p, const double* q4) {
   const int nc = ctx->nc, nv = ctx->nv, w = ctx->w, ncv = nc * nv;
@@ -259,6 +321,13 @@ int launch_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p, const double* q4) {
     a.fdeh = ctx->fdeh.as<double>();
   }
   a.vcv = nullptr;
+  a.Oc = a.Ov = nullptr;
+  if (ctx->prec == 1) {
+    if (int r = run_precision_overlaps(ctx, a.Uc, nv, nc, ctx->pOc)) return r;
+    if (int r = run_precision_overlaps(ctx, a.Uv, 0, nv, ctx->pOv)) return r;
+    a.Oc = ctx->pOc.as<float>();
+    a.Ov = ctx->pOv.as<float>();
+  }
   a.H = ctx->H.as<double2>();
   a.N = ctx->N;
   a.TK = TK;

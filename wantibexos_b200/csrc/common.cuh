@@ -1,6 +1,7 @@
 // Shared definitions for libwtbgpu.so (sm_100a).
 #pragma once
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
 #include <cstddef>
 #include <cstdint>
 #include <string>
@@ -91,6 +92,11 @@ struct wtbg_ctx {
   cudaGraphExec_t tri_exec = nullptr;
   std::vector<const void*> tri_sig;
   long long tri_launches = 0;
+
+  // precision form (0 = FP64; 1 = Fourier sums and band overlaps as 3-term split-BF16
+  // tensor-core products with FP32 accumulation)
+  int prec = 0;
+  DevBuf pOpA, pOpB, pHk, pOc, pOv, pErr;
 
   // fast form: split-BF16 planes of the kernel matrix for the tensor-core product
   int fast_mode = 0;
@@ -195,6 +201,26 @@ int launch_eigsys_all(wtbg_ctx* ctx, int nk, const double* d_kpt, double* d_eig,
 int launch_dos(wtbg_ctx* ctx, const double* d_etb, const double* d_w, long long ndim, int ncol, const double* d_en,
                int nw, double sme, long long nkpt, double* d_out);
 int autotune_hemv(wtbg_ctx* ctx, int* hs_out);
+// C^T (N x M, ldc) (+)= A (M x K, lda) B (N x K, ldb)^T, bf16 operands, FP32 accumulation on the
+// tensor cores (tcgen05); err is a device flag set when a pipeline wait times out
+int gemm_bf16(wtbg_ctx* ctx, int* err, const __nv_bfloat16* A, long long lda, int M, int K, const __nv_bfloat16* B,
+              long long ldb, int N, float* C, long long ldc, bool clear);
+int check_gemm_err(wtbg_ctx* ctx);
+
+// 3-term split of a double into bf16 hi + lo (x ~ hi + lo to about 16 significant bits)
+__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __double2bfloat16(x);
+  lo = __double2bfloat16(x - (double)__bfloat162float(hi));
+}
+// One operand row of the 3-term product sum_s a_s b_s ~ ah.bh + ah.bl + al.bh from its real
+// values: the A side is stored [hi | hi | lo], the B side [hi | lo | hi] (K = 3 * width)
+__device__ __forceinline__ void put_split_row(__nv_bfloat16* row, int width, int s, double x, bool a_side) {
+  __nv_bfloat16 hi, lo;
+  split_bf16(x, hi, lo);
+  row[s] = hi;
+  row[width + s] = a_side ? hi : lo;
+  row[2 * width + s] = a_side ? lo : hi;
+}
 int ensure_fdeh(wtbg_ctx* ctx, bool q_mesh);
 int fill_g_vectors(wtbg_ctx* ctx, double2* g);
 int run_fast_setup(wtbg_ctx* ctx);

@@ -29,7 +29,7 @@ EXPORTS = ["wtbg_create", "wtbg_destroy", "wtbg_error_string", "wtbg_last_error"
            "wtbg_net_features", "wtbg_net_add_sample", "wtbg_net_num_samples", "wtbg_net_train",
            "wtbg_net_eval_loss", "wtbg_net_predict", "wtbg_net_loss_grad", "wtbg_gemm_bf16",
            "wtbg_bse_build_q", "wtbg_set_temperature", "wtbg_eigsys", "wtbg_dos",
-           "wtbg_bands_batch", "wtbg_bse_q_batch"]
+           "wtbg_bands_batch", "wtbg_bse_q_batch", "wtbg_set_precision"]
 
 
 class WtbgError(RuntimeError):
@@ -93,6 +93,7 @@ def load_library(path: str = LIB_PATH):
                                              C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
                                              dp, fp]),
         "wtbg_set_fast_product": (C.c_int, [P, C.c_int]),
+        "wtbg_set_precision": (C.c_int, [P, C.c_int]),
         "wtbg_net_create": (C.c_int, [P, C.POINTER(P), C.c_ulonglong]),
         "wtbg_net_destroy": (C.c_int, [P]),
         "wtbg_net_num_params": (C.c_longlong, []),
@@ -359,6 +360,11 @@ class Context:
                                            float(ebse0), float(ebsef), float(numbse), float(sme),
                                            int(bool(renorm)), float(spinf), _dp(om), _fp(eps)))
         return om, eps
+
+    def set_precision(self, mode: int) -> None:
+        """0: FP64 form; 1: precision form (Fourier sums and band overlaps as 3-term split-BF16
+        tensor-core GEMMs, FP32 accumulation). Discards the context's bands and matrix."""
+        self._check(self.lib.wtbg_set_precision(self.h, int(mode)))
 
     def bse_build_q(self, kptq, q4, coul: Coulomb) -> None:
         kq = _f64(kptq)
