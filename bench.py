@@ -315,6 +315,21 @@ def cpu_baseline(wl, model, budget_s=30.0):
 
 
 # ----------------------------------------------------------------------------- main
+def solve_breakdown(st, nsteps):
+    """Per-step CUDA-event times of the dense solve's parts (profiling mode): the mat-vec, the
+    trailing rank-2k updates (with their FP64 tensor rate against the nominal 40 TFLOP/s: no
+    measured FP64 peak exists for this GPU), the rest of the reduction (column kernels), and
+    the tridiagonal eigenvalues + oscillators."""
+    if not st["tri_ms"]:
+        return None
+    her2k_tf = st["her2k_flops"] / (st["her2k_ms"] / 1e3) / 1e12 if st["her2k_ms"] else None
+    return {"tridiagonalise": st["tri_ms"] / 1e3 / nsteps, "hemv": st["hemv_ms"] / 1e3 / nsteps,
+            "her2k": st["her2k_ms"] / 1e3 / nsteps,
+            "column_kernels_and_gaps": (st["tri_ms"] - st["hemv_ms"] - st["her2k_ms"]) / 1e3 / nsteps,
+            "tridiagonal_solve": st["tdsolve_ms"] / 1e3 / nsteps,
+            "her2k_tflops": her2k_tf, "her2k_frac_of_nominal_fp64_40": (her2k_tf / 40.0) if her2k_tf else None}
+
+
 def max_over_ranks(values, dist):
     """Element-wise max of per-rank timings over the process group (the whole job ends when
     its slowest replica ends)."""
@@ -466,6 +481,8 @@ def main():
     ctx.close()
     if args.device_only:
         print(json.dumps({"metric": metric, "value": t_dev, "unit": unit, "stages_s": steps[-1] if steps else None,
+                          "solve_breakdown_s": solve_breakdown(st, max(1, len(steps))),
+                          "hemv_gbs": (st["hemv_bytes"] / (st["hemv_ms"] / 1e3) / 1e9) if st["hemv_ms"] else None,
                           "fast_form": fast, "config": cfg, "device_only": True}))
         return
     # e2e through the deck-level C entry (host buffers, files)
@@ -512,6 +529,7 @@ def main():
                      "launches": st["hemv_launches"], "avg_launch_ms": st["hemv_ms"] / max(1, st["hemv_launches"]),
                      "build_kernel": {"achieved": build_gbs, "frac": (build_gbs / hbm) if build_gbs else None,
                                       "algorithmic_bytes": "16 B x N(N+1)/2 (lower triangle written once)"}},
+        "solve_breakdown_s": solve_breakdown(st, max(1, len(steps))),
         "gpu_launches": int(st["launches"] / max(1, args.steps)),
         "clocks": ck,
         "fast_form": fast,

@@ -77,6 +77,11 @@ typedef struct wtbg_stats {
   double fast_bytes;         /* algorithmic: 8 N^2 (bf16 hi/lo planes of Re H, Im H) per product */
   long long dav_fast_iters;  /* Davidson iterations on the tensor-core product (last call) */
   long long dav_fp64_iters;  /* Davidson iterations on the FP64 product (last call) */
+  long long her2k_launches;  /* trailing rank-2k updates (k_her2k), timed when profiling */
+  double her2k_ms;
+  double her2k_flops;        /* algorithmic: 16 real flops x 2 x panel width per lower-triangle element */
+  double tri_ms;             /* whole tridiagonalisation (profiling) */
+  double tdsolve_ms;         /* tridiagonal eigenvalues + inverse iteration + oscillators (profiling) */
 } wtbg_stats;
 int wtbg_set_profiling(wtbg_ctx* ctx, int on);
 int wtbg_get_stats(const wtbg_ctx* ctx, wtbg_stats* out);

@@ -314,7 +314,28 @@ __global__ void k_gauge_last(double2* X, long long n, int nvec) {
 
 }  // namespace
 
+static int tridiagonal_solve_body(wtbg_ctx* ctx, int dtfull, int cpol, bool vectors);
+
+// Eigenvalues (bisection) and, with vectors, the fused oscillator sums of the tridiagonal
+// form; timed as a whole when profiling.
 int run_tridiagonal_solve(wtbg_ctx* ctx, int dtfull, int cpol, bool vectors) {
+  if (!ctx->profiling) return tridiagonal_solve_body(ctx, dtfull, cpol, vectors);
+  if (int r = ensure_events(ctx, 2)) return r;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  cudaEventRecord(e0, ctx->stream);
+  const int r = tridiagonal_solve_body(ctx, dtfull, cpol, vectors);
+  cudaEventRecord(e1, ctx->stream);
+  cudaEventSynchronize(e1);
+  float t = 0.f;
+  if (!r && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess) ctx->stats.tdsolve_ms += t;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return r;
+}
+
+static int tridiagonal_solve_body(wtbg_ctx* ctx, int dtfull, int cpol, bool vectors) {
   const long long n = ctx->N;
   cudaStream_t s = ctx->stream;
   std::vector<double> hd(n), he(n > 1 ? n - 1 : 1, 0.0);

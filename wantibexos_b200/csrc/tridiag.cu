@@ -389,8 +389,14 @@ __global__ void __launch_bounds__(RB) k_wfix_last(const double2* A, long long N,
 // Trailing update A22 -= V W^H + W V^H on the lower triangle with FP64 mma.sync.
 // Real form: C_re -= Vr Wr^T + Vi Wi^T + Wr Vr^T + Wi Vi^T
 //            C_im -= Vi Wr^T - Vr Wi^T + Wi Vr^T - Wr Vi^T
+// One CTA per 64x64 tile of the lower triangle. The panel columns arrive in chunks of HK
+// through a two-stage cp.async ring (the next chunk loads while the current one multiplies),
+// and the tile of A itself is prefetched into L2 at the start so that the read-modify-write
+// epilogue does not wait on HBM.
 constexpr int HK = 8;         // q-chunk staged per step
 constexpr int HKP = HK + 4;   // padded row stride (bank-conflict free 16-byte loads)
+constexpr int HSTAGE = 4 * TB * HKP;   // double2 per stage (Vr, Wr, Vc, Wc)
+constexpr size_t HER2K_SMEM = 2 * (size_t)HSTAGE * sizeof(double2);
 
 __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
   asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
@@ -398,8 +404,17 @@ __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, doubl
                : "d"(a0), "d"(a1), "d"(b0));
 }
 
-__global__ void __launch_bounds__(256) k_her2k(double2* A, long long N, const double2* Wp, int j0, int jb, int k0) {
-  __shared__ __align__(16) double2 sVr[TB][HKP], sWr[TB][HKP], sVc[TB][HKP], sWc[TB][HKP];
+// 16-byte asynchronous copy global -> shared; zero fill (no global read) when !valid
+__device__ __forceinline__ void cp_async16(double2* dst, const double2* src, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N_>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N_) : "memory"); }
+
+__global__ void __launch_bounds__(256, 2) k_her2k(double2* A, long long N, const double2* Wp, int j0, int jb, int k0) {
+  extern __shared__ __align__(16) double2 hsm[];
   const long long t = blockIdx.x;
   int bi = (int)floor((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
   while ((long long)(bi + 1) * (bi + 2) / 2 <= t) ++bi;
@@ -409,34 +424,63 @@ __global__ void __launch_bounds__(256) k_her2k(double2* A, long long N, const do
   const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   const int wr = wp & 3, wc = wp >> 2;
   const int gq = lane >> 2, tq = lane & 3;
+
+  // L2 prefetch of this thread's epilogue elements
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int k = 0; k < 4; k += 2) {
+      const long long row = r0 + wr * 16 + gq + ((k >> 1) ? 8 : 0);
+      const long long col = c0 + wc * 32 + n * 8 + 2 * tq;
+      if (row < N && col < N && row >= col) asm volatile("prefetch.global.L2 [%0];" ::"l"(A + row + col * N));
+    }
+
+  auto stage = [&](int c, int buf) {
+    double2* sVr = hsm + (size_t)buf * HSTAGE;
+    double2* sWr = sVr + TB * HKP;
+    double2* sVc = sWr + TB * HKP;
+    double2* sWc = sVc + TB * HKP;
+    const int qc = c * HK;
+    for (int it = tid; it < TB * HK; it += 256) {
+      const int rr = it % TB, q = it / TB;
+      const long long rg = r0 + rr, cg = c0 + rr;
+      const bool qv = (qc + q) < jb;
+      const long long qcol = (long long)(j0 + qc + q);
+      const bool vr = qv && rg < N, vc = qv && cg < N;
+      cp_async16(sVr + rr * HKP + q, vr ? A + rg + qcol * N : A, vr);
+      cp_async16(sWr + rr * HKP + q, vr ? Wp + rg + (long long)(qc + q) * N : Wp, vr);
+      cp_async16(sVc + rr * HKP + q, vc ? A + cg + qcol * N : A, vc);
+      cp_async16(sWc + rr * HKP + q, vc ? Wp + cg + (long long)(qc + q) * N : Wp, vc);
+    }
+    cp_async_commit();
+  };
+
   double accr[4][4], acci[4][4];
 #pragma unroll
   for (int n = 0; n < 4; ++n)
 #pragma unroll
     for (int k = 0; k < 4; ++k) accr[n][k] = acci[n][k] = 0.0;
 
-  for (int qc = 0; qc < jb; qc += HK) {
+  const int nch = (jb + HK - 1) / HK;
+  stage(0, 0);
+  if (nch > 1) stage(1, 1);
+  for (int c = 0; c < nch; ++c) {
+    if (c + 1 < nch) cp_async_wait<1>();
+    else cp_async_wait<0>();
     __syncthreads();
-    for (int it = tid; it < TB * HK; it += 256) {
-      const int rr = it % TB, q = it / TB;
-      const long long rg = r0 + rr, cg = c0 + rr;
-      const bool qv = (qc + q) < jb;
-      const long long qcol = (long long)(j0 + qc + q);
-      sVr[rr][q] = (qv && rg < N) ? A[rg + qcol * N] : make_double2(0, 0);
-      sWr[rr][q] = (qv && rg < N) ? Wp[rg + (long long)(qc + q) * N] : make_double2(0, 0);
-      sVc[rr][q] = (qv && cg < N) ? A[cg + qcol * N] : make_double2(0, 0);
-      sWc[rr][q] = (qv && cg < N) ? Wp[cg + (long long)(qc + q) * N] : make_double2(0, 0);
-    }
-    __syncthreads();
+    const double2* sVr = hsm + (size_t)(c & 1) * HSTAGE;
+    const double2* sWr = sVr + TB * HKP;
+    const double2* sVc = sWr + TB * HKP;
+    const double2* sWc = sVc + TB * HKP;
 #pragma unroll
     for (int kk = 0; kk < HK; kk += 4) {
       const int row = wr * 16 + gq;
-      const double2 v0 = sVr[row][kk + tq], v1 = sVr[row + 8][kk + tq];
-      const double2 w0 = sWr[row][kk + tq], w1 = sWr[row + 8][kk + tq];
+      const double2 v0 = sVr[row * HKP + kk + tq], v1 = sVr[(row + 8) * HKP + kk + tq];
+      const double2 w0 = sWr[row * HKP + kk + tq], w1 = sWr[(row + 8) * HKP + kk + tq];
 #pragma unroll
       for (int n = 0; n < 4; ++n) {
         const int col = wc * 32 + n * 8 + gq;
-        const double2 bw = sWc[col][kk + tq], bv = sVc[col][kk + tq];
+        const double2 bw = sWc[col * HKP + kk + tq], bv = sVc[col * HKP + kk + tq];
         dmma(accr[n], v0.x, v1.x, bw.x);
         dmma(accr[n], v0.y, v1.y, bw.y);
         dmma(accr[n], w0.x, w1.x, bv.x);
@@ -447,19 +491,29 @@ __global__ void __launch_bounds__(256) k_her2k(double2* A, long long N, const do
         dmma(acci[n], -w0.x, -w1.x, bv.y);
       }
     }
+    __syncthreads();
+    if (c + 2 < nch) stage(c + 2, c & 1);
   }
+  // epilogue per column block n: its four loads are issued before its stores, so a thread
+  // waits for one round trip per block instead of one per element
 #pragma unroll
   for (int n = 0; n < 4; ++n) {
+    double2 a[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const long long row = r0 + wr * 16 + gq + ((k >> 1) ? 8 : 0);
+      const long long col = c0 + wc * 32 + n * 8 + 2 * tq + (k & 1);
+      a[k] = (row < N && col < N && row >= col) ? __ldcg(A + row + col * N) : make_double2(0, 0);
+    }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const long long row = r0 + wr * 16 + gq + ((k >> 1) ? 8 : 0);
       const long long col = c0 + wc * 32 + n * 8 + 2 * tq + (k & 1);
       if (row < N && col < N && row >= col) {
-        double2* pa = A + row + col * N;
-        double2 a = *pa;
-        a.x -= accr[n][k];
-        a.y = (row == col) ? 0.0 : a.y - acci[n][k];
-        *pa = a;
+        double2 v = a[k];
+        v.x -= accr[n][k];
+        v.y = (row == col) ? 0.0 : v.y - acci[n][k];
+        A[row + col * N] = v;
       }
     }
   }
@@ -567,6 +621,7 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   CK(cudaStreamIsCapturing(s, &cap));
   if (cap == cudaStreamCaptureStatusNone) {
+    CK(cudaFuncSetAttribute(k_her2k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HER2K_SMEM));
     if (int r = autotune_hemv(ctx, &hs)) return r;
   } else {
     hs = ctx->hemv_hs > 0 ? ctx->hemv_hs : 8;   // chosen before the capture
@@ -585,8 +640,12 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
   }
   CKL("k_copy_g");
   const bool prof = ctx->profiling != 0;
+  const size_t npanel = (size_t)((N - 1 + NB - 1) / NB);
+  const size_t evh = 2 * (size_t)N;            // her2k event pairs follow the mat-vec ones
+  const size_t evt = evh + 2 * npanel;         // then the pair around the whole reduction
   if (prof) {
-    if (int r = ensure_events(ctx, 2 * (size_t)N)) return r;
+    if (int r = ensure_events(ctx, evt + 2)) return r;
+    cudaEventRecord(ctx->evpool[evt], s);
   }
 
   for (long long j0 = 0; j0 < N - 1; j0 += NB) {
@@ -611,14 +670,30 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
       k_wfix_last<<<(int)((N - k0 + RB - 1) / RB), RB, 0, s>>>(A, N, Wp, jb - 1, il, k0, st); WTBG_COUNT(ctx, 1);
       const long long T = (N - k0 + TB - 1) / TB;
       const long long ntile = T * (T + 1) / 2;
-      k_her2k<<<(unsigned)ntile, 256, 0, s>>>(A, N, Wp, (int)j0, jb, (int)k0); WTBG_COUNT(ctx, 1);
+      if (prof) cudaEventRecord(ctx->evpool[evh + 2 * (j0 / NB)], s);
+      k_her2k<<<(unsigned)ntile, 256, HER2K_SMEM, s>>>(A, N, Wp, (int)j0, jb, (int)k0); WTBG_COUNT(ctx, 1);
+      if (prof) cudaEventRecord(ctx->evpool[evh + 2 * (j0 / NB) + 1], s);
       CKL("k_her2k");
     }
   }
   k_last_diag<<<1, 1, 0, s>>>(A, N, d); WTBG_COUNT(ctx, 1);
   CKL("k_last_diag");
   if (prof) {
-    CK(cudaEventSynchronize(ctx->evpool[2 * (N - 2) + 1]));
+    cudaEventRecord(ctx->evpool[evt + 1], s);
+    CK(cudaEventSynchronize(ctx->evpool[evt + 1]));
+    float tt = 0.f;
+    CK(cudaEventElapsedTime(&tt, ctx->evpool[evt], ctx->evpool[evt + 1]));
+    ctx->stats.tri_ms += tt;
+    for (long long j0 = 0; j0 < N - 1; j0 += NB) {
+      const int jb = (int)((N - 1 - j0) < NB ? (N - 1 - j0) : NB);
+      const long long k0 = j0 + jb;
+      if (k0 >= N) continue;
+      CK(cudaEventElapsedTime(&tt, ctx->evpool[evh + 2 * (j0 / NB)], ctx->evpool[evh + 2 * (j0 / NB) + 1]));
+      const double nt = (double)(N - k0);
+      ctx->stats.her2k_ms += tt;
+      ctx->stats.her2k_flops += nt * (nt + 1.0) * 0.5 * 16.0 * (double)jb;   // 2 rank-jb products, 8 flop per cmac
+      ctx->stats.her2k_launches += 1;
+    }
     double ms = 0.0, bytes = 0.0;
     for (long long i = 0; i < N - 1; ++i) {
       float t = 0.f;

@@ -42,7 +42,9 @@ class Stats(C.Structure):
     _fields_ = [("launches", C.c_longlong), ("hemv_launches", C.c_longlong), ("hemv_ms", C.c_double),
                 ("hemv_bytes", C.c_double), ("build_launches", C.c_longlong), ("build_ms", C.c_double),
                 ("build_bytes", C.c_double), ("fast_launches", C.c_longlong), ("fast_ms", C.c_double),
-                ("fast_bytes", C.c_double), ("dav_fast_iters", C.c_longlong), ("dav_fp64_iters", C.c_longlong)]
+                ("fast_bytes", C.c_double), ("dav_fast_iters", C.c_longlong), ("dav_fp64_iters", C.c_longlong),
+                ("her2k_launches", C.c_longlong), ("her2k_ms", C.c_double), ("her2k_flops", C.c_double),
+                ("tri_ms", C.c_double), ("tdsolve_ms", C.c_double)]
 
 
 class Coulomb(C.Structure):
