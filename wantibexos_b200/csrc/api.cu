@@ -143,7 +143,7 @@ int wtbg_destroy(wtbg_ctx* ctx) {
                     &ctx->d, &ctx->e, &ctx->tau, &ctx->g, &ctx->fdeh, &ctx->Wp, &ctx->slots, &ctx->part, &ctx->scal,
                     &ctx->yv, &ctx->lam, &ctx->ws, &ctx->act, &ctx->zsel, &ctx->csz, &ctx->sp_in, &ctx->sp_out,
                     &ctx->sp_om, &ctx->tmp, &ctx->tmp2, &ctx->istat, &ctx->pOpA, &ctx->pOpB,
-                    &ctx->pHk, &ctx->pOc, &ctx->pOv, &ctx->pErr};
+                    &ctx->pHk, &ctx->pOc, &ctx->pOv, &ctx->pErr, &ctx->triErr};
   for (DevBuf* b : bufs) free_buf(*b);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
   if (ctx->tri_exec) cudaGraphExecDestroy(ctx->tri_exec);

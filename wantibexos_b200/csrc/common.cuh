@@ -89,6 +89,11 @@ struct wtbg_ctx {
   // tridiagonalisation: autotuned mat-vec chunk, and the captured CUDA graph of the whole
   // reduction for Q batches (valid while N and the work buffers stay the same)
   int hemv_hs = 0;
+  int nsm = 0;
+  alignas(64) unsigned char tmH[128];   // CUtensorMap of H for the mat-vec (see prepare_hemv)
+  const void* tmH_ptr = nullptr;
+  long long tmH_n = 0;
+  DevBuf triErr;                        // set by the mat-vec when a pipeline wait timed out
   cudaGraphExec_t tri_exec = nullptr;
   std::vector<const void*> tri_sig;
   long long tri_launches = 0;

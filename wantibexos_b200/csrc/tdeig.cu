@@ -341,7 +341,10 @@ static int tridiagonal_solve_body(wtbg_ctx* ctx, int dtfull, int cpol, bool vect
   std::vector<double> hd(n), he(n > 1 ? n - 1 : 1, 0.0);
   CK(cudaMemcpyAsync(hd.data(), ctx->d.as<double>(), n * 8, cudaMemcpyDeviceToHost, s));
   if (n > 1) CK(cudaMemcpyAsync(he.data(), ctx->e.as<double>(), (n - 1) * 8, cudaMemcpyDeviceToHost, s));
+  int tri_err = 0;
+  if (ctx->triErr.p) CK(cudaMemcpyAsync(&tri_err, ctx->triErr.p, 4, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  if (tri_err) return set_err(ctx, WTBG_ERR_CUDA, "tridiagonalise: a mat-vec pipeline wait timed out");
   double lo = hd[0], hi = hd[0], emax2 = 0.0;
   for (long long i = 0; i < n; ++i) {
     const double r = (i > 0 ? fabs(he[i - 1]) : 0.0) + (i < n - 1 ? fabs(he[i]) : 0.0);

@@ -18,10 +18,15 @@
 // All reductions are deterministic two-pass (no atomics).
 #include <cfloat>
 
-#include "common.cuh"
+#include <cudaTypedefs.h>
 
+#include "common.cuh"
+#include "tc_sm100.cuh"
+
+#include <algorithm>
 #include <map>
 #include <mutex>
+#include <string>
 
 namespace {
 
@@ -212,69 +217,123 @@ __global__ void __launch_bounds__(256) k_colC(double2* A, long long N, const dou
 }
 
 // (D) y = A22 v, A22 = rows/cols [i+1, N) of the lower-stored Hermitian matrix.
-// One CTA streams a chunk of up to HS 64x64 tiles down one block-column J: the row sums
-// A_IJ x_J go to slot[I][J] per tile; the column sums A_IJ^H x_I stay in registers across
-// the chunk and go to slot[J][I0] (I0 = first tile of the chunk, zeros in the rest of the
-// chunk's slots), so that y_a = sum_b slot[a][b] over b in the trailing block range.
-// HS (tiles per CTA chunk) is a template parameter; the autotuner below picks it per (device, N).
-template <int HS>
-__global__ void __launch_bounds__(256, 2) k_hemv(const double2* __restrict__ A, long long N, int i, int nblk,
-                                                 double2* __restrict__ slots) {
+// Work item = a chunk of up to hs 64x64 tiles down one block-column J. The row sums A_IJ x_J
+// go to slot[I][J] per tile; the column sums A_IJ^H x_I stay in registers across the chunk and
+// go to slot[J][I0] (I0 = first tile of the chunk, zeros in the rest of the chunk's slots), so
+// that y_a = sum_b slot[a][b] over b in the trailing block range.
+// Persistent: one CTA per SM walks its items round-robin; thread 0 keeps HV_STAGES tiles in
+// flight through TMA (one 64 KB box of 64 columns x 64 rows per tile, column-major as stored,
+// zero fill past N) into a shared-memory ring, across item boundaries, so that the HBM stream
+// does not drain between chunks. Every wait is bounded; a timed-out wait sets *err after the
+// CTA's own copies in flight have landed.
+constexpr int HV_STAGES = 3;
+constexpr uint32_t HV_TILE_BYTES = TB * TB * 16;
+constexpr size_t HV_SMEM = (size_t)HV_STAGES * HV_TILE_BYTES + 1024;
+
+__global__ void __launch_bounds__(256, 1) k_hemv(const __grid_constant__ CUtensorMap tm, const double2* __restrict__ A,
+                                                 long long N, int i, int nblk, int hs, double2* __restrict__ slots,
+                                                 int* err) {
+  extern __shared__ unsigned char hv_raw[];
   __shared__ double2 xJs[TB];
   __shared__ double2 rowp[2][8][TB];
   __shared__ double2 diagrow[TB];
   __shared__ double2 colp[TB];
-  const int b0 = (i + 1) / TB;
-  const int J = b0 + blockIdx.x;
-  const int I0 = J + blockIdx.y * HS;
-  if (I0 >= nblk) return;
-  const int I1 = min(I0 + HS, nblk);
+  __shared__ __align__(8) uint64_t full[HV_STAGES];
+  __shared__ int s_flag;
   const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  const uint32_t raw = tc::smem_u32(hv_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  const double2* tiles = reinterpret_cast<const double2*>(hv_raw + (base - raw));
+  const int b0 = (i + 1) / TB, nt = nblk - b0;
+  const int nyc = (nt + hs - 1) / hs;
+  const long long nitems = (long long)nt * nyc, stride = gridDim.x;
   const long long lo = (long long)i + 1;
   const double2* xcol = A + (long long)i * N;
-  const long long C0 = (long long)J * TB;
-  if (tid < TB) {
-    const long long c = C0 + tid;
-    xJs[tid] = (c >= lo && c < N) ? xcol[c] : make_double2(0, 0);
+  if (tid == 0) {
+    for (int s = 0; s < HV_STAGES; ++s) tc::mbar_init(tc::smem_u32(&full[s]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_flag = 0;
   }
   __syncthreads();
-  double2 cacc[8];
+
+  // producer state (thread 0): the same item/tile sequence as the consumers
+  long long p_it = (long long)blockIdx.x - stride;
+  int p_I = 0, p_I1 = 0, p_J = 0, issued = 0;
+  auto p_next = [&]() -> bool {
+    while (p_I >= p_I1) {
+      p_it += stride;
+      if (p_it >= nitems) return false;
+      const int jj = (int)(p_it % nt), y = (int)(p_it / nt);
+      p_J = b0 + jj;
+      p_I = p_J + y * hs;
+      p_I1 = min(p_I + hs, nblk);
+    }
+    return true;
+  };
+  auto issue = [&]() {
+    const int s = issued % HV_STAGES;
+    const uint32_t bar = tc::smem_u32(&full[s]);
+    tc::mbar_expect_tx(bar, HV_TILE_BYTES);
+    tc::tma_load_2d(base + (uint32_t)s * HV_TILE_BYTES, &tm, p_I * TB * 2, p_J * TB, bar);
+    ++p_I;
+    ++issued;
+  };
+  if (tid == 0)
+    for (int s = 0; s < HV_STAGES && p_next(); ++s) issue();
+
+  int t = 0;
+  bool aborted = false;
+  for (long long it = blockIdx.x; it < nitems && !aborted; it += stride) {
+    const int jj = (int)(it % nt), y = (int)(it / nt);
+    const int J = b0 + jj, I0 = J + y * hs;
+    if (I0 >= nblk) continue;
+    const int I1 = min(I0 + hs, nblk);
+    const long long C0 = (long long)J * TB;
+    __syncthreads();   // the previous item's readers of xJs and colp are done
+    if (tid < TB) {
+      const long long c = C0 + tid;
+      xJs[tid] = (c >= lo && c < N) ? xcol[c] : make_double2(0, 0);
+    }
+    __syncthreads();
+    double2 cacc[8];
+    bool cvalid[8];
 #pragma unroll
-  for (int m = 0; m < 8; ++m) cacc[m] = make_double2(0, 0);
-  bool cvalid[8];
+    for (int m = 0; m < 8; ++m) {
+      cacc[m] = make_double2(0, 0);
+      const long long c = C0 + wp + 8 * m;
+      cvalid[m] = (c >= lo && c < N);
+    }
+    // x rows of the next tile are loaded one tile ahead
+    double2 xa_n, xb_n;
+    {
+      const long long ra = (long long)I0 * TB + lane, rb = ra + 32;
+      xa_n = (ra >= lo && ra < N) ? xcol[ra] : make_double2(0, 0);
+      xb_n = (rb >= lo && rb < N) ? xcol[rb] : make_double2(0, 0);
+    }
+    for (int I = I0; I < I1; ++I, ++t) {
+      const double2 xa = xa_n, xb = xb_n;
+      if (I + 1 < I1) {
+        const long long ra = (long long)(I + 1) * TB + lane, rb = ra + 32;
+        xa_n = (ra >= lo && ra < N) ? xcol[ra] : make_double2(0, 0);
+        xb_n = (rb >= lo && rb < N) ? xcol[rb] : make_double2(0, 0);
+      }
+      const int s = t % HV_STAGES;
+      const bool ok = tc::mbar_wait(tc::smem_u32(&full[s]), (uint32_t)((t / HV_STAGES) & 1), &s_flag, false);
+      const double2* T = tiles + (size_t)s * TB * TB;   // T[c * 64 + r]
+      const int buf = (I - I0) & 1;
+      const long long R0 = (long long)I * TB;
+      const long long ra = R0 + lane, rb = ra + 32;
+      const bool diag = (I == J);
+      const bool va = (ra >= lo && ra < N), vb = (rb >= lo && rb < N);
+      double2 rp0 = make_double2(0, 0), rp1 = make_double2(0, 0);
 #pragma unroll
-  for (int m = 0; m < 8; ++m) {
-    const long long c = C0 + wp + 8 * m;
-    cvalid[m] = (c >= lo && c < N);
-  }
-  for (int I = I0; I < I1; ++I) {
-    const int buf = (I - I0) & 1;
-    const long long R0 = (long long)I * TB;
-    const long long ra = R0 + lane, rb = ra + 32;
-    const bool diag = (I == J);
-    const bool va = (ra >= lo && ra < N), vb = (rb >= lo && rb < N);
-    const double2 xa = va ? xcol[ra] : make_double2(0, 0);
-    const double2 xb = vb ? xcol[rb] : make_double2(0, 0);
-    double2 rp0 = make_double2(0, 0), rp1 = make_double2(0, 0);
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      double2 a0[4], a1[4];
-#pragma unroll
-      for (int mm = 0; mm < 4; ++mm) {
-        const int m = h * 4 + mm;
+      for (int m = 0; m < 8; ++m) {
         const int cl = wp + 8 * m;
-        const double2* colp_ = A + (C0 + cl) * N;
         const bool ok0 = cvalid[m] && va && (!diag || lane >= cl);
         const bool ok1 = cvalid[m] && vb && (!diag || lane + 32 >= cl);
-        a0[mm] = ok0 ? colp_[ra] : make_double2(0, 0);
-        a1[mm] = ok1 ? colp_[rb] : make_double2(0, 0);
-      }
-#pragma unroll
-      for (int mm = 0; mm < 4; ++mm) {
-        const int m = h * 4 + mm;
-        const int cl = wp + 8 * m;
+        double2 e0 = ok0 ? T[cl * TB + lane] : make_double2(0, 0);
+        double2 e1 = ok1 ? T[cl * TB + lane + 32] : make_double2(0, 0);
         const double2 xj = xJs[cl];
-        double2 e0 = a0[mm], e1 = a1[mm];
         const bool d0 = diag && (lane == cl), d1 = diag && (lane + 32 == cl);
         if (d0) e0.y = 0.0;
         if (d1) e1.y = 0.0;
@@ -283,32 +342,42 @@ __global__ void __launch_bounds__(256, 2) k_hemv(const double2* __restrict__ A, 
         if (!d0) cacc[m] = cadd(cacc[m], cmulc(e0, xa));
         if (!d1) cacc[m] = cadd(cacc[m], cmulc(e1, xb));
       }
+      rowp[buf][wp][lane] = rp0;
+      rowp[buf][wp][lane + 32] = rp1;
+      if (__syncthreads_or(!ok)) {   // every thread has left stage s (and agrees on failure)
+        aborted = true;
+        break;
+      }
+      if (tid == 0 && p_next()) issue();
+      if (tid < TB) {
+        double2 sm = make_double2(0, 0);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) sm = cadd(sm, rowp[buf][k][tid]);
+        if (diag) diagrow[tid] = sm;
+        else slots[((long long)I * nblk + J) * TB + tid] = sm;
+      }
     }
-    rowp[buf][wp][lane] = rp0;
-    rowp[buf][wp][lane + 32] = rp1;
+    if (aborted) break;
+    // column sums of the chunk
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const double2 sm = warp_sum2(cacc[m]);
+      if (lane == m) colp[wp + 8 * m] = sm;
+    }
     __syncthreads();
     if (tid < TB) {
-      double2 s = make_double2(0, 0);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) s = cadd(s, rowp[buf][k][tid]);
-      if (diag) diagrow[tid] = s;
-      else slots[((long long)I * nblk + J) * TB + tid] = s;
+      double2 v = colp[tid];
+      if (I0 == J) v = cadd(v, diagrow[tid]);
+      slots[((long long)J * nblk + I0) * TB + tid] = v;
+      for (int I = I0 + 1; I < I1; ++I) slots[((long long)J * nblk + I) * TB + tid] = make_double2(0, 0);
     }
   }
-  // column sums of the chunk
-#pragma unroll
-  for (int m = 0; m < 8; ++m) {
-    const double2 s = warp_sum2(cacc[m]);
-    if (lane == m) colp[wp + 8 * m] = s;
+  if (aborted && tid == 0) {
+    // let this CTA's copies in flight land before the shared memory is released
+    for (int u = t; u < issued; ++u)
+      tc::mbar_wait(tc::smem_u32(&full[u % HV_STAGES]), (uint32_t)((u / HV_STAGES) & 1), &s_flag, false);
+    atomicExch(err, 1);
   }
-  __syncthreads();
-  if (tid < TB) {
-    double2 v = colp[tid];
-    if (I0 == J) v = cadd(v, diagrow[tid]);
-    slots[((long long)J * nblk + I0) * TB + tid] = v;
-  }
-  for (int I = I0 + 1; I < I1; ++I)
-    if (tid < TB) slots[((long long)J * nblk + I) * TB + tid] = make_double2(0, 0);
 }
 
 // (E) y rows from the slots; w = tau (y - V z1 - W z2); g <- g - tau conj(v) s; partial
@@ -532,16 +601,51 @@ __global__ void k_copy_g(const double2* h, double2* g, long long n) {
 
 namespace {
 
-void launch_hemv(int hs, int nt, cudaStream_t s, const double2* A, long long N, int i, int nblk, double2* slots) {
-  if (hs == 4)
-    k_hemv<4><<<dim3(nt, (nt + 3) / 4), 256, 0, s>>>(A, N, i, nblk, slots);
-  else if (hs == 16)
-    k_hemv<16><<<dim3(nt, (nt + 15) / 16), 256, 0, s>>>(A, N, i, nblk, slots);
-  else
-    k_hemv<8><<<dim3(nt, (nt + 7) / 8), 256, 0, s>>>(A, N, i, nblk, slots);
+void launch_hemv(wtbg_ctx* ctx, int hs, int nt, cudaStream_t s, const double2* A, long long N, int i, int nblk,
+                 double2* slots) {
+  const long long nitems = (long long)nt * ((nt + hs - 1) / hs);
+  const int grid = (int)std::min<long long>(nitems, ctx->nsm);
+  k_hemv<<<grid, 256, HV_SMEM, s>>>(*reinterpret_cast<const CUtensorMap*>(ctx->tmH), A, N, i, nblk, hs, slots,
+                                    ctx->triErr.as<int>());
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
 }
 
 }  // namespace
+
+// TMA map of the BSE matrix for the mat-vec: FP64 view of the column-major complex array,
+// dims (2N doubles, N columns), box (128 doubles = 64 rows, 64 columns); kept while H and N
+// stay the same. Also sizes the error flag and reads the SM count.
+int prepare_hemv(wtbg_ctx* ctx) {
+  const long long N = ctx->N;
+  ENSURE(ctx->triErr, 16);
+  if (ctx->nsm <= 0) CK(cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device));
+  CK(cudaFuncSetAttribute(k_hemv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HV_SMEM));
+  if (ctx->tmH_ptr == ctx->H.p && ctx->tmH_n == N) return 0;
+  auto fn = tma_encoder();
+  if (!fn) return set_err(ctx, WTBG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  cuuint64_t dims[2] = {(cuuint64_t)(2 * N), (cuuint64_t)N};
+  cuuint64_t strides[1] = {(cuuint64_t)N * 16};
+  cuuint32_t box[2] = {(cuuint32_t)(2 * TB), (cuuint32_t)TB};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = fn(reinterpret_cast<CUtensorMap*>(ctx->tmH), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, ctx->H.p, dims, strides,
+                  box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_err(ctx, WTBG_ERR_CUDA, "cuTensorMapEncodeTiled(H) failed: " + std::to_string((int)r));
+  ctx->tmH_ptr = ctx->H.p;
+  ctx->tmH_n = N;
+  return 0;
+}
 
 // Autotuner for the mat-vec chunk (tiles per CTA, 4 / 8 / 16): times each variant on the
 // column N/4 (three launches each, CUDA events; the launches only write the slot partials,
@@ -563,6 +667,7 @@ int autotune_hemv(wtbg_ctx* ctx, int* hs_out) {
   *hs_out = 8;
   if (N < 4 * TB) return 0;
   ENSURE(ctx->slots, (size_t)nblk * nblk * TB * 16);
+  if (int r = prepare_hemv(ctx)) return r;
   if (int r = ensure_events(ctx, 2)) return r;
   const int i = (int)(N / 4);
   const int nt = nblk - (i + 1) / TB;
@@ -572,7 +677,7 @@ int autotune_hemv(wtbg_ctx* ctx, int* hs_out) {
     float tot = 0.f;
     for (int rep = 0; rep < 4; ++rep) {
       CK(cudaEventRecord(ctx->evpool[0], ctx->stream));
-      launch_hemv(c, nt, ctx->stream, ctx->H.as<double2>(), N, i, nblk, ctx->slots.as<double2>());
+      launch_hemv(ctx, c, nt, ctx->stream, ctx->H.as<double2>(), N, i, nblk, ctx->slots.as<double2>());
       CK(cudaEventRecord(ctx->evpool[1], ctx->stream));
       CK(cudaEventSynchronize(ctx->evpool[1]));
       float ms = 0.f;
@@ -622,12 +727,14 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
   CK(cudaStreamIsCapturing(s, &cap));
   if (cap == cudaStreamCaptureStatusNone) {
     CK(cudaFuncSetAttribute(k_her2k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HER2K_SMEM));
+    if (int r = prepare_hemv(ctx)) return r;
     if (int r = autotune_hemv(ctx, &hs)) return r;
   } else {
     hs = ctx->hemv_hs > 0 ? ctx->hemv_hs : 8;   // chosen before the capture
   }
   ctx->hemv_hs = hs;
   CK(cudaMemsetAsync(st, 0, sizeof(ColState), s));
+  CK(cudaMemsetAsync(ctx->triErr.p, 0, 4, s));
 
   const int ng = (ctx->have_velocity && ctx->temp_on) ? 10 : 5;
   ctx->ng = ng;
@@ -659,7 +766,7 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
       const int b0 = (i + 1) / TB;
       const int nt = nblk - b0;
       if (prof) cudaEventRecord(ctx->evpool[2 * i], s);
-      launch_hemv(hs, nt, s, A, N, i, nblk, slots); WTBG_COUNT(ctx, 1);
+      launch_hemv(ctx, hs, nt, s, A, N, i, nblk, slots); WTBG_COUNT(ctx, 1);
       if (prof) cudaEventRecord(ctx->evpool[2 * i + 1], s);
       k_colE<<<nt, 256, 0, s>>>(A, N, Wp, (int)j0, p, i, nblk, slots, st, g, ng, partE); WTBG_COUNT(ctx, 1);
     }
