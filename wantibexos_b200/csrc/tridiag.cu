@@ -303,6 +303,7 @@ __global__ void __launch_bounds__(256, 1) k_hemv(const __grid_constant__ CUtenso
       const long long c = C0 + wp + 8 * m;
       cvalid[m] = (c >= lo && c < N);
     }
+    const bool interior_cols = (C0 >= lo && C0 + TB <= N);
     // x rows of the next tile are loaded one tile ahead
     double2 xa_n, xb_n;
     {
@@ -326,6 +327,18 @@ __global__ void __launch_bounds__(256, 1) k_hemv(const __grid_constant__ CUtenso
       const bool diag = (I == J);
       const bool va = (ra >= lo && ra < N), vb = (rb >= lo && rb < N);
       double2 rp0 = make_double2(0, 0), rp1 = make_double2(0, 0);
+      if (interior_cols && !diag && R0 >= lo && R0 + TB <= N) {
+        // interior tile: every element is in the trailing matrix, no masks
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+          const int cl = wp + 8 * m;
+          const double2 e0 = T[cl * TB + lane], e1 = T[cl * TB + lane + 32];
+          const double2 xj = xJs[cl];
+          rp0 = cadd(rp0, cmul(e0, xj));
+          rp1 = cadd(rp1, cmul(e1, xj));
+          cacc[m] = cadd(cacc[m], cadd(cmulc(e0, xa), cmulc(e1, xb)));
+        }
+      } else
 #pragma unroll
       for (int m = 0; m < 8; ++m) {
         const int cl = wp + 8 * m;
