@@ -11,7 +11,7 @@
 //     (3) used in the Hermitian matrix-vector product y = A22 v (tiled over the lower triangle)
 //     (4) w = tau (y - V (W^H v) - W (V^H v)),  w += -tau/2 (w^H v) v
 //   and after the panel the trailing matrix gets A22 -= V W^H + W V^H on FP64 tensor cores
-//   (mma.sync m16n8k4 f64; Blackwell has no tcgen05 kind for f64).
+//   (mma.sync m16n8k16 f64; Blackwell has no tcgen05 kind for f64).
 // The oscillator sums need only A^T h = Z^T (Q^T h) (Z = eigenvectors of T), so the
 // reflectors are also applied to the five h vectors as they are generated,
 // g <- g - tau conj(v) (v^T g) -- the full O(N^3) eigenvector back-transform is never formed.
@@ -219,8 +219,8 @@ __global__ void __launch_bounds__(256) k_colC(double2* A, long long N, const dou
 // (D) y = A22 v, A22 = rows/cols [i+1, N) of the lower-stored Hermitian matrix.
 // Work item = a chunk of up to hs 64x64 tiles down one block-column J. The row sums A_IJ x_J
 // go to slot[I][J] per tile; the column sums A_IJ^H x_I stay in registers across the chunk and
-// go to slot[J][I0] (I0 = first tile of the chunk, zeros in the rest of the chunk's slots), so
-// that y_a = sum_b slot[a][b] over b in the trailing block range.
+// go to slot[J][I0] (I0 = first tile of the chunk, I0 = J + y*hs), so that
+// y_a = sum of slot[a][b] over b0 <= b <= a and over b = a + hs, a + 2 hs, ... < nblk.
 // Persistent: one CTA per SM walks its items round-robin; thread 0 keeps HV_STAGES tiles in
 // flight through TMA (one 64 KB box of 64 columns x 64 rows per tile, column-major as stored,
 // zero fill past N) into a shared-memory ring, across item boundaries, so that the HBM stream
@@ -382,7 +382,6 @@ __global__ void __launch_bounds__(256, 1) k_hemv(const __grid_constant__ CUtenso
       double2 v = colp[tid];
       if (I0 == J) v = cadd(v, diagrow[tid]);
       slots[((long long)J * nblk + I0) * TB + tid] = v;
-      for (int I = I0 + 1; I < I1; ++I) slots[((long long)J * nblk + I) * TB + tid] = make_double2(0, 0);
     }
   }
   if (aborted && tid == 0) {
@@ -396,7 +395,8 @@ __global__ void __launch_bounds__(256, 1) k_hemv(const __grid_constant__ CUtenso
 // (E) y rows from the slots; w = tau (y - V z1 - W z2); g <- g - tau conj(v) s; partial
 //     w^H v.  The last block computes alpha2 = -tau/2 w^H v for the next column kernel.
 __global__ void __launch_bounds__(256) k_colE(const double2* A, long long N, double2* Wp, int j0, int p, int i, int nblk,
-                                              const double2* slots, ColState* st, double2* g, int ng, double2* part) {
+                                              int hs, const double2* slots, ColState* st, double2* g, int ng,
+                                              double2* part) {
   __shared__ double2 acc4[4][TB];
   __shared__ double2 tq4[4][TB];
   __shared__ double2 zz[2 * NB + NG];
@@ -408,9 +408,15 @@ __global__ void __launch_bounds__(256) k_colE(const double2* A, long long N, dou
   const int b0 = (i + 1) / TB;
   const int a = b0 + blockIdx.x;
   const int el = tid & (TB - 1), grp = tid >> 6;
+  // slots of row block a: the tile row sums b0 <= b <= a, then the chunk column sums at
+  // b = a + hs, a + 2 hs, ... (the only slots the mat-vec writes above the diagonal)
+  const int n1 = a - b0 + 1, n2 = (nblk - 1 - a) / hs;
   double2 s = make_double2(0, 0);
 #pragma unroll 4
-  for (int b = b0 + grp; b < nblk; b += 4) s = cadd(s, slots[((long long)a * nblk + b) * TB + el]);
+  for (int u = grp; u < n1 + n2; u += 4) {
+    const int b = (u < n1) ? b0 + u : a + hs * (u - n1 + 1);
+    s = cadd(s, slots[((long long)a * nblk + b) * TB + el]);
+  }
   acc4[grp][el] = s;
   __syncthreads();
   const long long r = (long long)a * TB + el;
@@ -480,10 +486,15 @@ constexpr int HKP = HK + 4;   // padded row stride (bank-conflict free 16-byte l
 constexpr int HSTAGE = 4 * TB * HKP;   // double2 per stage (Vr, Wr, Vc, Wc)
 constexpr size_t HER2K_SMEM = 2 * (size_t)HSTAGE * sizeof(double2);
 
-__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
-  asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
-               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
-               : "d"(a0), "d"(a1), "d"(b0));
+// D += A B with A 16x16 (k = tq + 4*(i/2) for a_i, row gq + 8*(i%2)) and B 16x8 (k = tq + 4*j for
+// b_j, column gq): the four real products of one complex accumulator concatenated along k.
+__device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]), "d"(b[1]),
+        "d"(b[2]), "d"(b[3]));
 }
 
 // 16-byte asynchronous copy global -> shared; zero fill (no global read) when !valid
@@ -559,18 +570,16 @@ __global__ void __launch_bounds__(256, 2) k_her2k(double2* A, long long N, const
       const int row = wr * 16 + gq;
       const double2 v0 = sVr[row * HKP + kk + tq], v1 = sVr[(row + 8) * HKP + kk + tq];
       const double2 w0 = sWr[row * HKP + kk + tq], w1 = sWr[(row + 8) * HKP + kk + tq];
+      // k segments: [Vr | Vi | Wr | Wi] (re) and [Vi | -Vr | Wi | -Wr] (im) against [Wr; Wi; Vr; Vi]
+      const double are[8] = {v0.x, v1.x, v0.y, v1.y, w0.x, w1.x, w0.y, w1.y};
+      const double aim[8] = {v0.y, v1.y, -v0.x, -v1.x, w0.y, w1.y, -w0.x, -w1.x};
 #pragma unroll
       for (int n = 0; n < 4; ++n) {
         const int col = wc * 32 + n * 8 + gq;
         const double2 bw = sWc[col * HKP + kk + tq], bv = sVc[col * HKP + kk + tq];
-        dmma(accr[n], v0.x, v1.x, bw.x);
-        dmma(accr[n], v0.y, v1.y, bw.y);
-        dmma(accr[n], w0.x, w1.x, bv.x);
-        dmma(accr[n], w0.y, w1.y, bv.y);
-        dmma(acci[n], v0.y, v1.y, bw.x);
-        dmma(acci[n], -v0.x, -v1.x, bw.y);
-        dmma(acci[n], w0.y, w1.y, bv.x);
-        dmma(acci[n], -w0.x, -w1.x, bv.y);
+        const double b[4] = {bw.x, bw.y, bv.x, bv.y};
+        dmma16(accr[n], are, b);
+        dmma16(acci[n], aim, b);
       }
     }
     __syncthreads();
@@ -781,7 +790,7 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
       if (prof) cudaEventRecord(ctx->evpool[2 * i], s);
       launch_hemv(ctx, hs, nt, s, A, N, i, nblk, slots); WTBG_COUNT(ctx, 1);
       if (prof) cudaEventRecord(ctx->evpool[2 * i + 1], s);
-      k_colE<<<nt, 256, 0, s>>>(A, N, Wp, (int)j0, p, i, nblk, slots, st, g, ng, partE); WTBG_COUNT(ctx, 1);
+      k_colE<<<nt, 256, 0, s>>>(A, N, Wp, (int)j0, p, i, nblk, hs, slots, st, g, ng, partE); WTBG_COUNT(ctx, 1);
     }
     CKL("tridiagonal panel");
     const long long k0 = j0 + jb;
