@@ -81,12 +81,22 @@ __device__ __forceinline__ bool last_block(unsigned int* cnt) {
   return s_last;
 }
 
+// Programmatic dependent launch: every kernel of the column chain starts by waiting for its
+// predecessor grid (all of its memory operations visible), then lets its own dependent grid
+// be scheduled, so that launch latency and the CTA ramp of the next kernel overlap the tail of
+// this one. Outside a programmatic launch both instructions are no-ops.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // (A) apply the previous column's w correction, update column i with the panel's pending
 //     rank-2 terms, |x|^2 partials; the last block computes the reflector (ZLARFG).
 //     RA rows per block; the four 64-thread groups split the panel columns q (mod 4), so that
 //     each thread keeps few loads in flight and the grid covers the SMs at moderate N.
 __global__ void __launch_bounds__(256) k_colA(double2* A, long long N, double2* Wp, int j0, int p, int i, double* part,
                                               ColState* st, double* d, double* e, double2* tau_out) {
+  pdl_enter();
   __shared__ double2 wrow[NB], vrow[NB];
   __shared__ double2 sacc[4][RA];
   __shared__ double red[8];
@@ -171,6 +181,7 @@ __global__ void __launch_bounds__(256) k_colA(double2* A, long long N, double2* 
 //     partials into st->z, again one warp per dot with the lanes striding over the blocks.
 __global__ void __launch_bounds__(256) k_colC(double2* A, long long N, const double2* Wp, int j0, int p, int i,
                                               ColState* st, const double2* g, int ng, double2* part) {
+  pdl_enter();
   __shared__ double2 vs[RA];
   const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   const long long rbase = (long long)i + 1 + (long long)blockIdx.x * RA;
@@ -233,6 +244,7 @@ constexpr size_t HV_SMEM = (size_t)HV_STAGES * HV_TILE_BYTES + 1024;
 __global__ void __launch_bounds__(256, 1) k_hemv(const __grid_constant__ CUtensorMap tm, const double2* __restrict__ A,
                                                  long long N, int i, int nblk, int hs, double2* __restrict__ slots,
                                                  int* err) {
+  pdl_enter();
   extern __shared__ unsigned char hv_raw[];
   __shared__ double2 xJs[TB];
   __shared__ double2 rowp[2][8][TB];
@@ -397,6 +409,7 @@ __global__ void __launch_bounds__(256, 1) k_hemv(const __grid_constant__ CUtenso
 __global__ void __launch_bounds__(256) k_colE(const double2* A, long long N, double2* Wp, int j0, int p, int i, int nblk,
                                               int hs, const double2* slots, ColState* st, double2* g, int ng,
                                               double2* part) {
+  pdl_enter();
   __shared__ double2 acc4[4][TB];
   __shared__ double2 tq4[4][TB];
   __shared__ double2 zz[2 * NB + NG];
@@ -468,6 +481,7 @@ __global__ void __launch_bounds__(256) k_colE(const double2* A, long long N, dou
 // w(last column of the panel) += alpha2 v, rows [k0, N), before the trailing update
 __global__ void __launch_bounds__(RB) k_wfix_last(const double2* A, long long N, double2* Wp, int p, int i, long long k0,
                                                   const ColState* st) {
+  pdl_enter();
   const long long r = k0 + (long long)blockIdx.x * RB + threadIdx.x;
   if (r >= N) return;
   const double2 alpha2 = st->alpha2;
@@ -507,6 +521,7 @@ template <int N_>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N_) : "memory"); }
 
 __global__ void __launch_bounds__(256, 2) k_her2k(double2* A, long long N, const double2* Wp, int j0, int jb, int k0) {
+  pdl_enter();
   extern __shared__ __align__(16) double2 hsm[];
   const long long t = blockIdx.x;
   int bi = (int)floor((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
@@ -623,12 +638,28 @@ __global__ void k_copy_g(const double2* h, double2* g, long long n) {
 
 namespace {
 
-void launch_hemv(wtbg_ctx* ctx, int hs, int nt, cudaStream_t s, const double2* A, long long N, int i, int nblk,
-                 double2* slots) {
+// launch with programmatic stream serialisation (see pdl_enter)
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
+cudaError_t launch_hemv(wtbg_ctx* ctx, int hs, int nt, cudaStream_t s, const double2* A, long long N, int i, int nblk,
+                        double2* slots) {
   const long long nitems = (long long)nt * ((nt + hs - 1) / hs);
   const int grid = (int)std::min<long long>(nitems, ctx->nsm);
-  k_hemv<<<grid, 256, HV_SMEM, s>>>(*reinterpret_cast<const CUtensorMap*>(ctx->tmH), A, N, i, nblk, hs, slots,
-                                    ctx->triErr.as<int>());
+  return launch_pdl(k_hemv, dim3(grid), dim3(256), HV_SMEM, s, *reinterpret_cast<const CUtensorMap*>(ctx->tmH), A, N,
+                    i, nblk, hs, slots, ctx->triErr.as<int>());
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
@@ -699,7 +730,7 @@ int autotune_hemv(wtbg_ctx* ctx, int* hs_out) {
     float tot = 0.f;
     for (int rep = 0; rep < 4; ++rep) {
       CK(cudaEventRecord(ctx->evpool[0], ctx->stream));
-      launch_hemv(ctx, c, nt, ctx->stream, ctx->H.as<double2>(), N, i, nblk, ctx->slots.as<double2>());
+      CK(launch_hemv(ctx, c, nt, ctx->stream, ctx->H.as<double2>(), N, i, nblk, ctx->slots.as<double2>()));
       CK(cudaEventRecord(ctx->evpool[1], ctx->stream));
       CK(cudaEventSynchronize(ctx->evpool[1]));
       float ms = 0.f;
@@ -782,25 +813,29 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
     for (int p = 0; p < jb; ++p) {
       const int i = (int)(j0 + p);
       const int nA = (int)((N - i + RA - 1) / RA);
-      k_colA<<<nA, 256, 0, s>>>(A, N, Wp, (int)j0, p, i, partA, st, d, e, tau); WTBG_COUNT(ctx, 1);
+      CK(launch_pdl(k_colA, dim3(nA), dim3(256), 0, s, A, N, Wp, (int)j0, p, i, partA, st, d, e, tau)); WTBG_COUNT(ctx, 1);
       const int nC = (int)((N - i - 1 + RA - 1) / RA);
-      k_colC<<<nC, 256, 0, s>>>(A, N, Wp, (int)j0, p, i, st, g, ng, partC); WTBG_COUNT(ctx, 1);
+      CK(launch_pdl(k_colC, dim3(nC), dim3(256), 0, s, A, N, (const double2*)Wp, (int)j0, p, i, st, (const double2*)g, ng,
+                    partC)); WTBG_COUNT(ctx, 1);
       const int b0 = (i + 1) / TB;
       const int nt = nblk - b0;
       if (prof) cudaEventRecord(ctx->evpool[2 * i], s);
-      launch_hemv(ctx, hs, nt, s, A, N, i, nblk, slots); WTBG_COUNT(ctx, 1);
+      CK(launch_hemv(ctx, hs, nt, s, A, N, i, nblk, slots)); WTBG_COUNT(ctx, 1);
       if (prof) cudaEventRecord(ctx->evpool[2 * i + 1], s);
-      k_colE<<<nt, 256, 0, s>>>(A, N, Wp, (int)j0, p, i, nblk, hs, slots, st, g, ng, partE); WTBG_COUNT(ctx, 1);
+      CK(launch_pdl(k_colE, dim3(nt), dim3(256), 0, s, (const double2*)A, N, Wp, (int)j0, p, i, nblk, hs,
+                    (const double2*)slots, st, g, ng, partE)); WTBG_COUNT(ctx, 1);
     }
     CKL("tridiagonal panel");
     const long long k0 = j0 + jb;
     if (k0 < N) {
       const int il = (int)(j0 + jb - 1);
-      k_wfix_last<<<(int)((N - k0 + RB - 1) / RB), RB, 0, s>>>(A, N, Wp, jb - 1, il, k0, st); WTBG_COUNT(ctx, 1);
+      CK(launch_pdl(k_wfix_last, dim3((int)((N - k0 + RB - 1) / RB)), dim3(RB), 0, s, (const double2*)A, N, Wp, jb - 1, il,
+                    k0, (const ColState*)st)); WTBG_COUNT(ctx, 1);
       const long long T = (N - k0 + TB - 1) / TB;
       const long long ntile = T * (T + 1) / 2;
       if (prof) cudaEventRecord(ctx->evpool[evh + 2 * (j0 / NB)], s);
-      k_her2k<<<(unsigned)ntile, 256, HER2K_SMEM, s>>>(A, N, Wp, (int)j0, jb, (int)k0); WTBG_COUNT(ctx, 1);
+      CK(launch_pdl(k_her2k, dim3((unsigned)ntile), dim3(256), HER2K_SMEM, s, A, N, (const double2*)Wp, (int)j0, jb,
+                    (int)k0)); WTBG_COUNT(ctx, 1);
       if (prof) cudaEventRecord(ctx->evpool[evh + 2 * (j0 / NB) + 1], s);
       CKL("k_her2k");
     }
