@@ -27,91 +27,127 @@ constexpr int NG = 5;
 constexpr int kMaxRR = 80;    // largest Rayleigh-Ritz size (two 80x80 complex matrices fit in one CTA)
 
 // Y[part][N][m] partial of H X over the block-columns of chunk blockIdx.y; H lower-stored.
-// Thread layout: 256 threads = 32 row pairs x 8 vector groups; each thread owns rows
-// (r, r+32) and MV vectors.
+// The 64x64 tile H(I,J) (Hermitian-completed from the lower triangle) and the 64 rows of X
+// are staged in shared memory; the product runs on the FP64 tensor cores as
+// mma.sync m16n8k16 with the complex arithmetic concatenated along k:
+//   Yr += [Hr | -Hi] [Xr ; Xi],   Yi += [Hr | Hi] [Xi ; Xr]     (8 complex columns per MMA).
+// 8 warps = 4 row groups of 16 rows x 2 halves of the tile's 64 columns; the halves are
+// added through shared memory at the end. Fragment layout of m16n8k16 f64: a_i holds row
+// gq + 8 (i % 2), k = tq + 4 (i / 2); b_j holds k = tq + 4 j, column gq; c holds rows gq, gq + 8
+// and columns 2 tq, 2 tq + 1.
+constexpr int HT = TB + 2;   // tile column stride (conflict-free fragment loads)
+
+__device__ __forceinline__ void mma16(double (&c)[4], const double (&a)[8], double b0, double b1, double b2,
+                                      double b3) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b0), "d"(b1),
+        "d"(b2), "d"(b3));
+}
+
 template <int MV>
 __global__ void __launch_bounds__(256) k_hemm(const double2* __restrict__ A, long long N, const double2* __restrict__ X,
                                               int ldx, double2* __restrict__ Yp) {
   constexpr int M = 8 * MV;
+  constexpr int XS = M + 2;   // xs row stride
   extern __shared__ __align__(16) unsigned char hsm[];
-  double2 (*tile)[TB + 1] = reinterpret_cast<double2 (*)[TB + 1]>(hsm);                      // tile[c][r]
-  double2 (*xs)[M + 1] = reinterpret_cast<double2 (*)[M + 1]>(hsm + sizeof(double2) * TB * (TB + 1));  // xs[c][v]
+  double2* tile = reinterpret_cast<double2*>(hsm);                                   // tile[c * HT + r]
+  double2* xs = reinterpret_cast<double2*>(hsm + sizeof(double2) * TB * HT);         // xs[c * XS + v]
   const int I = blockIdx.x;
   const int nblk = (int)((N + TB - 1) / TB);
-  const int tid = threadIdx.x;
-  const int r = tid & 31, vg = tid >> 5;
-  double2 acc[2][MV];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gq = lane >> 2, tq = lane & 3;
+  const int rg = warp & 3, kh = warp >> 2;   // row group, column half
+  double accr[MV][4], acci[MV][4];
 #pragma unroll
-  for (int a = 0; a < 2; ++a)
+  for (int v = 0; v < MV; ++v)
 #pragma unroll
-    for (int v = 0; v < MV; ++v) acc[a][v] = make_double2(0, 0);
+    for (int k = 0; k < 4; ++k) accr[v][k] = acci[v][k] = 0.0;
   const int jper = (nblk + JCH - 1) / JCH;
   const int J0 = blockIdx.y * jper, J1 = min(nblk, J0 + jper);
   const long long R0 = (long long)I * TB;
   for (int J = J0; J < J1; ++J) {
     const long long C0 = (long long)J * TB;
     __syncthreads();
-    // load H(I,J): J < I from the lower tile (rows I, cols J); J > I from the conj
-    // transpose of the lower tile (rows J, cols I); J == I from the lower part of the
-    // diagonal tile, mirrored.
+    // H(I,J): J < I from the lower tile (rows I, cols J); J > I from the conj transpose of
+    // the lower tile (rows J, cols I); J == I from the lower part of the diagonal tile, mirrored
     for (int it = tid; it < TB * TB; it += 256) {
       const int a = it & (TB - 1), b = it >> 6;   // a fastest: coalesced global reads
       double2 v = make_double2(0, 0);
       if (J < I) {
         const long long rr = R0 + a, cc = C0 + b;
         if (rr < N && cc < N) v = A[rr + cc * N];
-        tile[b][a] = v;                 // H(R0+a, C0+b)
+        tile[b * HT + a] = v;                 // H(R0+a, C0+b)
       } else if (J > I) {
         const long long rr = C0 + a, cc = R0 + b;   // lower element (C0+a, R0+b)
         if (rr < N && cc < N) v = cconj(A[rr + cc * N]);
-        tile[a][b] = v;                 // H(R0+b, C0+a) = conj(L(C0+a, R0+b))
+        tile[a * HT + b] = v;                 // H(R0+b, C0+a) = conj(L(C0+a, R0+b))
       } else {
         const long long rr = R0 + a, cc = C0 + b;
         if (rr < N && cc < N) {
           if (a > b) {
             v = A[rr + cc * N];
-            tile[b][a] = v;
-            tile[a][b] = cconj(v);
+            tile[b * HT + a] = v;
+            tile[a * HT + b] = cconj(v);
           } else if (a == b) {
             v = A[rr + cc * N];
-            tile[a][a] = make_double2(v.x, 0.0);
+            tile[a * HT + a] = make_double2(v.x, 0.0);
           }
         } else {
-          tile[b][a] = make_double2(0, 0);
-          tile[a][b] = make_double2(0, 0);
+          tile[b * HT + a] = make_double2(0, 0);
+          tile[a * HT + b] = make_double2(0, 0);
         }
       }
     }
     for (int it = tid; it < TB * M; it += 256) {
       const int c = it % TB, v = it / TB;
       const long long rr = C0 + c;
-      xs[c][v] = (rr < N) ? X[rr + (long long)v * ldx] : make_double2(0, 0);
+      xs[c * XS + v] = (rr < N) ? X[rr + (long long)v * ldx] : make_double2(0, 0);
     }
     __syncthreads();
-#pragma unroll 4
-    for (int c = 0; c < TB; ++c) {
-      const double2 h0 = tile[c][r], h1 = tile[c][r + 32];
+    const int row = rg * 16 + gq;
 #pragma unroll
-      for (int v = 0; v < MV; ++v) {   // acc += h x as four FMAs each
-        const double2 x = xs[c][vg * MV + v];
-        acc[0][v].x = fma(h0.x, x.x, acc[0][v].x);
-        acc[0][v].x = fma(-h0.y, x.y, acc[0][v].x);
-        acc[0][v].y = fma(h0.x, x.y, acc[0][v].y);
-        acc[0][v].y = fma(h0.y, x.x, acc[0][v].y);
-        acc[1][v].x = fma(h1.x, x.x, acc[1][v].x);
-        acc[1][v].x = fma(-h1.y, x.y, acc[1][v].x);
-        acc[1][v].y = fma(h1.x, x.y, acc[1][v].y);
-        acc[1][v].y = fma(h1.y, x.x, acc[1][v].y);
+    for (int ks = 0; ks < 4; ++ks) {
+      const int c0 = kh * 32 + ks * 8;
+      const double2 h00 = tile[(c0 + tq) * HT + row], h10 = tile[(c0 + tq) * HT + row + 8];
+      const double2 h01 = tile[(c0 + tq + 4) * HT + row], h11 = tile[(c0 + tq + 4) * HT + row + 8];
+      const double are[8] = {h00.x, h10.x, h01.x, h11.x, -h00.y, -h10.y, -h01.y, -h11.y};
+      const double aim[8] = {h00.x, h10.x, h01.x, h11.x, h00.y, h10.y, h01.y, h11.y};
+#pragma unroll
+      for (int v = 0; v < MV; ++v) {
+        const double2 x0 = xs[(c0 + tq) * XS + v * 8 + gq], x1 = xs[(c0 + tq + 4) * XS + v * 8 + gq];
+        mma16(accr[v], are, x0.x, x1.x, x0.y, x1.y);
+        mma16(acci[v], aim, x0.y, x1.y, x0.x, x1.x);
       }
     }
   }
-#pragma unroll
-  for (int a = 0; a < 2; ++a) {
-    const long long rr = R0 + r + 32 * a;
-    if (rr >= N) continue;
+  // add the two column halves through shared memory, then store the partial
+  __syncthreads();
+  double2* red = tile;   // [64 rows][M] of the kh = 1 warps
+  if (kh == 1) {
 #pragma unroll
     for (int v = 0; v < MV; ++v)
-      Yp[((long long)blockIdx.y * M + vg * MV + v) * N + rr] = acc[a][v];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int rr = rg * 16 + gq + ((k >> 1) ? 8 : 0), cc = v * 8 + 2 * tq + (k & 1);
+        red[rr * M + cc] = make_double2(accr[v][k], acci[v][k]);
+      }
+  }
+  __syncthreads();
+  if (kh == 0) {
+#pragma unroll
+    for (int v = 0; v < MV; ++v)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int rr = rg * 16 + gq + ((k >> 1) ? 8 : 0), cc = v * 8 + 2 * tq + (k & 1);
+        const long long gr = R0 + rr;
+        if (gr < N) {
+          const double2 o = red[rr * M + cc];
+          Yp[((long long)blockIdx.y * M + cc) * N + gr] = make_double2(accr[v][k] + o.x, acci[v][k] + o.y);
+        }
+      }
   }
 }
 
@@ -851,7 +887,7 @@ static int hemm(wtbg_ctx* ctx, const double2* X, int ldx, int m, double2* Y, int
   const long long N = ctx->N;
   const int nblk = (int)((N + TB - 1) / TB);
   dim3 grid(nblk, JCH);
-  const size_t sm = sizeof(double2) * TB * (TB + 1) + sizeof(double2) * TB * (m + 1);
+  const size_t sm = sizeof(double2) * TB * HT + sizeof(double2) * TB * (m + 2);
   switch (m / 8) {
 #define WTBG_HEMM_CASE(MV)                                                                       \
   case MV:                                                                                       \
