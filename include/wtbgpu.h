@@ -296,6 +296,17 @@ int wtbg_bse_build_q(wtbg_ctx* ctx, int nk, const double* kptq, const double* q4
 int wtbg_bse_q_eigenvalues(wtbg_ctx* ctx, int nk, const double* kptq, const double* q4,
                            const wtbg_coulomb* p, double* W);
 
+/* ---- Berry curvature (berryct2, berry_curvature_subs.f90:1-128, as berrycurv and
+ *      berrycurvbz call it: berry_curvature_kpath-tool.f90, berry_curvature_bz-tool.f90):
+ *      eigsys of every band at each k (scissors on the states above E_F), the velocity
+ *      matrices dH/dk of hlm (optics.f90:1-97), and
+ *        b_ab(k) = sum_{n <= nocp < i} -2 <n|h_a|i> conj(<n|h_b|i>) / ((E_n - E_i)^2 + gamma^2),
+ *      pairs with |E_i - E_n| < degtol skipped.  The tools use gamma = 0.001 and degtol =
+ *      0.0001, both single-precision literals (pass (double)0.001f, (double)0.0001f).
+ *      kpt (nk,3); out (nk,6) = Im of b_xx, b_xy, b_xz, b_yy, b_yz, b_zz.  Leaves the BSE state
+ *      of the context alone. */
+int wtbg_berry(wtbg_ctx* ctx, int nk, const double* kpt, double gamma, double degtol, double* out);
+
 /* ---- precision form (mode 1): the Fourier sums H(k) = sum_R e^{ik.R} H(R)/deg(R) of the band
  *      stage (hamiltonian_tb.f90:73-77) and the band overlaps <c|c'>, <v|v'> of the BSE kernel
  *      build (bse_subs.f90:2-124) run as 3-term split-BF16 GEMMs on the tensor cores with FP32

@@ -802,6 +802,56 @@ def bandstool(model, ks, npts, orbw=None, dft="V"):
     return out, labels
 
 
+# berry tools: "double precision,parameter :: gammas= 0.001" and the degeneracy cut 0.0001
+# are default-real (single-precision) literals
+BERRY_GAMMA = float(np.float32(0.001))
+BERRY_DEGTOL = float(np.float32(0.0001))
+BERRY_PAIRS = [(0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2)]
+
+
+def berryct2(model, k, e, U, nocp, gamma=BERRY_GAMMA, degtol=BERRY_DEGTOL):
+    """berry_curvature_subs.f90:1-128: b_ab = sum over n <= nocp < i of
+    -2 v_a(n,i) conj(v_b(n,i)) / ((E_n - E_i)^2 + gamma^2) with v_a(n,i) = conj(u_n).(h_a u_i)
+    (vecconjg, matvec, prodintsq) and h_a from hlm; pairs with |E_i - E_n| < degtol give 0.
+    berryct2 passes hlm a kz it never sets; the k-point's own kz is used (2D models have
+    R_z = 0). Returns the complex [bxx, bxy, bxz, byy, byz, bzz], summed n outer, i inner."""
+    hs = hlm(model, k)
+    w = model.w
+    b = np.zeros(6, dtype=np.complex128)
+    for n in range(nocp):
+        vn = np.conj(U[n])
+        for i in range(nocp, w):
+            v = [np.sum(vn * (h @ U[i])) for h in hs]
+            if abs(e[i] - e[n]) < degtol:
+                continue
+            aux = (e[n] - e[i]) ** 2 + gamma ** 2
+            for c, (a, bb) in enumerate(BERRY_PAIRS):
+                b[c] += -2.0 * ((v[a] * np.conj(v[bb])) / aux)
+    return b
+
+
+def berry_bz(model, ngrid, mshift):
+    """berry_curvature_bz-tool.f90: rows (real(4) kx, ky, kz, Im b_yz, Im b_xz, Im b_xy)."""
+    kpts = monkhorst_pack(ngrid[0], ngrid[1], ngrid[2], mshift, model.rlat)
+    rows = []
+    for k in kpts:
+        e, U, nocp = eigsys(model, k)
+        b = berryct2(model, k, e, U, nocp)
+        rows.append([f32(k[0]), f32(k[1]), f32(k[2]), b[4].imag, b[2].imag, b[1].imag])
+    return np.array(rows)
+
+
+def berry_kpath(model, ks, npts):
+    """berry_curvature_kpath-tool.f90: rows (distance, Im b_yz, Im b_xz, Im b_xy) along kpath2."""
+    kp, labels = kpathbse(model.rlat, ks, npts)
+    rows = []
+    for j in range(kp.shape[0]):
+        e, U, nocp = eigsys(model, kp[j, 1:])
+        b = berryct2(model, kp[j, 1:], e, U, nocp)
+        rows.append([kp[j, 0], b[4].imag, b[2].imag, b[1].imag])
+    return np.array(rows), labels
+
+
 def dostool(model, ngrid, mshift, numdos, sme, orbw=None, dft="V"):
     """tdos-tool.f90: the dos.dat columns (energy, tdos, sumdos, [updos, -dndos,] awdos)."""
     kpts = monkhorst_pack(ngrid[0], ngrid[1], ngrid[2], mshift, model.rlat)

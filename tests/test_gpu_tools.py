@@ -1,6 +1,7 @@
 """Tools that share the per-k eigensolver (the next rows after the BSE path): eigsys for every
-band, the DOS smearing kernel, and the deck-level band-structure (BANDS=T) and DOS (DOS=T)
-runs against the CPU oracle."""
+band, the DOS smearing kernel, the Berry curvature (berryct2), and the deck-level
+band-structure (BANDS=T), DOS (DOS=T) and Berry-curvature (BERRY=T, BERRY_BZ=T) runs against
+the CPU oracle."""
 import copy
 import subprocess
 
@@ -36,6 +37,63 @@ def test_dos_kernel_matches_numpy(gpu_ctx):
     got = gpu_ctx.dos(etb, wts, 250, en, 0.05)
     want = (O.gaussian(en[:, None] - etb[None, :], 0.05) @ wts) / 250.0
     assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+
+
+def test_berry_curvature_matches_oracle(gpu_ctx):
+    """wtbg_berry (berryct2 on the device) against the oracle restatement, c1 and QWZ models."""
+    cases = [(synth.config_model("c1"), 4), (synth.qwz_model(-1.0), 6)]
+    for m, n in cases:
+        kp = O.monkhorst_pack(n, n, 1, [0, 0, 0], m.rlat) + np.array([0.013, -0.021, 0.0])
+        gpu_ctx.set_model(m)
+        got = gpu_ctx.berry(kp)
+        want = np.array([[x.imag for x in O.berryct2(m, k, *O.eigsys(m, k))] for k in kp])
+        assert np.abs(got - want).max() <= 1e-9 * max(1.0, np.abs(want).max())
+
+
+def test_berry_curvature_chern_numbers_on_device(gpu_ctx):
+    """Known answer: the QWZ lower band has Chern number +1, -1, 0 for u = -1, +1, -3."""
+    for u, chern in ((-1.0, 1.0), (1.0, -1.0), (-3.0, 0.0)):
+        m = synth.qwz_model(u)
+        gpu_ctx.set_model(m)
+        kp = O.monkhorst_pack(48, 48, 1, [0, 0, 0], m.rlat)
+        b = gpu_ctx.berry(kp)
+        b1, b2, _ = O.recvec(m.rlat[0], m.rlat[1], m.rlat[2])
+        area = abs(np.cross(b1, b2)[2])
+        assert abs(b[:, 1].sum() * area / len(kp) / (2 * np.pi) - chern) < 1e-4
+        assert np.abs(b[:, [0, 3, 5]]).max() < 1e-12   # diagonal components are real
+
+
+def test_berry_tool_runs_match_oracle(tmp_path):
+    """BERRY=T (berry_curv_kpath.dat, KLABELS.dat) and BERRY_BZ=T (berry_curv_bz.dat) decks."""
+    m = synth.config_model("c1")
+    synth.write_params(m, str(tmp_path / "tb.dat"))
+    ks = [(0, 0, 0), (0.5, 0, 0), (0.5, 0, 0), (1 / 3, 1 / 3, 0)]
+    (tmp_path / "kpath.dat").write_text("4\n6\n" + "\n".join(f"{a:.10f} {b:.10f} {c:.10f}" for a, b, c in ks) + "\n")
+    text = f"""BERRY= T
+BERRY_BZ= T
+NGX= 5
+NGY= 5
+NGZ= 1
+OUTPUT= "{tmp_path}/"
+CALC_DATA= "{tmp_path}/"
+PARAMS_FILE= "{tmp_path}/tb.dat"
+KPATH_FILE= "{tmp_path}/kpath.dat"
+"""
+    _run(tmp_path, text)
+    kin = [tuple(float(x) for x in l.split()) for l in (tmp_path / "kpath.dat").read_text().splitlines()[2:]]
+    want, labels = O.berry_kpath(m, kin, 6)
+    lines = (tmp_path / "berry_curv_kpath.dat").read_text().splitlines()
+    assert lines[0].split() == ["kp", "yz", "xz", "xy"]
+    got = np.array([[float(x) for x in l.split()] for l in lines[1:]])
+    assert got.shape == want.shape
+    assert np.abs(got - np.round(want, 4)).max() <= 1.0001e-4
+    assert np.allclose(_floats(tmp_path / "KLABELS.dat").ravel(), np.array(labels, dtype=np.float32), rtol=1e-6)
+    wb = O.berry_bz(m, [5, 5, 1], [0, 0, 0])
+    lines = (tmp_path / "berry_curv_bz.dat").read_text().splitlines()
+    assert lines[0].split() == ["kx", "ky", "kz", "yz", "xz", "xy"]
+    gb = np.array([[float(x) for x in l.split()] for l in lines[1:]])
+    assert gb.shape == wb.shape
+    assert np.abs(gb - np.round(wb, 4)).max() <= 1.0001e-4
 
 
 def _run(tmp_path, text):

@@ -201,3 +201,19 @@ def test_temperature_oracle_reduces_to_plain_at_unit_occupation():
     assert np.allclose(O.dielbseptemp(A, h[:, 0], h[:, 1], np.ones(h.shape[0])), O.dielbsep(A, h[:, 0], h[:, 1]))
     assert abs(O.gapcortemp(2.0, 0.02, 300.0) - (-2.0 * 0.02 * (1.0 / np.tanh(0.02 / (2 * O.KB_F32 * 300.0)) - 1.0))) < 1e-15
     assert O.gapcortemp2(1.0, 300.0, 300.0) == -(2.0 / (np.exp(1.0) - 1.0))
+
+
+def test_berry_oracle_gives_qwz_chern_numbers():
+    """Known answer for the Berry curvature restatement (berryct2): the lower band of the
+    Qi-Wu-Zhang model integrates to Chern number +1 (u = -1), -1 (u = +1) and 0 (u = -3)."""
+    for u, chern in ((-1.0, 1.0), (1.0, -1.0), (-3.0, 0.0)):
+        m = synth.qwz_model(u)
+        kp = O.monkhorst_pack(24, 24, 1, [0, 0, 0], m.rlat)
+        s = 0.0
+        for k in kp:
+            e, U, nocp = O.eigsys(m, k)
+            assert nocp == 1
+            s += O.berryct2(m, k, e, U, nocp)[1].imag
+        b1, b2, _ = O.recvec(m.rlat[0], m.rlat[1], m.rlat[2])
+        area = abs(np.cross(b1, b2)[2])
+        assert abs(s * area / len(kp) / (2 * np.pi) - chern) < 1e-4

@@ -395,6 +395,123 @@ __global__ void __launch_bounds__(kBandsThreads) k_velocity(VelArgs a) {
 }
 
 // ---------------------------------------------------------------------------------------
+// Berry curvature per k (berryct2, berry_curvature_subs.f90:1-128):
+//   b_ab = sum_{n <= nocp < i} -2 v_a(n,i) conj(v_b(n,i)) / ((E_n - E_i)^2 + gamma^2),
+//   v_a(n,i) = <n| dH/dk_a |i>  (hlm, optics.f90:1-97, as in k_velocity),
+// pairs with |E_i - E_n| < degtol skipped. One CTA per k; the three dH/dk matrices are built
+// in shared memory and overwritten by T_a = dH/dk_a U (unoccupied columns); the pair sums are
+// reduced over the block. out[c * nk + k] = Im b_c, c = xx, xy, xz, yy, yz, zz.
+struct BerryArgs {
+  const double2* HR;
+  const double* Rcart;
+  const double* Rf32;
+  const double* invdeg;
+  const int* isR0;
+  int nvec, w, nk;
+  const double* kpt;
+  const double* eig;    // [nk][w]
+  const double2* U;     // [nk][w][w], band-major
+  const int* nocp;      // [nk]
+  double gamma2, degtol;
+  double* out;          // [6][nk]
+};
+
+__global__ void __launch_bounds__(kBandsThreads) k_berry(BerryArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int w = a.w, nvec = a.nvec, tid = threadIdx.x, bs = blockDim.x;
+  const int ww = w * w;
+  double2* ph = reinterpret_cast<double2*>(smem);
+  double2* HX = ph + nvec;      // 3 matrices, column-major; then T_a
+  double2* Us = HX + 3 * ww;    // U[band][m]
+  double2* tmp = Us + ww;       // one T_a before it replaces dH/dk_a
+  __shared__ double red[kBandsThreads / 32][12];
+  for (int k = blockIdx.x; k < a.nk; k += gridDim.x) {
+    const double kx = a.kpt[3 * k], ky = a.kpt[3 * k + 1], kz = a.kpt[3 * k + 2];
+    const int nocp = a.nocp[k];
+    for (int R = tid; R < nvec; R += bs) ph[R] = phase_of(kx, ky, kz, a.Rcart + 3 * R);
+    for (int it = tid; it < ww; it += bs) Us[it] = a.U[(size_t)k * ww + it];
+    __syncthreads();
+    for (int el = tid; el < ww; el += bs) {
+      const int m = el % w, n = el / w;
+      double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+      const double2* hp = a.HR + el;
+      for (int R = 0; R < nvec; ++R) {
+        if (m == n && a.isR0[R]) continue;   // R=0 diagonal zeroed (optics.f90:59-68)
+        const double2 hr = hp[(size_t)R * ww];
+        const double2 p = ph[R];
+        const double inv = a.invdeg[R];
+#pragma unroll
+        for (int al = 0; al < 3; ++al) {
+          const double ra = a.Rf32[3 * R + al];
+          const double2 pre = make_double2(-ra * p.y, ra * p.x);   // (i*R_alpha) * phase
+          acc[al] = cadd(acc[al], cscale(cmul(pre, hr), inv));
+        }
+      }
+      HX[el] = acc[0];
+      HX[ww + el] = acc[1];
+      HX[2 * ww + el] = acc[2];
+    }
+    __syncthreads();
+    // T_a[m][i] = sum_l H_a[m][l] u_i[l] for the unoccupied bands i (matvec, general_subs.f90:132-160)
+    for (int al = 0; al < 3; ++al) {
+      double2* Ha = HX + al * ww;
+      for (int it = tid; it < w * (w - nocp); it += bs) {
+        const int m = it % w, i = nocp + it / w;
+        const double2* ui = Us + i * w;
+        double2 acc = make_double2(0, 0);
+        for (int l = 0; l < w; ++l) acc = cadd(acc, cmul(Ha[m + l * w], ui[l]));
+        tmp[m + i * w] = acc;
+      }
+      __syncthreads();
+      for (int it = tid; it < w * (w - nocp); it += bs) {
+        const int m = it % w, i = nocp + it / w;
+        Ha[m + i * w] = tmp[m + i * w];
+      }
+      __syncthreads();
+    }
+    double2 b[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) b[c] = make_double2(0, 0);
+    const int nun = w - nocp;
+    for (int it = tid; it < nocp * nun; it += bs) {
+      const int n = it / nun, i = nocp + it % nun;
+      const double en = a.eig[(size_t)k * w + n], ei = a.eig[(size_t)k * w + i];
+      if (fabs(ei - en) < a.degtol) continue;
+      const double2* un = Us + n * w;
+      double2 v[3];
+#pragma unroll
+      for (int al = 0; al < 3; ++al) {
+        const double2* t = HX + al * ww + i * w;
+        double2 acc = make_double2(0, 0);
+        for (int m = 0; m < w; ++m) acc = cadd(acc, cmulc(un[m], t[m]));   // prodintsq(conj(u_n), T u_i)
+        v[al] = acc;
+      }
+      const double aux = (en - ei) * (en - ei) + a.gamma2;
+      const int pa[6] = {0, 0, 0, 1, 1, 2}, pb[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        const double2 pr = cmul(v[pa[c]], cconj(v[pb[c]]));
+        b[c] = cadd(b[c], make_double2(-2.0 * (pr.x / aux), -2.0 * (pr.y / aux)));
+      }
+    }
+    // block reduction of the six sums (only the imaginary parts are kept)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      double x = b[c].y;
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      if ((tid & 31) == 0) red[tid >> 5][c] = x;
+    }
+    __syncthreads();
+    if (tid < 6) {
+      double s = 0.0;
+      for (int q = 0; q < bs / 32; ++q) s += red[q][tid];
+      a.out[(size_t)tid * a.nk + k] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // vecres rows (bse_solver-tool-diel.f90:379-393); key = column 7 (float32 dE)
 __global__ void k_sp_rows(const double* kpt, const double* eig, const int* nocp, const double2* h, const double* fdeh,
                           int nk, int nv, int nc, long long N, float* rows, float* key, int* idx) {
@@ -673,5 +790,33 @@ int launch_sp_table(wtbg_ctx* ctx, float* d_out) {
   CK(cub::DeviceRadixSort::SortPairs(ctmp, cub_bytes, kin, kout, iin, iout, (int)N, 0, 32, ctx->stream));
   k_sp_gather<<<gr, th, 0, ctx->stream>>>(rows, iout, N, d_out); WTBG_COUNT(ctx, 1);
   CKL("k_sp_gather");
+  return 0;
+}
+
+// Berry curvature of every k (berrycurv / berrycurvbz): eigsys of all bands, then k_berry
+int launch_berry(wtbg_ctx* ctx, int nk, const double* d_kpt, const double* d_eig, const double2* d_U, const int* d_nocp,
+                 double gamma, double degtol, double* d_out) {
+  const int w = ctx->w, nvec = ctx->nvec;
+  BerryArgs a;
+  a.HR = ctx->HR.as<double2>();
+  a.Rcart = ctx->Rcart.as<double>();
+  a.Rf32 = ctx->Rf32.as<double>();
+  a.invdeg = ctx->invdeg.as<double>();
+  a.isR0 = ctx->isR0.as<int>();
+  a.nvec = nvec;
+  a.w = w;
+  a.nk = nk;
+  a.kpt = d_kpt;
+  a.eig = d_eig;
+  a.U = d_U;
+  a.nocp = d_nocp;
+  a.gamma2 = gamma * gamma;
+  a.degtol = degtol;
+  a.out = d_out;
+  const size_t smem = sizeof(double2) * ((size_t)nvec + 5 * (size_t)w * w);
+  if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "berry: model too large for shared memory");
+  CK(cudaFuncSetAttribute(k_berry, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_berry<<<nk, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
+  CKL("k_berry");
   return 0;
 }

@@ -203,6 +203,8 @@ inline int set_device(wtbg_ctx* ctx) {
 int launch_bands_batch(wtbg_ctx* const* ctxs, int nmod);
 int launch_eigsys_all(wtbg_ctx* ctx, int nk, const double* d_kpt, double* d_eig, double2* d_U, int* d_nocp,
                       int* d_kstat);
+int launch_berry(wtbg_ctx* ctx, int nk, const double* d_kpt, const double* d_eig, const double2* d_U, const int* d_nocp,
+                 double gamma, double degtol, double* d_out);
 int launch_dos(wtbg_ctx* ctx, const double* d_etb, const double* d_w, long long ndim, int ncol, const double* d_en,
                int nw, double sme, long long nkpt, double* d_out);
 int autotune_hemv(wtbg_ctx* ctx, int* hs_out);

@@ -978,12 +978,12 @@ int spin_of(const std::string& systype, const std::string& dft, int i, int w) {
 
 // bandstool (bands-kpath-tool.f90): eigsys along the k path of KPATH_FILE=; bands.dat with
 // (k distance, E, <Sz>, layer weight) per band, KLABELS.dat from kpath2 (mhkpack_subs.f90:54-130)
-void bandstool(wtbg_ctx* ctx, const Deck& d, const Model& m) {
+// kpath2 (mhkpack_subs.f90:54-130) on the path of KPATH_FILE=: distances kp (nk) and
+// Cartesian points kc (nk,3), KLABELS.dat written to the output folder
+void kpath_points(const Deck& d, const Model& m, std::vector<double>& kp, std::vector<double>& kc) {
   const std::string of = d.outputfolder;
   std::ifstream kf(d.kpaths);
   if (!kf) throw Stop("Error opening kpath input file");
-  Out f300(join_path(of, "bands.dat"), "Error opening bands output file");
-  upload_model(ctx, m);
   std::vector<std::string> kl;
   {
     std::string l;
@@ -999,7 +999,6 @@ void bandstool(wtbg_ctx* ctx, const Deck& d, const Model& m) {
     auto t = items_of(kl[2 + i]);
     for (int c = 0; c < 3; ++c) ks[i][c] = num(t[c]);
   }
-  const std::vector<double> ow = orbital_weights(d, m.w);
   double b[3][3];
   recvec(m.rlat, b);
   std::vector<std::array<double, 3>> kx(nks);
@@ -1016,22 +1015,32 @@ void bandstool(wtbg_ctx* ctx, const Deck& d, const Model& m) {
   }
   for (auto& v : kdis) v = v / tot;
   const int nk = half * npts;
-  std::vector<double> kp(nk), kc(3 * (size_t)nk);
-  {
-    Out kl_out(join_path(of, "KLABELS.dat"), "Error opening KLABELS output file");
-    double acc = 0.0;
-    kl_out.line(LS(0.0f));
-    for (int j = 0; j < half; ++j) {
-      for (int i = 0; i < npts; ++i) {
-        const double t = (double)((float)i / (float)(npts - 1));
-        const size_t r = (size_t)j * npts + i;
-        kp[r] = acc + kdis[j] * t;
-        for (int c = 0; c < 3; ++c) kc[r + (size_t)nk * c] = kx[2 * j][c] + (kx[2 * j + 1][c] - kx[2 * j][c]) * t;
-      }
-      acc += kdis[j];
-      kl_out.line(LS((float)acc));
+  kp.assign(nk, 0.0);
+  kc.assign(3 * (size_t)nk, 0.0);
+  Out kl_out(join_path(of, "KLABELS.dat"), "Error opening KLABELS output file");
+  double acc = 0.0;
+  kl_out.line(LS(0.0f));
+  for (int j = 0; j < half; ++j) {
+    for (int i = 0; i < npts; ++i) {
+      const double t = (double)((float)i / (float)(npts - 1));
+      const size_t r = (size_t)j * npts + i;
+      kp[r] = acc + kdis[j] * t;
+      for (int c = 0; c < 3; ++c) kc[r + (size_t)nk * c] = kx[2 * j][c] + (kx[2 * j + 1][c] - kx[2 * j][c]) * t;
     }
+    acc += kdis[j];
+    kl_out.line(LS((float)acc));
   }
+}
+
+void bandstool(wtbg_ctx* ctx, const Deck& d, const Model& m) {
+  const std::string of = d.outputfolder;
+  if (!std::ifstream(d.kpaths)) throw Stop("Error opening kpath input file");
+  Out f300(join_path(of, "bands.dat"), "Error opening bands output file");
+  upload_model(ctx, m);
+  const std::vector<double> ow = orbital_weights(d, m.w);
+  std::vector<double> kp, kc;
+  kpath_points(d, m, kp, kc);
+  const int nk = (int)kp.size();
   const int w = m.w;
   std::vector<double> e((size_t)nk * w), vec((size_t)nk * w * w * 2);
   gpu_check(ctx, wtbg_eigsys(ctx, nk, kc.data(), e.data(), vec.data(), nullptr), "wtbg_eigsys");
@@ -1054,6 +1063,48 @@ void bandstool(wtbg_ctx* ctx, const Deck& d, const Model& m) {
              "\n";
     }
     buf += "\n";
+  }
+  fputs(buf.c_str(), f300.f);
+}
+
+// Berry curvature tools. berryct2 (berry_curvature_subs.f90:1-128) runs on the device
+// (wtbg_berry) with the tools' constants gammas = 0.001 and the degeneracy cut 0.0001, both
+// single-precision literals. berryct2 hands hlm a kz it never sets; the k-point's own kz is
+// used here (every 2D model has R_z = 0, where kz drops out of the phases).
+constexpr double kBerryGamma = (double)0.001f, kBerryDegTol = (double)0.0001f;
+
+// berrycurv (berry_curvature_kpath-tool.f90): berry_curv_kpath.dat, rows (kp, yz, xz, xy)
+void berrytool_kpath(wtbg_ctx* ctx, const Deck& d, const Model& m) {
+  const std::string of = d.outputfolder;
+  if (!std::ifstream(d.kpaths)) throw Stop("Error opening kpath input file");
+  Out f300(join_path(of, "berry_curv_kpath.dat"), "Error opening berry_curv_kpath output file");
+  upload_model(ctx, m);
+  std::vector<double> kp, kc;
+  kpath_points(d, m, kp, kc);
+  const int nk = (int)kp.size();
+  std::vector<double> b((size_t)nk * 6);
+  gpu_check(ctx, wtbg_berry(ctx, nk, kc.data(), kBerryGamma, kBerryDegTol, b.data()), "wtbg_berry");
+  std::string buf = " kp yz xz xy\n";
+  for (int k = 0; k < nk; ++k)
+    buf += F(kp[k], 15, 4) + F(b[k + (size_t)nk * 4], 15, 4) + F(b[k + (size_t)nk * 2], 15, 4) +
+           F(b[k + (size_t)nk * 1], 15, 4) + "\n";
+  fputs(buf.c_str(), f300.f);
+}
+
+// berrycurvbz (berry_curvature_bz-tool.f90): berry_curv_bz.dat on the Monkhorst-Pack mesh,
+// rows (real(4) kx, ky, kz, yz, xz, xy)
+void berrytool_bz(wtbg_ctx* ctx, const Deck& d, const Model& m) {
+  const std::string of = d.outputfolder;
+  Out f300(join_path(of, "berry_curv_bz.dat"), "Error opening berry_curv_bz output file");
+  upload_model(ctx, m);
+  const int nk = d.ngrid[0] * d.ngrid[1] * d.ngrid[2];
+  std::vector<double> kpt = kmesh(d.ngrid, d.mshift, m.rlat, nullptr);
+  std::vector<double> b((size_t)nk * 6);
+  gpu_check(ctx, wtbg_berry(ctx, nk, kpt.data(), kBerryGamma, kBerryDegTol, b.data()), "wtbg_berry");
+  std::string buf = " kx ky kz yz xz xy\n";
+  for (int k = 0; k < nk; ++k) {
+    for (int c = 0; c < 3; ++c) buf += F((double)(float)kpt[k + (size_t)nk * c], 15, 4);
+    buf += F(b[k + (size_t)nk * 4], 15, 4) + F(b[k + (size_t)nk * 2], 15, 4) + F(b[k + (size_t)nk * 1], 15, 4) + "\n";
   }
   fputs(buf.c_str(), f300.f);
 }
@@ -1312,7 +1363,8 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
     Deck d = parse_deck(deck_text ? deck_text : "");
     // params header + mesh (wtb_main.f90:77-104)
     Model m;
-    if (d.bse || d.bset || d.bsekpath || d.bsetbnd || d.spec || d.spdiel || d.bandscalc || d.doscalc)
+    if (d.bse || d.bset || d.bsekpath || d.bsetbnd || d.spec || d.spdiel || d.bandscalc || d.doscalc || d.berryk ||
+        d.berrybz)
       m = read_params(d.params);
     if (d.meshtype.rfind("RK3D", 0) == 0) rkmesh(d.rk, m.rlat, d.ngrid, false);
     else if (d.meshtype.rfind("RK2D", 0) == 0) rkmesh(d.rk, m.rlat, d.ngrid, true);
@@ -1360,6 +1412,17 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
       } else if (d.bsetbnd) {
         bsebnds(ctx, d, m);
         log.line(" BSE exciton band structure, with temperature, finished");
+        log.flush();
+      }
+      // wtb_main.f90:232-251
+      if (d.berryk) {
+        berrytool_kpath(ctx, d, m);
+        log.line(" Berry curvature in kpath finished");
+        log.flush();
+      }
+      if (d.berrybz) {
+        berrytool_bz(ctx, d, m);
+        log.line(" Berry curvature in BZ finished");
         log.flush();
       }
     }

@@ -138,6 +138,26 @@ def _bands_on_mesh(model: TBModel, n: int) -> np.ndarray:
     return np.array(ev)
 
 
+def qwz_model(u: float = -1.0, a: float = 1.0) -> TBModel:
+    """Qi-Wu-Zhang two-band Chern insulator on a square lattice (lattice constant a):
+    H(k) = sin(k_x a) sx + sin(k_y a) sy + (u + cos(k_x a) + cos(k_y a)) sz, i.e. H(0) = u sz,
+    H(+x) = (sz - i sx)/2, H(+y) = (sz - i sy)/2 and H(-R) = H(R)^dagger. The lower band has
+    Chern number +-1 for 0 < |u| < 2 and 0 for |u| > 2 (a known-answer model for the Berry
+    curvature; E_F = 0 lies in the gap)."""
+    sx = np.array([[0, 1], [1, 0]], dtype=np.complex128)
+    sy = np.array([[0, -1j], [1j, 0]], dtype=np.complex128)
+    sz = np.array([[1, 0], [0, -1]], dtype=np.complex128)
+    hx = 0.5 * sz - 0.5j * sx
+    hy = 0.5 * sz - 0.5j * sy
+    cells = [((0, 0, 0), u * sz), ((1, 0, 0), hx), ((-1, 0, 0), hx.conj().T),
+             ((0, 1, 0), hy), ((0, -1, 0), hy.conj().T)]
+    rvec = np.array([c[0] for c in cells], dtype=np.int32)
+    H = np.array([c[1] for c in cells])
+    return TBModel(systype="NP", scs=0.0, efermi=0.0,
+                   rlat=np.array([[a, 0.0, 0.0], [0.0, a, 0.0], [0.0, 0.0, 20.0]]), w=2, rvec=rvec,
+                   deg=np.ones(len(cells), dtype=np.int32), hre=H.real.copy(), him=H.imag.copy())
+
+
 def make_gapped_model(w: int, n_shell: int, onsite_lo: tuple, onsite_hi: tuple,
                       seed: int, check_mesh: int = 12, max_tries: int = 64) -> TBModel:
     """Re-seed (seed, seed+1, ...) until nocp = w/2 at every k of the check mesh and the gap > 0."""

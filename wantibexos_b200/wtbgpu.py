@@ -29,7 +29,7 @@ EXPORTS = ["wtbg_create", "wtbg_destroy", "wtbg_error_string", "wtbg_last_error"
            "wtbg_net_features", "wtbg_net_add_sample", "wtbg_net_num_samples", "wtbg_net_train",
            "wtbg_net_eval_loss", "wtbg_net_predict", "wtbg_net_loss_grad", "wtbg_gemm_bf16",
            "wtbg_bse_build_q", "wtbg_set_temperature", "wtbg_eigsys", "wtbg_dos",
-           "wtbg_bands_batch", "wtbg_bse_q_batch", "wtbg_set_precision"]
+           "wtbg_bands_batch", "wtbg_bse_q_batch", "wtbg_set_precision", "wtbg_berry"]
 
 
 class WtbgError(RuntimeError):
@@ -96,6 +96,7 @@ def load_library(path: str = LIB_PATH):
                                              dp, fp]),
         "wtbg_set_fast_product": (C.c_int, [P, C.c_int]),
         "wtbg_set_precision": (C.c_int, [P, C.c_int]),
+        "wtbg_berry": (C.c_int, [P, C.c_int, dp, C.c_double, C.c_double, dp]),
         "wtbg_net_create": (C.c_int, [P, C.POINTER(P), C.c_ulonglong]),
         "wtbg_net_destroy": (C.c_int, [P]),
         "wtbg_net_num_params": (C.c_longlong, []),
@@ -362,6 +363,13 @@ class Context:
                                            float(ebse0), float(ebsef), float(numbse), float(sme),
                                            int(bool(renorm)), float(spinf), _dp(om), _fp(eps)))
         return om, eps
+
+    def berry(self, kpt, gamma=float(np.float32(0.001)), degtol=float(np.float32(0.0001))):
+        """Berry curvature (berryct2) at each k: (nk, 6) = Im of b_xx, b_xy, b_xz, b_yy, b_yz, b_zz."""
+        k = _f64(kpt)
+        out = np.zeros((k.shape[0], 6), order="F")
+        self._check(self.lib.wtbg_berry(self.h, k.shape[0], _dp(k), float(gamma), float(degtol), _dp(out)))
+        return out
 
     def set_precision(self, mode: int) -> None:
         """0: FP64 form; 1: precision form (Fourier sums and band overlaps as 3-term split-BF16
