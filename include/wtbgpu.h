@@ -307,6 +307,15 @@ int wtbg_bse_q_eigenvalues(wtbg_ctx* ctx, int nk, const double* kptq, const doub
  *      of the context alone. */
 int wtbg_berry(wtbg_ctx* ctx, int nk, const double* kpt, double gamma, double degtol, double* out);
 
+/* ---- single-particle optical activity over the BZ (spoptpolbz, sp_opt_bz-tool.f90:81-175):
+ *      eigsys of every band at each k, then over the band pairs of the BSE window
+ *      (c = nocp_k+1 .. nocp_k+nc outer, v = nocp_k-nv+1 .. nocp of the FIRST k-point inner, the
+ *      first nc*nv pairs) the sums of |h_a|^2 with h_a = <c|dH/dk_a|v> / (E_c - E_v + i sme),
+ *      both terms of the denominator rounded to single precision as the reference's
+ *      default-kind cmplx does.  out (nk,5) = x, y, z, sigma+, sigma- (sigma-pm with
+ *      norm = f32(1/sqrt 2)).  WTBG_ERR_BANDWINDOW where a k-point has fewer than nc*nv pairs. */
+int wtbg_sp_optbz(wtbg_ctx* ctx, int nk, const double* kpt, int nv, int nc, double sme, double* out);
+
 /* ---- precision form (mode 1): the Fourier sums H(k) = sum_R e^{ik.R} H(R)/deg(R) of the band
  *      stage (hamiltonian_tb.f90:73-77) and the band overlaps <c|c'>, <v|v'> of the BSE kernel
  *      build (bse_subs.f90:2-124) run as 3-term split-BF16 GEMMs on the tensor cores with FP32

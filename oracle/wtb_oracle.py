@@ -852,6 +852,36 @@ def berry_kpath(model, ks, npts):
     return np.array(rows), labels
 
 
+def sp_optbz(model, ngrid, mshift, nv, nc, sme):
+    """sp_opt_bz-tool.f90:81-175 (spoptpolbz): per k of the mesh, over the pairs c = nocp_k+1 ..
+    nocp_k+nc (outer), v = nocp_k-nv+1 .. nocp of the FIRST k-point (inner), the first nc*nv of
+    them, h_a = optspbz / cmplx(E_c - E_v, sme) (a default-kind complex: both parts rounded to
+    single precision); rows (real(4) kx, ky, kz, sum|h_x|^2, sum|h_y|^2, sum|h_z|^2, sigma+,
+    sigma-, dichroism) with norm = f32(1/sqrt 2)."""
+    kpts = monkhorst_pack(ngrid[0], ngrid[1], ngrid[2], mshift, model.rlat)
+    norm = float(np.float32(1.0) / np.sqrt(np.float32(2.0)))
+    nocp1 = eigsys(model, kpts[0])[2]
+    rows = []
+    for k in kpts:
+        e, U, nocp = eigsys(model, k)
+        hs = hlm(model, k)
+        pairs = [(c, v) for c in range(nocp, nocp + nc) for v in range(nocp - nv, nocp1)][:nc * nv]
+        assert len(pairs) == nc * nv
+        s = np.zeros(5)
+        for c, v in pairs:
+            den = complex(f32(e[c] - e[v]), f32(sme))
+            h = [np.sum(np.conj(U[c]) * (H @ U[v])) / den for H in hs]
+            s[0] += (h[0] * np.conj(h[0])).real
+            s[1] += (h[1] * np.conj(h[1])).real
+            s[2] += (h[2] * np.conj(h[2])).real
+            p = norm * (h[0] + 1j * h[1])
+            m = norm * (h[0] - 1j * h[1])
+            s[3] += (p * np.conj(p)).real
+            s[4] += (m * np.conj(m)).real
+        rows.append([f32(k[0]), f32(k[1]), f32(k[2]), *s, (s[3] - s[4]) / (s[3] + s[4])])
+    return np.array(rows)
+
+
 def dostool(model, ngrid, mshift, numdos, sme, orbw=None, dft="V"):
     """tdos-tool.f90: the dos.dat columns (energy, tdos, sumdos, [updos, -dndos,] awdos)."""
     kpts = monkhorst_pack(ngrid[0], ngrid[1], ngrid[2], mshift, model.rlat)

@@ -96,6 +96,37 @@ KPATH_FILE= "{tmp_path}/kpath.dat"
     assert np.abs(gb - np.round(wb, 4)).max() <= 1.0001e-4
 
 
+def test_sp_optics_tools_match_oracle(tmp_path):
+    """OPT_BZ=T (bz_act_*.dat, dichroism.dat against the oracle) and DIEL=T (sp_optics files
+    identical to those of a BSE=T run on the same deck)."""
+    m = synth.config_model("c1")
+    synth.write_params(m, str(tmp_path / "tb.dat"))
+    common = f"""NGX= 5
+NGY= 5
+NGZ= 1
+NBANDSV= 2
+NBANDSC= 2
+CSHIFT= 0.05
+TMCOEF= T
+CALC_DATA= "{tmp_path}/"
+PARAMS_FILE= "{tmp_path}/tb.dat"
+"""
+    (tmp_path / "a").mkdir()
+    (tmp_path / "b").mkdir()
+    _run(tmp_path, "OPT_BZ= T\nDIEL= T\n" + common + f'OUTPUT= "{tmp_path}/a/"\n')
+    want = O.sp_optbz(m, [5, 5, 1], [0, 0, 0], 2, 2, float(np.float32(0.05)))
+    for c, name in enumerate(["x", "y", "z", "sp", "sm"]):
+        got = _floats(tmp_path / "a" / f"bz_act_{name}.dat")
+        assert got.shape == (25, 4)
+        assert np.array_equal(got[:, :3].astype(np.float32), want[:, :3].astype(np.float32))
+        assert np.allclose(got[:, 3], want[:, 3 + c], rtol=1e-10, atol=0)
+    got = _floats(tmp_path / "a" / "dichroism.dat")
+    assert np.allclose(got[:, 3], want[:, 8], rtol=1e-9, atol=1e-12)
+    _run(tmp_path, "BSE= T\n" + common + "COULOMB_POT= V2DRK\nR_0= 40\n" + f'OUTPUT= "{tmp_path}/b/"\n')
+    for f in ["sp_optics.dat", "sp_optics-pol.dat", "tm_coef.dat", "tm_coef-pol.dat"]:
+        assert (tmp_path / "a" / f).read_text() == (tmp_path / "b" / f).read_text(), f
+
+
 def _run(tmp_path, text):
     B.build()
     r = subprocess.run([B.DRIVER_EXE], input=text.encode(), capture_output=True, cwd=str(tmp_path), timeout=600)

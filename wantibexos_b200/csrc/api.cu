@@ -536,6 +536,44 @@ int wtbg_berry(wtbg_ctx* ctx, int nk, const double* kpt, double gamma, double de
   return WTBG_OK;
 }
 
+int wtbg_sp_optbz(wtbg_ctx* ctx, int nk, const double* kpt, int nv, int nc, double sme, double* out) {
+  if (!ctx || nk <= 0 || !kpt || !out || nv < 1 || nc < 1) return WTBG_ERR_ARG;
+  if (ctx->w == 0) return set_err(ctx, WTBG_ERR_STATE, "opt_bz: no model");
+  if (int r = set_device(ctx)) return r;
+  const int w = ctx->w;
+  std::vector<double> kp(3 * (size_t)nk);
+  for (int k = 0; k < nk; ++k)
+    for (int c = 0; c < 3; ++c) kp[3 * k + c] = kpt[k + (size_t)nk * c];
+  const size_t b_kpt = kp.size() * 8, b_eig = (size_t)nk * w * 8, b_int = (size_t)nk * 4, b_out = (size_t)nk * 5 * 8;
+  const size_t o_eig = (b_kpt + 255) / 256 * 256, o_int = o_eig + (b_eig + 255) / 256 * 256;
+  const size_t o_out = o_int + (2 * b_int + 255) / 256 * 256;
+  ENSURE(ctx->tmp, o_out + b_out + 256);
+  ENSURE(ctx->ws, (size_t)nk * w * w * 16);
+  char* base = ctx->tmp.as<char>();
+  double* dk = reinterpret_cast<double*>(base);
+  double* de = reinterpret_cast<double*>(base + o_eig);
+  int* dn = reinterpret_cast<int*>(base + o_int);
+  int* ds = dn + nk;
+  double* dout = reinterpret_cast<double*>(base + o_out);
+  Timer t(ctx);
+  CK(cudaMemcpyAsync(dk, kp.data(), b_kpt, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(ds, 0, b_int, ctx->stream));
+  if (int r = launch_eigsys_all(ctx, nk, dk, de, ctx->ws.as<double2>(), dn, ds)) return r;
+  if (int r = launch_optbz(ctx, nk, nv, nc, dk, de, ctx->ws.as<double2>(), dn, sme, dout, ds)) return r;
+  if (int r = t.stop()) return r;
+  std::vector<int> st(nk);
+  CK(cudaMemcpy(st.data(), ds, b_int, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < nk; ++k) {
+    if (st[k] == 1) return set_err(ctx, WTBG_ERR_NOCONV, "opt_bz: Jacobi did not converge at k-point " + std::to_string(k + 1));
+    if (st[k] == 4)
+      return set_err(ctx, WTBG_ERR_BANDWINDOW,
+                     "opt_bz: fewer than nc*nv band pairs at k-point " + std::to_string(k + 1) +
+                         " (the valence range ends at the first k-point's nocp)");
+  }
+  CK(cudaMemcpy(out, dout, b_out, cudaMemcpyDeviceToHost));
+  return WTBG_OK;
+}
+
 int wtbg_dos(wtbg_ctx* ctx, long long ndim, const double* etb, const double* weights, int ncol, long long nkpt,
              int nw, const double* en, double sme, double* out) {
   if (!ctx || ndim <= 0 || !etb || !weights || !en || !out || nw <= 0 || nkpt <= 0 || !(sme > 0))

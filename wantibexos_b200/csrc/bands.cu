@@ -401,6 +401,36 @@ __global__ void __launch_bounds__(kBandsThreads) k_velocity(VelArgs a) {
 // pairs with |E_i - E_n| < degtol skipped. One CTA per k; the three dH/dk matrices are built
 // in shared memory and overwritten by T_a = dH/dk_a U (unoccupied columns); the pair sums are
 // reduced over the block. out[c * nk + k] = Im b_c, c = xx, xy, xz, yy, yz, zz.
+// dH/dk_a of hlm (optics.f90:1-97) at one k into shared memory: HX = three column-major w x w
+// matrices, ph = the nvec phases (work area). Ends with a block barrier.
+__device__ void hlm_smem(const double2* HR, const double* Rcart, const double* Rf32, const double* invdeg,
+                         const int* isR0, int nvec, int w, double kx, double ky, double kz, double2* ph, double2* HX) {
+  const int tid = threadIdx.x, bs = blockDim.x, ww = w * w;
+  for (int R = tid; R < nvec; R += bs) ph[R] = phase_of(kx, ky, kz, Rcart + 3 * R);
+  __syncthreads();
+  for (int el = tid; el < ww; el += bs) {
+    const int m = el % w, n = el / w;
+    double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+    const double2* hp = HR + el;
+    for (int R = 0; R < nvec; ++R) {
+      if (m == n && isR0[R]) continue;   // R=0 diagonal zeroed (optics.f90:59-68)
+      const double2 hr = hp[(size_t)R * ww];
+      const double2 p = ph[R];
+      const double inv = invdeg[R];
+#pragma unroll
+      for (int al = 0; al < 3; ++al) {
+        const double ra = Rf32[3 * R + al];
+        const double2 pre = make_double2(-ra * p.y, ra * p.x);   // (i*R_alpha) * phase
+        acc[al] = cadd(acc[al], cscale(cmul(pre, hr), inv));
+      }
+    }
+    HX[el] = acc[0];
+    HX[ww + el] = acc[1];
+    HX[2 * ww + el] = acc[2];
+  }
+  __syncthreads();
+}
+
 struct BerryArgs {
   const double2* HR;
   const double* Rcart;
@@ -428,30 +458,8 @@ __global__ void __launch_bounds__(kBandsThreads) k_berry(BerryArgs a) {
   for (int k = blockIdx.x; k < a.nk; k += gridDim.x) {
     const double kx = a.kpt[3 * k], ky = a.kpt[3 * k + 1], kz = a.kpt[3 * k + 2];
     const int nocp = a.nocp[k];
-    for (int R = tid; R < nvec; R += bs) ph[R] = phase_of(kx, ky, kz, a.Rcart + 3 * R);
     for (int it = tid; it < ww; it += bs) Us[it] = a.U[(size_t)k * ww + it];
-    __syncthreads();
-    for (int el = tid; el < ww; el += bs) {
-      const int m = el % w, n = el / w;
-      double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
-      const double2* hp = a.HR + el;
-      for (int R = 0; R < nvec; ++R) {
-        if (m == n && a.isR0[R]) continue;   // R=0 diagonal zeroed (optics.f90:59-68)
-        const double2 hr = hp[(size_t)R * ww];
-        const double2 p = ph[R];
-        const double inv = a.invdeg[R];
-#pragma unroll
-        for (int al = 0; al < 3; ++al) {
-          const double ra = a.Rf32[3 * R + al];
-          const double2 pre = make_double2(-ra * p.y, ra * p.x);   // (i*R_alpha) * phase
-          acc[al] = cadd(acc[al], cscale(cmul(pre, hr), inv));
-        }
-      }
-      HX[el] = acc[0];
-      HX[ww + el] = acc[1];
-      HX[2 * ww + el] = acc[2];
-    }
-    __syncthreads();
+    hlm_smem(a.HR, a.Rcart, a.Rf32, a.invdeg, a.isR0, nvec, w, kx, ky, kz, ph, HX);
     // T_a[m][i] = sum_l H_a[m][l] u_i[l] for the unoccupied bands i (matvec, general_subs.f90:132-160)
     for (int al = 0; al < 3; ++al) {
       double2* Ha = HX + al * ww;
@@ -507,6 +515,90 @@ __global__ void __launch_bounds__(kBandsThreads) k_berry(BerryArgs a) {
       for (int q = 0; q < bs / 32; ++q) s += red[q][tid];
       a.out[(size_t)tid * a.nk + k] = s;
     }
+    __syncthreads();
+  }
+}
+
+// Single-particle optical activity over the BZ (spoptpolbz, sp_opt_bz-tool.f90:81-175): per k,
+// the pairs (c, v) with c = nocp_k .. nocp_k + nc - 1 (outer) and v = nocp_k - nv .. nocp_1 - 1
+// (inner; the reference bounds v by the FIRST k-point's nocp), the first nc * nv of them;
+// h_a = <c|dH/dk_a|v> / (f32(E_c - E_v) + i f32(sme)) (optspbz, optics.f90:246-300, divided by a
+// default-kind complex), and out[c * nk + k] = sum |h_x|^2, |h_y|^2, |h_z|^2,
+// |norm (h_x + i h_y)|^2, |norm (h_x - i h_y)|^2 with norm = f32(1/sqrt 2). kstat = 4 where
+// fewer than nc * nv pairs exist (the reference's pair table is then undefined).
+struct OptBzArgs {
+  const double2* HR;
+  const double* Rcart;
+  const double* Rf32;
+  const double* invdeg;
+  const int* isR0;
+  int nvec, w, nk, nv, nc;
+  const double* kpt;
+  const double* eig;    // [nk][w]
+  const double2* U;     // [nk][w][w]
+  const int* nocp;      // [nk]
+  double sme32, norm32;
+  double* out;          // [5][nk]
+  int* kstat;
+};
+
+__global__ void __launch_bounds__(kBandsThreads) k_optbz(OptBzArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int w = a.w, nvec = a.nvec, tid = threadIdx.x, bs = blockDim.x;
+  const int ww = w * w;
+  double2* ph = reinterpret_cast<double2*>(smem);
+  double2* HX = ph + nvec;
+  double2* Us = HX + 3 * ww;
+  __shared__ double red[kBandsThreads / 32][5];
+  const int nocp1 = a.nocp[0];
+  for (int k = blockIdx.x; k < a.nk; k += gridDim.x) {
+    const double kx = a.kpt[3 * k], ky = a.kpt[3 * k + 1], kz = a.kpt[3 * k + 2];
+    const int nocp = a.nocp[k];
+    const int vlo = nocp - a.nv, nvv = max(0, nocp1 - vlo);
+    const int npair_all = a.nc * nvv, npair = min(npair_all, a.nc * a.nv);
+    for (int it = tid; it < ww; it += bs) Us[it] = a.U[(size_t)k * ww + it];
+    hlm_smem(a.HR, a.Rcart, a.Rf32, a.invdeg, a.isR0, nvec, w, kx, ky, kz, ph, HX);
+    double s[5] = {0, 0, 0, 0, 0};
+    for (int p = tid; p < npair; p += bs) {
+      const int c = nocp + p / nvv, v = vlo + p % nvv;
+      if (c >= w || v < 0) continue;
+      const double2* uc = Us + c * w;
+      const double2* uv = Us + v * w;
+      double2 h[3];
+#pragma unroll
+      for (int al = 0; al < 3; ++al) {
+        const double2* Ha = HX + al * ww;
+        double2 acc = make_double2(0, 0);
+        for (int m = 0; m < w; ++m) {
+          double2 t = make_double2(0, 0);
+          for (int l = 0; l < w; ++l) t = cadd(t, cmul(Ha[m + l * w], uv[l]));
+          acc = cadd(acc, cmulc(uc[m], t));
+        }
+        h[al] = acc;
+      }
+      const double dr = (double)(float)(a.eig[(size_t)k * w + c] - a.eig[(size_t)k * w + v]);
+      const double den = dr * dr + a.sme32 * a.sme32;
+      const double2 sp = make_double2(h[0].x - h[1].y, h[0].y + h[1].x);   // h_x + i h_y
+      const double2 sm = make_double2(h[0].x + h[1].y, h[0].y - h[1].x);   // h_x - i h_y
+      s[0] += (h[0].x * h[0].x + h[0].y * h[0].y) / den;
+      s[1] += (h[1].x * h[1].x + h[1].y * h[1].y) / den;
+      s[2] += (h[2].x * h[2].x + h[2].y * h[2].y) / den;
+      s[3] += a.norm32 * a.norm32 * (sp.x * sp.x + sp.y * sp.y) / den;
+      s[4] += a.norm32 * a.norm32 * (sm.x * sm.x + sm.y * sm.y) / den;
+    }
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      double x = s[c];
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      if ((tid & 31) == 0) red[tid >> 5][c] = x;
+    }
+    __syncthreads();
+    if (tid < 5) {
+      double t = 0.0;
+      for (int q = 0; q < bs / 32; ++q) t += red[q][tid];
+      a.out[(size_t)tid * a.nk + k] = t;
+    }
+    if (tid == 0 && npair_all < a.nc * a.nv) a.kstat[k] = 4;
     __syncthreads();
   }
 }
@@ -818,5 +910,36 @@ int launch_berry(wtbg_ctx* ctx, int nk, const double* d_kpt, const double* d_eig
   CK(cudaFuncSetAttribute(k_berry, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_berry<<<nk, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
   CKL("k_berry");
+  return 0;
+}
+
+// single-particle optical activity of every k (spoptpolbz): eigsys of all bands, then k_optbz
+int launch_optbz(wtbg_ctx* ctx, int nk, int nv, int nc, const double* d_kpt, const double* d_eig, const double2* d_U,
+                 const int* d_nocp, double sme, double* d_out, int* d_kstat) {
+  const int w = ctx->w, nvec = ctx->nvec;
+  OptBzArgs a;
+  a.HR = ctx->HR.as<double2>();
+  a.Rcart = ctx->Rcart.as<double>();
+  a.Rf32 = ctx->Rf32.as<double>();
+  a.invdeg = ctx->invdeg.as<double>();
+  a.isR0 = ctx->isR0.as<int>();
+  a.nvec = nvec;
+  a.w = w;
+  a.nk = nk;
+  a.nv = nv;
+  a.nc = nc;
+  a.kpt = d_kpt;
+  a.eig = d_eig;
+  a.U = d_U;
+  a.nocp = d_nocp;
+  a.sme32 = (double)(float)sme;
+  a.norm32 = (double)(1.0f / sqrtf(2.0f));
+  a.out = d_out;
+  a.kstat = d_kstat;
+  const size_t smem = sizeof(double2) * ((size_t)nvec + 4 * (size_t)w * w);
+  if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "opt_bz: model too large for shared memory");
+  CK(cudaFuncSetAttribute(k_optbz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_optbz<<<nk, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
+  CKL("k_optbz");
   return 0;
 }

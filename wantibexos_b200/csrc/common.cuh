@@ -205,6 +205,8 @@ int launch_eigsys_all(wtbg_ctx* ctx, int nk, const double* d_kpt, double* d_eig,
                       int* d_kstat);
 int launch_berry(wtbg_ctx* ctx, int nk, const double* d_kpt, const double* d_eig, const double2* d_U, const int* d_nocp,
                  double gamma, double degtol, double* d_out);
+int launch_optbz(wtbg_ctx* ctx, int nk, int nv, int nc, const double* d_kpt, const double* d_eig, const double2* d_U,
+                 const int* d_nocp, double sme, double* d_out, int* d_kstat);
 int launch_dos(wtbg_ctx* ctx, const double* d_etb, const double* d_w, long long ndim, int ncol, const double* d_en,
                int nw, double sme, long long nkpt, double* d_out);
 int autotune_hemv(wtbg_ctx* ctx, int* hs_out);

@@ -29,6 +29,7 @@
 #include <fstream>
 #include <sstream>
 #include <stdexcept>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -656,6 +657,51 @@ void upload_model_temp(wtbg_ctx* ctx, const Model& m, const Deck& d, bool temp) 
 // bsesolver (bse_solver-tool-diel.f90) and, with d.bset, bsesolvertemp
 // (bse_solver-tool-diel-temp.f90): same files; the temperature run adds the log line, the
 // scissors tcor and the occupation factors.
+// sp_optics.dat, sp_optics-pol.dat and (TM_COEF) tm_coef*.dat from the device sp table
+// (bse_solver-tool-diel.f90:338-423, sp_solver-tool-diel.f90:98-175; Bubblem order)
+void write_sp_tables(const Deck& d, int nk, long long N, const std::vector<float>& vr, Out& f401, Out& f403, FILE* f402,
+                     FILE* f404) {
+  f401.line(" #  energy  xx  yy  zz  xy  xz  yz");
+  f403.line(" #  energy  xx  yy  zz  sp  sm");
+  if (d.tmcoef) {
+    fprintf(f402, " number of kpoints:%12d\n number of conduction states%12d\n number of valence states%12d\n", nk,
+            d.nc, d.nv);
+    fprintf(f402, " #  kx  ky  kz  nocp  nc  nv  energy  xx  yy  zz  xy  xz  yz\n");
+    fprintf(f404, " number of kpoints:%12d\n number of conduction states%12d\n number of valence states%12d\n", nk,
+            d.nc, d.nv);
+    fprintf(f404, " #  kx  ky  kz  nocp  nc  nv  energy  xx  yy  zz  sp  sm\n");
+  }
+  auto col = [&](long long i, int c) { return (double)vr[i + (size_t)N * c]; };
+  auto i100 = [](double v) {   // I10.0: a zero value prints as blanks
+    long long k = (long long)v;
+    return k == 0 ? std::string(10, ' ') : I(k, 10);
+  };
+  {
+    std::string b401, b403, b402, b404;
+    b401.reserve(N * 106);
+    b403.reserve(N * 91);
+    for (long long i = 0; i < N; ++i) {
+      b401 += F(col(i, 6), 15, 4) + F(col(i, 7), 15, 4) + F(col(i, 8), 15, 4) + F(col(i, 9), 15, 4) +
+              F(col(i, 10), 15, 4) + F(col(i, 11), 15, 4) + F(col(i, 12), 15, 4) + "\n";
+      b403 += F(col(i, 6), 15, 4) + F(col(i, 7), 15, 4) + F(col(i, 8), 15, 4) + F(col(i, 9), 15, 4) +
+              F(col(i, 13), 15, 4) + F(col(i, 14), 15, 4) + "\n";
+      if (d.tmcoef) {
+        std::string head = F(col(i, 0), 10, 4) + F(col(i, 1), 10, 4) + F(col(i, 2), 10, 4) + i100(col(i, 3)) +
+                           i100(col(i, 4)) + i100(col(i, 5)) + F(col(i, 6), 10, 4) + F(col(i, 7), 10, 4) +
+                           F(col(i, 8), 10, 4) + F(col(i, 9), 10, 4);
+        b402 += head + F(col(i, 10), 10, 4) + F(col(i, 11), 10, 4) + F(col(i, 12), 10, 4) + "\n";
+        b404 += head + F(col(i, 13), 10, 4) + F(col(i, 14), 10, 4) + "\n";
+      }
+    }
+    fputs(b401.c_str(), f401.f);
+    fputs(b403.c_str(), f403.f);
+    if (d.tmcoef) {
+      fputs(b402.c_str(), f402);
+      fputs(b404.c_str(), f404);
+    }
+  }
+}
+
 void bsesolver(wtbg_ctx* ctx, const Deck& d, const Model& m, Timings* tm) {
   const std::string of = d.outputfolder;
   Out log(join_path(of, "log_bse-diel.dat"), "Error opening log_bse-diel output file");
@@ -715,45 +761,7 @@ void bsesolver(wtbg_ctx* ctx, const Deck& d, const Model& m, Timings* tm) {
   gpu_check(ctx, wtbg_velocity(ctx, d.cshift, hr.data()), "wtbg_velocity");
   std::vector<float> vr(15 * (size_t)N);
   gpu_check(ctx, wtbg_sp_table(ctx, vr.data()), "wtbg_sp_table");
-  f401.line(" #  energy  xx  yy  zz  xy  xz  yz");
-  f403.line(" #  energy  xx  yy  zz  sp  sm");
-  if (d.tmcoef) {
-    fprintf(f402, " number of kpoints:%12d\n number of conduction states%12d\n number of valence states%12d\n", nk,
-            d.nc, d.nv);
-    fprintf(f402, " #  kx  ky  kz  nocp  nc  nv  energy  xx  yy  zz  xy  xz  yz\n");
-    fprintf(f404, " number of kpoints:%12d\n number of conduction states%12d\n number of valence states%12d\n", nk,
-            d.nc, d.nv);
-    fprintf(f404, " #  kx  ky  kz  nocp  nc  nv  energy  xx  yy  zz  sp  sm\n");
-  }
-  auto col = [&](long long i, int c) { return (double)vr[i + (size_t)N * c]; };
-  auto i100 = [](double v) {   // I10.0: a zero value prints as blanks
-    long long k = (long long)v;
-    return k == 0 ? std::string(10, ' ') : I(k, 10);
-  };
-  {
-    std::string b401, b403, b402, b404;
-    b401.reserve(N * 106);
-    b403.reserve(N * 91);
-    for (long long i = 0; i < N; ++i) {
-      b401 += F(col(i, 6), 15, 4) + F(col(i, 7), 15, 4) + F(col(i, 8), 15, 4) + F(col(i, 9), 15, 4) +
-              F(col(i, 10), 15, 4) + F(col(i, 11), 15, 4) + F(col(i, 12), 15, 4) + "\n";
-      b403 += F(col(i, 6), 15, 4) + F(col(i, 7), 15, 4) + F(col(i, 8), 15, 4) + F(col(i, 9), 15, 4) +
-              F(col(i, 13), 15, 4) + F(col(i, 14), 15, 4) + "\n";
-      if (d.tmcoef) {
-        std::string head = F(col(i, 0), 10, 4) + F(col(i, 1), 10, 4) + F(col(i, 2), 10, 4) + i100(col(i, 3)) +
-                           i100(col(i, 4)) + i100(col(i, 5)) + F(col(i, 6), 10, 4) + F(col(i, 7), 10, 4) +
-                           F(col(i, 8), 10, 4) + F(col(i, 9), 10, 4);
-        b402 += head + F(col(i, 10), 10, 4) + F(col(i, 11), 10, 4) + F(col(i, 12), 10, 4) + "\n";
-        b404 += head + F(col(i, 13), 10, 4) + F(col(i, 14), 10, 4) + "\n";
-      }
-    }
-    fputs(b401.c_str(), f401.f);
-    fputs(b403.c_str(), f403.f);
-    if (d.tmcoef) {
-      fputs(b402.c_str(), f402);
-      fputs(b404.c_str(), f404);
-    }
-  }
+  write_sp_tables(d, nk, N, vr, f401, f403, f402, f404);
   log.line(" single particle optics finished");
   log.flush();
   double t2 = now_s();
@@ -978,6 +986,59 @@ int spin_of(const std::string& systype, const std::string& dft, int i, int w) {
 
 // bandstool (bands-kpath-tool.f90): eigsys along the k path of KPATH_FILE=; bands.dat with
 // (k distance, E, <Sz>, layer weight) per band, KLABELS.dat from kpath2 (mhkpack_subs.f90:54-130)
+// spoptics (sp_solver-tool-diel.f90): the single-particle half of bsesolver on its own (DIEL=T)
+void spoptics_tool(wtbg_ctx* ctx, const Deck& d, const Model& m) {
+  const std::string of = d.outputfolder;
+  Out f401(join_path(of, "sp_optics.dat"), "Error opening sp_optics output file");
+  FILE* f402 = nullptr;
+  FILE* f404 = nullptr;
+  if (d.tmcoef) {
+    f402 = fopen(join_path(of, "tm_coef.dat").c_str(), "w");
+    if (!f402) throw Stop("Error opening tm_coef output file");
+    f404 = fopen(join_path(of, "tm_coef-pol.dat").c_str(), "w");
+    if (!f404) throw Stop("Error opening tm_coef-pol output file");
+  }
+  Out f403(join_path(of, "sp_optics-pol.dat"), "Error opening sp_optics-pol output file");
+  upload_model(ctx, m);
+  const int nk = d.ngrid[0] * d.ngrid[1] * d.ngrid[2];
+  const long long N = (long long)nk * d.nc * d.nv;
+  std::vector<double> kpt = kmesh(d.ngrid, d.mshift, m.rlat, nullptr);
+  gpu_check(ctx, wtbg_bands(ctx, nk, kpt.data(), d.nv, d.nc, nullptr, nullptr, nullptr, nullptr), "wtbg_bands");
+  gpu_check(ctx, wtbg_velocity(ctx, d.cshift, nullptr), "wtbg_velocity");
+  std::vector<float> vr(15 * (size_t)N);
+  gpu_check(ctx, wtbg_sp_table(ctx, vr.data()), "wtbg_sp_table");
+  write_sp_tables(d, nk, N, vr, f401, f403, f402, f404);
+  if (f402) fclose(f402);
+  if (f404) fclose(f404);
+}
+
+// spoptpolbz (sp_opt_bz-tool.f90): bz_act_{x,y,z,sp,sm}.dat and dichroism.dat, list-directed rows
+// (real(4) kx, ky, kz, value) on the Monkhorst-Pack mesh (OPT_BZ=T)
+void spoptpolbz_tool(wtbg_ctx* ctx, const Deck& d, const Model& m) {
+  const std::string of = d.outputfolder;
+  const char* names[6] = {"bz_act_x", "bz_act_y", "bz_act_z", "bz_act_sp", "bz_act_sm", "dichroism"};
+  std::vector<std::unique_ptr<Out>> files;
+  for (const char* n : names)
+  {
+    const std::string msg = std::string("Error opening ") + n + " output file";
+    files.emplace_back(new Out(join_path(of, std::string(n) + ".dat"), msg.c_str()));
+  }
+  upload_model(ctx, m);
+  const int nk = d.ngrid[0] * d.ngrid[1] * d.ngrid[2];
+  std::vector<double> kpt = kmesh(d.ngrid, d.mshift, m.rlat, nullptr);
+  std::vector<double> s((size_t)nk * 5);
+  gpu_check(ctx, wtbg_sp_optbz(ctx, nk, kpt.data(), d.nv, d.nc, d.cshift, s.data()), "wtbg_sp_optbz");
+  std::vector<std::string> buf(6);
+  for (int k = 0; k < nk; ++k) {
+    const std::string kk = LS((float)kpt[k]) + LS((float)kpt[k + (size_t)nk]) + LS((float)kpt[k + 2 * (size_t)nk]);
+    double v[6];
+    for (int c = 0; c < 5; ++c) v[c] = s[k + (size_t)nk * c];
+    v[5] = (v[3] - v[4]) / (v[3] + v[4]);
+    for (int c = 0; c < 6; ++c) buf[c] += kk + LD(v[c]) + "\n";
+  }
+  for (int c = 0; c < 6; ++c) fputs(buf[c].c_str(), files[c]->f);
+}
+
 // kpath2 (mhkpack_subs.f90:54-130) on the path of KPATH_FILE=: distances kp (nk) and
 // Cartesian points kc (nk,3), KLABELS.dat written to the output folder
 void kpath_points(const Deck& d, const Model& m, std::vector<double>& kp, std::vector<double>& kc) {
@@ -1364,7 +1425,7 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
     // params header + mesh (wtb_main.f90:77-104)
     Model m;
     if (d.bse || d.bset || d.bsekpath || d.bsetbnd || d.spec || d.spdiel || d.bandscalc || d.doscalc || d.berryk ||
-        d.berrybz)
+        d.berrybz || d.sppolbz)
       m = read_params(d.params);
     if (d.meshtype.rfind("RK3D", 0) == 0) rkmesh(d.rk, m.rlat, d.ngrid, false);
     else if (d.meshtype.rfind("RK2D", 0) == 0) rkmesh(d.rk, m.rlat, d.ngrid, true);
@@ -1412,6 +1473,17 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
       } else if (d.bsetbnd) {
         bsebnds(ctx, d, m);
         log.line(" BSE exciton band structure, with temperature, finished");
+        log.flush();
+      }
+      // wtb_main.f90:209-218
+      if (d.spdiel) {
+        spoptics_tool(ctx, d, m);
+        log.line(" Single particle dielectric calculation finished");
+        log.flush();
+      }
+      if (d.sppolbz) {
+        spoptpolbz_tool(ctx, d, m);
+        log.line(" Single particle optical activity in BZ finished");
         log.flush();
       }
       // wtb_main.f90:232-251

@@ -29,7 +29,7 @@ EXPORTS = ["wtbg_create", "wtbg_destroy", "wtbg_error_string", "wtbg_last_error"
            "wtbg_net_features", "wtbg_net_add_sample", "wtbg_net_num_samples", "wtbg_net_train",
            "wtbg_net_eval_loss", "wtbg_net_predict", "wtbg_net_loss_grad", "wtbg_gemm_bf16",
            "wtbg_bse_build_q", "wtbg_set_temperature", "wtbg_eigsys", "wtbg_dos",
-           "wtbg_bands_batch", "wtbg_bse_q_batch", "wtbg_set_precision", "wtbg_berry"]
+           "wtbg_bands_batch", "wtbg_bse_q_batch", "wtbg_set_precision", "wtbg_berry", "wtbg_sp_optbz"]
 
 
 class WtbgError(RuntimeError):
@@ -97,6 +97,7 @@ def load_library(path: str = LIB_PATH):
         "wtbg_set_fast_product": (C.c_int, [P, C.c_int]),
         "wtbg_set_precision": (C.c_int, [P, C.c_int]),
         "wtbg_berry": (C.c_int, [P, C.c_int, dp, C.c_double, C.c_double, dp]),
+        "wtbg_sp_optbz": (C.c_int, [P, C.c_int, dp, C.c_int, C.c_int, C.c_double, dp]),
         "wtbg_net_create": (C.c_int, [P, C.POINTER(P), C.c_ulonglong]),
         "wtbg_net_destroy": (C.c_int, [P]),
         "wtbg_net_num_params": (C.c_longlong, []),
@@ -369,6 +370,13 @@ class Context:
         k = _f64(kpt)
         out = np.zeros((k.shape[0], 6), order="F")
         self._check(self.lib.wtbg_berry(self.h, k.shape[0], _dp(k), float(gamma), float(degtol), _dp(out)))
+        return out
+
+    def sp_optbz(self, kpt, nv, nc, sme):
+        """spoptpolbz sums per k: (nk, 5) = x, y, z, sigma+, sigma-."""
+        k = _f64(kpt)
+        out = np.zeros((k.shape[0], 5), order="F")
+        self._check(self.lib.wtbg_sp_optbz(self.h, k.shape[0], _dp(k), int(nv), int(nc), float(sme), _dp(out)))
         return out
 
     def set_precision(self, mode: int) -> None:
