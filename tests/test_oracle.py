@@ -217,3 +217,15 @@ def test_berry_oracle_gives_qwz_chern_numbers():
         b1, b2, _ = O.recvec(m.rlat[0], m.rlat[1], m.rlat[2])
         area = abs(np.cross(b1, b2)[2])
         assert abs(s * area / len(kp) / (2 * np.pi) - chern) < 1e-4
+
+
+def test_sp_optbz_oracle_identities():
+    """spoptpolbz sums: |h_x + i h_y|^2 + |h_x - i h_y|^2 = 2 (|h_x|^2 + |h_y|^2), so
+    sigma+ + sigma- = 2 norm^2 (x + y) with norm = f32(1/sqrt 2), and the dichroism lies in [-1, 1]."""
+    m = synth.config_model("c1")
+    rows = O.sp_optbz(m, [3, 3, 1], [0, 0, 0], 2, 2, float(np.float32(0.05)))
+    norm = float(np.float32(1.0) / np.sqrt(np.float32(2.0)))
+    assert rows.shape == (9, 9)
+    assert np.allclose(rows[:, 6] + rows[:, 7], 2 * norm ** 2 * (rows[:, 3] + rows[:, 4]), rtol=1e-12)
+    assert np.all(np.abs(rows[:, 8]) <= 1.0)
+    assert np.all(rows[:, 3:8] >= 0.0)
