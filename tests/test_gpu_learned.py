@@ -1,6 +1,6 @@
 """Learned warm start on the GPU: the hand-written forward/backward kernels against the CPU
 oracle's gradient, and the trained network's gain over the cold-start block Davidson on
-held-out sweep points (r0, eps_env), with the plain dense FP64 solve as the judge."""
+held-out sweep points (r0, eps_env), with the plain dense FP64 solve as the arbiter."""
 import numpy as np
 import pytest
 

@@ -7,13 +7,13 @@ FP64 solve as training targets, trains the network on the first `ntrain` points 
 and compares, on the held-out rest, the block Davidson started from the network against the
 cold start (unit vectors at the smallest diagonal entries): subspace capture, error of the
 first Rayleigh-Ritz energies, iterations and device time to residual 1e-6 eV, with the dense
-solve as the judge.
+solve as the arbiter.
 
   python -m wantibexos_b200.warmstart_sweep --model c4_w16 --n 60 --points 256 --train 192
 
 prints one JSON object (and writes the trained parameters with --save FILE.npy). With
 --targets davidson the training targets come from the fast-form block Davidson instead of 256
-dense solves (the held-out points are still judged by the dense solve).
+dense solves (the held-out points are still checked against the dense solve).
 """
 from __future__ import annotations
 
@@ -51,7 +51,7 @@ def main(argv=None):
     ap.add_argument("--eval", type=int, default=0, help="held-out points evaluated (0 = all)")
     ap.add_argument("--targets", default="dense", choices=["dense", "davidson"],
                     help="training targets from the dense FP64 solve, or from the fast-form block Davidson "
-                         "(residual 1e-6 eV); the held-out points are always judged by the dense solve")
+                         "(residual 1e-6 eV); the held-out points are always checked against the dense solve")
     ap.add_argument("--save", default=None)
     a = ap.parse_args(argv)
 
