@@ -82,10 +82,22 @@ typedef struct wtbg_stats {
   double her2k_flops;        /* algorithmic: 16 real flops x 2 x panel width per lower-triangle element */
   double tri_ms;             /* whole tridiagonalisation (profiling) */
   double tdsolve_ms;         /* tridiagonal eigenvalues + inverse iteration + oscillators (profiling) */
+  long long dav_fallbacks;   /* wtbg_bse_lowest calls that fell back to the dense FP64 solve */
+  double stage1_ms;          /* two-stage reduction: dense -> band (profiling) */
+  double stage2_ms;          /* two-stage reduction: band -> tridiagonal (profiling) */
 } wtbg_stats;
 int wtbg_set_profiling(wtbg_ctx* ctx, int on);
 int wtbg_get_stats(const wtbg_ctx* ctx, wtbg_stats* out);
 int wtbg_reset_stats(wtbg_ctx* ctx);
+
+/* Reduction used by the dense solves (wtbg_bse_solve, the Q eigenvalues): 0 = automatic (the
+ * two-stage reduction, dense -> band of width 32 on the FP64 tensor cores -> tridiagonal by
+ * bulge chasing, for N >= 2048 where its panels fit on the device; else one-stage),
+ * 1 = one-stage (blocked Householder with a Hermitian mat-vec per column), 2 = two-stage
+ * wherever it fits.  Both give the tridiagonal form of ZHETRD('L') up to rounding; the eigenvalues,
+ * oscillator strengths and vectors agree within the tolerances of the dense path.  No counterpart
+ * in the reference (its ZHEEV is MKL's). */
+int wtbg_set_reduction(wtbg_ctx* ctx, int mode);
 
 /* ---- model: replaces the module globals filled by hamiltonian_input_read
  *      (subroutines/module_input_read.f90:32-176).
@@ -147,6 +159,20 @@ int wtbg_bse_eigvecs(wtbg_ctx* ctx, int n0, int n1, double* A);
 int wtbg_bse_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter, double tol,
                       const double* X0, int dtfull, int cpol, double* W, double* act, double* X,
                       int* iters, double* maxres);
+
+/* ---- the nev lowest excitons with the dense fallback (no counterpart in the reference, whose
+ *      only solver is ZHEEV; the fallback is that ZHEEV restated): block Davidson as
+ *      wtbg_bse_davidson (largest = 0); when it ends with a residual at or above tol after
+ *      max_iter iterations (or, with the temperature mode on and act requested, where the
+ *      Davidson oscillators do not exist), the dense FP64 solve of wtbg_bse_solve runs on the
+ *      same matrix and its nev lowest eigenpairs are returned, with *used_dense = 1 and the
+ *      stats counter dav_fallbacks incremented.  W (nev), act (nev,8) as wtbg_bse_solve (may be
+ *      NULL), X (N,nev) complex eigenvectors (may be NULL) normalised with the last component
+ *      real and >= 0 in both cases; iters and maxres describe the Davidson run.  After a
+ *      fallback the matrix has been overwritten by the reduction (as after wtbg_bse_solve) and
+ *      wtbg_bse_eigvecs serves further vectors; without one the matrix is kept. */
+int wtbg_bse_lowest(wtbg_ctx* ctx, int nev, int nb, int max_iter, double tol, const double* X0, int dtfull,
+                    int cpol, double* W, double* act, double* X, int* iters, double* maxres, int* used_dense);
 
 /* ---- bands of several models in one persistent launch (no counterpart in the reference,
  *      which loops eigsys per k per run): model m is the one set in ctxs[m] (all on one
@@ -272,8 +298,12 @@ int wtbg_spectrum(wtbg_ctx* ctx, int n, int ncomp, const double* ebse, const dou
  * (NULL = default stream).  The kernels' scratch is a fixed static device array of
  * 2*8*8192+32 doubles (about 1 MB) that every GPU loading this library keeps until exit, so
  * nw = int(numbse) must be <= 8192 and ncomp <= 8; larger sizes return WTBG_ERR_UNSUPPORTED
- * with a message in errbuf.  The first call on a device looks up the scratch address
- * (cudaGetSymbolAddress) and should come before any stream capture.  All calls share the
+ * with a message in errbuf.  The scratch address belongs to the CUDA context current on the
+ * calling thread: every call made outside stream capture looks it up again
+ * (cudaGetSymbolAddress, which allocates nothing), so calls after a cudaDeviceReset or under
+ * a non-primary context are safe; a call made while `stream` is being captured reuses the
+ * address found by an earlier call in the same context, so make one call in each context
+ * before any stream capture (otherwise WTBG_ERR_STATE).  All calls share the
  * scratch: calls whose work overlaps on the GPU (different streams or host threads without
  * ordering) race.  Nothing in the scratch has to start at zero.  The call is asynchronous on
  * `stream`; no memory is allocated or freed. */

@@ -74,3 +74,25 @@ def test_haydock_spectrum_matches_dense(gpu_ctx, dtfull, cpol):
         scale = np.abs(want[:, 1:]).max()
         assert np.abs(eps[:, 0, o] - want[:, 1]).max() <= 2e-5 * scale, o
         assert np.abs(eps[:, 1, o] - want[:, 2]).max() <= 2e-5 * scale, o
+
+
+def test_lowest_falls_back_to_dense_when_residual_fails(gpu_ctx):
+    """wtbg_bse_lowest: a Davidson run capped at 1 iteration cannot reach 1e-12 eV, so the dense
+    FP64 solve of the same matrix answers, bit for bit the dense solve's lowest pairs."""
+    setup(gpu_ctx)
+    s0 = gpu_ctx.stats()["dav_fallbacks"]
+    W, act, X, it, res, used = gpu_ctx.bse_lowest(8, nb=16, max_iter=1, tol=1e-12, dtfull=True, want_vectors=True)
+    assert used and res > 1e-12
+    assert gpu_ctx.stats()["dav_fallbacks"] == s0 + 1
+    setup(gpu_ctx)
+    Wd, actd = gpu_ctx.bse_solve(True, False)
+    Ad = gpu_ctx.bse_eigvecs(1, 8)
+    assert np.array_equal(W, Wd[:8])
+    assert np.array_equal(act, actd[:8])
+    assert np.abs(X - Ad).max() < 1e-12
+    # and without the cap the Davidson answer stands
+    setup(gpu_ctx)
+    W2, _, X2, it2, res2, used2 = gpu_ctx.bse_lowest(8, nb=16, tol=1e-8, want_vectors=True)
+    assert not used2 and res2 < 1e-8
+    assert np.abs(W2 - Wd[:8]).max() < 1e-9
+    assert np.abs(X2[-1].imag).max() == 0.0 and (X2[-1].real >= 0).all()

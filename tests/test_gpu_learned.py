@@ -25,7 +25,10 @@ def test_gradients_match_cpu_oracle(gpu_ctx):
     errs = {name: float(np.linalg.norm(P[name] - R[name]) / np.linalg.norm(R[name]))
             for name in ("W1", "b1", "W2", "b2", "W3", "b3")}
     print("gradient relative errors", errs)
-    assert max(errs.values()) < 2e-2, errs
+    # measured on B200: W1 4.2e-4, W2 1.8e-4, W3 7.5e-5, b1 6.2e-5, b2 2.6e-5, b3 1.5e-5
+    bound = {"W1": 2e-3, "b1": 5e-4, "W2": 1e-3, "b2": 2e-4, "W3": 5e-4, "b3": 1e-4}
+    for name, e in errs.items():
+        assert e < bound[name], (name, e)
     net.close()
 
 

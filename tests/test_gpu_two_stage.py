@@ -1,0 +1,102 @@
+"""Two-stage reduction (dense -> band on the FP64 tensor cores -> tridiagonal by bulge chasing)
+against the one-stage reduction and the CPU oracle: exciton energies 1e-9 eV, oscillator
+strengths 1e-7 of the largest, exciton vectors (through both back-transforms) 1e-8, on meshes
+whose BSE dimension is and is not a multiple of the band width, with and without the
+temperature factors, and for the eigenvalues of a centre-of-mass Q point."""
+import numpy as np
+import pytest
+
+from oracle import wtb_oracle as O
+from oracle.deck import parse_deck
+from wantibexos_b200 import synth, wtbgpu
+
+pytestmark = pytest.mark.gpu
+
+DECK = """BSE= T
+NGX= {n}
+NGY= {n}
+NGZ= 1
+NBANDSV= 2
+NBANDSC= 2
+COULOMB_POT= V2DRK
+R_0= 40
+KTOL= 0.001
+CSHIFT= 0.05
+DTDIAG= T
+CPOL= T
+SYSDIM= "2D"
+{extra}"""
+
+
+def run(ctx, m, deck, ref, mode):
+    ctx.set_reduction(mode)
+    ctx.set_model(m)
+    ctx.bands(ref["kpts"], deck["nv"], deck["nc"])
+    ctx.velocity(deck["cshift"], want=False)
+    c = wtbgpu.coulomb_params(deck["coultype"], ref["ngrid"], deck["ktol"], deck["ediel"], deck["lc"], deck["ez"],
+                              deck["w"], deck["r0"])
+    ctx.bse_build(c)
+    W, act = ctx.bse_solve(True, True)
+    A = ctx.bse_eigvecs(1, 6)
+    ctx.set_reduction(0)
+    return W, act, A
+
+
+@pytest.mark.parametrize("n", [12, 11, 9])
+def test_two_stage_matches_one_stage_and_oracle(n, gpu_ctx):
+    m = synth.config_model("c1")
+    deck = parse_deck(DECK.format(n=n, extra=""))
+    ref = O.run_bse(m, deck)
+    W2, act2, A2 = run(gpu_ctx, m, deck, ref, 2)
+    W1, act1, A1 = run(gpu_ctx, m, deck, ref, 1)
+    assert np.abs(W2 - ref["W"]).max() < 1e-9
+    assert np.abs(W2 - W1).max() < 1e-9
+    for c in range(8):
+        scale = max(np.abs(ref["act"][:, c]).max(), 1e-30)
+        assert np.abs(act2[:, c] - ref["act"][:, c]).max() < 1e-7 * scale, c
+    # vectors: same gauge (last component real >= 0) on the same band vectors -> equal
+    for k in range(6):
+        if (k == 0 or W1[k] - W1[k - 1] > 1e-6) and W1[k + 1] - W1[k] > 1e-6:
+            assert np.abs(A2[:, k] - A1[:, k]).max() < 1e-8, k
+    assert np.abs(A2[-1].imag).max() == 0.0
+
+
+def test_two_stage_temperature_factors(gpu_ctx):
+    m = synth.config_model("c1")
+    deck = parse_deck(DECK.format(n=10, extra="TEMP= 3000\n").replace("BSE= T", "BSET= T"))
+    ref = O.run_bse(m, deck)
+    gpu_ctx.set_temperature(True, deck["temp"])
+    try:
+        W2, act2, _ = run(gpu_ctx, m, deck, ref, 2)
+    finally:
+        gpu_ctx.set_temperature(False, 0.0)
+    assert np.abs(W2 - ref["W"]).max() < 1e-9
+    for c in range(6):
+        scale = max(np.abs(ref["act"][:, c]).max(), 1e-30)
+        assert np.abs(act2[:, c] - ref["act"][:, c]).max() < 1e-7 * scale, c
+
+
+def test_two_stage_q_eigenvalues(gpu_ctx):
+    m = synth.config_model("c1")
+    deck = parse_deck(DECK.format(n=10, extra=""))
+    ng = deck["ngrid"]
+    kpts = O.monkhorst_pack(ng[0], ng[1], ng[2], deck["mshift"], m.rlat)
+    e, v, _, _ = O.bands(m, kpts, 2, 2)
+    qpath, _ = O.kpathbse(m.rlat, [(0, 0, 0), (0.5, 0, 0)], 5)
+    p = O.CoulombParams(deck["coultype"], deck["ktol"], deck["ediel"], deck["lc"], deck["ez"], deck["w"],
+                        deck["r0"], ng, m.rlat)
+    gpu_ctx.set_model(m)
+    gpu_ctx.bands(kpts, 2, 2)
+    gpu_ctx.set_reduction(2)
+    try:
+        for iq in (1, 3):
+            q4 = qpath[iq]
+            kq = O.monkhorst_pack(ng[0], ng[1], ng[2], deck["mshift"], m.rlat, q=q4[1:])
+            eq, vq, _, _ = O.bands(m, kq, 2, 2)
+            H = O.bse_matrix_q(p, q4, kpts, e, v, eq, vq, 2, 2)
+            c = wtbgpu.coulomb_params(deck["coultype"], ng, deck["ktol"], deck["ediel"], deck["lc"], deck["ez"],
+                                      deck["w"], deck["r0"])
+            W = gpu_ctx.bse_q_eigenvalues(kq, q4, c)
+            assert np.abs(W - np.linalg.eigvalsh(H, UPLO="U")).max() < 1e-9, iq
+    finally:
+        gpu_ctx.set_reduction(0)

@@ -62,14 +62,36 @@ def test_noalloc_matches_regular_entry_twice(ncomp, rtype):
     ctx.close()
 
 
+def test_noalloc_at_the_scratch_limit():
+    """NESPEC = 8192 with 8 components fills the fixed scratch to its end (eta sits last)."""
+    lib = wtbgpu.load_library()
+    ctx = wtbgpu.Context(0)
+    rtype = [1, 1, 1, 0, 0, 0, 1, 1]
+    for call, seed in enumerate((21, 22)):
+        n = 40 + 3 * call
+        E, F = inputs(seed, n, 8)
+        F[:, 3:6] -= 1.0
+        om_ref, eps_ref = ctx.spectrum(E, F, [6, 6, 1], 321.5, 0.0, 6.0, 8192.0, 0.05, True, 1.0, rtype=rtype)
+        om, eps = call_noalloc(lib, E, F, rtype, [6, 6, 1], 321.5, 0.0, 6.0, 8192, 0.05, True, 1.0)
+        assert np.array_equal(om, om_ref)
+        tol = 4 * np.spacing(np.float32(np.abs(eps_ref).max()))
+        assert np.abs(eps.astype(np.float64) - eps_ref.astype(np.float64)).max() <= tol
+    ctx.close()
+
+
 def test_noalloc_rejects_oversize():
     import torch
     lib = wtbgpu.load_library()
     d = torch.zeros(16, dtype=torch.float64, device="cuda")
     err = C.create_string_buffer(256)
-    rt = np.ones(6, dtype=np.int32)
+    rt = np.ones(9, dtype=np.int32)
     ng = np.array([2, 2, 1], dtype=np.int32)
     st = lib.wtbg_spectrum_noalloc(4, 6, d.data_ptr(), d.data_ptr(), rt.ctypes.data_as(C.POINTER(C.c_int)),
                                    ng.ctypes.data_as(C.POINTER(C.c_int)), 1.0, 0.0, 1.0, 9000.0, 0.1, 1, 1.0,
                                    d.data_ptr(), d.data_ptr(), None, err, 256)
     assert st == -8 and b"8192" in err.value
+    for nw, ncomp in ((8193.0, 8), (8192.0, 9)):
+        st = lib.wtbg_spectrum_noalloc(4, ncomp, d.data_ptr(), d.data_ptr(), rt.ctypes.data_as(C.POINTER(C.c_int)),
+                                       ng.ctypes.data_as(C.POINTER(C.c_int)), 1.0, 0.0, 1.0, nw, 0.1, 1, 1.0,
+                                       d.data_ptr(), d.data_ptr(), None, err, 256)
+        assert st == -8

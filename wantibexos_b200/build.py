@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libwtbgpu.so")
-SOURCES = ["api.cu", "bands.cu", "bse_build.cu", "tridiag.cu", "tdeig.cu", "spectrum.cu", "davidson.cu", "haydock.cu", "fastprod.cu", "learned.cu", "temperature.cu"]
+SOURCES = ["api.cu", "bands.cu", "bse_build.cu", "tridiag.cu", "tridiag2.cu", "tdeig.cu", "spectrum.cu", "davidson.cu", "haydock.cu", "fastprod.cu", "learned.cu", "temperature.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
               "-I" + os.path.join(ROOT, "include")]
@@ -43,14 +43,18 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
-    for s in srcs:
-        o = os.path.join(objdir, os.path.basename(s) + ".o")
-        cmd = [nvcc()] + ARCH + NVCC_FLAGS + ["-c", s, "-o", o]
+    objs = [os.path.join(objdir, os.path.basename(s) + ".o") for s in srcs]
+
+    def compile_one(pair):
+        src, obj = pair
+        cmd = [nvcc()] + ARCH + NVCC_FLAGS + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
-        objs.append(o)
+
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 4)) as ex:
+        list(ex.map(compile_one, zip(srcs, objs)))
     cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", LIB + ".tmp"] + objs
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)

@@ -75,6 +75,12 @@ int check_gemm_err(wtbg_ctx* ctx) {
 
 extern "C" {
 
+int wtbg_set_reduction(wtbg_ctx* ctx, int mode) {
+  if (!ctx || mode < 0 || mode > 2) return WTBG_ERR_ARG;
+  ctx->tri_mode = mode;
+  return WTBG_OK;
+}
+
 int wtbg_set_profiling(wtbg_ctx* ctx, int on) {
   if (!ctx) return WTBG_ERR_ARG;
   ctx->profiling = on ? 1 : 0;
@@ -143,7 +149,8 @@ int wtbg_destroy(wtbg_ctx* ctx) {
                     &ctx->d, &ctx->e, &ctx->tau, &ctx->g, &ctx->fdeh, &ctx->Wp, &ctx->slots, &ctx->part, &ctx->scal,
                     &ctx->yv, &ctx->lam, &ctx->ws, &ctx->act, &ctx->zsel, &ctx->csz, &ctx->sp_in, &ctx->sp_out,
                     &ctx->sp_om, &ctx->tmp, &ctx->tmp2, &ctx->istat, &ctx->pOpA, &ctx->pOpB,
-                    &ctx->pHk, &ctx->pOc, &ctx->pOv, &ctx->pErr, &ctx->triErr};
+                    &ctx->pHk, &ctx->pOc, &ctx->pOv, &ctx->pErr, &ctx->triErr, &ctx->gwork,
+                    &ctx->t2V, &ctx->t2X, &ctx->t2D, &ctx->t2G, &ctx->t2T, &ctx->t2P, &ctx->t2AB, &ctx->t2prog};
   for (DevBuf* b : bufs) free_buf(*b);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
   if (ctx->tri_exec) cudaGraphExecDestroy(ctx->tri_exec);
@@ -399,6 +406,63 @@ int wtbg_bse_davidson(wtbg_ctx* ctx, int nev, int nb, int largest, int max_iter,
   if (iters) *iters = it;
   if (maxres) *maxres = mr;
   if (mr >= tol) return set_err(ctx, WTBG_ERR_NOCONV, "bse_davidson: residual above tolerance after max_iter");
+  return WTBG_OK;
+}
+
+// gauge of an exciton vector for the BSE_WF files: unit norm, last component real and >= 0
+// (the convention of wtbg_bse_eigvecs)
+static void gauge_last_real(double* x, long long N) {
+  double nrm = 0.0;
+  for (long long i = 0; i < N; ++i) nrm += x[2 * i] * x[2 * i] + x[2 * i + 1] * x[2 * i + 1];
+  const double lr = x[2 * (N - 1)], li = x[2 * (N - 1) + 1];
+  const double r = std::hypot(lr, li);
+  double cr = 1.0, ci = 0.0;   // multiply by conj(last)/|last|
+  if (r > 0.0) {
+    cr = lr / r;
+    ci = -li / r;
+  }
+  const double s = nrm > 0.0 ? 1.0 / std::sqrt(nrm) : 1.0;
+  for (long long i = 0; i < N; ++i) {
+    const double a = x[2 * i], b = x[2 * i + 1];
+    x[2 * i] = s * (a * cr - b * ci);
+    x[2 * i + 1] = s * (a * ci + b * cr);
+  }
+  x[2 * (N - 1) + 1] = 0.0;
+}
+
+int wtbg_bse_lowest(wtbg_ctx* ctx, int nev, int nb, int max_iter, double tol, const double* X0, int dtfull, int cpol,
+                    double* W, double* act, double* X, int* iters, double* maxres, int* used_dense) {
+  if (!ctx || !W || !used_dense) return WTBG_ERR_ARG;
+  *used_dense = 0;
+  if (!ctx->have_matrix) return set_err(ctx, WTBG_ERR_STATE, "bse_lowest: call wtbg_bse_build first");
+  const long long N = ctx->N;
+  if (nev < 1 || nev > N) return set_err(ctx, WTBG_ERR_ARG, "bse_lowest: bad nev");
+  int it = 0;
+  double mr = 0.0;
+  int st = WTBG_ERR_NOCONV;
+  if (!ctx->temp_on || !act)
+    st = wtbg_bse_davidson(ctx, nev, nb, 0, max_iter, tol, X0, dtfull, cpol, W, act, X, &it, &mr);
+  if (iters) *iters = it;
+  if (maxres) *maxres = mr;
+  if (st == WTBG_OK) {
+    if (X)
+      for (int n = 0; n < nev; ++n) gauge_last_real(X + 2 * (size_t)N * n, N);
+    return WTBG_OK;
+  }
+  if (st != WTBG_ERR_NOCONV && st != WTBG_ERR_UNSUPPORTED) return st;
+  // dense FP64 fallback: every eigenpair of the same matrix, the nev lowest returned
+  ctx->stats.dav_fallbacks += 1;
+  *used_dense = 1;
+  std::vector<double> w((size_t)N), a(act ? (size_t)N * 8 : 0);
+  if (int r = wtbg_bse_solve(ctx, dtfull, cpol, w.data(), act ? a.data() : nullptr)) return r;
+  const double ms = ctx->last_ms;
+  memcpy(W, w.data(), (size_t)nev * 8);
+  if (act)
+    for (int c = 0; c < 8; ++c) memcpy(act + (size_t)nev * c, a.data() + (size_t)N * c, (size_t)nev * 8);
+  if (X) {
+    if (int r = wtbg_bse_eigvecs(ctx, 1, nev, X)) return r;
+    ctx->last_ms += ms;
+  }
   return WTBG_OK;
 }
 
@@ -826,6 +890,7 @@ int wtbg_bse_q_eigenvalues(wtbg_ctx* ctx, int nk, const double* kptq, const doub
 // launch sequence into a graph, and every later call replays it. The graph reads the matrix
 // and writes the tridiagonal through the context's buffers, so it serves every Q of a batch.
 static int tridiagonalise_graph(wtbg_ctx* ctx) {
+  if (use_two_stage(ctx)) return run_tridiagonalise(ctx);   // a few launches per panel: no graph needed
   auto signature = [ctx]() {
     return std::vector<const void*>{ctx->H.p,     ctx->d.p,    ctx->e.p,     ctx->tau.p,  ctx->g.p,
                                      ctx->Wp.p,    ctx->slots.p, ctx->part.p, ctx->scal.p, ctx->h.p,

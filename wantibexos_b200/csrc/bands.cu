@@ -60,6 +60,8 @@ struct BandsArgs {
   int* kstat;      // [nk]
   int all;         // 1: every band (eigsys as the band and DOS tools call it), nb = w
   const float* Hk; // precision form: H(k) from the tensor-core Fourier sum, [2 w^2][nk] (Re, Im)
+  unsigned char* gwork;   // large models: per-CTA work areas in global memory (else shared memory)
+  long long gstride;      // bytes per CTA work area
 };
 
 // One k-point per iteration of the loop k = k0, k0 + kstride, ... (shared-memory work area
@@ -282,9 +284,15 @@ __global__ void k_hk_opB(const double2* HR, int nvec, int ww, int S, __nv_bfloat
   }
 }
 
+// work area of this CTA: dynamic shared memory, or its slice of the global work buffer when
+// the model's matrices exceed the shared-memory budget (w above ~70)
+__device__ __forceinline__ unsigned char* work_base(unsigned char* smem, unsigned char* gwork, long long gstride) {
+  return gwork ? gwork + (size_t)blockIdx.x * (size_t)gstride : smem;
+}
+
 __global__ void __launch_bounds__(kBandsThreads) k_bands(BandsArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
-  bands_body(a, blockIdx.x, gridDim.x, smem);
+  bands_body(a, blockIdx.x, gridDim.x, work_base(smem, a.gwork, a.gstride));
 }
 
 // Persistent ragged batch: every (model, k) item of several models (different w, nvec and
@@ -302,7 +310,7 @@ __global__ void __launch_bounds__(kBandsThreads) k_bands_batch(const BandsArgs* 
     if (it >= nitems) break;
     const BandsArgs a = mods[item_mod[it]];
     const int k = item_k[it];
-    bands_body(a, k, a.nk, smem);
+    bands_body(a, k, a.nk, work_base(smem, a.gwork, a.gstride));
   }
 }
 
@@ -322,13 +330,15 @@ struct VelArgs {
   double inv_sqrt2_f32;
   double2* h;      // [5][N]
   long long N;
+  unsigned char* gwork;
+  long long gstride;
 };
 
 __global__ void __launch_bounds__(kBandsThreads) k_velocity(VelArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int w = a.w, nvec = a.nvec, tid = threadIdx.x, bs = blockDim.x;
   const int ww = w * w, nb = a.nv + a.nc;
-  double2* ph = reinterpret_cast<double2*>(smem);
+  double2* ph = reinterpret_cast<double2*>(work_base(smem, a.gwork, a.gstride));
   double2* HX = ph + nvec;          // 3 matrices, column-major
   double2* Us = HX + 3 * ww;        // nb x w
   double2* T = Us + nb * w;         // [3][nv][w] = h_alpha * u_v
@@ -444,13 +454,15 @@ struct BerryArgs {
   const int* nocp;      // [nk]
   double gamma2, degtol;
   double* out;          // [6][nk]
+  unsigned char* gwork;
+  long long gstride;
 };
 
 __global__ void __launch_bounds__(kBandsThreads) k_berry(BerryArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int w = a.w, nvec = a.nvec, tid = threadIdx.x, bs = blockDim.x;
   const int ww = w * w;
-  double2* ph = reinterpret_cast<double2*>(smem);
+  double2* ph = reinterpret_cast<double2*>(work_base(smem, a.gwork, a.gstride));
   double2* HX = ph + nvec;      // 3 matrices, column-major; then T_a
   double2* Us = HX + 3 * ww;    // U[band][m]
   double2* tmp = Us + ww;       // one T_a before it replaces dH/dk_a
@@ -540,13 +552,15 @@ struct OptBzArgs {
   double sme32, norm32;
   double* out;          // [5][nk]
   int* kstat;
+  unsigned char* gwork;
+  long long gstride;
 };
 
 __global__ void __launch_bounds__(kBandsThreads) k_optbz(OptBzArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int w = a.w, nvec = a.nvec, tid = threadIdx.x, bs = blockDim.x;
   const int ww = w * w;
-  double2* ph = reinterpret_cast<double2*>(smem);
+  double2* ph = reinterpret_cast<double2*>(work_base(smem, a.gwork, a.gstride));
   double2* HX = ph + nvec;
   double2* Us = HX + 3 * ww;
   __shared__ double red[kBandsThreads / 32][5];
@@ -654,6 +668,30 @@ __global__ void k_sp_gather(const float* rows, const int* order, long long N, fl
 
 }  // namespace
 
+// Work-area placement of the per-k kernels: the model's matrices go to dynamic shared memory
+// when they fit the budget, else every CTA of a grid capped at 4 CTAs per SM gets a slice of
+// ctx->gwork in global memory (L2-resident at these sizes) and loops over k.
+constexpr size_t kSmemBudget = 200 * 1024;
+static int place_work(wtbg_ctx* ctx, size_t bytes, long long nk, unsigned char** gwork, long long* gstride,
+                      size_t* dyn, int* grid) {
+  if (bytes <= kSmemBudget) {
+    *gwork = nullptr;
+    *gstride = 0;
+    *dyn = bytes;
+    *grid = (int)nk;
+    return 0;
+  }
+  if (ctx->nsm <= 0) CK(cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device));
+  const long long g = std::min<long long>(nk, 4LL * ctx->nsm);
+  const size_t stride = (bytes + 255) / 256 * 256;
+  ENSURE(ctx->gwork, stride * (size_t)g);
+  *gwork = ctx->gwork.as<unsigned char>();
+  *gstride = (long long)stride;
+  *dyn = 0;
+  *grid = (int)g;
+  return 0;
+}
+
 static size_t bands_smem(int w, int nvec) {
   const int ww = w * w, m2 = w + (w & 1);
   return (size_t)nvec * 16 + 2 * (size_t)ww * 16 + (size_t)(m2 / 2) * sizeof(Rot) + (size_t)w * 8 +
@@ -709,10 +747,10 @@ int launch_bands(wtbg_ctx* ctx, bool q_mesh) {
     if (int r = run_precision_hk(ctx, a.kpt, ctx->nk)) return r;
     a.Hk = ctx->pHk.as<float>();
   }
-  const size_t smem = bands_smem(w, ctx->nvec);
-  if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bands: model too large for shared memory");
+  size_t smem = 0;
+  int grid = 0;
+  if (int r = place_work(ctx, bands_smem(w, ctx->nvec), ctx->nk, &a.gwork, &a.gstride, &smem, &grid)) return r;
   CK(cudaFuncSetAttribute(k_bands, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int grid = ctx->nk;
   k_bands<<<grid, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
   CKL("k_bands");
   return 0;
@@ -752,7 +790,6 @@ int launch_bands_batch(wtbg_ctx* const* ctxs, int nmod) {
     order.push_back({cm->w, m});
     nitems += cm->nk;
   }
-  if (smem > 200 * 1024) return set_err(c0, WTBG_ERR_UNSUPPORTED, "bands: model too large for shared memory");
   std::stable_sort(order.begin(), order.end(), [](const std::pair<int, int>& x, const std::pair<int, int>& y) {
     return x.first > y.first;
   });
@@ -777,11 +814,24 @@ int launch_bands_batch(wtbg_ctx* const* ctxs, int nmod) {
   CK(cudaMemcpyAsync(d_im, im.data(), b_it, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(d_ik, ik.data(), b_it, cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(d_cnt, 0, 4, s));
-  CK(cudaFuncSetAttribute(k_bands_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, nsm = 148, per = 1;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bands_batch, kBandsThreads, smem));
+  if (smem > kSmemBudget) {
+    // a model too large for shared memory: every CTA works in its slice of global memory
+    const long long g = std::min<long long>(nitems, 4LL * nsm);
+    const size_t stride = (smem + 255) / 256 * 256;
+    ENSURE(c0->gwork, stride * (size_t)g);
+    for (auto& a : mods) {
+      a.gwork = c0->gwork.as<unsigned char>();
+      a.gstride = (long long)stride;
+    }
+    CK(cudaMemcpyAsync(d_mod, mods.data(), b_mod, cudaMemcpyHostToDevice, s));
+    smem = 0;
+    per = 4;
+  }
+  CK(cudaFuncSetAttribute(k_bands_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (smem > 0) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bands_batch, kBandsThreads, smem));
   const int grid = (int)std::min<long long>(nitems, (long long)nsm * std::max(1, per));
   k_bands_batch<<<grid, kBandsThreads, smem, s>>>(d_mod, d_im, d_ik, (int)nitems, d_cnt);
   WTBG_COUNT(c0, 1);
@@ -814,10 +864,11 @@ int launch_eigsys_all(wtbg_ctx* ctx, int nk, const double* d_kpt, double* d_eig,
   a.kstat = d_kstat;
   a.all = 1;
   a.Hk = nullptr;   // the band and DOS tools run the FP64 form
-  const size_t smem = bands_smem(w, ctx->nvec);
-  if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "bands: model too large for shared memory");
+  size_t smem = 0;
+  int grid = 0;
+  if (int r = place_work(ctx, bands_smem(w, ctx->nvec), nk, &a.gwork, &a.gstride, &smem, &grid)) return r;
   CK(cudaFuncSetAttribute(k_bands, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_bands<<<nk, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
+  k_bands<<<grid, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
   CKL("k_bands(all)");
   return 0;
 }
@@ -842,11 +893,13 @@ int launch_velocity(wtbg_ctx* ctx, double eta32) {
   a.inv_sqrt2_f32 = (double)(1.0f / sqrtf(2.0f));
   a.h = ctx->h.as<double2>();
   a.N = ctx->N;
-  const size_t smem = (size_t)ctx->nvec * 16 + 3 * (size_t)w * w * 16 + (size_t)nb * w * 16 +
+  const size_t need = (size_t)ctx->nvec * 16 + 3 * (size_t)w * w * 16 + (size_t)nb * w * 16 +
                       3 * (size_t)ctx->nv * w * 16;
-  if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "velocity: model too large for shared memory");
+  size_t smem = 0;
+  int grid = 0;
+  if (int r = place_work(ctx, need, ctx->nk, &a.gwork, &a.gstride, &smem, &grid)) return r;
   CK(cudaFuncSetAttribute(k_velocity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_velocity<<<ctx->nk, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
+  k_velocity<<<grid, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
   CKL("k_velocity");
   return 0;
 }
@@ -905,10 +958,13 @@ int launch_berry(wtbg_ctx* ctx, int nk, const double* d_kpt, const double* d_eig
   a.gamma2 = gamma * gamma;
   a.degtol = degtol;
   a.out = d_out;
-  const size_t smem = sizeof(double2) * ((size_t)nvec + 5 * (size_t)w * w);
-  if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "berry: model too large for shared memory");
+  size_t smem = 0;
+  int grid = 0;
+  if (int r = place_work(ctx, sizeof(double2) * ((size_t)nvec + 5 * (size_t)w * w), nk, &a.gwork, &a.gstride, &smem,
+                         &grid))
+    return r;
   CK(cudaFuncSetAttribute(k_berry, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_berry<<<nk, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
+  k_berry<<<grid, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
   CKL("k_berry");
   return 0;
 }
@@ -936,10 +992,13 @@ int launch_optbz(wtbg_ctx* ctx, int nk, int nv, int nc, const double* d_kpt, con
   a.norm32 = (double)(1.0f / sqrtf(2.0f));
   a.out = d_out;
   a.kstat = d_kstat;
-  const size_t smem = sizeof(double2) * ((size_t)nvec + 4 * (size_t)w * w);
-  if (smem > 200 * 1024) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "opt_bz: model too large for shared memory");
+  size_t smem = 0;
+  int grid = 0;
+  if (int r = place_work(ctx, sizeof(double2) * ((size_t)nvec + 4 * (size_t)w * w), nk, &a.gwork, &a.gstride, &smem,
+                         &grid))
+    return r;
   CK(cudaFuncSetAttribute(k_optbz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_optbz<<<nk, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
+  k_optbz<<<grid, kBandsThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
   CKL("k_optbz");
   return 0;
 }

@@ -9,7 +9,7 @@
 
 #include "../../include/wtbgpu.h"
 
-#define WTBG_MAX_W 48          // largest orbital count of the per-k shared-memory eigensolver
+#define WTBG_MAX_W 256         // largest orbital count of the per-k eigensolver (one thread per band)
 #define WTBG_HEMV_TILE 64      // tile edge of the Hermitian matrix-vector kernel
 #define WTBG_PANEL 32          // Householder panel width of the tridiagonalisation
 
@@ -78,6 +78,7 @@ struct wtbg_ctx {
 
   // misc
   DevBuf tmp, tmp2, istat;
+  DevBuf gwork;   // per-CTA work areas of the per-k kernels for models too large for shared memory
 
   // counters
   // temperature BSE (BSET / BSET_BND): occupation factor f_v - f_c per basis state
@@ -94,6 +95,10 @@ struct wtbg_ctx {
   const void* tmH_ptr = nullptr;
   long long tmH_n = 0;
   DevBuf triErr;                        // set by the mat-vec when a pipeline wait timed out
+  // two-stage reduction (tridiag2.cu): mode 0 auto, 1 one-stage, 2 two-stage; which one ran last
+  int tri_mode = 0;
+  bool tri_two = false;
+  DevBuf t2V, t2X, t2D, t2G, t2T, t2P, t2AB, t2prog;
   cudaGraphExec_t tri_exec = nullptr;
   std::vector<const void*> tri_sig;
   long long tri_launches = 0;
@@ -210,6 +215,8 @@ int launch_optbz(wtbg_ctx* ctx, int nk, int nv, int nc, const double* d_kpt, con
 int launch_dos(wtbg_ctx* ctx, const double* d_etb, const double* d_w, long long ndim, int ncol, const double* d_en,
                int nw, double sme, long long nkpt, double* d_out);
 int autotune_hemv(wtbg_ctx* ctx, int* hs_out);
+int run_backtransform2(wtbg_ctx* ctx, double2* X, int nvec);
+bool use_two_stage(wtbg_ctx* ctx);
 // C^T (N x M, ldc) (+)= A (M x K, lda) B (N x K, ldb)^T, bf16 operands, FP32 accumulation on the
 // tensor cores (tcgen05); err is a device flag set when a pipeline wait times out
 int gemm_bf16(wtbg_ctx* ctx, int* err, const __nv_bfloat16* A, long long lda, int M, int K, const __nv_bfloat16* B,

@@ -11,6 +11,7 @@
 // One warp per photon energy reduces over the excitons with shuffles; the six tensor
 // components share the two divisions of each (w, n) term.
 #include <cstdio>
+#include <map>
 #include <mutex>
 
 #include "common.cuh"
@@ -186,20 +187,38 @@ int launch_dos(wtbg_ctx* ctx, const double* d_etb, const double* d_w, long long 
 // Allocation-free entry point.  The scratch of the three spectrum kernels (Re/Im sums per
 // component and photon energy, and eta) lives in this fixed file-scope device array instead
 // of context buffers, so the call performs no device allocation.  Host code must not use
-// the symbol itself as an address: the device address is looked up once per device with
-// cudaGetSymbolAddress while that device is current.
+// the symbol itself as an address: the device address belongs to the CUDA context that is
+// current, so it is looked up with cudaGetSymbolAddress on every call made outside stream
+// capture (a cheap query that allocates nothing) and remembered per context; a call made
+// while its stream is being captured uses the remembered address of the current context.
 namespace {
 constexpr int kNoAllocMaxNw = 8192;
 constexpr int kNoAllocMaxComp = 8;
 constexpr size_t kNoAllocScratch = 2 * (size_t)kNoAllocMaxComp * kNoAllocMaxNw + 32;
-constexpr int kMaxDevices = 64;
 
-double* g_noalloc_ptr[kMaxDevices] = {nullptr};
+typedef int (*CtxGetCurrentFn)(void**);   // cuCtxGetCurrent(CUcontext*)
 std::mutex g_noalloc_mu;
+std::map<void*, double*> g_noalloc_ptr;   // current CUDA context -> scratch address in it
 
 int noalloc_fail(char* errbuf, int errlen, int code, const char* msg) {
   if (errbuf && errlen > 0) snprintf(errbuf, (size_t)errlen, "%s", msg);
   return code;
+}
+
+// the CUcontext current on this host thread (nullptr if the driver entry is unavailable)
+void* current_context() {
+  static CtxGetCurrentFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrentFn>(p);
+  });
+  void* c = nullptr;
+  if (fn && fn(&c) != 0) c = nullptr;
+  return c;
 }
 }  // namespace
 
@@ -218,25 +237,40 @@ extern "C" int wtbg_spectrum_noalloc(int n, int ncomp, const double* d_ebse, con
     return noalloc_fail(errbuf, errlen, WTBG_ERR_UNSUPPORTED,
                         "spectrum_noalloc: NESPEC above 8192 or more than 8 components exceeds the fixed scratch");
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+  if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
     return noalloc_fail(errbuf, errlen, WTBG_ERR_CUDA, "spectrum_noalloc: no current device");
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    return noalloc_fail(errbuf, errlen, WTBG_ERR_CUDA, "spectrum_noalloc: cannot query the stream");
   }
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    void* cctx = current_context();
+    if (cap == cudaStreamCaptureStatusNone) {
+      // outside capture: resolve the address in the context that is current now (after a
+      // cudaDeviceReset or under another context the old address would be invalid)
       void* p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_spectrum_scratch);
       if (e != cudaSuccess || !p) {
         cudaGetLastError();
         return noalloc_fail(errbuf, errlen, WTBG_ERR_CUDA, "spectrum_noalloc: cudaGetSymbolAddress failed");
       }
-      g_noalloc_ptr[dev] = static_cast<double*>(p);
+      scratch = static_cast<double*>(p);
+      if (cctx) g_noalloc_ptr[cctx] = scratch;
+    } else {
+      auto it = cctx ? g_noalloc_ptr.find(cctx) : g_noalloc_ptr.end();
+      if (it == g_noalloc_ptr.end())
+        return noalloc_fail(errbuf, errlen, WTBG_ERR_STATE,
+                            "spectrum_noalloc: first call in this CUDA context made under stream capture; "
+                            "call once before capturing");
+      scratch = it->second;
     }
-    scratch = g_noalloc_ptr[dev];
   }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   double* re = scratch;
   double* im = re + (size_t)ncomp * nw;
   double* eta = im + (size_t)ncomp * nw;

@@ -302,14 +302,23 @@ __global__ void k_real_to_complex(const double* z, double2* X, long long cnt) {
 }
 
 // rotate each vector so that its last component is real and >= 0 (ZHEEV 'U' convention)
+// each vector times conj(last)/|last|: the last component becomes real >= 0 (exactly real, as
+// ZHEEV('V','U') returns it).  The last component is read before any thread writes.
 __global__ void k_gauge_last(double2* X, long long n, int nvec) {
   const int c = blockIdx.x;
   if (c >= nvec) return;
-  const double2 last = X[(long long)c * n + n - 1];
+  __shared__ double2 s_last;
+  if (threadIdx.x == 0) s_last = X[(long long)c * n + n - 1];
+  __syncthreads();
+  const double2 last = s_last;
   const double r = hypot(last.x, last.y);
   double2 ph = make_double2(1, 0);
   if (r > 0) ph = make_double2(last.x / r, -last.y / r);
-  for (long long k = threadIdx.x; k < n; k += blockDim.x) X[(long long)c * n + k] = cmul(X[(long long)c * n + k], ph);
+  for (long long k = threadIdx.x; k < n; k += blockDim.x) {
+    double2 v = cmul(X[(long long)c * n + k], ph);
+    if (k == n - 1) v = make_double2(r, 0.0);
+    X[(long long)c * n + k] = v;
+  }
 }
 
 }  // namespace
@@ -478,6 +487,12 @@ int run_eigvecs(wtbg_ctx* ctx, int n0, int n1, double2* d_out) {
   const long long cnt = (long long)nvec * n;
   k_real_to_complex<<<(int)((cnt + 255) / 256), 256, 0, s>>>(ctx->zsel.as<double>(), d_out, cnt); WTBG_COUNT(ctx, 1);
   CKL("k_real_to_complex");
+  if (ctx->tri_two) {
+    if (int r = run_backtransform2(ctx, d_out, nvec)) return r;
+    k_gauge_last<<<nvec, 256, 0, s>>>(d_out, n, nvec); WTBG_COUNT(ctx, 1);
+    CKL("k_gauge_last");
+    return 0;
+  }
   const int nparts_max = (int)((n + BT_RB - 1) / BT_RB) + 1;
   ENSURE(ctx->tmp, (size_t)nparts_max * PB * (PB + 64) * 16 + PB * 64 * 16 + 1024);
   double2* part = ctx->tmp.as<double2>();

@@ -520,7 +520,10 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N_>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N_) : "memory"); }
 
-__global__ void __launch_bounds__(256, 2) k_her2k(double2* A, long long N, const double2* Wp, int j0, int jb, int k0) {
+// V (row, q) = Vs[row + (vc0 + q) * N]: the panel columns of A in the one-stage reduction, the
+// dense V of the two-stage panel otherwise.
+__global__ void __launch_bounds__(256, 2) k_her2k(double2* A, long long N, const double2* Wp, const double2* Vs,
+                                                  int vc0, int jb, int k0) {
   pdl_enter();
   extern __shared__ __align__(16) double2 hsm[];
   const long long t = blockIdx.x;
@@ -553,11 +556,11 @@ __global__ void __launch_bounds__(256, 2) k_her2k(double2* A, long long N, const
       const int rr = it % TB, q = it / TB;
       const long long rg = r0 + rr, cg = c0 + rr;
       const bool qv = (qc + q) < jb;
-      const long long qcol = (long long)(j0 + qc + q);
+      const long long qcol = (long long)(vc0 + qc + q);
       const bool vr = qv && rg < N, vc = qv && cg < N;
-      cp_async16(sVr + rr * HKP + q, vr ? A + rg + qcol * N : A, vr);
+      cp_async16(sVr + rr * HKP + q, vr ? Vs + rg + qcol * N : Vs, vr);
       cp_async16(sWr + rr * HKP + q, vr ? Wp + rg + (long long)(qc + q) * N : Wp, vr);
-      cp_async16(sVc + rr * HKP + q, vc ? A + cg + qcol * N : A, vc);
+      cp_async16(sVc + rr * HKP + q, vc ? Vs + cg + qcol * N : Vs, vc);
       cp_async16(sWc + rr * HKP + q, vc ? Wp + cg + (long long)(qc + q) * N : Wp, vc);
     }
     cp_async_commit();
@@ -749,9 +752,35 @@ int autotune_hemv(wtbg_ctx* ctx, int* hs_out) {
   return 0;
 }
 
+// Trailing update of the two-stage panel: A22 -= V W^H + W V^H with V (row, q) = V[row + (vc0 + q) vld]
+int launch_her2k_v(wtbg_ctx* ctx, double2* A, long long N, const double2* Wp, const double2* V, long long vld, int vc0,
+                   int jb, long long k0) {
+  if (vld != N) return set_err(ctx, WTBG_ERR_ARG, "her2k: V must have leading dimension N");
+  CK(cudaFuncSetAttribute(k_her2k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HER2K_SMEM));
+  const long long T = (N - k0 + TB - 1) / TB;
+  const long long ntile = T * (T + 1) / 2;
+  CK(launch_pdl(k_her2k, dim3((unsigned)ntile), dim3(256), HER2K_SMEM, ctx->stream, A, N, Wp, V, vc0, jb, (int)k0));
+  WTBG_COUNT(ctx, 1);
+  return 0;
+}
+
+bool use_two_stage(wtbg_ctx* ctx);
+int run_tridiagonalise2(wtbg_ctx* ctx);
+static int run_tridiagonalise1(wtbg_ctx* ctx);
+
+// Reduction of the current matrix to tridiagonal form: two-stage (tridiag2.cu) where it is
+// selected and fits, else the one-stage column loop below.
 int run_tridiagonalise(wtbg_ctx* ctx) {
+  if (ctx->N < 2) return set_err(ctx, WTBG_ERR_ARG, "tridiagonalise: N < 2");
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(ctx->stream, &cap));
+  if (cap == cudaStreamCaptureStatusNone && use_two_stage(ctx)) return run_tridiagonalise2(ctx);
+  return run_tridiagonalise1(ctx);
+}
+
+static int run_tridiagonalise1(wtbg_ctx* ctx) {
   const long long N = ctx->N;
-  if (N < 2) return set_err(ctx, WTBG_ERR_ARG, "tridiagonalise: N < 2");
+  ctx->tri_two = false;
   const int nblk = (int)((N + TB - 1) / TB);
   const int maxRB = (int)((N + RA - 1) / RA) + 1;   // blocks of k_colA / k_colC
   ENSURE(ctx->d, (size_t)N * 8);
@@ -834,8 +863,8 @@ int run_tridiagonalise(wtbg_ctx* ctx) {
       const long long T = (N - k0 + TB - 1) / TB;
       const long long ntile = T * (T + 1) / 2;
       if (prof) cudaEventRecord(ctx->evpool[evh + 2 * (j0 / NB)], s);
-      CK(launch_pdl(k_her2k, dim3((unsigned)ntile), dim3(256), HER2K_SMEM, s, A, N, (const double2*)Wp, (int)j0, jb,
-                    (int)k0)); WTBG_COUNT(ctx, 1);
+      CK(launch_pdl(k_her2k, dim3((unsigned)ntile), dim3(256), HER2K_SMEM, s, A, N, (const double2*)Wp,
+                    (const double2*)A, (int)j0, jb, (int)k0)); WTBG_COUNT(ctx, 1);
       if (prof) cudaEventRecord(ctx->evpool[evh + 2 * (j0 / NB) + 1], s);
       CKL("k_her2k");
     }

@@ -1,0 +1,1106 @@
+// Kernel (c), two-stage form: reduction of the Hermitian BSE matrix to real symmetric
+// tridiagonal form in two steps, dense -> band (bandwidth b = 32) -> tridiagonal.
+//
+// Reference: the dense ZHEEV('V','U') of bsesolver (subprograms/bse_solver-tool-diel.f90:
+// 485-492) and ZHEEV('N','U') of bsebnds (bse_kpath-tool.f90:384-387).  The one-stage
+// reduction (tridiag.cu) streams the whole trailing matrix once per column in a Hermitian
+// matrix-vector product, so half of its flops run at HBM speed.  Here:
+//
+// Stage 1 (dense -> band), per panel of b columns j0..j0+b-1 with k0 = j0 + b:
+//   (1) k_panel_qr: Householder QR of the panel A[k0:N, j0:j0+b] (ZLARFG reflectors, one
+//       cooperative launch whose CTAs keep their row slices in shared memory, two bounded grid
+//       barriers per column); the T factor of the block reflector Q = I - V T V^H; the velocity
+//       vectors g <- Q^T g = g - conj(V) T^T (V^T g).
+//   (2) k_hemm2: X = A22 V on the FP64 tensor cores (mma.sync m16n8k16), A22 = A[k0:N, k0:N]
+//       read once from its stored lower triangle (tiles above the diagonal are read transposed
+//       and conjugated, the diagonal tiles from a symmetrised copy), split over K into
+//       deterministic partial sums.
+//   (3) k_xreduce / k_mform / k_wform: X <- X T, M = T^H V^H X, W = X - 1/2 V M.
+//   (4) k_her2k (tridiag.cu): A22 -= V W^H + W V^H, so that A22 <- Q^H A22 Q.
+//   Both large products are GEMM-shaped, so the stage runs at tensor-core speed where the
+//   one-stage mat-vec runs at HBM speed.
+// Stage 2 (band -> tridiagonal, bulge chasing) is in the second half of this file.
+// The oscillator strengths need only A^T h = Z^T (Q^T h), so no O(N^3) back-transform is formed.
+#include <cfloat>
+
+#include "common.cuh"
+
+#include <algorithm>
+#include <string>
+
+// implemented in tridiag.cu
+int launch_her2k_v(wtbg_ctx* ctx, double2* A, long long N, const double2* Wp, const double2* V, long long vld, int vc0,
+                   int jb, long long k0);
+
+namespace {
+
+constexpr int BW = 32;            // band width b of the two-stage reduction (= WTBG_PANEL)
+constexpr int PQ_THREADS = 256;   // threads of the panel QR kernel
+constexpr int NGMAX = 10;         // velocity vectors carried through (x, y, z, sp, sm [, times f])
+
+__device__ __forceinline__ double2 warp_sum2(double2 v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned int* p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+constexpr unsigned long long kWaitNs = 2000000000ull;   // 2 s bound on every spin wait
+
+// Grid barrier among the co-resident CTAs of a cooperative launch: arrival counter plus a
+// generation word.  The wait is bounded (2 s of %globaltimer); on time-out (or when another
+// CTA has already failed) the CTA sets *err and the barrier reports failure, after which every
+// CTA leaves the kernel.
+struct GridBar {
+  unsigned int count;
+  unsigned int gen;
+};
+__device__ bool grid_barrier(GridBar* gb, int* err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int g = ld_acquire(&gb->gen);
+    __threadfence();
+    const unsigned int arrived = atomicAdd(&gb->count, 1u);
+    int ok = 1;
+    if (arrived == gridDim.x - 1) {
+      atomicExch(&gb->count, 0u);
+      __threadfence();
+      st_release(&gb->gen, g + 1u);
+    } else {
+      const unsigned long long t0 = globaltimer();
+      while (ld_acquire(&gb->gen) == g) {
+        if (ld_acquire(reinterpret_cast<unsigned int*>(err)) != 0u || globaltimer() - t0 > kWaitNs) {
+          atomicExch(err, 1);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// ----------------------------------------------------------------------------- stage 1
+// Panel QR.  CTA c owns rows [k0 + c*R, k0 + min((c+1)*R, m)) of the panel, kept in shared
+// memory as P[col][row] (row fastest).  Per column p: ZLARFG from the grid-reduced norm (every
+// CTA sums the same partials in the same order, so all hold identical scalars), then the
+// reflector is applied to the panel's remaining columns with grid-reduced dot products.
+struct PanelArgs {
+  double2* A;
+  long long N;
+  int j0, k0, jb;      // panel columns j0 .. j0+jb-1, first panel row k0
+  int nref;            // reflectors: min(jb, N - k0)
+  int R;               // rows per CTA
+  double2* Vp;         // [32][N] dense V (rows k0.. written, explicit unit and zeros)
+  double2* Tout;       // [32][32] column-major T factor
+  double2* g;          // [ng][N]
+  int ng;
+  double* partN;       // [grid]
+  double2* partW;      // [grid][32]
+  double2* partG;      // [grid][32*32]
+  double2* partVg;     // [grid][32*NGMAX]
+  double2* alpha;      // [1] diagonal element of the current column
+  GridBar* bar;
+  int* err;
+};
+
+__device__ __forceinline__ double2 ldcg2(const double2* p) { return __ldcg(p); }
+
+__global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
+  extern __shared__ __align__(16) double2 P[];   // [jb][R]
+  __shared__ double2 s_tau[BW];
+  __shared__ double2 s_w[BW];
+  __shared__ double2 s_scal;
+  __shared__ double s_beta;
+  __shared__ double s_red[PQ_THREADS / 32];
+  __shared__ double2 s_T[BW * BW];
+  __shared__ double2 s_y[BW * NGMAX];
+  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  constexpr int NW = PQ_THREADS / 32;
+  const int R = a.R, jb = a.jb;
+  const long long N = a.N;
+  const int G = (int)gridDim.x;
+  const long long rbeg = (long long)a.k0 + (long long)blockIdx.x * R;
+  const long long rend = min((long long)a.k0 + (long long)(blockIdx.x + 1) * R, N);
+  const int nr = (int)max(0LL, rend - rbeg);
+  for (int q = 0; q < jb; ++q)
+    for (int i = tid; i < R; i += PQ_THREADS)
+      P[(size_t)q * R + i] = (i < nr) ? a.A[(rbeg + i) + (long long)(a.j0 + q) * N] : make_double2(0, 0);
+  __syncthreads();
+
+  // norm partial of column p over the own rows below row k0 + p; the owner of row k0 + p
+  // posts the diagonal element alpha
+  auto norm_partial = [&](int p) {
+    const long long rp = (long long)a.k0 + p;
+    double t = 0.0;
+    for (int i = tid; i < nr; i += PQ_THREADS)
+      if (rbeg + i > rp) {
+        const double2 x = P[(size_t)p * R + i];
+        t += x.x * x.x + x.y * x.y;
+      }
+    t = warp_sum(t);
+    if (lane == 0) s_red[wp] = t;
+    __syncthreads();
+    if (tid == 0) {
+      double s = 0.0;
+      for (int k = 0; k < NW; ++k) s += s_red[k];
+      a.partN[blockIdx.x] = s;
+      if (rp >= rbeg && rp < rend) *a.alpha = P[(size_t)p * R + (rp - rbeg)];
+    }
+  };
+
+  norm_partial(0);
+  for (int p = 0; p < a.nref; ++p) {
+    if (!grid_barrier(a.bar, a.err)) return;
+    const long long rp = (long long)a.k0 + p;
+    if (wp == 0) {
+      double xn2 = 0.0;
+      for (int c = lane; c < G; c += 32) xn2 += __ldcg(a.partN + c);
+      xn2 = warp_sum(xn2);
+      if (lane == 0) {
+        const double2 al = ldcg2(a.alpha);
+        double2 tau, scal;
+        double beta;
+        if (xn2 == 0.0 && al.y == 0.0) {
+          tau = make_double2(0, 0);
+          scal = make_double2(0, 0);
+          beta = al.x;
+        } else {
+          beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xn2), al.x);
+          tau = make_double2((beta - al.x) / beta, -al.y / beta);
+          const double2 den = make_double2(al.x - beta, al.y);
+          const double dd = den.x * den.x + den.y * den.y;
+          scal = make_double2(den.x / dd, -den.y / dd);
+        }
+        s_tau[p] = tau;
+        s_scal = scal;
+        s_beta = beta;
+      }
+    }
+    __syncthreads();
+    {
+      const double2 scal = s_scal;
+      const double beta = s_beta;
+      for (int i = tid; i < nr; i += PQ_THREADS) {
+        const long long r = rbeg + i;
+        if (r > rp) P[(size_t)p * R + i] = cmul(P[(size_t)p * R + i], scal);
+        else if (r == rp) P[(size_t)p * R + i] = make_double2(beta, 0.0);
+      }
+    }
+    __syncthreads();
+    // partial dots w_q = sum_{r >= k0+p} conj(v_r) P[r, q] for q = p+1 .. jb-1: one warp per q
+    const int nq = jb - p - 1;
+    for (int qq = wp; qq < nq; qq += NW) {
+      const int q = p + 1 + qq;
+      double2 s = make_double2(0, 0);
+      for (int i = lane; i < nr; i += 32) {
+        const long long r = rbeg + i;
+        if (r < rp) continue;
+        const double2 v = (r == rp) ? make_double2(1.0, 0.0) : P[(size_t)p * R + i];
+        s = cadd(s, cmulc(v, P[(size_t)q * R + i]));
+      }
+      s = warp_sum2(s);
+      if (lane == 0) a.partW[(size_t)blockIdx.x * BW + q] = s;
+    }
+    if (!grid_barrier(a.bar, a.err)) return;
+    for (int qq = wp; qq < nq; qq += NW) {
+      const int q = p + 1 + qq;
+      double2 s = make_double2(0, 0);
+      for (int c = lane; c < G; c += 32) s = cadd(s, ldcg2(a.partW + (size_t)c * BW + q));
+      s = warp_sum2(s);
+      if (lane == 0) s_w[q] = s;
+    }
+    __syncthreads();
+    {
+      // P[r, q] -= conj(tau) v_r w_q
+      const double2 ct = cconj(s_tau[p]);
+      for (int it = tid; it < nq * nr; it += PQ_THREADS) {
+        const int i = it % nr, q = p + 1 + it / nr;
+        const long long r = rbeg + i;
+        if (r < rp) continue;
+        const double2 v = (r == rp) ? make_double2(1.0, 0.0) : P[(size_t)p * R + i];
+        P[(size_t)q * R + i] = csub(P[(size_t)q * R + i], cmul(ct, cmul(v, s_w[q])));
+      }
+    }
+    __syncthreads();
+    if (p + 1 < a.nref) norm_partial(p + 1);
+  }
+  __syncthreads();
+  // write back: A keeps R (rows <= k0+q) and v below; Vp gets V with its unit and zeros
+  auto vval = [&](int q, int i) -> double2 {
+    const long long r = rbeg + i, rq = (long long)a.k0 + q;
+    if (q >= a.nref || r < rq) return make_double2(0, 0);
+    if (r == rq) return make_double2(1.0, 0.0);
+    return P[(size_t)q * R + i];
+  };
+  for (int q = 0; q < jb; ++q)
+    for (int i = tid; i < nr; i += PQ_THREADS) {
+      a.A[(rbeg + i) + (long long)(a.j0 + q) * N] = P[(size_t)q * R + i];
+      a.Vp[(rbeg + i) + (long long)q * N] = vval(q, i);
+    }
+  // Gram partial V^H V over the own rows, and V^T g
+  const int nref = a.nref;
+  for (int e = tid; e < BW * BW; e += PQ_THREADS) {
+    const int qi = e % BW, qj = e / BW;
+    double2 s = make_double2(0, 0);
+    if (qi < nref && qj < nref)
+      for (int i = 0; i < nr; ++i) s = cadd(s, cmulc(vval(qi, i), vval(qj, i)));
+    a.partG[(size_t)blockIdx.x * BW * BW + e] = s;
+  }
+  for (int e = tid; e < BW * a.ng; e += PQ_THREADS) {
+    const int q = e % BW, al = e / BW;
+    double2 s = make_double2(0, 0);
+    if (q < nref)
+      for (int i = 0; i < nr; ++i) s = cadd(s, cmul(vval(q, i), a.g[(long long)al * N + rbeg + i]));
+    a.partVg[(size_t)blockIdx.x * BW * NGMAX + e] = s;
+  }
+  if (!grid_barrier(a.bar, a.err)) return;
+  // T factor (ZLARFT forward columnwise): T[i][i] = tau_i, T[0:i, i] = -tau_i T[0:i, 0:i] G[0:i, i]
+  if (blockIdx.x == 0) {
+    for (int e = tid; e < BW * BW; e += PQ_THREADS) {
+      double2 s = make_double2(0, 0);
+      for (int c = 0; c < G; ++c) s = cadd(s, ldcg2(a.partG + (size_t)c * BW * BW + e));
+      s_T[e] = s;   // G for now, column-major (qi + qj * BW)
+    }
+    __syncthreads();
+    // column by column; column i of T is built in s_w from G(:, i) before T(:, i) is stored
+    for (int i = 0; i < BW; ++i) {
+      if (tid < BW) s_w[tid] = (tid < i && i < nref) ? s_T[tid + i * BW] : make_double2(0, 0);
+      __syncthreads();
+      if (tid < BW) {
+        double2 t = make_double2(0, 0);
+        if (i < nref && tid < i) {
+          for (int l = tid; l < i; ++l) t = cadd(t, cmul(s_T[tid + l * BW], s_w[l]));   // T[tid][l] for l < i
+          t = cscale(cmul(s_tau[i], t), -1.0);
+        } else if (i < nref && tid == i) {
+          t = s_tau[i];
+        }
+        // column i of the G storage is no longer needed below the diagonal: the T entries of
+        // rows < i overwrite G(0:i, i); rows >= i become T's diagonal and zeros
+        s_T[tid + i * BW] = t;
+      }
+      __syncthreads();
+    }
+    // s_T now holds T upper triangular; G entries below the diagonal were overwritten with 0
+    for (int e = tid; e < BW * BW; e += PQ_THREADS) a.Tout[e] = s_T[e];
+  }
+  if (!grid_barrier(a.bar, a.err)) return;
+  // g <- g - conj(V) T^T (V^T g)
+  for (int e = tid; e < BW * BW; e += PQ_THREADS) s_T[e] = ldcg2(a.Tout + e);
+  for (int e = tid; e < BW * a.ng; e += PQ_THREADS) {
+    double2 s = make_double2(0, 0);
+    for (int c = 0; c < G; ++c) s = cadd(s, ldcg2(a.partVg + (size_t)c * BW * NGMAX + e));
+    s_y[e] = s;   // (V^T g)[q][al] at q + al*BW
+  }
+  __syncthreads();
+  // z = T^T y into s_w-sized scratch: z[j][al] = sum_{i <= j} T[i][j] y[i][al]
+  __shared__ double2 s_z[BW * NGMAX];
+  for (int e = tid; e < BW * a.ng; e += PQ_THREADS) {
+    const int j = e % BW, al = e / BW;
+    double2 s = make_double2(0, 0);
+    for (int i = 0; i <= j; ++i) s = cadd(s, cmul(s_T[i + j * BW], s_y[i + al * BW]));
+    s_z[e] = s;
+  }
+  __syncthreads();
+  for (int e = tid; e < nr * a.ng; e += PQ_THREADS) {
+    const int i = e % nr, al = e / nr;
+    double2 s = make_double2(0, 0);
+    for (int q = 0; q < nref; ++q) s = cadd(s, cmul(cconj(vval(q, i)), s_z[q + al * BW]));
+    double2* gp = a.g + (long long)al * N + rbeg + i;
+    *gp = csub(*gp, s);
+  }
+}
+
+
+// Diagonal 64 x 64 tiles of A22 made full Hermitian (lower stored, upper = conj of lower,
+// diagonal real), column-major per tile: Dsym[I][c*64 + r].  Rows/columns past N are zero.
+__global__ void __launch_bounds__(256) k_symdiag(const double2* __restrict__ A, long long N, long long k0,
+                                                 double2* __restrict__ Dsym) {
+  const long long I0 = k0 + (long long)blockIdx.x * 64;
+  double2* D = Dsym + (size_t)blockIdx.x * 64 * 64;
+  for (int e = threadIdx.x; e < 64 * 64; e += 256) {
+    const int r = e & 63, c = e >> 6;
+    const long long gr = I0 + r, gc = I0 + c;
+    double2 v = make_double2(0, 0);
+    if (gr < N && gc < N) {
+      if (r > c) v = A[gr + gc * N];
+      else if (r < c) v = cconj(A[gc + gr * N]);
+      else v = make_double2(A[gr + gc * N].x, 0.0);
+    }
+    D[e] = v;
+  }
+}
+
+// D += A B with A 16x16 (a_i: row gq + 8*(i%2), k = tq + 4*(i/2)) and B 16x8 (b_j: k = tq + 4*j,
+// column gq): FP64 tensor-core MMA.
+__device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]), "d"(b[1]),
+        "d"(b[2]), "d"(b[3]));
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+  const unsigned sh = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sh), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N_>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N_) : "memory"); }
+
+// X = A22 V, A22 Hermitian (lower triangle of A from row/column k0), V = Vp (32 columns).
+// CTA (I, s): the 64 rows I of X, column blocks J of A22 in split s, K staged in chunks of 32
+// through a two-stage cp.async ring.  The A operand of chunk (J, kc) is A[I, J] (J < I, staged
+// k-major), conj(A[J, I])^T (J > I, staged row-major, conjugated when the fragment is built) or
+// the symmetrised diagonal tile (J = I).  Complex products as real MMAs with the real and
+// imaginary parts concatenated along k: X_re = [Ar | Ai] [Vr; -Vi], X_im = [Ar | Ai] [Vi; Vr].
+// Warp (wr, wc): rows 16 wr .. +16, columns 16 wc .. +16 (two 8-wide n blocks).
+constexpr int HM_LDA = 66;   // sA[k][row], 64 rows + 2 (conflict-free fragment loads)
+constexpr int HM_LDT = 36;   // sAT[row][k], 32 k + 4
+constexpr int HM_LDV = 34;   // sV[k][col], 32 columns + 2
+constexpr int HM_ABUF = 64 * HM_LDT;   // >= 32 * HM_LDA; union of the two A layouts
+constexpr int HM_STAGE = HM_ABUF + 32 * HM_LDV;
+constexpr size_t HM_SMEM = 2 * (size_t)HM_STAGE * sizeof(double2);
+
+__global__ void __launch_bounds__(256, 2) k_hemm2(const double2* __restrict__ A, long long N, long long k0,
+                                                  const double2* __restrict__ Dsym, const double2* __restrict__ V,
+                                                  int nI, int chunkJ, double2* __restrict__ Xpart) {
+  extern __shared__ __align__(16) double2 hs[];
+  const int I = blockIdx.x, sp = blockIdx.y;
+  const int J0 = sp * chunkJ, J1 = min(J0 + chunkJ, nI);
+  const long long m = N - k0;
+  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  const int wr = wp & 3, wc = wp >> 2, gq = lane >> 2, tq = lane & 3;
+  const long long rI = k0 + (long long)I * 64;
+
+  double accr[2][4], acci[2][4];
+#pragma unroll
+  for (int nb = 0; nb < 2; ++nb)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) accr[nb][k] = acci[nb][k] = 0.0;
+  const int nch = 2 * max(0, J1 - J0);
+
+  auto stage = [&](int c, int buf) {
+    const int J = J0 + (c >> 1), kc = (c & 1) * 32;
+    double2* sA = hs + (size_t)buf * HM_STAGE;
+    double2* sV = sA + HM_ABUF;
+    const long long cJ = k0 + (long long)J * 64 + kc;   // first global index of the k range
+    if (J < I) {
+      for (int e = tid; e < 64 * 32; e += 256) {
+        const int r = e & 63, k = e >> 6;
+        const long long gr = rI + r, gc = cJ + k;
+        const bool ok = gr < N && gc < N;
+        cp_async16(sA + k * HM_LDA + r, ok ? A + gr + gc * N : A, ok);
+      }
+    } else if (J > I) {
+      for (int e = tid; e < 64 * 32; e += 256) {
+        const int k = e & 31, r = e >> 5;
+        const long long gr = cJ + k, gc = rI + r;   // stored element A[gr, gc], gr > gc
+        const bool ok = gr < N && gc < N;
+        cp_async16(sA + r * HM_LDT + k, ok ? A + gr + gc * N : A, ok);
+      }
+    } else {
+      const double2* D = Dsym + (size_t)I * 64 * 64;
+      for (int e = tid; e < 64 * 32; e += 256) {
+        const int r = e & 63, k = e >> 6;
+        cp_async16(sA + k * HM_LDA + r, D + (size_t)(kc + k) * 64 + r, true);
+      }
+    }
+    for (int e = tid; e < 32 * 32; e += 256) {
+      const int k = e & 31, col = e >> 5;
+      const long long gr = cJ + k;
+      const bool ok = gr < N;
+      cp_async16(sV + k * HM_LDV + col, ok ? V + gr + (long long)col * N : V, ok);
+    }
+    cp_async_commit();
+  };
+
+  if (nch > 0) stage(0, 0);
+  if (nch > 1) stage(1, 1);
+  for (int c = 0; c < nch; ++c) {
+    if (c + 1 < nch) cp_async_wait<1>();
+    else cp_async_wait<0>();
+    __syncthreads();
+    const double2* sA = hs + (size_t)(c & 1) * HM_STAGE;
+    const double2* sV = sA + HM_ABUF;
+    const bool tr = (J0 + (c >> 1)) > I;
+    const int r0 = wr * 16 + gq, r1 = r0 + 8;
+#pragma unroll
+    for (int kk = 0; kk < 32; kk += 8) {
+      const int ka = kk + tq, kb = ka + 4;
+      double2 x00, x10, x01, x11;
+      if (tr) {
+        x00 = cconj(sA[r0 * HM_LDT + ka]);
+        x10 = cconj(sA[r1 * HM_LDT + ka]);
+        x01 = cconj(sA[r0 * HM_LDT + kb]);
+        x11 = cconj(sA[r1 * HM_LDT + kb]);
+      } else {
+        x00 = sA[ka * HM_LDA + r0];
+        x10 = sA[ka * HM_LDA + r1];
+        x01 = sA[kb * HM_LDA + r0];
+        x11 = sA[kb * HM_LDA + r1];
+      }
+      const double a[8] = {x00.x, x10.x, x01.x, x11.x, x00.y, x10.y, x01.y, x11.y};
+#pragma unroll
+      for (int nb = 0; nb < 2; ++nb) {
+        const int col = wc * 16 + nb * 8 + gq;
+        const double2 v0 = sV[ka * HM_LDV + col], v1 = sV[kb * HM_LDV + col];
+        const double bre[4] = {v0.x, v1.x, -v0.y, -v1.y};
+        const double bim[4] = {v0.y, v1.y, v0.x, v1.x};
+        dmma16(accr[nb], a, bre);
+        dmma16(acci[nb], a, bim);
+      }
+    }
+    __syncthreads();
+    if (c + 2 < nch) stage(c + 2, c & 1);
+  }
+#pragma unroll
+  for (int nb = 0; nb < 2; ++nb)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const long long row = rI + wr * 16 + gq + ((k >> 1) ? 8 : 0);
+      const int col = wc * 16 + nb * 8 + 2 * tq + (k & 1);
+      if (row < N) Xpart[((size_t)sp * 32 + col) * (size_t)m + (size_t)(row - k0)] = make_double2(accr[nb][k], acci[nb][k]);
+    }
+}
+
+constexpr size_t XR_SMEM = (size_t)(32 * 64 + 32 * 32 + 32 * 64) * sizeof(double2);
+// X = sum of the split partials; Y = X T into Wp; partial G_b = V_b^H Y_b over the 64 rows of
+// this block (Gpart[b][i + 32 j]).
+__global__ void __launch_bounds__(256) k_xreduce(const double2* __restrict__ Xpart, int S, long long N, long long k0,
+                                                 const double2* __restrict__ T, const double2* __restrict__ V,
+                                                 double2* __restrict__ Wp, double2* __restrict__ Gpart) {
+  extern __shared__ __align__(16) double2 xsm[];   // sX [32][64], sT [32][32], sV [32][64]
+  double2* sX = xsm;
+  double2* sT = sX + 32 * 64;
+  double2* sV = sT + 32 * 32;
+  const long long m = N - k0;
+  const long long rb = (long long)blockIdx.x * 64;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < 32 * 32; e += 256) sT[e] = T[e];
+  for (int e = tid; e < 32 * 64; e += 256) {
+    const int r = e & 63, c = e >> 6;
+    const long long rr = rb + r;
+    double2 x = make_double2(0, 0), v = make_double2(0, 0);
+    if (rr < m) {
+      for (int s = 0; s < S; ++s) x = cadd(x, Xpart[((size_t)s * 32 + c) * (size_t)m + rr]);
+      v = V[k0 + rr + (long long)c * N];
+    }
+    sX[e] = x;
+    sV[e] = v;
+  }
+  __syncthreads();
+  double2 y[8];
+  for (int u = 0; u < 8; ++u) {
+    const int e = tid + u * 256;
+    const int r = e & 63, j = e >> 6;
+    double2 t = make_double2(0, 0);
+    for (int i = 0; i <= j; ++i) t = cadd(t, cmul(sX[i * 64 + r], sT[i + j * 32]));
+    y[u] = t;
+  }
+  __syncthreads();
+  for (int u = 0; u < 8; ++u) {
+    const int e = tid + u * 256;
+    const int r = e & 63, j = e >> 6;
+    sX[e] = y[u];
+    if (rb + r < m) Wp[k0 + rb + r + (long long)j * N] = y[u];
+  }
+  __syncthreads();
+  for (int e = tid; e < 32 * 32; e += 256) {
+    const int i = e & 31, j = e >> 5;
+    double2 t = make_double2(0, 0);
+    for (int r = 0; r < 64; ++r) t = cadd(t, cmulc(sV[i * 64 + r], sX[j * 64 + r]));
+    Gpart[(size_t)blockIdx.x * 1024 + i + 32 * j] = t;
+  }
+}
+
+// M = T^H G, G = sum of the block partials (one CTA, fixed summation order)
+__global__ void __launch_bounds__(1024) k_mform(const double2* __restrict__ Gpart, int nb, const double2* __restrict__ T,
+                                                double2* __restrict__ M) {
+  __shared__ double2 sG[1024];
+  __shared__ double2 sT[1024];
+  const int e = threadIdx.x;
+  double2 t = make_double2(0, 0);
+  for (int b = 0; b < nb; ++b) t = cadd(t, Gpart[(size_t)b * 1024 + e]);
+  sG[e] = t;
+  sT[e] = T[e];
+  __syncthreads();
+  const int i = e & 31, j = e >> 5;
+  double2 s = make_double2(0, 0);
+  for (int l = 0; l <= i; ++l) s = cadd(s, cmulc(sT[l + i * 32], sG[l + j * 32]));   // conj(T[l][i]) G[l][j]
+  M[i + 32 * j] = s;
+}
+
+// W = Y - 1/2 V M (in place in Wp, rows k0..N-1)
+__global__ void __launch_bounds__(256) k_wform(long long N, long long k0, const double2* __restrict__ V,
+                                               const double2* __restrict__ M, double2* __restrict__ Wp) {
+  __shared__ double2 sM[1024];
+  for (int e = threadIdx.x; e < 1024; e += 256) sM[e] = M[e];
+  __syncthreads();
+  const long long r = k0 + (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int j = threadIdx.x & 31;
+  if (r >= N) return;
+  double2 t = make_double2(0, 0);
+  for (int i = 0; i < 32; ++i) t = cadd(t, cmul(V[r + (long long)i * N], sM[i + 32 * j]));
+  Wp[r + (long long)j * N] = csub(Wp[r + (long long)j * N], cscale(t, 0.5));
+}
+
+
+// ----------------------------------------------------------------------------- stage 2
+// Band storage: column j holds A[j + o, j] for o = 0 .. LDB-1 (the band, o <= b, and room for
+// the bulges, o <= 2b - 1).
+constexpr int LDB = 2 * BW + 2;
+constexpr int BG_WARPS = 4;                 // sweep workers per CTA
+constexpr int BG_LD = BW + 1;               // padded row length of the per-warp work tiles
+
+__device__ __forceinline__ long long nsteps_of(long long N, long long s) { return (N - 1 - s + BW - 1) / BW; }
+// sum_{u=1}^{U} ceil(u / b)
+__device__ __host__ __forceinline__ long long ceil_sum(long long U) {
+  if (U <= 0) return 0;
+  const long long q = U / BW, r = U % BW;
+  return BW * q * (q + 1) / 2 + r * (q + 1);
+}
+// index of the first reflector of sweep s in the flat tau2 array
+__device__ __host__ __forceinline__ long long tau2_offset(long long N, long long s) {
+  return ceil_sum(N - 1) - ceil_sum(N - 1 - s);
+}
+
+__global__ void __launch_bounds__(256) k_band_extract(const double2* __restrict__ A, long long N, double2* __restrict__ AB) {
+  const long long j = blockIdx.x;
+  for (int o = threadIdx.x; o < LDB; o += blockDim.x) {
+    double2 v = make_double2(0, 0);
+    if (o <= BW && j + o < N) v = A[(j + o) + j * N];
+    if (o == 0) v.y = 0.0;
+    AB[j * LDB + o] = v;
+  }
+}
+
+struct BulgeArgs {
+  double2* AB;
+  long long N;
+  double2* A;            // upper triangle: reflector vectors (sweep s in column N-1-s, rows 0..)
+  double2* tau2;         // [tau2_offset(N, s) + t]
+  double2* g;            // [ng][N]
+  int ng;
+  unsigned int* prog;    // [N] steps published per sweep
+  int* err;
+  int store;             // keep the reflectors for the eigenvector back-transform
+};
+
+// One step of sweep s (warp-wide; lane i <-> row r0 + i of the step's blocks).
+__device__ void bulge_step(const BulgeArgs& a, long long s, long long t, double2* Bs, double2* Ds, double2* vs,
+                           double2* ws) {
+  const int lane = threadIdx.x & 31;
+  const long long N = a.N;
+  double2* AB = a.AB;
+  const long long r0 = s + 1 + t * BW;
+  const int L = (int)min((long long)BW, N - r0);
+  const long long c0 = r0 - BW;   // first column of the bulge block (t >= 1)
+  // the column to annihilate: column s (t = 0) or column c0 of the bulge block
+  double2 x = make_double2(0, 0);
+  if (lane < L) x = (t == 0) ? __ldcg(AB + s * LDB + 1 + lane) : __ldcg(AB + c0 * LDB + BW + lane);
+  double xn2 = (lane >= 1 && lane < L) ? x.x * x.x + x.y * x.y : 0.0;
+  xn2 = warp_sum(xn2);
+  const double2 al = make_double2(__shfl_sync(0xffffffffu, x.x, 0), __shfl_sync(0xffffffffu, x.y, 0));
+  double2 tau, scal;
+  double beta;
+  if (xn2 == 0.0 && al.y == 0.0) {
+    tau = make_double2(0, 0);
+    scal = make_double2(0, 0);
+    beta = al.x;
+  } else {
+    beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xn2), al.x);
+    tau = make_double2((beta - al.x) / beta, -al.y / beta);
+    const double2 den = make_double2(al.x - beta, al.y);
+    const double dd = den.x * den.x + den.y * den.y;
+    scal = make_double2(den.x / dd, -den.y / dd);
+  }
+  const double2 v = (lane == 0) ? make_double2(1.0, 0.0) : (lane < L ? cmul(x, scal) : make_double2(0, 0));
+  vs[lane] = v;
+  // annihilated column: (beta, 0, ..., 0)
+  if (lane < L) {
+    const double2 nv = (lane == 0) ? make_double2(beta, 0.0) : make_double2(0, 0);
+    if (t == 0) AB[s * LDB + 1 + lane] = nv;
+    else AB[c0 * LDB + BW + lane] = nv;
+  }
+  __syncwarp();
+  if (t > 0) {
+    // left application to the other columns of the bulge block: B <- H^H B
+    for (int q = 1; q < BW; ++q) {
+      const long long o = BW + lane - q;
+      Bs[lane * BG_LD + q] = (lane < L) ? __ldcg(AB + (c0 + q) * LDB + o) : make_double2(0, 0);
+    }
+    __syncwarp();
+    if (lane >= 1) {   // w_q = sum_i conj(v_i) B(i, q), lane q
+      double2 w = make_double2(0, 0);
+      for (int i = 0; i < L; ++i) w = cadd(w, cmulc(vs[i], Bs[i * BG_LD + lane]));
+      ws[lane] = w;
+    }
+    __syncwarp();
+    if (lane < L) {
+      const double2 cv = cmul(cconj(tau), v);
+      for (int q = 1; q < BW; ++q) {
+        const double2 b = csub(Bs[lane * BG_LD + q], cmul(cv, ws[q]));
+        AB[(c0 + q) * LDB + (BW + lane - q)] = b;
+      }
+    }
+    __syncwarp();
+  }
+  // two-sided update of the diagonal block D (rows/cols r0 .. r0+L-1): D <- H^H D H
+  for (int q = 0; q < L; ++q) {
+    if (lane >= q && lane < L) {
+      double2 d = __ldcg(AB + (r0 + q) * LDB + (lane - q));
+      if (lane == q) d.y = 0.0;
+      Ds[lane * BG_LD + q] = d;
+      Ds[q * BG_LD + lane] = cconj(d);
+    }
+  }
+  __syncwarp();
+  double2 y = make_double2(0, 0);
+  if (lane < L)
+    for (int q = 0; q < L; ++q) y = cadd(y, cmul(Ds[lane * BG_LD + q], vs[q]));
+  double2 pv = cmulc(v, y);   // v^H y (real for Hermitian D)
+  pv = warp_sum2(pv);
+  const double t2 = tau.x * tau.x + tau.y * tau.y;
+  const double2 w = csub(cmul(tau, y), cscale(v, 0.5 * t2 * pv.x));
+  ws[lane] = w;
+  __syncwarp();
+  if (lane < L)
+    for (int q = 0; q <= lane; ++q) {
+      double2 d = csub(Ds[lane * BG_LD + q], cadd(cmulc(ws[q], v), cmulc(vs[q], w)));   // v_i conj(w_q) + w_i conj(v_q)
+      if (q == lane) d.y = 0.0;
+      AB[(r0 + q) * LDB + (lane - q)] = d;
+    }
+  // right application to the block below: B1 <- B1 H (rows r1 .. r1+L1-1, cols r0 .. r0+L-1)
+  const long long r1 = r0 + L;
+  if (r1 < N) {
+    const int L1 = (int)min((long long)BW, N - r1);
+    __syncwarp();
+    for (int q = 0; q < L; ++q)
+      Bs[lane * BG_LD + q] = (lane < L1) ? __ldcg(AB + (r0 + q) * LDB + (L + lane - q)) : make_double2(0, 0);
+    __syncwarp();
+    double2 z = make_double2(0, 0);
+    if (lane < L1)
+      for (int q = 0; q < L; ++q) z = cadd(z, cmul(Bs[lane * BG_LD + q], vs[q]));
+    if (lane < L1) {
+      const double2 tz = cmul(tau, z);
+      for (int q = 0; q < L; ++q)
+        AB[(r0 + q) * LDB + (L + lane - q)] = csub(Bs[lane * BG_LD + q], cmul(tz, cconj(vs[q])));
+    }
+  }
+  // velocity vectors: g <- g - tau conj(v) (v^T g)
+  for (int al2 = 0; al2 < a.ng; ++al2) {
+    double2* gp = a.g + (long long)al2 * N + r0;
+    const double2 gv = (lane < L) ? __ldcg(gp + lane) : make_double2(0, 0);
+    double2 sg = warp_sum2(cmul(v, gv));
+    if (lane < L) gp[lane] = csub(gv, cmul(tau, cmul(cconj(v), sg)));
+  }
+  if (a.store) {
+    if (lane < L) a.A[(r0 + lane - s - 1) + (N - 1 - s) * N] = v;
+    if (lane == 0) a.tau2[tau2_offset(N, s) + t] = tau;
+  }
+  __syncwarp();
+}
+
+// Persistent bulge chasing: warp w of the grid runs sweeps w, w + W, w + 2W, ...; sweep s
+// starts step t after sweep s-1 has published step t+3 (or finished).
+__global__ void __launch_bounds__(32 * BG_WARPS, 1) k_bulge(BulgeArgs a) {
+  extern __shared__ __align__(16) double2 bsm[];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2* Bs = bsm + (size_t)wid * (2 * BW * BG_LD + 2 * BW);
+  double2* Ds = Bs + BW * BG_LD;
+  double2* vs = Ds + BW * BG_LD;
+  double2* ws = vs + BW;
+  const long long W = (long long)gridDim.x * BG_WARPS;
+  const long long N = a.N;
+  for (long long s = (long long)blockIdx.x * BG_WARPS + wid; s < N - 1; s += W) {
+    const long long ns = nsteps_of(N, s);
+    const long long nprev = (s > 0) ? nsteps_of(N, s - 1) : 0;
+    for (long long t = 0; t < ns; ++t) {
+      if (s > 0) {
+        const unsigned int need = (unsigned int)min(t + 4, nprev);
+        int bad = 0;
+        if (lane == 0) {
+          const unsigned long long t0 = globaltimer();
+          while (ld_acquire(a.prog + s - 1) < need) {
+            if (ld_acquire(reinterpret_cast<unsigned int*>(a.err)) != 0u || globaltimer() - t0 > kWaitNs) {
+              atomicExch(a.err, 1);
+              bad = 1;
+              break;
+            }
+          }
+        }
+        bad = __shfl_sync(0xffffffffu, bad, 0);
+        if (bad) return;
+      }
+      bulge_step(a, s, t, Bs, Ds, vs, ws);
+      __threadfence();
+      __syncwarp();
+      if (lane == 0) st_release(a.prog + s, (unsigned int)(t + 1));
+    }
+  }
+}
+
+__global__ void k_band_to_tridiag(const double2* __restrict__ AB, long long N, double* __restrict__ d,
+                                  double* __restrict__ e) {
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  d[j] = AB[j * LDB].x;
+  if (j < N - 1) e[j] = AB[j * LDB + 1].x;
+}
+
+// ----------------------------------------------------------------------------- back-transform
+// Stage-2 reflectors in reverse: sweeps from the last, each step after the next sweep has
+// finished its steps up to t (the ranges are then disjoint); X (n x nvec, column-major).
+__global__ void __launch_bounds__(32 * BG_WARPS, 1) k_bulge_back(const double2* __restrict__ A, long long N,
+                                                                  const double2* __restrict__ tau2, double2* X, int nvec,
+                                                                  unsigned int* prog, int* err) {
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long W = (long long)gridDim.x * BG_WARPS;
+  for (long long u = (long long)blockIdx.x * BG_WARPS + wid; u < N - 1; u += W) {
+    const long long s = N - 2 - u;
+    const long long ns = nsteps_of(N, s);
+    const long long nnext = (s + 1 < N - 1) ? nsteps_of(N, s + 1) : 0;
+    for (long long t = 0; t < ns; ++t) {
+      if (s + 1 < N - 1) {
+        const unsigned int need = (unsigned int)min(t + 1, nnext);
+        int bad = 0;
+        if (lane == 0) {
+          const unsigned long long t0 = globaltimer();
+          while (ld_acquire(prog + s + 1) < need) {
+            if (ld_acquire(reinterpret_cast<unsigned int*>(err)) != 0u || globaltimer() - t0 > kWaitNs) {
+              atomicExch(err, 1);
+              bad = 1;
+              break;
+            }
+          }
+        }
+        bad = __shfl_sync(0xffffffffu, bad, 0);
+        if (bad) return;
+      }
+      const long long r0 = s + 1 + t * BW;
+      const int L = (int)min((long long)BW, N - r0);
+      const double2 v = (lane < L) ? A[(r0 + lane - s - 1) + (N - 1 - s) * N] : make_double2(0, 0);
+      const double2 tau = tau2[tau2_offset(N, s) + t];
+      for (int c = 0; c < nvec; ++c) {
+        double2* xp = X + (long long)c * N + r0;
+        const double2 xv = (lane < L) ? __ldcg(xp + lane) : make_double2(0, 0);
+        const double2 sv = warp_sum2(cmulc(v, xv));   // v^H x
+        if (lane < L) xp[lane] = csub(xv, cmul(tau, cmul(v, sv)));
+      }
+      __threadfence();
+      __syncwarp();
+      if (lane == 0) st_release(prog + s, (unsigned int)(t + 1));
+    }
+  }
+}
+
+// Stage-1 block reflectors in reverse: X[k0:] -= V (T (V^H X[k0:])).  V from the panel's
+// columns of A (unit at row k0+q, v below, zero above).
+constexpr int BT1_RB = 128;
+__device__ __forceinline__ double2 panel_v(const double2* A, long long N, int j0, int k0, int q, long long r) {
+  const long long rq = (long long)k0 + q;
+  if (r < rq) return make_double2(0, 0);
+  if (r == rq) return make_double2(1.0, 0.0);
+  return A[r + (long long)(j0 + q) * N];
+}
+__global__ void __launch_bounds__(256) k_bt1_partial(const double2* __restrict__ A, long long N, int j0, int k0, int nref,
+                                                     const double2* __restrict__ X, int nvec, double2* __restrict__ part) {
+  // part[b][q + 32 c] = sum over this block's rows of conj(V[r][q]) X[r][c]
+  const long long rb = (long long)k0 + (long long)blockIdx.x * BT1_RB;
+  for (int e = threadIdx.x; e < 32 * nvec; e += 256) {
+    const int q = e & 31, c = e >> 5;
+    double2 t = make_double2(0, 0);
+    if (q < nref)
+      for (int i = 0; i < BT1_RB; ++i) {
+        const long long r = rb + i;
+        if (r >= N) break;
+        t = cadd(t, cmulc(panel_v(A, N, j0, k0, q, r), X[r + (long long)c * N]));
+      }
+    part[(size_t)blockIdx.x * 32 * 32 + e] = t;
+  }
+}
+__global__ void __launch_bounds__(1024) k_bt1_tmat(const double2* __restrict__ part, int nb, int nvec,
+                                                   const double2* __restrict__ T, double2* __restrict__ Y) {
+  __shared__ double2 sY[32 * 32];
+  const int e = threadIdx.x;
+  const int q = e & 31, c = e >> 5;
+  double2 t = make_double2(0, 0);
+  if (c < nvec)
+    for (int b = 0; b < nb; ++b) t = cadd(t, part[(size_t)b * 32 * 32 + e]);
+  sY[e] = t;
+  __syncthreads();
+  if (c < nvec) {   // (T Y)[q][c] = sum_{l >= q} T[q][l] Y[l][c]
+    double2 s = make_double2(0, 0);
+    for (int l = q; l < 32; ++l) s = cadd(s, cmul(T[q + 32 * l], sY[l + 32 * c]));
+    Y[e] = s;
+  }
+}
+__global__ void __launch_bounds__(256) k_bt1_apply(const double2* __restrict__ A, long long N, int j0, int k0, int nref,
+                                                   double2* X, int nvec, const double2* __restrict__ Y) {
+  __shared__ double2 sY[32 * 32];
+  for (int e = threadIdx.x; e < 32 * nvec; e += 256) sY[e] = Y[e];
+  __syncthreads();
+  const long long r = (long long)k0 + (long long)blockIdx.x * 256 + threadIdx.x;
+  if (r >= N) return;
+  double2 vq[32];
+#pragma unroll
+  for (int q = 0; q < 32; ++q) vq[q] = (q < nref) ? panel_v(A, N, j0, k0, q, r) : make_double2(0, 0);
+  for (int c = 0; c < nvec; ++c) {
+    double2 t = make_double2(0, 0);
+#pragma unroll
+    for (int q = 0; q < 32; ++q) t = cadd(t, cmul(vq[q], sY[q + 32 * c]));
+    X[r + (long long)c * N] = csub(X[r + (long long)c * N], t);
+  }
+}
+
+}  // namespace
+
+// Largest N whose panels fit the aggregate shared memory of the panel QR (one CTA per SM,
+// at most PQ_MAX_R rows of the 32-wide panel each).
+constexpr int PQ_MAX_R = 384;
+static bool two_stage_fits(wtbg_ctx* ctx, long long N) {
+  if (ctx->nsm <= 0) cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+  return N > BW + 1 && (N + ctx->nsm - 1) / ctx->nsm <= PQ_MAX_R;
+}
+
+// The reduction used for the current matrix: two-stage for large N (auto) where it fits.
+bool use_two_stage(wtbg_ctx* ctx) {
+  const long long N = ctx->N;
+  if (ctx->tri_mode == 1) return false;
+  if (!two_stage_fits(ctx, N)) return false;
+  if (ctx->tri_mode == 2) return true;
+  return false;
+}
+
+int run_tridiagonalise2(wtbg_ctx* ctx) {
+  const long long N = ctx->N;
+  cudaStream_t s = ctx->stream;
+  const int nsm = ctx->nsm > 0 ? ctx->nsm : 148;
+  const long long npan = (N - BW - 1 + BW - 1) / BW;   // panels j0 = 0, 32, ... with j0 + 32 < N - 1
+  const long long nI = (N + 63) / 64;
+  const int SMAX = 8;
+  ENSURE(ctx->d, (size_t)N * 8);
+  ENSURE(ctx->e, (size_t)N * 8);
+  ENSURE(ctx->g, (size_t)N * 16 * NGMAX);
+  ENSURE(ctx->Wp, (size_t)N * 16 * BW);
+  ENSURE(ctx->t2V, (size_t)N * 16 * BW);
+  ENSURE(ctx->t2X, (size_t)SMAX * BW * N * 16);
+  ENSURE(ctx->t2D, (size_t)nI * 64 * 64 * 16);
+  ENSURE(ctx->t2G, (size_t)nI * 1024 * 16 + 1024 * 16);
+  ENSURE(ctx->t2T, (size_t)std::max<long long>(npan, 1) * 1024 * 16);
+  ENSURE(ctx->t2P, (size_t)nsm * (16 + 16 * BW + 16 * BW * BW + 16 * BW * NGMAX) + 4096);
+  ENSURE(ctx->t2AB, (size_t)N * LDB * 16);
+  const long long ntau = ceil_sum(N - 1);
+  ENSURE(ctx->tau, (size_t)std::max<long long>(ntau, 1) * 16);
+  ENSURE(ctx->t2prog, (size_t)N * 4 + 64);
+  ENSURE(ctx->triErr, 16);
+  double2* A = ctx->H.as<double2>();
+  double2* g = ctx->g.as<double2>();
+  double2* Vp = ctx->t2V.as<double2>();
+  double2* Wp = ctx->Wp.as<double2>();
+  double2* Xpart = ctx->t2X.as<double2>();
+  double2* Dsym = ctx->t2D.as<double2>();
+  double2* Gpart = ctx->t2G.as<double2>();
+  double2* Mbuf = Gpart + (size_t)nI * 1024;
+  double2* Tbuf = ctx->t2T.as<double2>();
+  char* pb = ctx->t2P.as<char>();
+  double* partN = reinterpret_cast<double*>(pb);
+  double2* partW = reinterpret_cast<double2*>(pb + (size_t)nsm * 16);   // 16-byte aligned for any SM count
+  double2* partG = partW + (size_t)nsm * BW;
+  double2* partVg = partG + (size_t)nsm * BW * BW;
+  double2* alpha = partVg + (size_t)nsm * BW * NGMAX;
+  GridBar* bar = reinterpret_cast<GridBar*>(alpha + 2);
+  int* err = ctx->triErr.as<int>();
+  CK(cudaMemsetAsync(err, 0, 4, s));
+  CK(cudaMemsetAsync(bar, 0, sizeof(GridBar), s));
+  // velocity vectors g (as the one-stage reduction)
+  const int ng = ctx->have_velocity ? (ctx->temp_on ? 10 : 5) : 0;
+  ctx->ng = ctx->have_velocity ? ng : 5;
+  if (ctx->have_velocity && ctx->temp_on) {
+    if (int r = fill_g_vectors(ctx, g)) return r;
+  } else if (ctx->have_velocity) {
+    CK(cudaMemcpyAsync(g, ctx->h.p, (size_t)N * 16 * 5, cudaMemcpyDeviceToDevice, s));
+  } else {
+    CK(cudaMemsetAsync(g, 0, (size_t)N * 16 * 5, s));
+  }
+  CK(cudaFuncSetAttribute(k_hemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HM_SMEM));
+  CK(cudaFuncSetAttribute(k_xreduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XR_SMEM));
+  const bool prof = ctx->profiling != 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  if (prof) {
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    cudaEventRecord(ev[0], s);
+  }
+  for (long long pnl = 0; pnl < npan; ++pnl) {
+    const int j0 = (int)(pnl * BW), k0 = j0 + BW;
+    const long long m = N - k0;
+    const int nref = (int)std::min<long long>(BW, m);
+    // panel QR: G CTAs of R rows
+    int R = (int)std::max<long long>(64, (m + nsm - 1) / nsm);
+    const int G = (int)((m + R - 1) / R);
+    PanelArgs pa;
+    pa.A = A;
+    pa.N = N;
+    pa.j0 = j0;
+    pa.k0 = k0;
+    pa.jb = BW;
+    pa.nref = nref;
+    pa.R = R;
+    pa.Vp = Vp;
+    pa.Tout = Tbuf + (size_t)pnl * 1024;
+    pa.g = g;
+    pa.ng = ng;
+    pa.partN = partN;
+    pa.partW = partW;
+    pa.partG = partG;
+    pa.partVg = partVg;
+    pa.alpha = alpha;
+    pa.bar = bar;
+    pa.err = err;
+    const size_t psm = (size_t)BW * R * 16;
+    CK(cudaFuncSetAttribute(k_panel_qr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+    {
+      void* args[] = {&pa};
+      CK(cudaLaunchCooperativeKernel((const void*)k_panel_qr, dim3(G), dim3(PQ_THREADS), args, psm, s));
+    }
+    // X = A22 V (split K), W, trailing update
+    const int nIm = (int)((m + 63) / 64);
+    k_symdiag<<<nIm, 256, 0, s>>>(A, N, k0, Dsym);
+    int S = (int)std::min<long long>(SMAX, std::max<long long>(1, (4LL * nsm + nIm - 1) / nIm));
+    S = std::min(S, nIm);
+    const int chunkJ = (nIm + S - 1) / S;
+    S = (nIm + chunkJ - 1) / chunkJ;
+    k_hemm2<<<dim3(nIm, S), 256, HM_SMEM, s>>>(A, N, k0, Dsym, Vp, nIm, chunkJ, Xpart);
+    k_xreduce<<<nIm, 256, XR_SMEM, s>>>(Xpart, S, N, k0, Tbuf + (size_t)pnl * 1024, Vp, Wp, Gpart);
+    k_mform<<<1, 1024, 0, s>>>(Gpart, nIm, Tbuf + (size_t)pnl * 1024, Mbuf);
+    k_wform<<<(int)((m + 7) / 8), 256, 0, s>>>(N, k0, Vp, Mbuf, Wp);
+    WTBG_COUNT(ctx, 6);
+    CKL("two-stage panel");
+    if (prof) cudaEventRecord(ev[2], s);
+    if (int r = launch_her2k_v(ctx, A, N, Wp, Vp, N, 0, nref, k0)) return r;
+    if (prof) {
+      cudaEventRecord(ev[3], s);
+      CK(cudaEventSynchronize(ev[3]));
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[2], ev[3]);
+      const double nt = (double)m;
+      ctx->stats.her2k_ms += t;
+      ctx->stats.her2k_flops += nt * (nt + 1.0) * 0.5 * 16.0 * (double)nref;
+      ctx->stats.her2k_launches += 1;
+    }
+  }
+  if (prof) {
+    cudaEventRecord(ev[1], s);
+    CK(cudaEventSynchronize(ev[1]));
+    float t = 0.f;
+    cudaEventElapsedTime(&t, ev[0], ev[1]);
+    ctx->stats.stage1_ms += t;
+    cudaEventRecord(ev[0], s);
+  }
+  // stage 2: band -> tridiagonal
+  double2* AB = ctx->t2AB.as<double2>();
+  unsigned int* prog = ctx->t2prog.as<unsigned int>();
+  k_band_extract<<<(unsigned)N, 128, 0, s>>>(A, N, AB);
+  CK(cudaMemsetAsync(prog, 0, (size_t)N * 4, s));
+  BulgeArgs ba;
+  ba.AB = AB;
+  ba.N = N;
+  ba.A = A;
+  ba.tau2 = ctx->tau.as<double2>();
+  ba.g = g;
+  ba.ng = ng;
+  ba.prog = prog;
+  ba.err = err;
+  ba.store = 1;
+  const size_t bsm = (size_t)BG_WARPS * (2 * BW * BG_LD + 2 * BW) * 16;
+  CK(cudaFuncSetAttribute(k_bulge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
+  int per = 1;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bulge, 32 * BG_WARPS, bsm));
+  const long long nsweep = N - 1;
+  const int gb = (int)std::max<long long>(1, std::min<long long>((long long)nsm * std::max(per, 1),
+                                                                  (nsweep + BG_WARPS - 1) / BG_WARPS));
+  {
+    void* args[] = {&ba};
+    CK(cudaLaunchCooperativeKernel((const void*)k_bulge, dim3(gb), dim3(32 * BG_WARPS), args, bsm, s));
+  }
+  k_band_to_tridiag<<<(int)((N + 255) / 256), 256, 0, s>>>(AB, N, ctx->d.as<double>(), ctx->e.as<double>());
+  WTBG_COUNT(ctx, 3);
+  CKL("two-stage bulge chasing");
+  if (prof) {
+    cudaEventRecord(ev[1], s);
+    CK(cudaEventSynchronize(ev[1]));
+    float t = 0.f;
+    cudaEventElapsedTime(&t, ev[0], ev[1]);
+    ctx->stats.stage2_ms += t;
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+  ctx->tri_two = true;
+  return 0;
+}
+
+// Exciton vectors through both stages: X <- Q1 (Q2 X), Q2 the bulge-chasing reflectors in
+// reverse, Q1 the panels' block reflectors in reverse.
+int run_backtransform2(wtbg_ctx* ctx, double2* X, int nvec) {
+  const long long N = ctx->N;
+  cudaStream_t s = ctx->stream;
+  const int nsm = ctx->nsm > 0 ? ctx->nsm : 148;
+  unsigned int* prog = ctx->t2prog.as<unsigned int>();
+  int* err = ctx->triErr.as<int>();
+  CK(cudaMemsetAsync(prog, 0, (size_t)N * 4, s));
+  CK(cudaMemsetAsync(err, 0, 4, s));
+  const long long nsweep = N - 1;
+  const int gb = (int)std::max<long long>(1, std::min<long long>(nsm, (nsweep + BG_WARPS - 1) / BG_WARPS));
+  {
+    const double2* A = ctx->H.as<double2>();
+    const double2* tau2 = ctx->tau.as<double2>();
+    long long NN = N;
+    void* args[] = {(void*)&A, (void*)&NN, (void*)&tau2, (void*)&X, (void*)&nvec, (void*)&prog, (void*)&err};
+    CK(cudaLaunchCooperativeKernel((const void*)k_bulge_back, dim3(gb), dim3(32 * BG_WARPS), args, 0, s));
+  }
+  const long long npan = (N - BW - 1 + BW - 1) / BW;
+  const int nbmax = (int)((N + BT1_RB - 1) / BT1_RB);
+  ENSURE(ctx->t2G, (size_t)nbmax * 1024 * 16 + 1024 * 16);
+  double2* part = ctx->t2G.as<double2>();
+  double2* Y = part + (size_t)nbmax * 1024;
+  for (long long pnl = npan - 1; pnl >= 0; --pnl) {
+    const int j0 = (int)(pnl * BW), k0 = j0 + BW;
+    const long long m = N - k0;
+    const int nref = (int)std::min<long long>(BW, m);
+    const int nb = (int)((m + BT1_RB - 1) / BT1_RB);
+    k_bt1_partial<<<nb, 256, 0, s>>>(ctx->H.as<double2>(), N, j0, k0, nref, X, nvec, part);
+    k_bt1_tmat<<<1, 1024, 0, s>>>(part, nb, nvec, ctx->t2T.as<double2>() + (size_t)pnl * 1024, Y);
+    k_bt1_apply<<<(int)((m + 255) / 256), 256, 0, s>>>(ctx->H.as<double2>(), N, j0, k0, nref, X, nvec, Y);
+  }
+  WTBG_COUNT(ctx, 1 + 3 * npan);
+  CKL("two-stage back-transform");
+  int herr = 0;
+  CK(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (herr) return set_err(ctx, WTBG_ERR_CUDA, "back-transform: a sweep wait timed out");
+  return 0;
+}

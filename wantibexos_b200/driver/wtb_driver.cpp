@@ -73,6 +73,19 @@ struct Deck {
   double ez = 1.0, w = 0.0, lc = 1.0, r0 = 1.0;
   double st = 0, phavg = 0, temp = 0;
   double ctemp = (double)298.15f, tmax = (double)5e-6f, eg = 0, egd = 0, egs = 0, ebgs = 0;
+  // keys of this implementation (the reference ignores unknown keys, so decks stay valid there):
+  // GPU_SOLVER= DENSE | DAVIDSON, GPU_PRECISION= FP64 | BF16X3 (alias FAST), GPU_NEV=, GPU_TOL= (eV),
+  // GPU_MAXIT=, GPU_HAYDOCK= (Lanczos steps of the fast spectrum), GPU_WARMSTART= (.npy network file)
+  std::string gpu_solver = "DENSE", gpu_precision = "FP64", gpu_warmstart;
+  int gpu_nev = 32, gpu_maxit = 400, gpu_haydock = 150;
+  double gpu_tol = 1e-6;
+};
+
+// what bsesolver leaves for the spectrum stage of the same run
+struct RunState {
+  bool fast = false;      // the fast form produced the exciton table (GPU_SOLVER= DAVIDSON, converged)
+  long long rows = 0;     // rows of bse_opt_diel.dat
+  double e1 = 0, emax = 0;
 };
 
 // one record split into list-directed character items (quotes keep blanks)
@@ -98,6 +111,11 @@ std::vector<std::string> items_of(const std::string& line) {
     i = j;
   }
   return out;
+}
+
+std::string upper(std::string s) {
+  for (char& c : s) c = (char)toupper(c);
+  return s;
 }
 
 double num(const std::string& s) {
@@ -217,7 +235,20 @@ Deck parse_deck(const std::string& text) {
     else if (a == "SHIFT_1=") d.mshift[0] = num(b);
     else if (a == "SHIFT_2=") d.mshift[1] = num(b);
     else if (a == "SHIFT_3=") d.mshift[2] = num(b);
+    else if (a == "GPU_SOLVER=") d.gpu_solver = upper(trunc(b, 10));
+    else if (a == "GPU_PRECISION=") d.gpu_precision = upper(trunc(b, 10));
+    else if (a == "GPU_NEV=") d.gpu_nev = (int)num(b);
+    else if (a == "GPU_TOL=") d.gpu_tol = num(b);
+    else if (a == "GPU_MAXIT=") d.gpu_maxit = (int)num(b);
+    else if (a == "GPU_HAYDOCK=") d.gpu_haydock = (int)num(b);
+    else if (a == "GPU_WARMSTART=") d.gpu_warmstart = trunc(b, 200);
   }
+  if (d.gpu_solver != "DENSE" && d.gpu_solver != "DAVIDSON") throw Stop("GPU_SOLVER= must be DENSE or DAVIDSON");
+  if (d.gpu_precision == "FAST") d.gpu_precision = "BF16X3";
+  if (d.gpu_precision != "FP64" && d.gpu_precision != "BF16X3")
+    throw Stop("GPU_PRECISION= must be FP64 or BF16X3 (FAST)");
+  if (d.gpu_nev < 1 || d.gpu_nev > 32) throw Stop("GPU_NEV= must be between 1 and 32");
+  if (!(d.gpu_tol > 0) || d.gpu_maxit < 1 || d.gpu_haydock < 2) throw Stop("bad GPU_TOL=, GPU_MAXIT= or GPU_HAYDOCK=");
   return d;
 }
 
@@ -702,7 +733,116 @@ void write_sp_tables(const Deck& d, int nk, long long N, const std::vector<float
   }
 }
 
-void bsesolver(wtbg_ctx* ctx, const Deck& d, const Model& m, Timings* tm) {
+// Network parameters of the learned warm start as saved by warmstart_sweep (--save FILE.npy):
+// a little-endian float32 .npy vector of wtbg_net_num_params() values.
+std::vector<float> read_npy_f32(const std::string& path, long long n) {
+  FILE* f = fopen(path.c_str(), "rb");
+  if (!f) throw Stop("Error opening GPU_WARMSTART file " + path);
+  unsigned char magic[8];
+  if (fread(magic, 1, 8, f) != 8 || memcmp(magic, "\x93NUMPY", 6) != 0) {
+    fclose(f);
+    throw Stop("GPU_WARMSTART file is not a .npy file");
+  }
+  size_t hlen = 0;
+  if (magic[6] == 1) {
+    unsigned char b[2];
+    if (fread(b, 1, 2, f) != 2) hlen = 0;
+    else hlen = b[0] | (b[1] << 8);
+  } else {
+    unsigned char b[4];
+    if (fread(b, 1, 4, f) != 4) hlen = 0;
+    else hlen = b[0] | (b[1] << 8) | (b[2] << 16) | ((size_t)b[3] << 24);
+  }
+  std::string hdr(hlen, ' ');
+  if (hlen == 0 || fread(&hdr[0], 1, hlen, f) != hlen || hdr.find("<f4") == std::string::npos ||
+      hdr.find("'fortran_order': False") == std::string::npos) {
+    fclose(f);
+    throw Stop("GPU_WARMSTART file must hold a C-ordered float32 vector");
+  }
+  std::vector<float> p((size_t)n);
+  const size_t got = fread(p.data(), 4, (size_t)n, f);
+  fclose(f);
+  if ((long long)got != n) throw Stop("GPU_WARMSTART file holds fewer values than the network has parameters");
+  return p;
+}
+
+// Start block of the fast form from the learned network: the 32 predicted vectors, then
+// nb - 32 fixed pseudo-random columns (glob = Q = 0, R_0, EDIEL_T as in the training sweep).
+std::vector<double> warm_start_block(wtbg_ctx* ctx, const Deck& d, long long N, int nb) {
+  std::vector<float> p = read_npy_f32(d.gpu_warmstart, wtbg_net_num_params());
+  wtbg_net* net = nullptr;
+  gpu_check(ctx, wtbg_net_create(ctx, &net, 1), "wtbg_net_create");
+  std::vector<double> X0(2 * (size_t)N * nb, 0.0);
+  const double glob[5] = {0.0, 0.0, 0.0, d.r0, d.ediel[0]};
+  int st = wtbg_net_set_params(net, p.data());
+  if (st == 0) st = wtbg_net_predict(net, glob, X0.data());
+  wtbg_net_destroy(net);
+  gpu_check(ctx, st, "wtbg_net_predict");
+  uint64_t x = 0x9E3779B97F4A7C15ull;
+  for (size_t i = 2 * (size_t)N * 32; i < X0.size(); ++i) {
+    x ^= x << 13;
+    x ^= x >> 7;
+    x ^= x << 17;
+    X0[i] = (double)(x >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+  }
+  return X0;
+}
+
+// The exciton solve of bsesolver.  GPU_SOLVER= DENSE (default): ZHEEV's role, every eigenpair
+// (wtbg_bse_solve).  GPU_SOLVER= DAVIDSON: the GPU_NEV lowest excitons by block Davidson to
+// residual GPU_TOL, with the split-BF16 tensor-core product under GPU_PRECISION= BF16X3, and the
+// highest exciton to 1e-3 eV for the broadening rule; if the Davidson run ends above GPU_TOL after
+// GPU_MAXIT iterations, or in the temperature form, the dense solve runs instead and the run
+// continues exactly as a dense run (logged in log_bse-diel.dat).
+RunState exciton_solve(wtbg_ctx* ctx, const Deck& d, long long N, bool temp, Out& log, std::vector<double>& W,
+                       std::vector<double>& act, std::vector<double>& Xfast) {
+  RunState rs;
+  rs.rows = N;
+  if (d.gpu_solver == "DAVIDSON") {
+    const int nev = (int)std::min<long long>(d.gpu_nev, N);
+    const int nb = std::min(40, ((nev + 8 + 7) / 8) * 8);
+    if (temp) {
+      log.line(" fast form: no temperature form; dense FP64 solve used");
+    } else if (N < 4LL * nb) {
+      log.line(" fast form: BSE dimension below four Davidson blocks; dense FP64 solve used");
+    } else {
+      gpu_check(ctx, wtbg_set_fast_product(ctx, d.gpu_precision == "BF16X3" ? 1 : 0), "wtbg_set_fast_product");
+      std::vector<double> X0;
+      if (!d.gpu_warmstart.empty()) X0 = warm_start_block(ctx, d, N, nb);
+      std::vector<double> w(nev), a(8 * (size_t)nev), X(d.bsewf ? 2 * (size_t)N * nev : 0);
+      int it = 0;
+      double mr = 0.0;
+      const int st = wtbg_bse_davidson(ctx, nev, nb, 0, d.gpu_maxit, d.gpu_tol, X0.empty() ? nullptr : X0.data(),
+                                       d.dtfull, d.cpol, w.data(), a.data(), d.bsewf ? X.data() : nullptr, &it, &mr);
+      if (st == WTBG_OK) {
+        double top = 0.0, mr2 = 0.0;
+        int it2 = 0;
+        const int st2 = wtbg_bse_davidson(ctx, 1, 8, 1, 300, 1e-3, nullptr, 0, 0, &top, nullptr, nullptr, &it2, &mr2);
+        if (st2 != WTBG_OK && st2 != WTBG_ERR_NOCONV) gpu_check(ctx, st2, "wtbg_bse_davidson (highest exciton)");
+        rs.fast = true;
+        rs.rows = nev;
+        rs.e1 = w[0];
+        rs.emax = top;
+        W = w;
+        act = a;
+        Xfast = X;
+        log.line(" fast form: lowest" + LI(nev) + " excitons by block Davidson," + LI(it) +
+                 " iterations, max residual" + LD(mr) + " eV");
+        return rs;
+      }
+      if (st != WTBG_ERR_NOCONV) gpu_check(ctx, st, "wtbg_bse_davidson");
+      log.line(" fast form: block Davidson stopped at max residual" + LD(mr) + " eV after" + LI(it) +
+               " iterations; dense FP64 solve used");
+    }
+    log.flush();
+  }
+  W.assign((size_t)N, 0.0);
+  act.assign(8 * (size_t)N, 0.0);
+  gpu_check(ctx, wtbg_bse_solve(ctx, d.dtfull, d.cpol, W.data(), act.data()), "wtbg_bse_solve");
+  return rs;
+}
+
+RunState bsesolver(wtbg_ctx* ctx, const Deck& d, const Model& m, Timings* tm) {
   const std::string of = d.outputfolder;
   Out log(join_path(of, "log_bse-diel.dat"), "Error opening log_bse-diel output file");
   Out f301(join_path(of, "bse_opt_diel.dat"), "Error opening bse_opt_diel output file");
@@ -719,6 +859,7 @@ void bsesolver(wtbg_ctx* ctx, const Deck& d, const Model& m, Timings* tm) {
   double t0 = now_s();
   const bool temp = d.bset && !d.bse;
   upload_model_temp(ctx, m, d, temp);
+  gpu_check(ctx, wtbg_set_precision(ctx, d.gpu_precision == "BF16X3" ? 1 : 0), "wtbg_set_precision");
   f301.line(" #  exciton energy  xx  yy  zz xy  xz  yz");
   f302.line(" #  exciton energy  xx  yy  zz sp  sm");
   const int nk = d.ngrid[0] * d.ngrid[1] * d.ngrid[2];
@@ -772,15 +913,33 @@ void bsesolver(wtbg_ctx* ctx, const Deck& d, const Model& m, Timings* tm) {
   log.flush();
   double t3 = now_s();
   if (tm) tm->build = t3 - t2;
-  std::vector<double> W(N), act(8 * (size_t)N);
-  gpu_check(ctx, wtbg_bse_solve(ctx, d.dtfull, d.cpol, W.data(), act.data()), "wtbg_bse_solve");
+  if (d.gpu_precision == "BF16X3") log.line(" GPU_PRECISION= BF16X3: split-BF16 tensor-core Fourier sums and overlaps");
+  std::vector<double> W, act, Xfast;
+  RunState rs = exciton_solve(ctx, d, N, temp, log, W, act, Xfast);
+  const long long rows = rs.rows;
   double t4 = now_s();
   if (tm) tm->solve = t4 - t3;
   if (d.bsewf) {
-    const int a0 = std::max(1, d.excwf0), a1 = std::min<long long>(d.excwff, N);
+    const int a0 = std::max(1, d.excwf0), a1 = (int)std::min<long long>(d.excwff, rows);
     if (a1 >= a0) {
       std::vector<double> A(2 * (size_t)N * (a1 - a0 + 1));
-      gpu_check(ctx, wtbg_bse_eigvecs(ctx, a0, a1, A.data()), "wtbg_bse_eigvecs");
+      if (rs.fast) {
+        for (int n = a0; n <= a1; ++n) {   // gauge of wtbg_bse_eigvecs: unit norm, last component real >= 0
+          const double* x = Xfast.data() + 2 * (size_t)N * (n - 1);
+          double* y = A.data() + 2 * (size_t)N * (n - a0);
+          double nrm = 0.0;
+          for (long long i = 0; i < N; ++i) nrm += x[2 * i] * x[2 * i] + x[2 * i + 1] * x[2 * i + 1];
+          const double lr = x[2 * (N - 1)], li = x[2 * (N - 1) + 1], r = std::hypot(lr, li);
+          const double cr = r > 0 ? lr / r : 1.0, ci = r > 0 ? -li / r : 0.0, sc = nrm > 0 ? 1.0 / std::sqrt(nrm) : 1.0;
+          for (long long i = 0; i < N; ++i) {
+            y[2 * i] = sc * (x[2 * i] * cr - x[2 * i + 1] * ci);
+            y[2 * i + 1] = sc * (x[2 * i] * ci + x[2 * i + 1] * cr);
+          }
+          y[2 * (N - 1) + 1] = 0.0;
+        }
+      } else {
+        gpu_check(ctx, wtbg_bse_eigvecs(ctx, a0, a1, A.data()), "wtbg_bse_eigvecs");
+      }
       for (int n = a0; n <= a1; ++n) {
         // excwf2 (bse_subs.f90:534-576)
         Out o(join_path(of, "exc_wf_" + std::to_string(n) + ".dat"), "Error opening wf BSE output file");
@@ -823,14 +982,15 @@ void bsesolver(wtbg_ctx* ctx, const Deck& d, const Model& m, Timings* tm) {
   log.flush();
   {
     std::string b301, b302;
-    b301.reserve(N * 106);
-    for (long long i = 0; i < N; ++i) {
+    b301.reserve(rows * 106);
+    for (long long i = 0; i < rows; ++i) {
       b301 += F(W[i], 15, 4);
-      for (int c = 0; c < 6; ++c) b301 += F(act[i + (size_t)N * c], 15, 4);
+      for (int c = 0; c < 6; ++c) b301 += F(act[i + (size_t)rows * c], 15, 4);
       b301 += "\n";
       if (d.cpol) {
-        b302 += F(W[i], 15, 4) + F(act[i], 15, 4) + F(act[i + (size_t)N], 15, 4) + F(act[i + 2 * (size_t)N], 15, 4) +
-                F(act[i + 6 * (size_t)N], 15, 4) + F(act[i + 7 * (size_t)N], 15, 4) + "\n";
+        b302 += F(W[i], 15, 4) + F(act[i], 15, 4) + F(act[i + (size_t)rows], 15, 4) +
+                F(act[i + 2 * (size_t)rows], 15, 4) + F(act[i + 6 * (size_t)rows], 15, 4) +
+                F(act[i + 7 * (size_t)rows], 15, 4) + "\n";
       }
     }
     fputs(b301.c_str(), f301.f);
@@ -842,6 +1002,7 @@ void bsesolver(wtbg_ctx* ctx, const Deck& d, const Model& m, Timings* tm) {
   if (f402) fclose(f402);
   if (f404) fclose(f404);
   if (tm) tm->write_opt = now_s() - t4;
+  return rs;
 }
 
 // ------------------------------------------------------------------------------ bsebnds
@@ -1437,6 +1598,7 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
     log.flush();
     int st = wtbg_create(&ctx, device);
     if (st != 0) return fail(std::string("wtbg_create: ") + wtbg_error_string(st));
+    RunState rs;
     if (!d.pponly) {
       if (d.bandscalc) {
         bandstool(ctx, d, m);
@@ -1454,11 +1616,11 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
         log.flush();
         throw Stop("ERROR: Choose BSE=T or BSET=T not both");
       } else if (d.bse) {
-        bsesolver(ctx, d, m, tm);
+        rs = bsesolver(ctx, d, m, tm);
         log.line(" BSE and Single particle dielectric calculation finished");
         log.flush();
       } else if (d.bset) {
-        bsesolver(ctx, d, m, tm);
+        rs = bsesolver(ctx, d, m, tm);
         log.line(" BSE and Single particle dielectric calculation, with temperature, finished");
         log.flush();
       }
@@ -1503,10 +1665,26 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
     const int N = nk * d.nc * d.nv;
     const std::string of = d.outputfolder;
     const bool bsex = d.bse || d.bset;
+    // the fast form's spectrum: Haydock recursion on the BSE matrix still on the device (all
+    // eight components at once; the -pol files take x, y, z, sp, sm = 0, 1, 2, 6, 7)
+    Spec sfast;
+    if (d.spec && bsex && rs.fast) {
+      sfast.nw = (int)d.numbse;
+      sfast.ncomp = 8;
+      sfast.om.resize(sfast.nw);
+      sfast.eps.resize((size_t)sfast.nw * 2 * 8);
+      std::string sty = m.systype;
+      while (!sty.empty() && sty.back() == ' ') sty.pop_back();
+      gpu_check(ctx, wtbg_bse_spectrum_fast(ctx, d.gpu_haydock, d.dtfull, d.cpol, rs.e1, rs.emax, d.ngrid,
+                                            vcell3d(m.rlat), d.ebse0, d.ebsef, d.numbse, d.cshift, d.renorm,
+                                            (sty == "NP") ? 2.0 : 1.0, sfast.om.data(), sfast.eps.data()),
+                "wtbg_bse_spectrum_fast");
+    }
+    const long long nrow = rs.fast ? rs.rows : (long long)N;
     if (d.spec && bsex) {
       // bsedielraw / bseoptprop / lifetime (wtb_main.f90:257-300; no lifetime after BSET)
-      Table t = read_table(of + "bse_opt_diel.dat", N, 7, "Error opening bse_opt_diel input file");
-      Spec s = run_spectrum(ctx, d, m, t, {1, 1, 1, 0, 0, 0});
+      Table t = read_table(of + "bse_opt_diel.dat", (int)nrow, 7, "Error opening bse_opt_diel input file");
+      Spec s = rs.fast ? sfast : run_spectrum(ctx, d, m, t, {1, 1, 1, 0, 0, 0});
       const char* nm[6] = {"xx", "yy", "zz", "xy", "xz", "yz"};
       for (int c = 0; c < 6; ++c) write_diel(of + "bse_diel_" + nm[c] + ".dat", s, c);
       if (tm) tm->spectrum = now_s() - t1;
@@ -1516,10 +1694,11 @@ extern "C" int wtb_run(const char* deck_text, int device, Timings* tm, char* err
       log.line(" BSE dielectric properties calculated");
       log.flush();
       if (d.cpol) {
-        Table tp = read_table(of + "bse_opt_diel-pol.dat", N, 6, "Error opening bse_opt_diel-pol input file");
-        Spec sp = run_spectrum(ctx, d, m, tp, {1, 1, 1, 1, 1});
+        Table tp = read_table(of + "bse_opt_diel-pol.dat", (int)nrow, 6, "Error opening bse_opt_diel-pol input file");
+        Spec sp = rs.fast ? sfast : run_spectrum(ctx, d, m, tp, {1, 1, 1, 1, 1});
         const char* pn[5] = {"x", "y", "z", "sp", "sm"};
-        for (int c = 0; c < 5; ++c) write_diel(of + "bse_diel-pol_" + pn[c] + ".dat", sp, c);
+        const int fast_col[5] = {0, 1, 2, 6, 7};
+        for (int c = 0; c < 5; ++c) write_diel(of + "bse_diel-pol_" + pn[c] + ".dat", sp, rs.fast ? fast_col[c] : c);
         optprop_files(of, "bse_", {"bse_diel-pol_x.dat", "bse_diel-pol_y.dat", "bse_diel-pol_z.dat",
                                    "bse_diel-pol_sp.dat", "bse_diel-pol_sm.dat"}, {0, 1, 2, 3, 4}, "-pol", sp.nw);
         if (!d.bset) lifetime_file(of, d, m, tp, true);

@@ -29,7 +29,8 @@ EXPORTS = ["wtbg_create", "wtbg_destroy", "wtbg_error_string", "wtbg_last_error"
            "wtbg_net_features", "wtbg_net_add_sample", "wtbg_net_num_samples", "wtbg_net_train",
            "wtbg_net_eval_loss", "wtbg_net_predict", "wtbg_net_loss_grad", "wtbg_gemm_bf16",
            "wtbg_bse_build_q", "wtbg_set_temperature", "wtbg_eigsys", "wtbg_dos",
-           "wtbg_bands_batch", "wtbg_bse_q_batch", "wtbg_set_precision", "wtbg_berry", "wtbg_sp_optbz"]
+           "wtbg_bands_batch", "wtbg_bse_q_batch", "wtbg_set_precision", "wtbg_berry", "wtbg_sp_optbz",
+           "wtbg_bse_lowest", "wtbg_set_reduction"]
 
 
 class WtbgError(RuntimeError):
@@ -44,7 +45,8 @@ class Stats(C.Structure):
                 ("build_bytes", C.c_double), ("fast_launches", C.c_longlong), ("fast_ms", C.c_double),
                 ("fast_bytes", C.c_double), ("dav_fast_iters", C.c_longlong), ("dav_fp64_iters", C.c_longlong),
                 ("her2k_launches", C.c_longlong), ("her2k_ms", C.c_double), ("her2k_flops", C.c_double),
-                ("tri_ms", C.c_double), ("tdsolve_ms", C.c_double)]
+                ("tri_ms", C.c_double), ("tdsolve_ms", C.c_double), ("dav_fallbacks", C.c_longlong),
+                ("stage1_ms", C.c_double), ("stage2_ms", C.c_double)]
 
 
 class Coulomb(C.Structure):
@@ -91,6 +93,9 @@ def load_library(path: str = LIB_PATH):
         "wtbg_reset_stats": (C.c_int, [P]),
         "wtbg_bse_davidson": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, dp, C.c_int, C.c_int,
                                         dp, dp, dp, ip, dp]),
+        "wtbg_set_reduction": (C.c_int, [P, C.c_int]),
+        "wtbg_bse_lowest": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_double, dp, C.c_int, C.c_int, dp, dp, dp,
+                                      ip, dp, ip]),
         "wtbg_bse_spectrum_fast": (C.c_int, [P, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, ip, C.c_double,
                                              C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
                                              dp, fp]),
@@ -281,6 +286,30 @@ class Context:
         if check or st not in (0, -4):
             self._check(st)
         return W, act, X, it.value, mr.value
+
+    def set_reduction(self, mode: int) -> None:
+        """0 automatic, 1 one-stage, 2 two-stage reduction for the dense solves."""
+        self._check(self.lib.wtbg_set_reduction(self.h, int(mode)))
+
+    def bse_lowest(self, nev: int, nb: int = 40, max_iter: int = 200, tol: float = 1e-6, X0=None,
+                   dtfull: bool = False, cpol: bool = False, want_act: bool = True, want_vectors: bool = False):
+        """The nev lowest excitons by block Davidson with the dense FP64 solve as fallback; returns
+        (W, act, X, iters, maxres, used_dense)."""
+        W = np.zeros(nev)
+        act = np.zeros((nev, 8), order="F") if want_act else None
+        X = np.zeros((self.N, nev), dtype=np.complex128, order="F") if want_vectors else None
+        x0 = None
+        if X0 is not None:
+            x0 = np.asfortranarray(np.asarray(X0, dtype=np.complex128))
+        it = C.c_int(0)
+        mr = C.c_double(0.0)
+        used = C.c_int(0)
+        self._check(self.lib.wtbg_bse_lowest(self.h, nev, nb, max_iter, float(tol),
+                                             x0.ctypes.data_as(C.POINTER(C.c_double)) if x0 is not None else None,
+                                             int(dtfull), int(cpol), _dp(W), _dp(act),
+                                             X.ctypes.data_as(C.POINTER(C.c_double)) if X is not None else None,
+                                             C.byref(it), C.byref(mr), C.byref(used)))
+        return W, act, X, it.value, mr.value, bool(used.value)
 
     def bse_spectrum_fast(self, nsteps, e1, emax, ngrid, vcell3d, ebse0, ebsef, numbse, sme, renorm, spinf,
                           dtfull=False, cpol=False):
