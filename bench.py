@@ -323,6 +323,16 @@ def solve_breakdown(st, nsteps):
     if not st["tri_ms"]:
         return None
     her2k_tf = st["her2k_flops"] / (st["her2k_ms"] / 1e3) / 1e12 if st["her2k_ms"] else None
+    if st.get("stage1_ms"):
+        hemm_tf = st["hemm_flops"] / (st["hemm_ms"] / 1e3) / 1e12 if st["hemm_ms"] else None
+        return {"reduction": "two-stage", "tridiagonalise": st["tri_ms"] / 1e3 / nsteps,
+                "stage1_dense_to_band": st["stage1_ms"] / 1e3 / nsteps,
+                "panel_qr": st["panel_ms"] / 1e3 / nsteps,
+                "hemm": st["hemm_ms"] / 1e3 / nsteps, "hemm_tflops": hemm_tf,
+                "her2k": st["her2k_ms"] / 1e3 / nsteps, "her2k_tflops": her2k_tf,
+                "stage1_other": (st["stage1_ms"] - st["panel_ms"] - st["hemm_ms"] - st["her2k_ms"]) / 1e3 / nsteps,
+                "stage2_band_to_tridiagonal": st["stage2_ms"] / 1e3 / nsteps,
+                "tridiagonal_solve": st["tdsolve_ms"] / 1e3 / nsteps}
     return {"tridiagonalise": st["tri_ms"] / 1e3 / nsteps, "hemv": st["hemv_ms"] / 1e3 / nsteps,
             "her2k": st["her2k_ms"] / 1e3 / nsteps,
             "column_kernels_and_gaps": (st["tri_ms"] - st["hemv_ms"] - st["her2k_ms"]) / 1e3 / nsteps,
@@ -383,6 +393,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", default="both", choices=["both", "plain", "fast"],
                     help="plain FP64 path (the headline), the fast form, or both (default)")
+    ap.add_argument("--reduction", default="auto", choices=["auto", "one", "two"],
+                    help="tridiagonal reduction of the dense solve: automatic (two-stage for N >= 2048), "
+                         "one-stage or two-stage")
     ap.add_argument("--device-only", action="store_true",
                     help="only the device-resident steps (no e2e run, no CPU baseline): profiling captures")
     args = ap.parse_args()
@@ -428,6 +441,7 @@ def main():
 
     wbuild.build()
     ctx = wtbgpu.Context(local)   # one replica per GPU (LOCAL_RANK)
+    ctx.set_reduction({"auto": 0, "one": 1, "two": 2}[args.reduction])
     ctx.set_model(model)
     kpt = kmesh(wl["n"], model.rlat)
     c = wtbgpu.coulomb_params("V2DRK", [wl["n"], wl["n"], 1], 1e-3, [1, 1, 1], 1.0, 1.0, 0.0, wl["r0"])

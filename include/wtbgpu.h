@@ -85,6 +85,9 @@ typedef struct wtbg_stats {
   long long dav_fallbacks;   /* wtbg_bse_lowest calls that fell back to the dense FP64 solve */
   double stage1_ms;          /* two-stage reduction: dense -> band (profiling) */
   double stage2_ms;          /* two-stage reduction: band -> tridiagonal (profiling) */
+  double panel_ms;           /* two-stage: panel QR (profiling) */
+  double hemm_ms;            /* two-stage: X = A22 V on the FP64 tensor cores (profiling) */
+  double hemm_flops;         /* algorithmic: 8 m^2 nref per panel */
 } wtbg_stats;
 int wtbg_set_profiling(wtbg_ctx* ctx, int on);
 int wtbg_get_stats(const wtbg_ctx* ctx, wtbg_stats* out);

@@ -44,11 +44,16 @@ def run(tmp_path, template, model, **kw):
 
 
 def rows(path):
+    """Numeric rows of an output file (header lines, with or without '#', skipped)."""
     out = []
     for line in open(path).read().splitlines():
         t = line.split()
-        if t and not t[0].startswith("#"):
+        if not t or t[0].startswith("#"):
+            continue
+        try:
             out.append([float(x) for x in t])
+        except ValueError:
+            continue
     return np.array(out)
 
 
@@ -108,7 +113,8 @@ def test_example3_bse_files(ex6):
         want = O.exclft("2D", ng, mos2.rlat, f, E)
         fin = np.isfinite(want)
         assert np.array_equal(fin, np.isfinite(lt[:, 1 + k])), k
-        assert fin.sum() == 0 or np.all(np.abs(lt[fin, 1 + k] - want[fin]) <= 1.2e-4 * np.abs(want[fin])), k
+        # E15.4 keeps four significant digits: relative rounding up to 5e-4
+        assert fin.sum() == 0 or np.all(np.abs(lt[fin, 1 + k] - want[fin]) <= 5.01e-4 * np.abs(want[fin])), k
 
 
 def test_example3_single_particle_table(ex6):

@@ -894,7 +894,7 @@ bool use_two_stage(wtbg_ctx* ctx) {
   if (ctx->tri_mode == 1) return false;
   if (!two_stage_fits(ctx, N)) return false;
   if (ctx->tri_mode == 2) return true;
-  return false;
+  return N >= 2048;
 }
 
 int run_tridiagonalise2(wtbg_ctx* ctx) {
@@ -950,12 +950,18 @@ int run_tridiagonalise2(wtbg_ctx* ctx) {
   }
   CK(cudaFuncSetAttribute(k_hemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HM_SMEM));
   CK(cudaFuncSetAttribute(k_xreduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XR_SMEM));
+  // profiling: event pairs around the panel QR, the Hermitian product and the rank-2k update
+  // of every panel (read after the reduction), and around each stage
   const bool prof = ctx->profiling != 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   if (prof) {
     for (auto& e : ev) CK(cudaEventCreate(&e));
+    if (int r = ensure_events(ctx, 6 * (size_t)std::max<long long>(npan, 1))) return r;
     cudaEventRecord(ev[0], s);
   }
+  auto mark = [&](long long pnl, int k) {
+    if (prof) cudaEventRecord(ctx->evpool[6 * pnl + k], s);
+  };
   for (long long pnl = 0; pnl < npan; ++pnl) {
     const int j0 = (int)(pnl * BW), k0 = j0 + BW;
     const long long m = N - k0;
@@ -984,10 +990,12 @@ int run_tridiagonalise2(wtbg_ctx* ctx) {
     pa.err = err;
     const size_t psm = (size_t)BW * R * 16;
     CK(cudaFuncSetAttribute(k_panel_qr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+    mark(pnl, 0);
     {
       void* args[] = {&pa};
       CK(cudaLaunchCooperativeKernel((const void*)k_panel_qr, dim3(G), dim3(PQ_THREADS), args, psm, s));
     }
+    mark(pnl, 1);
     // X = A22 V (split K), W, trailing update
     const int nIm = (int)((m + 63) / 64);
     k_symdiag<<<nIm, 256, 0, s>>>(A, N, k0, Dsym);
@@ -995,24 +1003,17 @@ int run_tridiagonalise2(wtbg_ctx* ctx) {
     S = std::min(S, nIm);
     const int chunkJ = (nIm + S - 1) / S;
     S = (nIm + chunkJ - 1) / chunkJ;
+    mark(pnl, 2);
     k_hemm2<<<dim3(nIm, S), 256, HM_SMEM, s>>>(A, N, k0, Dsym, Vp, nIm, chunkJ, Xpart);
+    mark(pnl, 3);
     k_xreduce<<<nIm, 256, XR_SMEM, s>>>(Xpart, S, N, k0, Tbuf + (size_t)pnl * 1024, Vp, Wp, Gpart);
     k_mform<<<1, 1024, 0, s>>>(Gpart, nIm, Tbuf + (size_t)pnl * 1024, Mbuf);
     k_wform<<<(int)((m + 7) / 8), 256, 0, s>>>(N, k0, Vp, Mbuf, Wp);
     WTBG_COUNT(ctx, 6);
     CKL("two-stage panel");
-    if (prof) cudaEventRecord(ev[2], s);
+    mark(pnl, 4);
     if (int r = launch_her2k_v(ctx, A, N, Wp, Vp, N, 0, nref, k0)) return r;
-    if (prof) {
-      cudaEventRecord(ev[3], s);
-      CK(cudaEventSynchronize(ev[3]));
-      float t = 0.f;
-      cudaEventElapsedTime(&t, ev[2], ev[3]);
-      const double nt = (double)m;
-      ctx->stats.her2k_ms += t;
-      ctx->stats.her2k_flops += nt * (nt + 1.0) * 0.5 * 16.0 * (double)nref;
-      ctx->stats.her2k_launches += 1;
-    }
+    mark(pnl, 5);
   }
   if (prof) {
     cudaEventRecord(ev[1], s);
@@ -1020,6 +1021,20 @@ int run_tridiagonalise2(wtbg_ctx* ctx) {
     float t = 0.f;
     cudaEventElapsedTime(&t, ev[0], ev[1]);
     ctx->stats.stage1_ms += t;
+    ctx->stats.tri_ms += t;
+    for (long long pnl = 0; pnl < npan; ++pnl) {
+      const double m = (double)(N - (pnl + 1) * BW), nref = std::min(m, (double)BW);
+      float a = 0.f, b = 0.f, c = 0.f;
+      cudaEventElapsedTime(&a, ctx->evpool[6 * pnl + 0], ctx->evpool[6 * pnl + 1]);
+      cudaEventElapsedTime(&b, ctx->evpool[6 * pnl + 2], ctx->evpool[6 * pnl + 3]);
+      cudaEventElapsedTime(&c, ctx->evpool[6 * pnl + 4], ctx->evpool[6 * pnl + 5]);
+      ctx->stats.panel_ms += a;
+      ctx->stats.hemm_ms += b;
+      ctx->stats.hemm_flops += 8.0 * m * m * nref;
+      ctx->stats.her2k_ms += c;
+      ctx->stats.her2k_flops += m * (m + 1.0) * 0.5 * 16.0 * nref;
+      ctx->stats.her2k_launches += 1;
+    }
     cudaEventRecord(ev[0], s);
   }
   // stage 2: band -> tridiagonal
@@ -1057,6 +1072,7 @@ int run_tridiagonalise2(wtbg_ctx* ctx) {
     float t = 0.f;
     cudaEventElapsedTime(&t, ev[0], ev[1]);
     ctx->stats.stage2_ms += t;
+    ctx->stats.tri_ms += t;
     for (auto& e : ev) cudaEventDestroy(e);
   }
   ctx->tri_two = true;

@@ -46,7 +46,8 @@ class Stats(C.Structure):
                 ("fast_bytes", C.c_double), ("dav_fast_iters", C.c_longlong), ("dav_fp64_iters", C.c_longlong),
                 ("her2k_launches", C.c_longlong), ("her2k_ms", C.c_double), ("her2k_flops", C.c_double),
                 ("tri_ms", C.c_double), ("tdsolve_ms", C.c_double), ("dav_fallbacks", C.c_longlong),
-                ("stage1_ms", C.c_double), ("stage2_ms", C.c_double)]
+                ("stage1_ms", C.c_double), ("stage2_ms", C.c_double), ("panel_ms", C.c_double),
+                ("hemm_ms", C.c_double), ("hemm_flops", C.c_double)]
 
 
 class Coulomb(C.Structure):
