@@ -576,6 +576,7 @@ __global__ void __launch_bounds__(256) k_wform(long long N, long long k0, const 
 constexpr int LDB = 2 * BW + 2;
 constexpr int BG_WARPS = 4;                 // sweep workers per CTA
 constexpr int BG_LD = BW + 1;               // padded row length of the per-warp work tiles
+constexpr int BG_WARP_TILE = 3 * BW * BG_LD + 2 * BW;   // Bs, Ds, B1s, v, w (double2) per warp
 
 __device__ __forceinline__ long long nsteps_of(long long N, long long s) { return (N - 1 - s + BW - 1) / BW; }
 // sum_{u=1}^{U} ceil(u / b)
@@ -611,18 +612,46 @@ struct BulgeArgs {
   int store;             // keep the reflectors for the eigenvector back-transform
 };
 
-// One step of sweep s (warp-wide; lane i <-> row r0 + i of the step's blocks).
-__device__ void bulge_step(const BulgeArgs& a, long long s, long long t, double2* Bs, double2* Ds, double2* vs,
-                           double2* ws) {
+// One step of sweep s (warp-wide; lane i <-> row r0 + i of the step's blocks).  All the
+// blocks the step reads (bulge block B_t, diagonal block D_t, block below B_{t+1}) are fetched
+// at once with cp.async into the warp's shared tiles, so the step pays one L2 round trip; the
+// dot products run with four independent partial sums per lane.
+__device__ __forceinline__ void cpa16(double2* dst, const double2* src, bool valid) {
+  const unsigned sh = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sh), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+
+__device__ void bulge_step(const BulgeArgs& a, long long s, long long t, double2* Bs, double2* Ds, double2* B1s,
+                           double2* vs, double2* ws) {
   const int lane = threadIdx.x & 31;
   const long long N = a.N;
   double2* AB = a.AB;
   const long long r0 = s + 1 + t * BW;
   const int L = (int)min((long long)BW, N - r0);
   const long long c0 = r0 - BW;   // first column of the bulge block (t >= 1)
-  // the column to annihilate: column s (t = 0) or column c0 of the bulge block
+  const long long r1 = r0 + L;
+  const int L1 = (r1 < N) ? (int)min((long long)BW, N - r1) : 0;
+  // ---- fetch
+  if (t > 0) {
+#pragma unroll 8
+    for (int q = 0; q < BW; ++q) cpa16(Bs + lane * BG_LD + q, AB + (c0 + q) * LDB + (BW + lane - q), lane < L);
+  }
+  for (int q = 0; q < L; ++q) {
+    const bool ok = lane >= q && lane < L;
+    cpa16(Ds + lane * BG_LD + q, ok ? AB + (r0 + q) * LDB + (lane - q) : AB, ok);
+  }
+  for (int q = 0; q < L; ++q) cpa16(B1s + lane * BG_LD + q, AB + (r0 + q) * LDB + (L + lane - q), lane < L1);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  double2 gv[NGMAX];
+#pragma unroll
+  for (int al2 = 0; al2 < NGMAX; ++al2)
+    gv[al2] = (al2 < a.ng && lane < L) ? __ldcg(a.g + (long long)al2 * N + r0 + lane) : make_double2(0, 0);
   double2 x = make_double2(0, 0);
-  if (lane < L) x = (t == 0) ? __ldcg(AB + s * LDB + 1 + lane) : __ldcg(AB + c0 * LDB + BW + lane);
+  if (t == 0 && lane < L) x = __ldcg(AB + s * LDB + 1 + lane);
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncwarp();
+  if (t > 0) x = Bs[lane * BG_LD];
+  // ---- reflector (ZLARFG)
   double xn2 = (lane >= 1 && lane < L) ? x.x * x.x + x.y * x.y : 0.0;
   xn2 = warp_sum(xn2);
   const double2 al = make_double2(__shfl_sync(0xffffffffu, x.x, 0), __shfl_sync(0xffffffffu, x.y, 0));
@@ -641,83 +670,107 @@ __device__ void bulge_step(const BulgeArgs& a, long long s, long long t, double2
   }
   const double2 v = (lane == 0) ? make_double2(1.0, 0.0) : (lane < L ? cmul(x, scal) : make_double2(0, 0));
   vs[lane] = v;
-  // annihilated column: (beta, 0, ..., 0)
+  // Hermitian fill of D (upper = conj of lower, real diagonal)
+  if (lane < L)
+    for (int q = 0; q <= lane; ++q) {
+      double2 d = Ds[lane * BG_LD + q];
+      if (q == lane) {
+        d.y = 0.0;
+        Ds[lane * BG_LD + q] = d;
+      } else {
+        Ds[q * BG_LD + lane] = cconj(d);
+      }
+    }
+  __syncwarp();
+  // ---- annihilated column and the left application to the rest of the bulge block
   if (lane < L) {
     const double2 nv = (lane == 0) ? make_double2(beta, 0.0) : make_double2(0, 0);
     if (t == 0) AB[s * LDB + 1 + lane] = nv;
     else AB[c0 * LDB + BW + lane] = nv;
   }
-  __syncwarp();
   if (t > 0) {
-    // left application to the other columns of the bulge block: B <- H^H B
-    for (int q = 1; q < BW; ++q) {
-      const long long o = BW + lane - q;
-      Bs[lane * BG_LD + q] = (lane < L) ? __ldcg(AB + (c0 + q) * LDB + o) : make_double2(0, 0);
-    }
-    __syncwarp();
     if (lane >= 1) {   // w_q = sum_i conj(v_i) B(i, q), lane q
-      double2 w = make_double2(0, 0);
-      for (int i = 0; i < L; ++i) w = cadd(w, cmulc(vs[i], Bs[i * BG_LD + lane]));
-      ws[lane] = w;
+      double2 w0 = make_double2(0, 0), w1 = w0, w2 = w0, w3 = w0;
+      for (int i = 0; i < L; i += 4) {
+        w0 = cadd(w0, cmulc(vs[i], Bs[i * BG_LD + lane]));
+        if (i + 1 < L) w1 = cadd(w1, cmulc(vs[i + 1], Bs[(i + 1) * BG_LD + lane]));
+        if (i + 2 < L) w2 = cadd(w2, cmulc(vs[i + 2], Bs[(i + 2) * BG_LD + lane]));
+        if (i + 3 < L) w3 = cadd(w3, cmulc(vs[i + 3], Bs[(i + 3) * BG_LD + lane]));
+      }
+      ws[lane] = cadd(cadd(w0, w1), cadd(w2, w3));
     }
     __syncwarp();
     if (lane < L) {
       const double2 cv = cmul(cconj(tau), v);
-      for (int q = 1; q < BW; ++q) {
-        const double2 b = csub(Bs[lane * BG_LD + q], cmul(cv, ws[q]));
-        AB[(c0 + q) * LDB + (BW + lane - q)] = b;
-      }
+#pragma unroll 4
+      for (int q = 1; q < BW; ++q)
+        AB[(c0 + q) * LDB + (BW + lane - q)] = csub(Bs[lane * BG_LD + q], cmul(cv, ws[q]));
     }
     __syncwarp();
   }
-  // two-sided update of the diagonal block D (rows/cols r0 .. r0+L-1): D <- H^H D H
-  for (int q = 0; q < L; ++q) {
-    if (lane >= q && lane < L) {
-      double2 d = __ldcg(AB + (r0 + q) * LDB + (lane - q));
-      if (lane == q) d.y = 0.0;
-      Ds[lane * BG_LD + q] = d;
-      Ds[q * BG_LD + lane] = cconj(d);
+  // ---- two-sided update of D: D <- H^H D H
+  double2 y = make_double2(0, 0);
+  if (lane < L) {
+    double2 y1 = y, y2 = y, y3 = y;
+    for (int q = 0; q < L; q += 4) {
+      y = cadd(y, cmul(Ds[lane * BG_LD + q], vs[q]));
+      if (q + 1 < L) y1 = cadd(y1, cmul(Ds[lane * BG_LD + q + 1], vs[q + 1]));
+      if (q + 2 < L) y2 = cadd(y2, cmul(Ds[lane * BG_LD + q + 2], vs[q + 2]));
+      if (q + 3 < L) y3 = cadd(y3, cmul(Ds[lane * BG_LD + q + 3], vs[q + 3]));
+    }
+    y = cadd(cadd(y, y1), cadd(y2, y3));
+  }
+  // v^H y (real for Hermitian D) and, interleaved, v^T g of the velocity vectors
+  double pvx = cmulc(v, y).x;
+  double2 sg[NGMAX];
+#pragma unroll
+  for (int al2 = 0; al2 < NGMAX; ++al2) sg[al2] = cmul(v, gv[al2]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    pvx += __shfl_xor_sync(0xffffffffu, pvx, o);
+#pragma unroll
+    for (int al2 = 0; al2 < NGMAX; ++al2) {
+      if (al2 < a.ng) {
+        sg[al2].x += __shfl_xor_sync(0xffffffffu, sg[al2].x, o);
+        sg[al2].y += __shfl_xor_sync(0xffffffffu, sg[al2].y, o);
+      }
     }
   }
-  __syncwarp();
-  double2 y = make_double2(0, 0);
-  if (lane < L)
-    for (int q = 0; q < L; ++q) y = cadd(y, cmul(Ds[lane * BG_LD + q], vs[q]));
-  double2 pv = cmulc(v, y);   // v^H y (real for Hermitian D)
-  pv = warp_sum2(pv);
   const double t2 = tau.x * tau.x + tau.y * tau.y;
-  const double2 w = csub(cmul(tau, y), cscale(v, 0.5 * t2 * pv.x));
+  const double2 w = csub(cmul(tau, y), cscale(v, 0.5 * t2 * pvx));
   ws[lane] = w;
   __syncwarp();
   if (lane < L)
+#pragma unroll 4
     for (int q = 0; q <= lane; ++q) {
       double2 d = csub(Ds[lane * BG_LD + q], cadd(cmulc(ws[q], v), cmulc(vs[q], w)));   // v_i conj(w_q) + w_i conj(v_q)
       if (q == lane) d.y = 0.0;
       AB[(r0 + q) * LDB + (lane - q)] = d;
     }
-  // right application to the block below: B1 <- B1 H (rows r1 .. r1+L1-1, cols r0 .. r0+L-1)
-  const long long r1 = r0 + L;
-  if (r1 < N) {
-    const int L1 = (int)min((long long)BW, N - r1);
-    __syncwarp();
-    for (int q = 0; q < L; ++q)
-      Bs[lane * BG_LD + q] = (lane < L1) ? __ldcg(AB + (r0 + q) * LDB + (L + lane - q)) : make_double2(0, 0);
-    __syncwarp();
+  // ---- right application to the block below: B1 <- B1 H
+  if (L1 > 0) {
     double2 z = make_double2(0, 0);
-    if (lane < L1)
-      for (int q = 0; q < L; ++q) z = cadd(z, cmul(Bs[lane * BG_LD + q], vs[q]));
     if (lane < L1) {
+      double2 z1 = z, z2 = z, z3 = z;
+      for (int q = 0; q < L; q += 4) {
+        z = cadd(z, cmul(B1s[lane * BG_LD + q], vs[q]));
+        if (q + 1 < L) z1 = cadd(z1, cmul(B1s[lane * BG_LD + q + 1], vs[q + 1]));
+        if (q + 2 < L) z2 = cadd(z2, cmul(B1s[lane * BG_LD + q + 2], vs[q + 2]));
+        if (q + 3 < L) z3 = cadd(z3, cmul(B1s[lane * BG_LD + q + 3], vs[q + 3]));
+      }
+      z = cadd(cadd(z, z1), cadd(z2, z3));
       const double2 tz = cmul(tau, z);
+#pragma unroll 4
       for (int q = 0; q < L; ++q)
-        AB[(r0 + q) * LDB + (L + lane - q)] = csub(Bs[lane * BG_LD + q], cmul(tz, cconj(vs[q])));
+        AB[(r0 + q) * LDB + (L + lane - q)] = csub(B1s[lane * BG_LD + q], cmul(tz, cconj(vs[q])));
     }
   }
-  // velocity vectors: g <- g - tau conj(v) (v^T g)
-  for (int al2 = 0; al2 < a.ng; ++al2) {
-    double2* gp = a.g + (long long)al2 * N + r0;
-    const double2 gv = (lane < L) ? __ldcg(gp + lane) : make_double2(0, 0);
-    double2 sg = warp_sum2(cmul(v, gv));
-    if (lane < L) gp[lane] = csub(gv, cmul(tau, cmul(cconj(v), sg)));
+  // ---- velocity vectors: g <- g - tau conj(v) (v^T g)
+  if (lane < L) {
+    const double2 tcv = cmul(tau, cconj(v));
+#pragma unroll
+    for (int al2 = 0; al2 < NGMAX; ++al2)
+      if (al2 < a.ng) a.g[(long long)al2 * N + r0 + lane] = csub(gv[al2], cmul(tcv, sg[al2]));
   }
   if (a.store) {
     if (lane < L) a.A[(r0 + lane - s - 1) + (N - 1 - s) * N] = v;
@@ -727,13 +780,16 @@ __device__ void bulge_step(const BulgeArgs& a, long long s, long long t, double2
 }
 
 // Persistent bulge chasing: warp w of the grid runs sweeps w, w + W, w + 2W, ...; sweep s
-// starts step t after sweep s-1 has published step t+3 (or finished).
+// starts step t after sweep s-1 has published step t+2 (or finished): the elements of step t
+// of sweep s have rows and columns <= s + 1 + (t+2) b, those of step t+3 of sweep s-1 rows
+// >= s + (t+3) b + 1, so the two never touch the same element (nor the same rows of g).
 __global__ void __launch_bounds__(32 * BG_WARPS, 1) k_bulge(BulgeArgs a) {
   extern __shared__ __align__(16) double2 bsm[];
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double2* Bs = bsm + (size_t)wid * (2 * BW * BG_LD + 2 * BW);
+  double2* Bs = bsm + (size_t)wid * BG_WARP_TILE;
   double2* Ds = Bs + BW * BG_LD;
-  double2* vs = Ds + BW * BG_LD;
+  double2* B1s = Ds + BW * BG_LD;
+  double2* vs = B1s + BW * BG_LD;
   double2* ws = vs + BW;
   const long long W = (long long)gridDim.x * BG_WARPS;
   const long long N = a.N;
@@ -742,7 +798,7 @@ __global__ void __launch_bounds__(32 * BG_WARPS, 1) k_bulge(BulgeArgs a) {
     const long long nprev = (s > 0) ? nsteps_of(N, s - 1) : 0;
     for (long long t = 0; t < ns; ++t) {
       if (s > 0) {
-        const unsigned int need = (unsigned int)min(t + 4, nprev);
+        const unsigned int need = (unsigned int)min(t + 3, nprev);
         int bad = 0;
         if (lane == 0) {
           const unsigned long long t0 = globaltimer();
@@ -757,7 +813,7 @@ __global__ void __launch_bounds__(32 * BG_WARPS, 1) k_bulge(BulgeArgs a) {
         bad = __shfl_sync(0xffffffffu, bad, 0);
         if (bad) return;
       }
-      bulge_step(a, s, t, Bs, Ds, vs, ws);
+      bulge_step(a, s, t, Bs, Ds, B1s, vs, ws);
       __threadfence();
       __syncwarp();
       if (lane == 0) st_release(a.prog + s, (unsigned int)(t + 1));
@@ -1052,7 +1108,7 @@ int run_tridiagonalise2(wtbg_ctx* ctx) {
   ba.prog = prog;
   ba.err = err;
   ba.store = 1;
-  const size_t bsm = (size_t)BG_WARPS * (2 * BW * BG_LD + 2 * BW) * 16;
+  const size_t bsm = (size_t)BG_WARPS * BG_WARP_TILE * 16;
   CK(cudaFuncSetAttribute(k_bulge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
   int per = 1;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bulge, 32 * BG_WARPS, bsm));
