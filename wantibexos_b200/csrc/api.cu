@@ -150,7 +150,7 @@ int wtbg_destroy(wtbg_ctx* ctx) {
                     &ctx->yv, &ctx->lam, &ctx->ws, &ctx->act, &ctx->zsel, &ctx->csz, &ctx->sp_in, &ctx->sp_out,
                     &ctx->sp_om, &ctx->tmp, &ctx->tmp2, &ctx->istat, &ctx->pOpA, &ctx->pOpB,
                     &ctx->pHk, &ctx->pOc, &ctx->pOv, &ctx->pErr, &ctx->triErr, &ctx->gwork,
-                    &ctx->t2V, &ctx->t2X, &ctx->t2D, &ctx->t2G, &ctx->t2T, &ctx->t2P, &ctx->t2AB, &ctx->t2prog};
+                    &ctx->t2V, &ctx->t2X, &ctx->t2D, &ctx->t2G, &ctx->t2T, &ctx->t2P, &ctx->t2AB, &ctx->t2prog, &ctx->t2de};
   for (DevBuf* b : bufs) free_buf(*b);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
   if (ctx->tri_exec) cudaGraphExecDestroy(ctx->tri_exec);
@@ -939,12 +939,80 @@ static int tridiagonalise_graph(wtbg_ctx* ctx) {
   return 0;
 }
 
+// Q points of the two-stage path in groups of up to kQGroup: stage 1 of each Q into its own band
+// slot (the N x N matrix buffer is reused), one bulge-chasing launch for the group's bands, then
+// the eigenvalues of each tridiagonal form.  ms_q gets the group's device time divided evenly.
+constexpr int kQGroup = 64;
+static int q_group_two_stage(wtbg_ctx* ctx, int nk, int g0, int gn, const double* kptq, const double* q4,
+                             const wtbg_coulomb* p, double* W, double* ms_q) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int r = 0;
+  long long N = 0;
+  const bool hv = ctx->have_velocity;
+  cudaEventRecord(e0, ctx->stream);
+  for (int i = 0; i < gn && !r; ++i) {
+    const int iq = g0 + i;
+    if ((r = wtbg_bse_build_q(ctx, nk, kptq + (size_t)iq * nk * 3, q4 + (size_t)iq * 4, p))) break;
+    if (i == 0) {
+      N = ctx->N;
+      if ((r = two_stage_group_begin(ctx, gn))) break;
+    }
+    ctx->have_velocity = false;
+    r = two_stage_group_add(ctx, i);
+    ctx->have_velocity = hv;
+  }
+  double* dd = nullptr;
+  double* ee = nullptr;
+  if (!r) r = two_stage_group_finish(ctx, gn, &dd, &ee);
+  for (int i = 0; i < gn && !r; ++i) {
+    cudaError_t ce = cudaMemcpyAsync(ctx->d.p, dd + (size_t)i * N, (size_t)N * 8, cudaMemcpyDeviceToDevice, ctx->stream);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpyAsync(ctx->e.p, ee + (size_t)i * N, (size_t)N * 8, cudaMemcpyDeviceToDevice, ctx->stream);
+    if (ce != cudaSuccess) {
+      r = cuda_fail(ctx, ce, "Q group: tridiagonal copy");
+      break;
+    }
+    if ((r = run_tridiagonal_solve(ctx, 0, 0, false))) break;
+    memcpy(W + (size_t)(g0 + i) * N, ctx->lam_host.data(), (size_t)N * 8);
+  }
+  if (!r) {
+    cudaEventRecord(e1, ctx->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms_q)
+      for (int i = 0; i < gn; ++i) ms_q[g0 + i] = ms / gn;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return r;
+}
+
 int wtbg_bse_q_batch(wtbg_ctx* ctx, int nk, int nq, const double* kptq, const double* q4, const wtbg_coulomb* p,
                      int use_graph, double* W, double* ms_q) {
   if (!ctx || !kptq || !q4 || !p || !W || nq < 0) return WTBG_ERR_ARG;
   if (nq == 0) return WTBG_OK;
+  if (!ctx->have_bands) return set_err(ctx, WTBG_ERR_STATE, "bse_q_batch: call wtbg_bands first");
   const bool hv = ctx->have_velocity;
   int r = 0;
+  {
+    // the reduction is decided by N = nk nc nv, the same for every Q
+    const long long N0 = ctx->N;
+    ctx->N = (long long)nk * ctx->nc * ctx->nv;
+    const bool two = use_two_stage(ctx);
+    ctx->N = N0;
+    if (two) {
+      for (int g0 = 0; g0 < nq && !r; g0 += kQGroup)
+        r = q_group_two_stage(ctx, nk, g0, std::min(kQGroup, nq - g0), kptq, q4, p, W, ms_q);
+      ctx->have_velocity = hv;
+      ctx->have_matrix = false;
+      ctx->fast_ready = false;
+      ctx->have_solution = false;
+      return r ? r : WTBG_OK;
+    }
+  }
   for (int iq = 0; iq < nq && !r; ++iq) {
     if ((r = wtbg_bse_build_q(ctx, nk, kptq + (size_t)iq * nk * 3, q4 + (size_t)iq * 4, p))) break;
     const double ms_build = ctx->last_ms;

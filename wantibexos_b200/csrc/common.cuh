@@ -98,7 +98,7 @@ struct wtbg_ctx {
   // two-stage reduction (tridiag2.cu): mode 0 auto, 1 one-stage, 2 two-stage; which one ran last
   int tri_mode = 0;
   bool tri_two = false;
-  DevBuf t2V, t2X, t2D, t2G, t2T, t2P, t2AB, t2prog;
+  DevBuf t2V, t2X, t2D, t2G, t2T, t2P, t2AB, t2prog, t2de;
   cudaGraphExec_t tri_exec = nullptr;
   std::vector<const void*> tri_sig;
   long long tri_launches = 0;
@@ -216,6 +216,9 @@ int launch_dos(wtbg_ctx* ctx, const double* d_etb, const double* d_w, long long 
                int nw, double sme, long long nkpt, double* d_out);
 int autotune_hemv(wtbg_ctx* ctx, int* hs_out);
 int run_backtransform2(wtbg_ctx* ctx, double2* X, int nvec);
+int two_stage_group_begin(wtbg_ctx* ctx, int nq);
+int two_stage_group_add(wtbg_ctx* ctx, int slot);
+int two_stage_group_finish(wtbg_ctx* ctx, int nq, double** dd, double** ee);
 bool use_two_stage(wtbg_ctx* ctx);
 // C^T (N x M, ldc) (+)= A (M x K, lda) B (N x K, ldb)^T, bf16 operands, FP32 accumulation on the
 // tensor cores (tcgen05); err is a device flag set when a pipeline wait times out

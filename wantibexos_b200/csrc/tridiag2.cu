@@ -610,6 +610,9 @@ struct BulgeArgs {
   unsigned int* prog;    // [N] steps published per sweep
   int* err;
   int store;             // keep the reflectors for the eigenvector back-transform
+  int nprob;             // independent bands chased in one launch (eigenvalues only when > 1)
+  long long ab_stride;   // elements between consecutive bands in AB
+  long long prog_stride; // entries between consecutive progress arrays
 };
 
 // One step of sweep s (warp-wide; lane i <-> row r0 + i of the step's blocks).  All the
@@ -793,7 +796,15 @@ __global__ void __launch_bounds__(32 * BG_WARPS, 1) k_bulge(BulgeArgs a) {
   double2* ws = vs + BW;
   const long long W = (long long)gridDim.x * BG_WARPS;
   const long long N = a.N;
-  for (long long s = (long long)blockIdx.x * BG_WARPS + wid; s < N - 1; s += W) {
+  const long long np = a.nprob;
+  // sweep u of the launch = sweep s = u / np of band q = u % np: sweeps are taken in increasing
+  // u, and a sweep waits only on sweep s-1 of its own band (index u - np), so every wait is on a
+  // sweep that some resident warp has already started or finished
+  for (long long u = (long long)blockIdx.x * BG_WARPS + wid; u < np * (N - 1); u += W) {
+    const long long q = u % np, s = u / np;
+    BulgeArgs b = a;
+    b.AB = a.AB + q * a.ab_stride;
+    unsigned int* prog = a.prog + q * a.prog_stride;
     const long long ns = nsteps_of(N, s);
     const long long nprev = (s > 0) ? nsteps_of(N, s - 1) : 0;
     for (long long t = 0; t < ns; ++t) {
@@ -802,7 +813,7 @@ __global__ void __launch_bounds__(32 * BG_WARPS, 1) k_bulge(BulgeArgs a) {
         int bad = 0;
         if (lane == 0) {
           const unsigned long long t0 = globaltimer();
-          while (ld_acquire(a.prog + s - 1) < need) {
+          while (ld_acquire(prog + s - 1) < need) {
             if (ld_acquire(reinterpret_cast<unsigned int*>(a.err)) != 0u || globaltimer() - t0 > kWaitNs) {
               atomicExch(a.err, 1);
               bad = 1;
@@ -813,10 +824,10 @@ __global__ void __launch_bounds__(32 * BG_WARPS, 1) k_bulge(BulgeArgs a) {
         bad = __shfl_sync(0xffffffffu, bad, 0);
         if (bad) return;
       }
-      bulge_step(a, s, t, Bs, Ds, B1s, vs, ws);
+      bulge_step(b, s, t, Bs, Ds, B1s, vs, ws);
       __threadfence();
       __syncwarp();
-      if (lane == 0) st_release(a.prog + s, (unsigned int)(t + 1));
+      if (lane == 0) st_release(prog + s, (unsigned int)(t + 1));
     }
   }
 }
@@ -953,28 +964,37 @@ bool use_two_stage(wtbg_ctx* ctx) {
   return N >= 2048;
 }
 
-int run_tridiagonalise2(wtbg_ctx* ctx) {
+// Work buffers of the two-stage reduction for N (nband bands side by side for Q groups).
+static int two_stage_buffers(wtbg_ctx* ctx, int nband) {
   const long long N = ctx->N;
-  cudaStream_t s = ctx->stream;
   const int nsm = ctx->nsm > 0 ? ctx->nsm : 148;
-  const long long npan = (N - BW - 1 + BW - 1) / BW;   // panels j0 = 0, 32, ... with j0 + 32 < N - 1
+  const long long npan = (N - BW - 1 + BW - 1) / BW;
   const long long nI = (N + 63) / 64;
-  const int SMAX = 8;
   ENSURE(ctx->d, (size_t)N * 8);
   ENSURE(ctx->e, (size_t)N * 8);
   ENSURE(ctx->g, (size_t)N * 16 * NGMAX);
   ENSURE(ctx->Wp, (size_t)N * 16 * BW);
   ENSURE(ctx->t2V, (size_t)N * 16 * BW);
-  ENSURE(ctx->t2X, (size_t)SMAX * BW * N * 16);
+  ENSURE(ctx->t2X, (size_t)8 * BW * N * 16);
   ENSURE(ctx->t2D, (size_t)nI * 64 * 64 * 16);
   ENSURE(ctx->t2G, (size_t)nI * 1024 * 16 + 1024 * 16);
   ENSURE(ctx->t2T, (size_t)std::max<long long>(npan, 1) * 1024 * 16);
   ENSURE(ctx->t2P, (size_t)nsm * (16 + 16 * BW + 16 * BW * BW + 16 * BW * NGMAX) + 4096);
-  ENSURE(ctx->t2AB, (size_t)N * LDB * 16);
-  const long long ntau = ceil_sum(N - 1);
-  ENSURE(ctx->tau, (size_t)std::max<long long>(ntau, 1) * 16);
-  ENSURE(ctx->t2prog, (size_t)N * 4 + 64);
+  ENSURE(ctx->t2AB, (size_t)nband * N * LDB * 16);
+  ENSURE(ctx->t2prog, (size_t)nband * N * 4 + 64);
   ENSURE(ctx->triErr, 16);
+  return 0;
+}
+
+// Stage 1 (dense -> band) of the context's matrix; the band goes to slot `band` of ctx->t2AB.
+// ng velocity vectors in ctx->g follow the reflectors.
+static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
+  const long long N = ctx->N;
+  cudaStream_t s = ctx->stream;
+  const int nsm = ctx->nsm > 0 ? ctx->nsm : 148;
+  const long long npan = (N - BW - 1 + BW - 1) / BW;
+  const long long nI = (N + 63) / 64;
+  const int SMAX = 8;
   double2* A = ctx->H.as<double2>();
   double2* g = ctx->g.as<double2>();
   double2* Vp = ctx->t2V.as<double2>();
@@ -992,24 +1012,13 @@ int run_tridiagonalise2(wtbg_ctx* ctx) {
   double2* alpha = partVg + (size_t)nsm * BW * NGMAX;
   GridBar* bar = reinterpret_cast<GridBar*>(alpha + 2);
   int* err = ctx->triErr.as<int>();
-  CK(cudaMemsetAsync(err, 0, 4, s));
   CK(cudaMemsetAsync(bar, 0, sizeof(GridBar), s));
-  // velocity vectors g (as the one-stage reduction)
-  const int ng = ctx->have_velocity ? (ctx->temp_on ? 10 : 5) : 0;
-  ctx->ng = ctx->have_velocity ? ng : 5;
-  if (ctx->have_velocity && ctx->temp_on) {
-    if (int r = fill_g_vectors(ctx, g)) return r;
-  } else if (ctx->have_velocity) {
-    CK(cudaMemcpyAsync(g, ctx->h.p, (size_t)N * 16 * 5, cudaMemcpyDeviceToDevice, s));
-  } else {
-    CK(cudaMemsetAsync(g, 0, (size_t)N * 16 * 5, s));
-  }
   CK(cudaFuncSetAttribute(k_hemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HM_SMEM));
   CK(cudaFuncSetAttribute(k_xreduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XR_SMEM));
   // profiling: event pairs around the panel QR, the Hermitian product and the rank-2k update
-  // of every panel (read after the reduction), and around each stage
+  // of every panel (read after the stage), and around the stage
   const bool prof = ctx->profiling != 0;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
   if (prof) {
     for (auto& e : ev) CK(cudaEventCreate(&e));
     if (int r = ensure_events(ctx, 6 * (size_t)std::max<long long>(npan, 1))) return r;
@@ -1071,6 +1080,9 @@ int run_tridiagonalise2(wtbg_ctx* ctx) {
     if (int r = launch_her2k_v(ctx, A, N, Wp, Vp, N, 0, nref, k0)) return r;
     mark(pnl, 5);
   }
+  k_band_extract<<<(unsigned)N, 128, 0, s>>>(A, N, ctx->t2AB.as<double2>() + (size_t)band * N * LDB);
+  WTBG_COUNT(ctx, 1);
+  CKL("k_band_extract");
   if (prof) {
     cudaEventRecord(ev[1], s);
     CK(cudaEventSynchronize(ev[1]));
@@ -1091,36 +1103,58 @@ int run_tridiagonalise2(wtbg_ctx* ctx) {
       ctx->stats.her2k_flops += m * (m + 1.0) * 0.5 * 16.0 * nref;
       ctx->stats.her2k_launches += 1;
     }
-    cudaEventRecord(ev[0], s);
+    for (auto& e : ev) cudaEventDestroy(e);
   }
-  // stage 2: band -> tridiagonal
+  return 0;
+}
+
+// Stage 2 (band -> tridiagonal) of nband bands of ctx->t2AB in one persistent launch; the
+// tridiagonal forms go to dd/ee ([nband][N] each).  With store (one band only; ctx->tau must
+// hold ceil_sum(N-1) entries) the ng velocity vectors follow the reflectors and the reflectors
+// are kept for the eigenvector back-transform; without, only the band is reduced.
+static int run_stage2(wtbg_ctx* ctx, int nband, int ng, bool store, double* dd, double* ee) {
+  if (store && (nband != 1 || ctx->tau.bytes < (size_t)std::max<long long>(ceil_sum(ctx->N - 1), 1) * 16))
+    return set_err(ctx, WTBG_ERR_STATE, "two-stage: reflector storage not sized");
+  const long long N = ctx->N;
+  cudaStream_t s = ctx->stream;
+  const int nsm = ctx->nsm > 0 ? ctx->nsm : 148;
   double2* AB = ctx->t2AB.as<double2>();
   unsigned int* prog = ctx->t2prog.as<unsigned int>();
-  k_band_extract<<<(unsigned)N, 128, 0, s>>>(A, N, AB);
-  CK(cudaMemsetAsync(prog, 0, (size_t)N * 4, s));
+  const bool prof = ctx->profiling != 0;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  if (prof) {
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    cudaEventRecord(ev[0], s);
+  }
+  CK(cudaMemsetAsync(prog, 0, (size_t)nband * N * 4, s));
   BulgeArgs ba;
   ba.AB = AB;
   ba.N = N;
-  ba.A = A;
+  ba.A = ctx->H.as<double2>();
   ba.tau2 = ctx->tau.as<double2>();
-  ba.g = g;
-  ba.ng = ng;
+  ba.g = ctx->g.as<double2>();
+  ba.ng = store ? ng : 0;
   ba.prog = prog;
-  ba.err = err;
-  ba.store = 1;
+  ba.err = ctx->triErr.as<int>();
+  ba.store = store ? 1 : 0;
+  ba.nprob = nband;
+  ba.ab_stride = N * LDB;
+  ba.prog_stride = N;
   const size_t bsm = (size_t)BG_WARPS * BG_WARP_TILE * 16;
   CK(cudaFuncSetAttribute(k_bulge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
   int per = 1;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bulge, 32 * BG_WARPS, bsm));
-  const long long nsweep = N - 1;
+  const long long nsweep = (long long)nband * (N - 1);
   const int gb = (int)std::max<long long>(1, std::min<long long>((long long)nsm * std::max(per, 1),
                                                                   (nsweep + BG_WARPS - 1) / BG_WARPS));
   {
     void* args[] = {&ba};
     CK(cudaLaunchCooperativeKernel((const void*)k_bulge, dim3(gb), dim3(32 * BG_WARPS), args, bsm, s));
   }
-  k_band_to_tridiag<<<(int)((N + 255) / 256), 256, 0, s>>>(AB, N, ctx->d.as<double>(), ctx->e.as<double>());
-  WTBG_COUNT(ctx, 3);
+  for (int q = 0; q < nband; ++q)
+    k_band_to_tridiag<<<(int)((N + 255) / 256), 256, 0, s>>>(AB + (size_t)q * N * LDB, N, dd + (size_t)q * N,
+                                                              ee + (size_t)q * N);
+  WTBG_COUNT(ctx, 1 + nband);
   CKL("two-stage bulge chasing");
   if (prof) {
     cudaEventRecord(ev[1], s);
@@ -1131,7 +1165,48 @@ int run_tridiagonalise2(wtbg_ctx* ctx) {
     ctx->stats.tri_ms += t;
     for (auto& e : ev) cudaEventDestroy(e);
   }
+  return 0;
+}
+
+int run_tridiagonalise2(wtbg_ctx* ctx) {
+  const long long N = ctx->N;
+  cudaStream_t s = ctx->stream;
+  if (int r = two_stage_buffers(ctx, 1)) return r;
+  ENSURE(ctx->tau, (size_t)std::max<long long>(ceil_sum(N - 1), 1) * 16);
+  CK(cudaMemsetAsync(ctx->triErr.p, 0, 4, s));
+  double2* g = ctx->g.as<double2>();
+  // velocity vectors g (as the one-stage reduction)
+  const int ng = ctx->have_velocity ? (ctx->temp_on ? 10 : 5) : 0;
+  ctx->ng = ctx->have_velocity ? ng : 5;
+  if (ctx->have_velocity && ctx->temp_on) {
+    if (int r = fill_g_vectors(ctx, g)) return r;
+  } else if (ctx->have_velocity) {
+    CK(cudaMemcpyAsync(g, ctx->h.p, (size_t)N * 16 * 5, cudaMemcpyDeviceToDevice, s));
+  } else {
+    CK(cudaMemsetAsync(g, 0, (size_t)N * 16 * 5, s));
+  }
+  if (int r = run_stage1(ctx, ng, 0)) return r;
+  if (int r = run_stage2(ctx, 1, ng, true, ctx->d.as<double>(), ctx->e.as<double>())) return r;
   ctx->tri_two = true;
+  return 0;
+}
+
+// Q groups of the exciton band structure (eigenvalues only): group_begin sizes the work
+// buffers for nq bands, group_add runs stage 1 of the matrix just built into band slot i, and
+// group_finish chases all nq bands in one persistent launch; the tridiagonal forms of the group
+// land in dd/ee ([nq][N] each).
+int two_stage_group_begin(wtbg_ctx* ctx, int nq) {
+  if (int r = two_stage_buffers(ctx, nq)) return r;
+  ENSURE(ctx->t2de, (size_t)2 * nq * ctx->N * 8);
+  CK(cudaMemsetAsync(ctx->triErr.p, 0, 4, ctx->stream));
+  return 0;
+}
+int two_stage_group_add(wtbg_ctx* ctx, int slot) { return run_stage1(ctx, 0, slot); }
+int two_stage_group_finish(wtbg_ctx* ctx, int nq, double** dd, double** ee) {
+  *dd = ctx->t2de.as<double>();
+  *ee = *dd + (size_t)nq * ctx->N;
+  if (int r = run_stage2(ctx, nq, 0, false, *dd, *ee)) return r;
+  ctx->tri_two = false;   // no reflectors kept: exciton vectors need a wtbg_bse_solve
   return 0;
 }
 
