@@ -458,7 +458,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", default="both", choices=["both", "plain", "fast"],
                     help="plain FP64 path (the headline), the fast form, or both (default)")
-    ap.add_argument("--reduction", default="auto", choices=["auto", "one", "two"],
+    ap.add_argument("--reduction", default="auto", choices=["auto", "one", "two", "two-warp"],
                     help="tridiagonal reduction of the dense solve: automatic (two-stage for N >= 2048), "
                          "one-stage or two-stage")
     ap.add_argument("--device-only", action="store_true",
@@ -512,7 +512,7 @@ def main():
 
     wbuild.build()
     ctx = wtbgpu.Context(local)   # one replica per GPU (LOCAL_RANK)
-    ctx.set_reduction({"auto": 0, "one": 1, "two": 2}[args.reduction])
+    ctx.set_reduction({"auto": 0, "one": 1, "two": 2, "two-warp": 3}[args.reduction])
     ctx.set_model(model)
     kpt = kmesh(wl["n"], model.rlat)
     c = wtbgpu.coulomb_params("V2DRK", [wl["n"], wl["n"], 1], 1e-3, [1, 1, 1], 1.0, 1.0, 0.0, wl["r0"])

@@ -97,7 +97,8 @@ int wtbg_reset_stats(wtbg_ctx* ctx);
  * two-stage reduction, dense -> band of width 32 on the FP64 tensor cores -> tridiagonal by
  * bulge chasing, for N >= 2048 where its panels fit on the device; else one-stage),
  * 1 = one-stage (blocked Householder with a Hermitian mat-vec per column), 2 = two-stage
- * wherever it fits.  Both give the tridiagonal form of ZHETRD('L') up to rounding; the eigenvalues,
+ * wherever it fits, 3 = as 2 with the bulge chasing run one warp per sweep instead of one CTA
+ * of four warps per sweep (for comparison).  Both give the tridiagonal form of ZHETRD('L') up to rounding; the eigenvalues,
  * oscillator strengths and vectors agree within the tolerances of the dense path.  No counterpart
  * in the reference (its ZHEEV is MKL's). */
 int wtbg_set_reduction(wtbg_ctx* ctx, int mode);

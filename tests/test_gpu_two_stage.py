@@ -42,12 +42,13 @@ def run(ctx, m, deck, ref, mode):
     return W, act, A
 
 
-@pytest.mark.parametrize("n", [12, 11, 9])
-def test_two_stage_matches_one_stage_and_oracle(n, gpu_ctx):
+@pytest.mark.parametrize("n,mode", [(12, 2), (11, 2), (9, 2), (12, 3), (9, 3)])
+def test_two_stage_matches_one_stage_and_oracle(n, mode, gpu_ctx):
+    """mode 2: bulge chasing one CTA of four warps per sweep; mode 3: one warp per sweep."""
     m = synth.config_model("c1")
     deck = parse_deck(DECK.format(n=n, extra=""))
     ref = O.run_bse(m, deck)
-    W2, act2, A2 = run(gpu_ctx, m, deck, ref, 2)
+    W2, act2, A2 = run(gpu_ctx, m, deck, ref, mode)
     W1, act1, A1 = run(gpu_ctx, m, deck, ref, 1)
     assert np.abs(W2 - ref["W"]).max() < 1e-9
     assert np.abs(W2 - W1).max() < 1e-9

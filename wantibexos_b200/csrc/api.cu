@@ -76,8 +76,9 @@ int check_gemm_err(wtbg_ctx* ctx) {
 extern "C" {
 
 int wtbg_set_reduction(wtbg_ctx* ctx, int mode) {
-  if (!ctx || mode < 0 || mode > 2) return WTBG_ERR_ARG;
-  ctx->tri_mode = mode;
+  if (!ctx || mode < 0 || mode > 3) return WTBG_ERR_ARG;
+  ctx->tri_mode = (mode == 3) ? 2 : mode;
+  ctx->bulge_warp_mode = (mode == 3) ? 1 : 0;
   return WTBG_OK;
 }
 

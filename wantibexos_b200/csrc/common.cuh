@@ -98,6 +98,7 @@ struct wtbg_ctx {
   // two-stage reduction (tridiag2.cu): mode 0 auto, 1 one-stage, 2 two-stage; which one ran last
   int tri_mode = 0;
   bool tri_two = false;
+  int bulge_warp_mode = 0;   // stage 2: 0 = one CTA of four warps per sweep, 1 = one warp per sweep
   DevBuf t2V, t2X, t2D, t2G, t2T, t2P, t2AB, t2prog, t2de;
   cudaGraphExec_t tri_exec = nullptr;
   std::vector<const void*> tri_sig;

@@ -119,10 +119,10 @@ struct PanelArgs {
   double2* g;          // [ng][N]
   int ng;
   double* partN;       // [grid]
-  double2* partW;      // [grid][32]
+  double2* partW;      // [2][grid][32] partial norms (column p) and unscaled dots, by parity of p
   double2* partG;      // [grid][32*32]
   double2* partVg;     // [grid][32*NGMAX]
-  double2* alpha;      // [1] diagonal element of the current column
+  double2* alpha;      // [2][32] posted row k0 + p (alpha = its column-p entry), by parity of p
   GridBar* bar;
   int* err;
 };
@@ -135,7 +135,6 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
   __shared__ double2 s_w[BW];
   __shared__ double2 s_scal;
   __shared__ double s_beta;
-  __shared__ double s_red[PQ_THREADS / 32];
   __shared__ double2 s_T[BW * BW];
   __shared__ double2 s_y[BW * NGMAX];
   const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
@@ -151,102 +150,87 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
       P[(size_t)q * R + i] = (i < nr) ? a.A[(rbeg + i) + (long long)(a.j0 + q) * N] : make_double2(0, 0);
   __syncthreads();
 
-  // norm partial of column p over the own rows below row k0 + p; the owner of row k0 + p
-  // posts the diagonal element alpha
-  auto norm_partial = [&](int p) {
+  // Partials of column p over the own rows below row k0 + p, one reduction for both the norm
+  // and the unscaled dot products: S_q = sum_{r > k0+p} conj(P[r,p]) P[r,q] for q = p .. jb-1
+  // (S_p = |x|^2).  The owner of row k0 + p posts that row (alpha = P[k0+p, p] and P[k0+p, q]).
+  // Buffers alternate with the parity of p: a CTA writes the partials of column p+1 while others
+  // may still read those of p, but never those of p+2 before everyone passed the barrier of p+1.
+  auto partials = [&](int p) {
     const long long rp = (long long)a.k0 + p;
-    double t = 0.0;
-    for (int i = tid; i < nr; i += PQ_THREADS)
-      if (rbeg + i > rp) {
-        const double2 x = P[(size_t)p * R + i];
-        t += x.x * x.x + x.y * x.y;
-      }
-    t = warp_sum(t);
-    if (lane == 0) s_red[wp] = t;
-    __syncthreads();
-    if (tid == 0) {
-      double s = 0.0;
-      for (int k = 0; k < NW; ++k) s += s_red[k];
-      a.partN[blockIdx.x] = s;
-      if (rp >= rbeg && rp < rend) *a.alpha = P[(size_t)p * R + (rp - rbeg)];
+    const int buf = p & 1;
+    for (int q = p + wp; q < jb; q += NW) {
+      double2 sacc = make_double2(0, 0);
+      for (int i = lane; i < nr; i += 32)
+        if (rbeg + i > rp) sacc = cadd(sacc, cmulc(P[(size_t)p * R + i], P[(size_t)q * R + i]));
+      sacc = warp_sum2(sacc);
+      if (lane == 0) a.partW[((size_t)buf * G + blockIdx.x) * BW + q] = sacc;
     }
+    if (rp >= rbeg && rp < rend)
+      for (int q = p + tid; q < jb; q += PQ_THREADS) a.alpha[buf * BW + q] = P[(size_t)q * R + (rp - rbeg)];
   };
 
-  norm_partial(0);
+  partials(0);
   for (int p = 0; p < a.nref; ++p) {
     if (!grid_barrier(a.bar, a.err)) return;
     const long long rp = (long long)a.k0 + p;
-    if (wp == 0) {
-      double xn2 = 0.0;
-      for (int c = lane; c < G; c += 32) xn2 += __ldcg(a.partN + c);
-      xn2 = warp_sum(xn2);
-      if (lane == 0) {
-        const double2 al = ldcg2(a.alpha);
-        double2 tau, scal;
-        double beta;
-        if (xn2 == 0.0 && al.y == 0.0) {
-          tau = make_double2(0, 0);
-          scal = make_double2(0, 0);
-          beta = al.x;
-        } else {
-          beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xn2), al.x);
-          tau = make_double2((beta - al.x) / beta, -al.y / beta);
-          const double2 den = make_double2(al.x - beta, al.y);
-          const double dd = den.x * den.x + den.y * den.y;
-          scal = make_double2(den.x / dd, -den.y / dd);
-        }
-        s_tau[p] = tau;
-        s_scal = scal;
-        s_beta = beta;
-      }
+    const int buf = p & 1;
+    const int nq = jb - p;   // columns p .. jb-1
+    for (int qq = wp; qq < nq; qq += NW) {
+      const int q = p + qq;
+      double2 sacc = make_double2(0, 0);
+      for (int c = lane; c < G; c += 32) sacc = cadd(sacc, ldcg2(a.partW + ((size_t)buf * G + c) * BW + q));
+      sacc = warp_sum2(sacc);
+      if (lane == 0) s_w[q] = sacc;
     }
+    __syncthreads();
+    if (tid == 0) {
+      const double xn2 = s_w[p].x;
+      const double2 al = ldcg2(a.alpha + buf * BW + p);
+      double2 tau, scal;
+      double beta;
+      if (xn2 == 0.0 && al.y == 0.0) {
+        tau = make_double2(0, 0);
+        scal = make_double2(0, 0);
+        beta = al.x;
+      } else {
+        beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xn2), al.x);
+        tau = make_double2((beta - al.x) / beta, -al.y / beta);
+        const double2 den = make_double2(al.x - beta, al.y);
+        const double dd = den.x * den.x + den.y * den.y;
+        scal = make_double2(den.x / dd, -den.y / dd);
+      }
+      s_tau[p] = tau;
+      s_scal = scal;
+      s_beta = beta;
+    }
+    __syncthreads();
+    // w_q = sum_{r >= k0+p} conj(v_r) P[r,q] = P[k0+p, q] + conj(scal) S_q   (q > p)
+    if (tid > p && tid < jb) s_w[tid] = cadd(ldcg2(a.alpha + buf * BW + tid), cmul(cconj(s_scal), s_w[tid]));
     __syncthreads();
     {
       const double2 scal = s_scal;
-      const double beta = s_beta;
+      const double2 ct = cconj(s_tau[p]);
+      const int nu = jb - p - 1;
       for (int i = tid; i < nr; i += PQ_THREADS) {
         const long long r = rbeg + i;
-        if (r > rp) P[(size_t)p * R + i] = cmul(P[(size_t)p * R + i], scal);
-        else if (r == rp) P[(size_t)p * R + i] = make_double2(beta, 0.0);
-      }
-    }
-    __syncthreads();
-    // partial dots w_q = sum_{r >= k0+p} conj(v_r) P[r, q] for q = p+1 .. jb-1: one warp per q
-    const int nq = jb - p - 1;
-    for (int qq = wp; qq < nq; qq += NW) {
-      const int q = p + 1 + qq;
-      double2 s = make_double2(0, 0);
-      for (int i = lane; i < nr; i += 32) {
-        const long long r = rbeg + i;
         if (r < rp) continue;
-        const double2 v = (r == rp) ? make_double2(1.0, 0.0) : P[(size_t)p * R + i];
-        s = cadd(s, cmulc(v, P[(size_t)q * R + i]));
-      }
-      s = warp_sum2(s);
-      if (lane == 0) a.partW[(size_t)blockIdx.x * BW + q] = s;
-    }
-    if (!grid_barrier(a.bar, a.err)) return;
-    for (int qq = wp; qq < nq; qq += NW) {
-      const int q = p + 1 + qq;
-      double2 s = make_double2(0, 0);
-      for (int c = lane; c < G; c += 32) s = cadd(s, ldcg2(a.partW + (size_t)c * BW + q));
-      s = warp_sum2(s);
-      if (lane == 0) s_w[q] = s;
-    }
-    __syncthreads();
-    {
-      // P[r, q] -= conj(tau) v_r w_q
-      const double2 ct = cconj(s_tau[p]);
-      for (int it = tid; it < nq * nr; it += PQ_THREADS) {
-        const int i = it % nr, q = p + 1 + it / nr;
-        const long long r = rbeg + i;
-        if (r < rp) continue;
-        const double2 v = (r == rp) ? make_double2(1.0, 0.0) : P[(size_t)p * R + i];
-        P[(size_t)q * R + i] = csub(P[(size_t)q * R + i], cmul(ct, cmul(v, s_w[q])));
+        double2 v;
+        if (r == rp) {
+          v = make_double2(1.0, 0.0);
+          P[(size_t)p * R + i] = make_double2(s_beta, 0.0);
+        } else {
+          v = cmul(P[(size_t)p * R + i], scal);
+          P[(size_t)p * R + i] = v;
+        }
+        const double2 cv = cmul(ct, v);
+        for (int u = 0; u < nu; ++u) {
+          const int q = p + 1 + u;
+          P[(size_t)q * R + i] = csub(P[(size_t)q * R + i], cmul(cv, s_w[q]));
+        }
       }
     }
     __syncthreads();
-    if (p + 1 < a.nref) norm_partial(p + 1);
+    if (p + 1 < a.nref) partials(p + 1);
   }
   __syncthreads();
   // write back: A keeps R (rows <= k0+q) and v below; Vp gets V with its unit and zeros
@@ -832,6 +816,222 @@ __global__ void __launch_bounds__(32 * BG_WARPS, 1) k_bulge(BulgeArgs a) {
   }
 }
 
+// Stage 2 with one CTA of four warps per sweep.  After the fetch (all 128 threads) warp 0
+// forms the reflector while warp 2 completes the Hermitian diagonal block; then the four updates,
+// which need only v and tau, run concurrently: warp 0 the annihilated column, the velocity
+// vectors and the stored reflector, warp 1 the left application to the bulge block, warp 2 the
+// two-sided update of the diagonal block, warp 3 the right application to the block below.
+constexpr int B4_THREADS = 128;
+constexpr int B4_TILE = 3 * BW * BG_LD + 4 * BW + 8;   // Bs, Ds, B1s, v, w1, w2, scalars (double2)
+constexpr size_t B4_SMEM = (size_t)B4_TILE * 16;
+
+__device__ void bulge_step4(const BulgeArgs& a, long long s, long long t, double2* sm) {
+  double2* Bs = sm;
+  double2* Ds = Bs + BW * BG_LD;
+  double2* B1s = Ds + BW * BG_LD;
+  double2* vs = B1s + BW * BG_LD;
+  double2* w1 = vs + BW;
+  double2* w2 = w1 + BW;
+  double2* sc = w2 + BW;   // [0] tau, [1] (beta, 0)
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const long long N = a.N;
+  double2* AB = a.AB;
+  const long long r0 = s + 1 + t * BW;
+  const int L = (int)min((long long)BW, N - r0);
+  const long long c0 = r0 - BW;
+  const long long r1 = r0 + L;
+  const int L1 = (r1 < N) ? (int)min((long long)BW, N - r1) : 0;
+  // ---- fetch (element e of each tile: row e % 32, column e / 32)
+  if (t > 0)
+    for (int e = tid; e < BW * BW; e += B4_THREADS) {
+      const int i = e & 31, q = e >> 5;
+      cpa16(Bs + i * BG_LD + q, AB + (c0 + q) * LDB + (BW + i - q), i < L);
+    }
+  for (int e = tid; e < BW * BW; e += B4_THREADS) {
+    const int i = e & 31, q = e >> 5;
+    if (q < L) {
+      const bool ok = i >= q && i < L;
+      cpa16(Ds + i * BG_LD + q, ok ? AB + (r0 + q) * LDB + (i - q) : AB, ok);
+      cpa16(B1s + i * BG_LD + q, AB + (r0 + q) * LDB + (L + i - q), i < L1);
+    }
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  double2 gv[NGMAX];
+  if (wid == 0) {
+#pragma unroll
+    for (int al2 = 0; al2 < NGMAX; ++al2)
+      gv[al2] = (al2 < a.ng && lane < L) ? __ldcg(a.g + (long long)al2 * N + r0 + lane) : make_double2(0, 0);
+  }
+  double2 x = make_double2(0, 0);
+  if (wid == 0 && t == 0 && lane < L) x = __ldcg(AB + s * LDB + 1 + lane);
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncthreads();
+  // ---- reflector (warp 0) | Hermitian fill of D (warp 2)
+  if (wid == 0) {
+    if (t > 0) x = Bs[lane * BG_LD];
+    double xn2 = (lane >= 1 && lane < L) ? x.x * x.x + x.y * x.y : 0.0;
+    xn2 = warp_sum(xn2);
+    const double2 al = make_double2(__shfl_sync(0xffffffffu, x.x, 0), __shfl_sync(0xffffffffu, x.y, 0));
+    double2 tau, scal;
+    double beta;
+    if (xn2 == 0.0 && al.y == 0.0) {
+      tau = make_double2(0, 0);
+      scal = make_double2(0, 0);
+      beta = al.x;
+    } else {
+      beta = -copysign(sqrt(al.x * al.x + al.y * al.y + xn2), al.x);
+      tau = make_double2((beta - al.x) / beta, -al.y / beta);
+      const double2 den = make_double2(al.x - beta, al.y);
+      const double dd = den.x * den.x + den.y * den.y;
+      scal = make_double2(den.x / dd, -den.y / dd);
+    }
+    vs[lane] = (lane == 0) ? make_double2(1.0, 0.0) : (lane < L ? cmul(x, scal) : make_double2(0, 0));
+    if (lane == 0) {
+      sc[0] = tau;
+      sc[1] = make_double2(beta, 0.0);
+    }
+  } else if (wid == 2 && lane < L) {
+    for (int q = 0; q <= lane; ++q) {
+      double2 d = Ds[lane * BG_LD + q];
+      if (q == lane) {
+        d.y = 0.0;
+        Ds[lane * BG_LD + q] = d;
+      } else {
+        Ds[q * BG_LD + lane] = cconj(d);
+      }
+    }
+  }
+  __syncthreads();
+  const double2 tau = sc[0];
+  const double2 v = vs[lane];
+  if (wid == 0) {
+    // annihilated column, velocity vectors, stored reflector
+    if (lane < L) {
+      const double2 nv = (lane == 0) ? sc[1] : make_double2(0, 0);
+      if (t == 0) AB[s * LDB + 1 + lane] = nv;
+      else AB[c0 * LDB + BW + lane] = nv;
+    }
+    double2 sg[NGMAX];
+#pragma unroll
+    for (int al2 = 0; al2 < NGMAX; ++al2) sg[al2] = cmul(v, gv[al2]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int al2 = 0; al2 < NGMAX; ++al2)
+        if (al2 < a.ng) {
+          sg[al2].x += __shfl_xor_sync(0xffffffffu, sg[al2].x, o);
+          sg[al2].y += __shfl_xor_sync(0xffffffffu, sg[al2].y, o);
+        }
+    if (lane < L) {
+      const double2 tcv = cmul(tau, cconj(v));
+#pragma unroll
+      for (int al2 = 0; al2 < NGMAX; ++al2)
+        if (al2 < a.ng) a.g[(long long)al2 * N + r0 + lane] = csub(gv[al2], cmul(tcv, sg[al2]));
+      if (a.store) a.A[(r0 + lane - s - 1) + (N - 1 - s) * N] = v;
+    }
+    if (a.store && lane == 0) a.tau2[tau2_offset(N, s) + t] = tau;
+  } else if (wid == 1) {
+    // left application to the bulge block: B <- H^H B (columns 1..31)
+    if (t > 0) {
+      if (lane >= 1) {
+        double2 a0 = make_double2(0, 0), a1 = a0, a2 = a0, a3 = a0;
+        for (int i = 0; i < L; i += 4) {
+          a0 = cadd(a0, cmulc(vs[i], Bs[i * BG_LD + lane]));
+          if (i + 1 < L) a1 = cadd(a1, cmulc(vs[i + 1], Bs[(i + 1) * BG_LD + lane]));
+          if (i + 2 < L) a2 = cadd(a2, cmulc(vs[i + 2], Bs[(i + 2) * BG_LD + lane]));
+          if (i + 3 < L) a3 = cadd(a3, cmulc(vs[i + 3], Bs[(i + 3) * BG_LD + lane]));
+        }
+        w1[lane] = cadd(cadd(a0, a1), cadd(a2, a3));
+      }
+      __syncwarp();
+      if (lane < L) {
+        const double2 cv = cmul(cconj(tau), v);
+#pragma unroll 4
+        for (int q = 1; q < BW; ++q) AB[(c0 + q) * LDB + (BW + lane - q)] = csub(Bs[lane * BG_LD + q], cmul(cv, w1[q]));
+      }
+    }
+  } else if (wid == 2) {
+    // two-sided update of the diagonal block: D <- H^H D H
+    double2 y = make_double2(0, 0);
+    if (lane < L) {
+      double2 y1 = y, y2 = y, y3 = y;
+      for (int q = 0; q < L; q += 4) {
+        y = cadd(y, cmul(Ds[lane * BG_LD + q], vs[q]));
+        if (q + 1 < L) y1 = cadd(y1, cmul(Ds[lane * BG_LD + q + 1], vs[q + 1]));
+        if (q + 2 < L) y2 = cadd(y2, cmul(Ds[lane * BG_LD + q + 2], vs[q + 2]));
+        if (q + 3 < L) y3 = cadd(y3, cmul(Ds[lane * BG_LD + q + 3], vs[q + 3]));
+      }
+      y = cadd(cadd(y, y1), cadd(y2, y3));
+    }
+    const double pv = warp_sum(cmulc(v, y).x);
+    const double t2 = tau.x * tau.x + tau.y * tau.y;
+    const double2 w = csub(cmul(tau, y), cscale(v, 0.5 * t2 * pv));
+    w2[lane] = w;
+    __syncwarp();
+    if (lane < L)
+#pragma unroll 4
+      for (int q = 0; q <= lane; ++q) {
+        double2 d = csub(Ds[lane * BG_LD + q], cadd(cmulc(w2[q], v), cmulc(vs[q], w)));
+        if (q == lane) d.y = 0.0;
+        AB[(r0 + q) * LDB + (lane - q)] = d;
+      }
+  } else if (L1 > 0 && lane < L1) {
+    // right application to the block below: B1 <- B1 H
+    double2 z = make_double2(0, 0), z1 = z, z2 = z, z3 = z;
+    for (int q = 0; q < L; q += 4) {
+      z = cadd(z, cmul(B1s[lane * BG_LD + q], vs[q]));
+      if (q + 1 < L) z1 = cadd(z1, cmul(B1s[lane * BG_LD + q + 1], vs[q + 1]));
+      if (q + 2 < L) z2 = cadd(z2, cmul(B1s[lane * BG_LD + q + 2], vs[q + 2]));
+      if (q + 3 < L) z3 = cadd(z3, cmul(B1s[lane * BG_LD + q + 3], vs[q + 3]));
+    }
+    z = cadd(cadd(z, z1), cadd(z2, z3));
+    const double2 tz = cmul(tau, z);
+#pragma unroll 4
+    for (int q = 0; q < L; ++q) AB[(r0 + q) * LDB + (L + lane - q)] = csub(B1s[lane * BG_LD + q], cmul(tz, cconj(vs[q])));
+  }
+}
+
+__global__ void __launch_bounds__(B4_THREADS) k_bulge4(BulgeArgs a) {
+  extern __shared__ __align__(16) double2 b4sm[];
+  __shared__ int s_bad;
+  const int tid = threadIdx.x;
+  const long long W = (long long)gridDim.x;
+  const long long N = a.N;
+  const long long np = a.nprob;
+  // same sweep order and wait rule as k_bulge, one CTA per sweep
+  for (long long u = blockIdx.x; u < np * (N - 1); u += W) {
+    const long long q = u % np, s = u / np;
+    BulgeArgs b = a;
+    b.AB = a.AB + q * a.ab_stride;
+    unsigned int* prog = a.prog + q * a.prog_stride;
+    const long long ns = nsteps_of(N, s);
+    const long long nprev = (s > 0) ? nsteps_of(N, s - 1) : 0;
+    for (long long t = 0; t < ns; ++t) {
+      if (tid == 0) {
+        int bad = 0;
+        if (s > 0) {
+          const unsigned int need = (unsigned int)min(t + 3, nprev);
+          const unsigned long long t0 = globaltimer();
+          while (ld_acquire(prog + s - 1) < need) {
+            if (ld_acquire(reinterpret_cast<unsigned int*>(a.err)) != 0u || globaltimer() - t0 > kWaitNs) {
+              atomicExch(a.err, 1);
+              bad = 1;
+              break;
+            }
+          }
+        }
+        s_bad = bad;
+      }
+      __syncthreads();
+      if (s_bad) return;
+      bulge_step4(b, s, t, b4sm);
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) st_release(prog + s, (unsigned int)(t + 1));
+    }
+  }
+}
+
 __global__ void k_band_to_tridiag(const double2* __restrict__ AB, long long N, double* __restrict__ d,
                                   double* __restrict__ e) {
   const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -979,7 +1179,7 @@ static int two_stage_buffers(wtbg_ctx* ctx, int nband) {
   ENSURE(ctx->t2D, (size_t)nI * 64 * 64 * 16);
   ENSURE(ctx->t2G, (size_t)nI * 1024 * 16 + 1024 * 16);
   ENSURE(ctx->t2T, (size_t)std::max<long long>(npan, 1) * 1024 * 16);
-  ENSURE(ctx->t2P, (size_t)nsm * (16 + 16 * BW + 16 * BW * BW + 16 * BW * NGMAX) + 4096);
+  ENSURE(ctx->t2P, (size_t)nsm * (16 + 2 * 16 * BW + 16 * BW * BW + 16 * BW * NGMAX) + 4096);
   ENSURE(ctx->t2AB, (size_t)nband * N * LDB * 16);
   ENSURE(ctx->t2prog, (size_t)nband * N * 4 + 64);
   ENSURE(ctx->triErr, 16);
@@ -1007,10 +1207,10 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
   char* pb = ctx->t2P.as<char>();
   double* partN = reinterpret_cast<double*>(pb);
   double2* partW = reinterpret_cast<double2*>(pb + (size_t)nsm * 16);   // 16-byte aligned for any SM count
-  double2* partG = partW + (size_t)nsm * BW;
+  double2* partG = partW + (size_t)2 * nsm * BW;
   double2* partVg = partG + (size_t)nsm * BW * BW;
   double2* alpha = partVg + (size_t)nsm * BW * NGMAX;
-  GridBar* bar = reinterpret_cast<GridBar*>(alpha + 2);
+  GridBar* bar = reinterpret_cast<GridBar*>(alpha + 2 * BW);
   int* err = ctx->triErr.as<int>();
   CK(cudaMemsetAsync(bar, 0, sizeof(GridBar), s));
   CK(cudaFuncSetAttribute(k_hemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HM_SMEM));
@@ -1031,8 +1231,9 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
     const int j0 = (int)(pnl * BW), k0 = j0 + BW;
     const long long m = N - k0;
     const int nref = (int)std::min<long long>(BW, m);
-    // panel QR: G CTAs of R rows
-    int R = (int)std::max<long long>(64, (m + nsm - 1) / nsm);
+    // panel QR: G CTAs of R rows (at most 64 CTAs while the rows fit: the panel is latency-bound,
+    // and fewer CTAs make the grid barrier and the cross-CTA reductions cheaper)
+    const int R = (int)std::min<long long>(PQ_MAX_R, std::max<long long>(64, (m + 63) / 64));
     const int G = (int)((m + R - 1) / R);
     PanelArgs pa;
     pa.A = A;
@@ -1140,16 +1341,23 @@ static int run_stage2(wtbg_ctx* ctx, int nband, int ng, bool store, double* dd, 
   ba.nprob = nband;
   ba.ab_stride = N * LDB;
   ba.prog_stride = N;
-  const size_t bsm = (size_t)BG_WARPS * BG_WARP_TILE * 16;
-  CK(cudaFuncSetAttribute(k_bulge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
-  int per = 1;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bulge, 32 * BG_WARPS, bsm));
   const long long nsweep = (long long)nband * (N - 1);
-  const int gb = (int)std::max<long long>(1, std::min<long long>((long long)nsm * std::max(per, 1),
-                                                                  (nsweep + BG_WARPS - 1) / BG_WARPS));
-  {
+  if (ctx->bulge_warp_mode) {   // one warp per sweep
+    const size_t bsm = (size_t)BG_WARPS * BG_WARP_TILE * 16;
+    CK(cudaFuncSetAttribute(k_bulge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
+    int per = 1;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bulge, 32 * BG_WARPS, bsm));
+    const int gb = (int)std::max<long long>(1, std::min<long long>((long long)nsm * std::max(per, 1),
+                                                                    (nsweep + BG_WARPS - 1) / BG_WARPS));
     void* args[] = {&ba};
     CK(cudaLaunchCooperativeKernel((const void*)k_bulge, dim3(gb), dim3(32 * BG_WARPS), args, bsm, s));
+  } else {   // one CTA of four warps per sweep
+    CK(cudaFuncSetAttribute(k_bulge4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B4_SMEM));
+    int per = 1;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bulge4, B4_THREADS, B4_SMEM));
+    const int gb = (int)std::max<long long>(1, std::min<long long>((long long)nsm * std::max(per, 1), nsweep));
+    void* args[] = {&ba};
+    CK(cudaLaunchCooperativeKernel((const void*)k_bulge4, dim3(gb), dim3(B4_THREADS), args, B4_SMEM, s));
   }
   for (int q = 0; q < nband; ++q)
     k_band_to_tridiag<<<(int)((N + 255) / 256), 256, 0, s>>>(AB + (size_t)q * N * LDB, N, dd + (size_t)q * N,
