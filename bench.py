@@ -228,6 +228,27 @@ def fast_step(ctx, model, kpt, wl, c):
     return {k: v / 1e3 for k, v in t.items()}, W, eps[:, 1, 0].astype(np.float64), dav
 
 
+def learned_leg(device=0, evaluated=16, judged=4):
+    """Config-5 learned warm start, bounded for the bench: w = 16 model, 60x60 mesh, nv = nc = 2
+    (N = 14400), 256 seeded (Q, r0, eps_env) points, the network trained on the first 192 against
+    the 32 lowest block-Davidson eigenvectors (residual 1e-6 eV), then on `evaluated` held-out
+    points cold start against learned start (iterations and device ms to residual 1e-6 eV, FP64
+    and tensor-core products), the first `judged` of them checked against the dense FP64 solve."""
+    from wantibexos_b200 import warmstart_sweep as ws
+    a = ws.parser().parse_args(["--model", "c4_w16", "--n", "60", "--points", "256", "--train", "192",
+                                "--targets", "davidson", "--eval", str(evaluated), "--judge", str(judged)])
+    t0 = time.perf_counter()
+    summ = ws.sweep(a, device)
+    mi, ms = summ["mean_iters"], summ["mean_ms"]
+    return {"protocol": "256 points (Q <= 0.05 b, r0 in [10, 60] A, eps_env in [1, 5]), 192 trained, "
+                        f"{evaluated} held out evaluated, {judged} judged by the dense FP64 solve",
+            "N": summ["N"], "heldout_loss_before_after": summ["heldout_loss"],
+            "mean_capture_learned": summ["mean_capture_learned"], "mean_iters": mi, "mean_device_ms": ms,
+            "gain_fp64_product": 1.0 - ms["fp64_learned"] / ms["fp64_cold"],
+            "gain_tensor_core_product": 1.0 - ms["fast_learned"] / ms["fast_cold"],
+            "max_final_err_meV_vs_dense": summ["max_final_err_meV"], "wall_s": time.perf_counter() - t0}
+
+
 def peak_rel_error(ref, x):
     """max |x - ref| at the local maxima of ref, relative to max |ref|."""
     pk = np.where((ref[1:-1] > ref[:-2]) & (ref[1:-1] >= ref[2:]))[0] + 1
@@ -458,6 +479,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", default="both", choices=["both", "plain", "fast"],
                     help="plain FP64 path (the headline), the fast form, or both (default)")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start leg")
     ap.add_argument("--reduction", default="auto", choices=["auto", "one", "two", "two-warp"],
                     help="tridiagonal reduction of the dense solve: automatic (two-stage for N >= 2048), "
                          "one-stage or two-stage")
@@ -656,6 +678,8 @@ def main():
         "clocks": ck,
         "fast_form": fast,
     }
+    if not args.no_learned and args.form != "plain":
+        out["learned_warm_start"] = learned_leg(local)
     if not args.no_cpu_baseline:
         fit = zheev_fit(sizes=(N,) if N <= ZHEEV_FIT_SIZES[-1] else ZHEEV_FIT_SIZES)
         v, parts, _ = cpu_baseline(wl, model, fit)
