@@ -477,7 +477,9 @@ constexpr size_t XR_SMEM = (size_t)(32 * 64 + 32 * 32 + 32 * 64) * sizeof(double
 // this block (Gpart[b][i + 32 j]).
 __global__ void __launch_bounds__(256) k_xreduce(const double2* __restrict__ Xpart, int S, long long N, long long k0,
                                                  const double2* __restrict__ T, const double2* __restrict__ V,
-                                                 double2* __restrict__ Wp, double2* __restrict__ Gpart) {
+                                                 double2* __restrict__ Wp, double2* __restrict__ Gpart,
+                                                 const double2* __restrict__ Vl, const double2* __restrict__ Wl,
+                                                 const double2* __restrict__ C12) {
   extern __shared__ __align__(16) double2 xsm[];   // sX [32][64], sT [32][32], sV [32][64]
   double2* sX = xsm;
   double2* sT = sX + 32 * 64;
@@ -493,6 +495,14 @@ __global__ void __launch_bounds__(256) k_xreduce(const double2* __restrict__ Xpa
     if (rr < m) {
       for (int s = 0; s < S; ++s) x = cadd(x, Xpart[((size_t)s * 32 + c) * (size_t)m + rr]);
       v = V[k0 + rr + (long long)c * N];
+      if (C12) {
+        // look-ahead: the product used the matrix before the previous panel's update;
+        // X -= Vl C1 + Wl C2 with C1 = Wl^H V, C2 = Vl^H V (Vl, Wl: the previous panel)
+        for (int i = 0; i < 32; ++i) {
+          const long long ri = k0 + rr + (long long)i * N;
+          x = csub(x, cadd(cmul(Vl[ri], C12[i + 32 * c]), cmul(Wl[ri], C12[1024 + i + 32 * c])));
+        }
+      }
     }
     sX[e] = x;
     sV[e] = v;
@@ -553,6 +563,57 @@ __global__ void __launch_bounds__(256) k_wform(long long N, long long k0, const 
   Wp[r + (long long)j * N] = csub(Wp[r + (long long)j * N], cscale(t, 0.5));
 }
 
+
+// Look-ahead strip: the next panel's 32 columns c in [k0, k0+32), rows r >= c, get the current
+// panel's update A[r,c] -= V[r] W[c]^H + W[r] V[c]^H (V, W: rows of the panel's 32 columns)
+__global__ void __launch_bounds__(256) k_strip_update(double2* __restrict__ A, long long N, long long k0,
+                                                      const double2* __restrict__ V, const double2* __restrict__ W) {
+  __shared__ double2 sVc[32 * 32], sWc[32 * 32];   // [q][c]
+  for (int e = threadIdx.x; e < 32 * 32; e += 256) {
+    const int q = e >> 5, c = e & 31;
+    const long long rc = k0 + c;
+    sVc[e] = rc < N ? V[rc + (long long)q * N] : make_double2(0, 0);
+    sWc[e] = rc < N ? W[rc + (long long)q * N] : make_double2(0, 0);
+  }
+  __syncthreads();
+  const long long r = k0 + (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int c = threadIdx.x & 31;
+  if (r >= N || k0 + c >= N || r < k0 + c) return;
+  double2 t = make_double2(0, 0);
+  for (int q = 0; q < 32; ++q) {
+    const double2 vr = V[r + (long long)q * N], wr = W[r + (long long)q * N];
+    t = cadd(t, cadd(cmulc(sWc[q * 32 + c], vr), cmulc(sVc[q * 32 + c], wr)));   // v_r conj(w_c) + w_r conj(v_c)
+  }
+  const long long idx = r + (k0 + c) * N;
+  double2 a = csub(A[idx], t);
+  if (r == k0 + c) a.y = 0.0;
+  A[idx] = a;
+}
+
+// Look-ahead corrections, per 64-row block from row k1: C1 = Wl^H V2, C2 = Vl^H V2
+__global__ void __launch_bounds__(256) k_cpart(long long N, long long k1, const double2* __restrict__ Vl,
+                                               const double2* __restrict__ Wl, const double2* __restrict__ V2,
+                                               double2* __restrict__ part) {
+  const long long rb = k1 + (long long)blockIdx.x * 64;
+  for (int e = threadIdx.x; e < 2048; e += 256) {
+    const int which = e >> 10, i = e & 31, j = (e >> 5) & 31;
+    const double2* L = which ? Vl : Wl;
+    double2 t = make_double2(0, 0);
+    for (int u = 0; u < 64; ++u) {
+      const long long r = rb + u;
+      if (r >= N) break;
+      t = cadd(t, cmulc(L[r + (long long)i * N], V2[r + (long long)j * N]));
+    }
+    part[(size_t)blockIdx.x * 2048 + e] = t;
+  }
+}
+__global__ void __launch_bounds__(1024) k_creduce(const double2* __restrict__ part, int nb, double2* __restrict__ C12) {
+  for (int e = threadIdx.x; e < 2048; e += 1024) {
+    double2 t = make_double2(0, 0);
+    for (int b = 0; b < nb; ++b) t = cadd(t, part[(size_t)b * 2048 + e]);
+    C12[e] = t;
+  }
+}
 
 // ----------------------------------------------------------------------------- stage 2
 // Band storage: column j holds A[j + o, j] for o = 0 .. LDB-1 (the band, o <= b, and room for
@@ -1173,11 +1234,11 @@ static int two_stage_buffers(wtbg_ctx* ctx, int nband) {
   ENSURE(ctx->d, (size_t)N * 8);
   ENSURE(ctx->e, (size_t)N * 8);
   ENSURE(ctx->g, (size_t)N * 16 * NGMAX);
-  ENSURE(ctx->Wp, (size_t)N * 16 * BW);
-  ENSURE(ctx->t2V, (size_t)N * 16 * BW);
+  ENSURE(ctx->Wp, (size_t)N * 16 * 2 * BW);
+  ENSURE(ctx->t2V, (size_t)N * 16 * 2 * BW);
   ENSURE(ctx->t2X, (size_t)8 * BW * N * 16);
   ENSURE(ctx->t2D, (size_t)nI * 64 * 64 * 16);
-  ENSURE(ctx->t2G, (size_t)nI * 1024 * 16 + 1024 * 16);
+  ENSURE(ctx->t2G, (size_t)nI * 1024 * 16 + 1024 * 16 + (size_t)nI * 2048 * 16 + 2048 * 16);
   ENSURE(ctx->t2T, (size_t)std::max<long long>(npan, 1) * 1024 * 16);
   ENSURE(ctx->t2P, (size_t)nsm * (16 + 2 * 16 * BW + 16 * BW * BW + 16 * BW * NGMAX) + 4096);
   ENSURE(ctx->t2AB, (size_t)nband * N * LDB * 16);
@@ -1203,6 +1264,8 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
   double2* Dsym = ctx->t2D.as<double2>();
   double2* Gpart = ctx->t2G.as<double2>();
   double2* Mbuf = Gpart + (size_t)nI * 1024;
+  double2* Cpart = Mbuf + 1024;                 // look-ahead correction partials [nI][2048]
+  double2* Cbuf = Cpart + (size_t)nI * 2048;    // C1 (1024) then C2 (1024)
   double2* Tbuf = ctx->t2T.as<double2>();
   char* pb = ctx->t2P.as<char>();
   double* partN = reinterpret_cast<double*>(pb);
@@ -1227,7 +1290,10 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
   auto mark = [&](long long pnl, int k) {
     if (prof) cudaEventRecord(ctx->evpool[6 * pnl + k], s);
   };
-  for (long long pnl = 0; pnl < npan; ++pnl) {
+  // Panel QR of panel pnl into V (its 32 columns), then X = A22 V (split K) and W.  With
+  // lookahead (Vl, Wl != nullptr) A22 still lacks the previous panel's update and the product
+  // is corrected by -Vl C1 - Wl C2.
+  auto panel = [&](long long pnl, double2* V, double2* Wout, const double2* Vl, const double2* Wl) -> int {
     const int j0 = (int)(pnl * BW), k0 = j0 + BW;
     const long long m = N - k0;
     const int nref = (int)std::min<long long>(BW, m);
@@ -1243,7 +1309,7 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
     pa.jb = BW;
     pa.nref = nref;
     pa.R = R;
-    pa.Vp = Vp;
+    pa.Vp = V;
     pa.Tout = Tbuf + (size_t)pnl * 1024;
     pa.g = g;
     pa.ng = ng;
@@ -1262,24 +1328,59 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
       CK(cudaLaunchCooperativeKernel((const void*)k_panel_qr, dim3(G), dim3(PQ_THREADS), args, psm, s));
     }
     mark(pnl, 1);
-    // X = A22 V (split K), W, trailing update
     const int nIm = (int)((m + 63) / 64);
+    double2* C12 = nullptr;
+    if (Vl) {
+      k_cpart<<<nIm, 256, 0, s>>>(N, k0, Vl, Wl, V, Cpart);
+      k_creduce<<<1, 1024, 0, s>>>(Cpart, nIm, Cbuf);
+      C12 = Cbuf;
+      WTBG_COUNT(ctx, 2);
+    }
     k_symdiag<<<nIm, 256, 0, s>>>(A, N, k0, Dsym);
     int S = (int)std::min<long long>(SMAX, std::max<long long>(1, (4LL * nsm + nIm - 1) / nIm));
     S = std::min(S, nIm);
     const int chunkJ = (nIm + S - 1) / S;
     S = (nIm + chunkJ - 1) / chunkJ;
     mark(pnl, 2);
-    k_hemm2<<<dim3(nIm, S), 256, HM_SMEM, s>>>(A, N, k0, Dsym, Vp, nIm, chunkJ, Xpart);
+    k_hemm2<<<dim3(nIm, S), 256, HM_SMEM, s>>>(A, N, k0, Dsym, V, nIm, chunkJ, Xpart);
     mark(pnl, 3);
-    k_xreduce<<<nIm, 256, XR_SMEM, s>>>(Xpart, S, N, k0, Tbuf + (size_t)pnl * 1024, Vp, Wp, Gpart);
+    k_xreduce<<<nIm, 256, XR_SMEM, s>>>(Xpart, S, N, k0, Tbuf + (size_t)pnl * 1024, V, Wout, Gpart, Vl, Wl, C12);
     k_mform<<<1, 1024, 0, s>>>(Gpart, nIm, Tbuf + (size_t)pnl * 1024, Mbuf);
-    k_wform<<<(int)((m + 7) / 8), 256, 0, s>>>(N, k0, Vp, Mbuf, Wp);
+    k_wform<<<(int)((m + 7) / 8), 256, 0, s>>>(N, k0, V, Mbuf, Wout);
     WTBG_COUNT(ctx, 6);
     CKL("two-stage panel");
-    mark(pnl, 4);
-    if (int r = launch_her2k_v(ctx, A, N, Wp, Vp, N, 0, nref, k0)) return r;
-    mark(pnl, 5);
+    return 0;
+  };
+  // Panels in pairs: panel p, then the next panel's columns updated with p alone (strip), the
+  // next panel's QR and product from the matrix without p's update (corrected), and one rank-2k
+  // update with both panels (K = 64); a last unpaired panel updates alone (K = 32).
+  std::vector<double> her2k_flops(npan, 0.0);
+  for (long long pnl = 0; pnl < npan;) {
+    const int k0 = (int)(pnl * BW) + BW;
+    const long long m = N - k0;
+    const int nref = (int)std::min<long long>(BW, m);
+    if (int r = panel(pnl, Vp, Wp, nullptr, nullptr)) return r;
+    if (pnl + 1 < npan) {
+      const long long k1 = k0 + BW;
+      mark(pnl, 4);
+      k_strip_update<<<(int)((m + 7) / 8), 256, 0, s>>>(A, N, k0, Vp, Wp);
+      WTBG_COUNT(ctx, 1);
+      mark(pnl, 5);
+      her2k_flops[pnl] = 8.0 * (double)m * BW * 2 * BW;
+      if (int r = panel(pnl + 1, Vp + (size_t)BW * N, Wp + (size_t)BW * N, Vp, Wp)) return r;
+      const long long m1 = N - k1;
+      mark(pnl + 1, 4);
+      if (int r = launch_her2k_v(ctx, A, N, Wp, Vp, N, 0, 2 * BW, k1)) return r;
+      mark(pnl + 1, 5);
+      her2k_flops[pnl + 1] = (double)m1 * (m1 + 1.0) * 0.5 * 16.0 * 2 * BW;
+      pnl += 2;
+    } else {
+      mark(pnl, 4);
+      if (int r = launch_her2k_v(ctx, A, N, Wp, Vp, N, 0, nref, k0)) return r;
+      mark(pnl, 5);
+      her2k_flops[pnl] = (double)m * (m + 1.0) * 0.5 * 16.0 * nref;
+      pnl += 1;
+    }
   }
   k_band_extract<<<(unsigned)N, 128, 0, s>>>(A, N, ctx->t2AB.as<double2>() + (size_t)band * N * LDB);
   WTBG_COUNT(ctx, 1);
@@ -1300,8 +1401,8 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
       ctx->stats.panel_ms += a;
       ctx->stats.hemm_ms += b;
       ctx->stats.hemm_flops += 8.0 * m * m * nref;
-      ctx->stats.her2k_ms += c;
-      ctx->stats.her2k_flops += m * (m + 1.0) * 0.5 * 16.0 * nref;
+      ctx->stats.her2k_ms += c;   // rank-2k updates (K = 64 per pair) and the look-ahead strips
+      ctx->stats.her2k_flops += her2k_flops[pnl];
       ctx->stats.her2k_launches += 1;
     }
     for (auto& e : ev) cudaEventDestroy(e);
