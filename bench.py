@@ -228,6 +228,42 @@ def fast_step(ctx, model, kpt, wl, c):
     return {k: v / 1e3 for k, v in t.items()}, W, eps[:, 1, 0].astype(np.float64), dav
 
 
+def config4_leg(device=0):
+    """Config-4 exciton band structure: w = 16 model, 30x30 mesh, nv = nc = 3 (N = 8100), 64 Q on
+    Gamma-M-K-Gamma (22 points per segment with the float32 fraction of kpathbse, the two repeated
+    junction points dropped), V2DRK r0 = 35 A, eps_env = 2.5, all Q in one wtbg_bse_q_batch call
+    (after one sizing call on the first Q)."""
+    model = synth.config_model("c4_w16")
+    n, nv, nc, npts = 30, 3, 3, 22
+    b1, b2, b3 = recvec(model.rlat)
+    nodes = [(0, 0, 0), (0.5, 0, 0), (0.5, 0, 0), (1 / 3, 1 / 3, 0), (1 / 3, 1 / 3, 0), (0, 0, 0)]
+    cart = [u[0] * b1 + u[1] * b2 + u[2] * b3 for u in nodes]
+    qs = []
+    for j in range(3):
+        for i in range(npts):
+            if j > 0 and i == 0:
+                continue
+            t = float(np.float32(i) / np.float32(npts - 1))
+            q = cart[2 * j] + (cart[2 * j + 1] - cart[2 * j]) * t
+            qs.append([0.0, q[0], q[1], q[2]])
+    qs = np.array(qs)
+    k = kmesh(n, model.rlat)
+    kqs = [k + q[1:][None, :] for q in qs]
+    c = wtbgpu.coulomb_params("V2DRK", [n, n, 1], 1e-3, [2.5] * 3, 1.0, 1.0, 0.0, 35.0)
+    ctx = wtbgpu.Context(device)
+    ctx.set_model(model)
+    ctx.bands(k, nv, nc, want_vectors=False)
+    ctx.bse_q_batch(kqs[:1], qs[:1], c, graph=False)
+    t0 = time.perf_counter()
+    W, ms = ctx.bse_q_batch(kqs, qs, c, graph=False)
+    wall = time.perf_counter() - t0
+    ctx.close()
+    return {"workload": "config 4: w=16, 61 cells, 30x30 mesh, nv=nc=3, N=8100, 64 Q on Gamma-M-K-Gamma, "
+                        "V2DRK r0=35, eps_env=2.5", "n_q": int(qs.shape[0]), "N": int(W.shape[1]),
+            "device_s": float(ms.sum() / 1e3), "ms_per_q": float(ms.sum() / qs.shape[0]), "wall_s": wall,
+            "lowest_exciton_eV": [float(W[:, 0].min()), float(W[:, 0].max())]}
+
+
 def learned_leg(device=0, evaluated=16, judged=4):
     """Config-5 learned warm start, bounded for the bench: w = 16 model, 60x60 mesh, nv = nc = 2
     (N = 14400), 256 seeded (Q, r0, eps_env) points, the network trained on the first 192 against
@@ -479,7 +515,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", default="both", choices=["both", "plain", "fast"],
                     help="plain FP64 path (the headline), the fast form, or both (default)")
-    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start leg")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start and config-4 legs")
     ap.add_argument("--reduction", default="auto", choices=["auto", "one", "two", "two-warp"],
                     help="tridiagonal reduction of the dense solve: automatic (two-stage for N >= 2048), "
                          "one-stage or two-stage")
@@ -680,6 +716,8 @@ def main():
     }
     if not args.no_learned and args.form != "plain":
         out["learned_warm_start"] = learned_leg(local)
+    if not args.no_learned:
+        out["config4_q_batch"] = config4_leg(local)
     if not args.no_cpu_baseline:
         fit = zheev_fit(sizes=(N,) if N <= ZHEEV_FIT_SIZES[-1] else ZHEEV_FIT_SIZES)
         v, parts, _ = cpu_baseline(wl, model, fit)

@@ -477,9 +477,7 @@ constexpr size_t XR_SMEM = (size_t)(32 * 64 + 32 * 32 + 32 * 64) * sizeof(double
 // this block (Gpart[b][i + 32 j]).
 __global__ void __launch_bounds__(256) k_xreduce(const double2* __restrict__ Xpart, int S, long long N, long long k0,
                                                  const double2* __restrict__ T, const double2* __restrict__ V,
-                                                 double2* __restrict__ Wp, double2* __restrict__ Gpart,
-                                                 const double2* __restrict__ Vl, const double2* __restrict__ Wl,
-                                                 const double2* __restrict__ C12) {
+                                                 double2* __restrict__ Wp, double2* __restrict__ Gpart) {
   extern __shared__ __align__(16) double2 xsm[];   // sX [32][64], sT [32][32], sV [32][64]
   double2* sX = xsm;
   double2* sT = sX + 32 * 64;
@@ -495,14 +493,6 @@ __global__ void __launch_bounds__(256) k_xreduce(const double2* __restrict__ Xpa
     if (rr < m) {
       for (int s = 0; s < S; ++s) x = cadd(x, Xpart[((size_t)s * 32 + c) * (size_t)m + rr]);
       v = V[k0 + rr + (long long)c * N];
-      if (C12) {
-        // look-ahead: the product used the matrix before the previous panel's update;
-        // X -= Vl C1 + Wl C2 with C1 = Wl^H V, C2 = Vl^H V (Vl, Wl: the previous panel)
-        for (int i = 0; i < 32; ++i) {
-          const long long ri = k0 + rr + (long long)i * N;
-          x = csub(x, cadd(cmul(Vl[ri], C12[i + 32 * c]), cmul(Wl[ri], C12[1024 + i + 32 * c])));
-        }
-      }
     }
     sX[e] = x;
     sV[e] = v;
@@ -564,55 +554,103 @@ __global__ void __launch_bounds__(256) k_wform(long long N, long long k0, const 
 }
 
 
-// Look-ahead strip: the next panel's 32 columns c in [k0, k0+32), rows r >= c, get the current
-// panel's update A[r,c] -= V[r] W[c]^H + W[r] V[c]^H (V, W: rows of the panel's 32 columns)
-__global__ void __launch_bounds__(256) k_strip_update(double2* __restrict__ A, long long N, long long k0,
+// Look-ahead group of panels.  Vacc, Wacc hold the group's V and W side by side (32 columns per
+// panel, leading dimension N); K = 32 * (panels already factored in the group).
+
+// Strip of the next panel: columns c in [c0, c0+32), rows r >= c, get the pending updates of the
+// group's earlier panels, A[r,c] -= sum_{q<K} V[r,q] conj(W[c,q]) + W[r,q] conj(V[c,q]).
+// One warp per row (lane = column); the column rows of V and W in shared memory.
+__global__ void __launch_bounds__(256) k_strip_update(double2* __restrict__ A, long long N, long long c0, int K,
                                                       const double2* __restrict__ V, const double2* __restrict__ W) {
-  __shared__ double2 sVc[32 * 32], sWc[32 * 32];   // [q][c]
-  for (int e = threadIdx.x; e < 32 * 32; e += 256) {
+  extern __shared__ __align__(16) double2 ssm[];   // sVc [K][32], sWc [K][32]
+  double2* sVc = ssm;
+  double2* sWc = ssm + (size_t)K * 32;
+  for (int e = threadIdx.x; e < K * 32; e += 256) {
     const int q = e >> 5, c = e & 31;
-    const long long rc = k0 + c;
+    const long long rc = c0 + c;
     sVc[e] = rc < N ? V[rc + (long long)q * N] : make_double2(0, 0);
     sWc[e] = rc < N ? W[rc + (long long)q * N] : make_double2(0, 0);
   }
   __syncthreads();
-  const long long r = k0 + (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+  const long long r = c0 + (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
   const int c = threadIdx.x & 31;
-  if (r >= N || k0 + c >= N || r < k0 + c) return;
-  double2 t = make_double2(0, 0);
-  for (int q = 0; q < 32; ++q) {
-    const double2 vr = V[r + (long long)q * N], wr = W[r + (long long)q * N];
-    t = cadd(t, cadd(cmulc(sWc[q * 32 + c], vr), cmulc(sVc[q * 32 + c], wr)));   // v_r conj(w_c) + w_r conj(v_c)
+  if (r >= N || c0 + c >= N || r < c0 + c) return;
+  double2 t0 = make_double2(0, 0), t1 = t0;
+  for (int q = 0; q < K; q += 2) {
+    t0 = cadd(t0, cadd(cmulc(sWc[q * 32 + c], V[r + (long long)q * N]), cmulc(sVc[q * 32 + c], W[r + (long long)q * N])));
+    t1 = cadd(t1, cadd(cmulc(sWc[(q + 1) * 32 + c], V[r + (long long)(q + 1) * N]),
+                       cmulc(sVc[(q + 1) * 32 + c], W[r + (long long)(q + 1) * N])));
   }
-  const long long idx = r + (k0 + c) * N;
-  double2 a = csub(A[idx], t);
-  if (r == k0 + c) a.y = 0.0;
+  const long long idx = r + (c0 + c) * N;
+  double2 a = csub(A[idx], cadd(t0, t1));
+  if (r == c0 + c) a.y = 0.0;
   A[idx] = a;
 }
 
-// Look-ahead corrections, per 64-row block from row k1: C1 = Wl^H V2, C2 = Vl^H V2
-__global__ void __launch_bounds__(256) k_cpart(long long N, long long k1, const double2* __restrict__ Vl,
-                                               const double2* __restrict__ Wl, const double2* __restrict__ V2,
+// Correction Gram matrices over 64-row blocks from row k1: which = 0: C1 = Wacc^H V2,
+// which = 1: C2 = Vacc^H V2 (K x 32 each, part[b][which][i + K j]).  Rows staged in shared memory.
+__global__ void __launch_bounds__(256) k_cpart(long long N, long long k1, int K, const double2* __restrict__ Vacc,
+                                               const double2* __restrict__ Wacc, const double2* __restrict__ V2,
                                                double2* __restrict__ part) {
+  extern __shared__ __align__(16) double2 csm[];   // sL [K][64], sV [32][64]
+  const int which = blockIdx.y;
+  const double2* L = which ? Vacc : Wacc;
+  double2* sL = csm;
+  double2* sV = csm + (size_t)K * 64;
   const long long rb = k1 + (long long)blockIdx.x * 64;
-  for (int e = threadIdx.x; e < 2048; e += 256) {
-    const int which = e >> 10, i = e & 31, j = (e >> 5) & 31;
-    const double2* L = which ? Vl : Wl;
-    double2 t = make_double2(0, 0);
-    for (int u = 0; u < 64; ++u) {
-      const long long r = rb + u;
-      if (r >= N) break;
-      t = cadd(t, cmulc(L[r + (long long)i * N], V2[r + (long long)j * N]));
+  for (int e = threadIdx.x; e < K * 64; e += 256) {
+    const int u = e & 63, i = e >> 6;
+    const long long r = rb + u;
+    sL[e] = r < N ? L[r + (long long)i * N] : make_double2(0, 0);
+  }
+  for (int e = threadIdx.x; e < 32 * 64; e += 256) {
+    const int u = e & 63, j = e >> 6;
+    const long long r = rb + u;
+    sV[e] = r < N ? V2[r + (long long)j * N] : make_double2(0, 0);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < K * 32; e += 256) {
+    const int i = e % K, j = e / K;
+    double2 t0 = make_double2(0, 0), t1 = t0;
+    for (int u = 0; u < 64; u += 2) {
+      t0 = cadd(t0, cmulc(sL[i * 64 + u], sV[j * 64 + u]));
+      t1 = cadd(t1, cmulc(sL[i * 64 + u + 1], sV[j * 64 + u + 1]));
     }
-    part[(size_t)blockIdx.x * 2048 + e] = t;
+    part[((size_t)blockIdx.x * 2 + which) * K * 32 + e] = cadd(t0, t1);
   }
 }
-__global__ void __launch_bounds__(1024) k_creduce(const double2* __restrict__ part, int nb, double2* __restrict__ C12) {
-  for (int e = threadIdx.x; e < 2048; e += 1024) {
-    double2 t = make_double2(0, 0);
-    for (int b = 0; b < nb; ++b) t = cadd(t, part[(size_t)b * 2048 + e]);
-    C12[e] = t;
+// C12[which][i + K j] = sum over the blocks (fixed order); grid over entries
+__global__ void __launch_bounds__(256) k_creduce(const double2* __restrict__ part, int nb, int K, double2* __restrict__ C12) {
+  const int e = blockIdx.x * 256 + threadIdx.x;
+  if (e >= 2 * K * 32) return;
+  double2 t0 = make_double2(0, 0), t1 = t0;
+  int b = 0;
+  for (; b + 1 < nb; b += 2) {
+    t0 = cadd(t0, part[(size_t)b * 2 * K * 32 + e]);
+    t1 = cadd(t1, part[(size_t)(b + 1) * 2 * K * 32 + e]);
   }
+  if (b < nb) t0 = cadd(t0, part[(size_t)b * 2 * K * 32 + e]);
+  C12[e] = cadd(t0, t1);
+}
+// X (the first split partial, [32][m]) -= Vacc C1 + Wacc C2 for the rows from k1: one warp per
+// row, lane = column; C1, C2 in shared memory.
+__global__ void __launch_bounds__(256) k_xcorr(double2* __restrict__ X0, long long N, long long k1, int K,
+                                               const double2* __restrict__ Vacc, const double2* __restrict__ Wacc,
+                                               const double2* __restrict__ C12) {
+  extern __shared__ __align__(16) double2 xsm2[];   // C1 [K][32] (i + K j), C2
+  for (int e = threadIdx.x; e < 2 * K * 32; e += 256) xsm2[e] = C12[e];
+  __syncthreads();
+  const long long m = N - k1;
+  const long long rr = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int c = threadIdx.x & 31;
+  if (rr >= m) return;
+  const long long r = k1 + rr;
+  double2 t0 = make_double2(0, 0), t1 = t0;
+  for (int i = 0; i < K; ++i) {
+    t0 = cadd(t0, cmul(Vacc[r + (long long)i * N], xsm2[i + K * c]));
+    t1 = cadd(t1, cmul(Wacc[r + (long long)i * N], xsm2[K * 32 + i + K * c]));
+  }
+  X0[(size_t)c * m + rr] = csub(X0[(size_t)c * m + rr], cadd(t0, t1));
 }
 
 // ----------------------------------------------------------------------------- stage 2
@@ -1211,6 +1249,7 @@ __global__ void __launch_bounds__(256) k_bt1_apply(const double2* __restrict__ A
 // Largest N whose panels fit the aggregate shared memory of the panel QR (one CTA per SM,
 // at most PQ_MAX_R rows of the 32-wide panel each).
 constexpr int PQ_MAX_R = 384;
+constexpr int LOOKAHEAD = 2;   // panels applied per rank-2k update (K = 64)
 static bool two_stage_fits(wtbg_ctx* ctx, long long N) {
   if (ctx->nsm <= 0) cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
   return N > BW + 1 && (N + ctx->nsm - 1) / ctx->nsm <= PQ_MAX_R;
@@ -1234,11 +1273,12 @@ static int two_stage_buffers(wtbg_ctx* ctx, int nband) {
   ENSURE(ctx->d, (size_t)N * 8);
   ENSURE(ctx->e, (size_t)N * 8);
   ENSURE(ctx->g, (size_t)N * 16 * NGMAX);
-  ENSURE(ctx->Wp, (size_t)N * 16 * 2 * BW);
-  ENSURE(ctx->t2V, (size_t)N * 16 * 2 * BW);
+  ENSURE(ctx->Wp, (size_t)N * 16 * LOOKAHEAD * BW);
+  ENSURE(ctx->t2V, (size_t)N * 16 * LOOKAHEAD * BW);
   ENSURE(ctx->t2X, (size_t)8 * BW * N * 16);
   ENSURE(ctx->t2D, (size_t)nI * 64 * 64 * 16);
-  ENSURE(ctx->t2G, (size_t)nI * 1024 * 16 + 1024 * 16 + (size_t)nI * 2048 * 16 + 2048 * 16);
+  ENSURE(ctx->t2G, (size_t)nI * 1024 * 16 + 1024 * 16 + (size_t)nI * 2 * (LOOKAHEAD - 1) * 1024 * 16 +
+                        (size_t)2 * (LOOKAHEAD - 1) * 1024 * 16);
   ENSURE(ctx->t2T, (size_t)std::max<long long>(npan, 1) * 1024 * 16);
   ENSURE(ctx->t2P, (size_t)nsm * (16 + 2 * 16 * BW + 16 * BW * BW + 16 * BW * NGMAX) + 4096);
   ENSURE(ctx->t2AB, (size_t)nband * N * LDB * 16);
@@ -1264,8 +1304,8 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
   double2* Dsym = ctx->t2D.as<double2>();
   double2* Gpart = ctx->t2G.as<double2>();
   double2* Mbuf = Gpart + (size_t)nI * 1024;
-  double2* Cpart = Mbuf + 1024;                 // look-ahead correction partials [nI][2048]
-  double2* Cbuf = Cpart + (size_t)nI * 2048;    // C1 (1024) then C2 (1024)
+  double2* Cpart = Mbuf + 1024;                                        // look-ahead correction partials
+  double2* Cbuf = Cpart + (size_t)nI * 2 * (LOOKAHEAD - 1) * 1024;     // C1 (K x 32) then C2
   double2* Tbuf = ctx->t2T.as<double2>();
   char* pb = ctx->t2P.as<char>();
   double* partN = reinterpret_cast<double*>(pb);
@@ -1290,10 +1330,10 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
   auto mark = [&](long long pnl, int k) {
     if (prof) cudaEventRecord(ctx->evpool[6 * pnl + k], s);
   };
-  // Panel QR of panel pnl into V (its 32 columns), then X = A22 V (split K) and W.  With
-  // lookahead (Vl, Wl != nullptr) A22 still lacks the previous panel's update and the product
-  // is corrected by -Vl C1 - Wl C2.
-  auto panel = [&](long long pnl, double2* V, double2* Wout, const double2* Vl, const double2* Wl) -> int {
+  // Panel QR of panel pnl into V (its 32 columns), then X = A22 V (split K) and W.  Inside a
+  // look-ahead group (K > 0) A22 still lacks the updates of the group's K/32 earlier panels
+  // (Vacc, Wacc) and the product is corrected by -Vacc C1 - Wacc C2.
+  auto panel = [&](long long pnl, double2* V, double2* Wout, int K) -> int {
     const int j0 = (int)(pnl * BW), k0 = j0 + BW;
     const long long m = N - k0;
     const int nref = (int)std::min<long long>(BW, m);
@@ -1329,13 +1369,6 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
     }
     mark(pnl, 1);
     const int nIm = (int)((m + 63) / 64);
-    double2* C12 = nullptr;
-    if (Vl) {
-      k_cpart<<<nIm, 256, 0, s>>>(N, k0, Vl, Wl, V, Cpart);
-      k_creduce<<<1, 1024, 0, s>>>(Cpart, nIm, Cbuf);
-      C12 = Cbuf;
-      WTBG_COUNT(ctx, 2);
-    }
     k_symdiag<<<nIm, 256, 0, s>>>(A, N, k0, Dsym);
     int S = (int)std::min<long long>(SMAX, std::max<long long>(1, (4LL * nsm + nIm - 1) / nIm));
     S = std::min(S, nIm);
@@ -1344,43 +1377,52 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
     mark(pnl, 2);
     k_hemm2<<<dim3(nIm, S), 256, HM_SMEM, s>>>(A, N, k0, Dsym, V, nIm, chunkJ, Xpart);
     mark(pnl, 3);
-    k_xreduce<<<nIm, 256, XR_SMEM, s>>>(Xpart, S, N, k0, Tbuf + (size_t)pnl * 1024, V, Wout, Gpart, Vl, Wl, C12);
+    if (K > 0) {
+      const size_t cps = ((size_t)K * 64 + 32 * 64) * 16, xcs = (size_t)2 * K * 32 * 16;
+      CK(cudaFuncSetAttribute(k_cpart, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cps));
+      CK(cudaFuncSetAttribute(k_xcorr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xcs));
+      k_cpart<<<dim3(nIm, 2), 256, cps, s>>>(N, k0, K, Vp, Wp, V, Cpart);
+      k_creduce<<<(2 * K * 32 + 255) / 256, 256, 0, s>>>(Cpart, nIm, K, Cbuf);
+      k_xcorr<<<(int)((m + 7) / 8), 256, xcs, s>>>(Xpart, N, k0, K, Vp, Wp, Cbuf);
+      WTBG_COUNT(ctx, 3);
+    }
+    k_xreduce<<<nIm, 256, XR_SMEM, s>>>(Xpart, S, N, k0, Tbuf + (size_t)pnl * 1024, V, Wout, Gpart);
     k_mform<<<1, 1024, 0, s>>>(Gpart, nIm, Tbuf + (size_t)pnl * 1024, Mbuf);
     k_wform<<<(int)((m + 7) / 8), 256, 0, s>>>(N, k0, V, Mbuf, Wout);
     WTBG_COUNT(ctx, 6);
     CKL("two-stage panel");
     return 0;
   };
-  // Panels in pairs: panel p, then the next panel's columns updated with p alone (strip), the
-  // next panel's QR and product from the matrix without p's update (corrected), and one rank-2k
-  // update with both panels (K = 64); a last unpaired panel updates alone (K = 32).
+  // Panels in look-ahead groups of up to LOOKAHEAD: panel j of a group first gets the pending
+  // updates of the group's earlier panels on its own 32 columns (strip), is factored, and forms
+  // its product from the matrix that still lacks those updates (corrected); one rank-2k update
+  // with K = 32 x (panels in the group) then applies the whole group to the trailing matrix.
   std::vector<double> her2k_flops(npan, 0.0);
-  for (long long pnl = 0; pnl < npan;) {
-    const int k0 = (int)(pnl * BW) + BW;
-    const long long m = N - k0;
-    const int nref = (int)std::min<long long>(BW, m);
-    if (int r = panel(pnl, Vp, Wp, nullptr, nullptr)) return r;
-    if (pnl + 1 < npan) {
-      const long long k1 = k0 + BW;
-      mark(pnl, 4);
-      k_strip_update<<<(int)((m + 7) / 8), 256, 0, s>>>(A, N, k0, Vp, Wp);
-      WTBG_COUNT(ctx, 1);
-      mark(pnl, 5);
-      her2k_flops[pnl] = 8.0 * (double)m * BW * 2 * BW;
-      if (int r = panel(pnl + 1, Vp + (size_t)BW * N, Wp + (size_t)BW * N, Vp, Wp)) return r;
-      const long long m1 = N - k1;
-      mark(pnl + 1, 4);
-      if (int r = launch_her2k_v(ctx, A, N, Wp, Vp, N, 0, 2 * BW, k1)) return r;
-      mark(pnl + 1, 5);
-      her2k_flops[pnl + 1] = (double)m1 * (m1 + 1.0) * 0.5 * 16.0 * 2 * BW;
-      pnl += 2;
-    } else {
-      mark(pnl, 4);
-      if (int r = launch_her2k_v(ctx, A, N, Wp, Vp, N, 0, nref, k0)) return r;
-      mark(pnl, 5);
-      her2k_flops[pnl] = (double)m * (m + 1.0) * 0.5 * 16.0 * nref;
-      pnl += 1;
+  for (long long p0 = 0; p0 < npan; p0 += LOOKAHEAD) {
+    const int gsz = (int)std::min<long long>(LOOKAHEAD, npan - p0);
+    for (int j = 0; j < gsz; ++j) {
+      const long long pnl = p0 + j;
+      if (j > 0) {
+        const long long c0 = pnl * BW;   // the panel's first column (= the previous panel's k0)
+        const long long mc = N - c0;
+        const size_t sss = (size_t)2 * 32 * j * 32 * 16;
+        CK(cudaFuncSetAttribute(k_strip_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sss));
+        mark(pnl - 1, 4);
+        k_strip_update<<<(int)((mc + 7) / 8), 256, sss, s>>>(A, N, c0, 32 * j, Vp, Wp);
+        WTBG_COUNT(ctx, 1);
+        mark(pnl - 1, 5);
+        her2k_flops[pnl - 1] = 8.0 * (double)mc * 32 * 2 * 32 * j;
+      }
+      if (int r = panel(pnl, Vp + (size_t)32 * j * N, Wp + (size_t)32 * j * N, 32 * j)) return r;
     }
+    const long long pl = p0 + gsz - 1;
+    const long long kl = (pl + 1) * BW;
+    const long long ml = N - kl;
+    const int Kg = 32 * (gsz - 1) + (int)std::min<long long>(BW, ml);
+    mark(pl, 4);
+    if (int r = launch_her2k_v(ctx, A, N, Wp, Vp, N, 0, Kg, kl)) return r;
+    mark(pl, 5);
+    her2k_flops[pl] = (double)ml * (ml + 1.0) * 0.5 * 16.0 * Kg;
   }
   k_band_extract<<<(unsigned)N, 128, 0, s>>>(A, N, ctx->t2AB.as<double2>() + (size_t)band * N * LDB);
   WTBG_COUNT(ctx, 1);
