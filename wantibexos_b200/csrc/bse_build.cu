@@ -14,9 +14,18 @@
 // <c|c'> and <v|v'> of the tile are small complex GEMMs (K = w) computed once per tile in
 // shared memory; the Coulomb factor W(k-k') is evaluated once per (k, k') pair; the
 // Kronecker expansion into the (nc*nv) x (nc*nv) blocks happens in the store loop, so every
-// element of the 16*N^2-byte matrix is written to HBM exactly once with coalesced 16-byte
-// stores.  The kernel is bound by the HBM write of the matrix.
+// element of the 16*N^2-byte matrix is written to HBM exactly once.  Off-diagonal tiles are
+// staged in shared memory in chunks of CW columns (double-buffered, in the space the band
+// vectors occupied) and leave through one TMA bulk tensor store per chunk, which overlaps the
+// write of one chunk with the evaluation of the next; the TMA unit clips the rows past N of the
+// last block row.  Diagonal tiles (lower half only) use plain coalesced 16-byte stores.  The
+// kernel is bound by the HBM write of the matrix.
+#include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <string>
+
+#include <cudaTypedefs.h>
 
 #include "common.cuh"
 #include "coulomb.cuh"
@@ -44,10 +53,24 @@ struct BuildArgs {
   // n = nk * nc (conduction) and nk * nv (valence); nullptr for the FP64 form
   const float* Oc;
   const float* Ov;
+  // TMA-staged stores of the off-diagonal tiles: CW columns per chunk (0: plain stores only)
+  int cw;
 };
 
-__global__ void __launch_bounds__(kBuildThreads) k_bse_build(BuildArgs a) {
-  extern __shared__ __align__(16) unsigned char smem[];
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"((unsigned)__cvta_generic_to_shared(src)), "r"(x), "r"(y)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+template <int N_>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N_) : "memory");
+}
+
+__global__ void __launch_bounds__(kBuildThreads) k_bse_build(const __grid_constant__ CUtensorMap tmH, BuildArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
   const long long t = blockIdx.x;
   int bi = (int)floor((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
   while ((long long)(bi + 1) * (bi + 2) / 2 <= t) ++bi;
@@ -60,11 +83,13 @@ __global__ void __launch_bounds__(kBuildThreads) k_bse_build(BuildArgs a) {
   const int RC = TK * nc, RV = TK * nv;
   const int ws = w | 1;   // odd row stride: conflict-free 16-byte shared loads across rows
 
+  // region 0: the band-vector rows, later the two store-staging buffers [CW][TK*ncv]
   double2* UcR = reinterpret_cast<double2*>(smem);
   double2* UcC = UcR + RC * ws;
   double2* UvR = UcC + RC * ws;
   double2* UvC = UvR + RV * ws;
-  double2* Mc = UvC + RV * ws;         // col-major [RC x RC]
+  const int r0len = max(2 * RC * ws + 2 * RV * ws, 2 * ((a.cw * TK * ncv + 7) & ~7));
+  double2* Mc = UcR + ((r0len + 7) & ~7);   // col-major [RC x RC], 128-byte aligned
   double2* Mv = Mc + RC * RC;          // col-major [RV x RV]
   double* Vt = reinterpret_cast<double*>(Mv + RV * RV);   // [kc][kr]
   double* dE = Vt + TK * TK;           // [TK*ncv]
@@ -135,23 +160,23 @@ __global__ void __launch_bounds__(kBuildThreads) k_bse_build(BuildArgs a) {
   }
   __syncthreads();
 
-  const int rows = nkr * ncv, cols = nkc * ncv;
   const long long N = a.N;
   const long long I0 = (long long)kr0 * ncv, J0 = (long long)kc0 * ncv;
   const bool diag_tile = (bi == bj);
-  if (tid >= (bs / rows) * rows) return;
-  const int ii = tid % rows;
+  const bool staged = a.cw > 0 && !diag_tile;
+  // staged tiles evaluate all TK*ncv rows (those past N are clipped by the TMA store)
+  const int rows = staged ? TK * ncv : nkr * ncv, cols = nkc * ncv;
   const int njp = bs / rows;
+  const int ii = tid % rows;
+  const bool thr_on = tid < njp * rows;
   const int kr = ii / ncv, c = (ii % ncv) / nv, v = ii % nv;
   const long long I = I0 + ii;
-  const double2 vcvI = a.exch ? a.vcv[I] : make_double2(0, 0);
+  const double2 vcvI = (a.exch && thr_on && I < N) ? a.vcv[I] : make_double2(0, 0);
   const double dEi = dE[ii];
   const double2* Mc_r = Mc + kr * nc + c;   // + col*RC
   const double2* Mv_r = Mv + kr * nv + v;   // + col*RV
-  double2* Hcol = a.H + I;
-  for (int jj = tid / rows; jj < cols; jj += njp) {
-    const long long J = J0 + jj;
-    if (diag_tile && I < J) continue;
+  // element (I, J) of tile column jj
+  auto elem = [&](int jj, long long J) -> double2 {
     const int ci = colinfo[jj];
     const int kc = ci >> 16, cc = (ci >> 8) & 0xff, vv = ci & 0xff;
     const double vk = Vt[kc * TK + kr];
@@ -176,7 +201,38 @@ __global__ void __launch_bounds__(kBuildThreads) k_bse_build(BuildArgs a) {
       val = cscale(inter, a.fdeh[J]);
       if (I == J) val.x += dEi;
     }
-    Hcol[J * N] = val;
+    return val;
+  };
+  if (staged) {
+    // off-diagonal tile (a full block column: cols = TK*ncv, a multiple of CW): chunk ch of CW
+    // columns goes to buffer ch&1 and leaves with one store issued by thread 0.  One CTA
+    // barrier per chunk: thread 0 reaches it only after the store of chunk ch-1 has finished
+    // reading its buffer, which chunk ch+1 refills after that barrier; the store of chunk ch
+    // proceeds while chunk ch+1 is evaluated into the other buffer.
+    const int CW = a.cw;
+    double2* stg = reinterpret_cast<double2*>(smem);
+    const int bstride = (CW * rows + 7) & ~7;   // 128-byte aligned buffers
+    for (int ch = 0; ch * CW < cols; ++ch) {
+      double2* buf = stg + (size_t)(ch & 1) * bstride;
+      if (thr_on)
+        for (int cl = tid / rows; cl < CW; cl += njp) {
+          const int jj = ch * CW + cl;
+          buf[cl * rows + ii] = (I < N) ? elem(jj, J0 + jj) : make_double2(0, 0);
+        }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      if (tid == 0) bulk_wait_read<0>();
+      __syncthreads();
+      if (tid == 0) tma_store_2d(&tmH, buf, (int)(2 * I0), (int)(J0 + (long long)ch * CW));
+    }
+    if (tid == 0) bulk_wait_read<0>();
+    return;
+  }
+  if (!thr_on) return;
+  double2* Hcol = a.H + I;
+  for (int jj = tid / rows; jj < cols; jj += njp) {
+    const long long J = J0 + jj;
+    if (diag_tile && I < J) continue;
+    Hcol[J * N] = elem(jj, J);
   }
 }
 
@@ -194,12 +250,58 @@ __global__ void k_exchange_overlap(const double2* Uq, const double2* U, int nk, 
   vcv[i] = acc;
 }
 
+// Columns per staged store chunk: the largest divisor of the tile width TK*ncv up to 16 whose
+// two buffers fit in region 0 as sized by the band-vector rows (8 when region 0 must grow);
+// 0 when a tile is taller than one TMA box (256 doubles) or wider than a 32-bit coordinate.
+int build_cw(int TK, int nc, int nv, int w) {
+  const int RC = TK * nc, RV = TK * nv, ncv = nc * nv, ws = w | 1, TR = TK * ncv;
+  if (TR > 128) return 0;
+  const long long u = 2LL * RC * ws + 2LL * RV * ws;
+  int best = 0;
+  for (int cw = 1; cw <= 16; ++cw)
+    if (TR % cw == 0 && 2LL * ((cw * TR + 7) & ~7) <= u) best = cw;
+  if (best >= 4) return best;
+  for (int cw = 8; cw >= 1; --cw)
+    if (TR % cw == 0) return cw;
+  return 1;
+}
+
 size_t build_smem(int TK, int nc, int nv, int w) {
   const int RC = TK * nc, RV = TK * nv, ncv = nc * nv, ws = w | 1;
-  return 16ull * (2ull * RC * ws + 2ull * RV * ws + (size_t)RC * RC + (size_t)RV * RV) + 8ull * TK * TK +
+  const long long r0len = std::max(2LL * RC * ws + 2LL * RV * ws, 2LL * ((build_cw(TK, nc, nv, w) * TK * ncv + 7) & ~7));
+  return 16ull * ((size_t)((r0len + 7) & ~7LL) + (size_t)RC * RC + (size_t)RV * RV) + 8ull * TK * TK +
          8ull * TK * ncv + 4ull * TK * ncv + 64;
 }
 
+}  // namespace
+
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 build_encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// H (N x N complex, column-major) as a FLOAT64 tensor {2N, N}; box = rows x cw of one staged chunk
+int encode_h_map(wtbg_ctx* ctx, CUtensorMap* map, void* H, long long N, int rows, int cw) {
+  auto fn = build_encode_fn();
+  if (!fn) return set_err(ctx, WTBG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  cuuint64_t dims[2] = {(cuuint64_t)(2 * N), (cuuint64_t)N};
+  cuuint64_t strides[1] = {(cuuint64_t)(16 * N)};
+  cuuint32_t box[2] = {(cuuint32_t)(2 * rows), (cuuint32_t)cw};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, H, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    return set_err(ctx, WTBG_ERR_CUDA, "bse_build: cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return WTBG_OK;
+}
 }  // namespace
 
 CoulombDev make_coulomb_dev(const wtbg_coulomb* p, const double* L) {
@@ -332,6 +434,12 @@ int launch_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p, const double* q4) {
   a.N = ctx->N;
   a.TK = TK;
   a.nbk = (ctx->nk + TK - 1) / TK;
+  // TMA-staged stores for the off-diagonal tiles (there are none with a single block row)
+  CUtensorMap tmH;
+  memset(&tmH, 0, sizeof(tmH));
+  a.cw = (a.nbk > 1 && 2 * a.N < 0x7fffffffLL) ? build_cw(TK, nc, nv, w) : 0;
+  if (a.cw > 0)
+    if (int r = encode_h_map(ctx, &tmH, a.H, a.N, TK * ncv, a.cw)) return r;
   if (q) {
     const double modq = sqrt((q4[1]) * (q4[1]) + (q4[2]) * (q4[2]) + (q4[3]) * (q4[3]));
     if (modq != 0.0) {
@@ -361,7 +469,7 @@ int launch_bse_build(wtbg_ctx* ctx, const wtbg_coulomb* p, const double* q4) {
     if (int r = ensure_events(ctx, 2)) return r;
     cudaEventRecord(ctx->evpool[0], ctx->stream);
   }
-  k_bse_build<<<(unsigned)ntile, kBuildThreads, smem, ctx->stream>>>(a); WTBG_COUNT(ctx, 1);
+  k_bse_build<<<(unsigned)ntile, kBuildThreads, smem, ctx->stream>>>(tmH, a); WTBG_COUNT(ctx, 1);
   CKL("k_bse_build");
   if (prof) {
     cudaEventRecord(ctx->evpool[1], ctx->stream);

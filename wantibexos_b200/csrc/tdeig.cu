@@ -6,7 +6,8 @@
 //   f_n = |sum_j A_jn h_j|^2 = |z_n^T g|^2,  g = Q^T h,  A = Q Z,
 // so after the reduction only the tridiagonal eigenvectors z_n are needed, and only inside
 // the dot products with the five g vectors.
-//   * eigenvalues: Sturm-count bisection, one thread per eigenvalue index, to full precision;
+//   * eigenvalues: Sturm-count multisection, L lanes per eigenvalue index (L = 1: bisection),
+//     to full precision;
 //   * eigenvectors: inverse iteration with a partial-pivoting tridiagonal LU, three steps
 //     from a deterministic pseudo-random start vector; eigenvalues closer than
 //     1e-7 * ||T|| form a cluster that one thread processes in sequence with modified
@@ -46,20 +47,55 @@ __global__ void k_e2(const double* e, long long n, double* e2) {
   if (i < n - 1) e2[i] = e[i] * e[i];
 }
 
+// Multisection: L consecutive lanes (L a power of two, L <= 32) share eigenvalue m and, per
+// round, take Sturm counts at L interior points of its interval [a, b]; the new interval runs
+// from the highest point with count <= m to the next point (or b), so count(a) <= m < count(b)
+// holds whatever the counts at the other points.  A round divides the interval by L + 1 (by 2,
+// at the midpoint, for L = 1: plain bisection), so the chain of dependent Sturm passes per
+// eigenvalue is log2(L + 1) times shorter, for L times more total passes; the host picks L.
+// Stopping rule as in bisection: width <= 2 eps max(|a|, |b|) + pivmin, or no double between.
 __global__ void __launch_bounds__(128) k_bisect(const double* __restrict__ d, const double* __restrict__ e2, long long n,
-                                                double lo, double hi, double pivmin, double* lam) {
-  const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (m >= n) return;
+                                                double lo, double hi, double pivmin, int L, double* lam) {
+  const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long m = gt / L;
+  const int lane = threadIdx.x & 31, sl = lane & (L - 1), base = lane - sl;
+  const bool active = m < n;
   double a = lo, b = hi;
   for (int it = 0; it < 256; ++it) {
     const double mid = 0.5 * (a + b);
-    if (!(mid > a && mid < b)) break;
-    if (b - a <= 2.0 * DBL_EPSILON * fmax(fabs(a), fabs(b)) + pivmin) break;
-    const int c = sturm_count(d, e2, n, mid, pivmin);
-    if (c <= m) a = mid;
-    else b = mid;
+    const bool done = !active || !(mid > a && mid < b) || (b - a <= 2.0 * DBL_EPSILON * fmax(fabs(a), fabs(b)) + pivmin);
+    if (__all_sync(0xffffffffu, done)) break;
+    const double x = (L == 1) ? mid : a + (b - a) * ((double)(sl + 1) / (double)(L + 1));
+    const bool le = !done && sturm_count(d, e2, n, x, pivmin) <= m;
+    const unsigned gb = (__ballot_sync(0xffffffffu, le) >> base) & (L == 32 ? 0xffffffffu : ((1u << L) - 1u));
+    const int jhi = gb ? 31 - __clz(gb) : -1;   // highest point with count <= m
+    const double xa = __shfl_sync(0xffffffffu, x, base + max(jhi, 0));
+    const double xb = __shfl_sync(0xffffffffu, x, base + min(jhi + 1, L - 1));
+    if (!done) {
+      if (jhi >= 0) a = xa;
+      if (jhi + 1 < L) b = xb;
+    }
   }
-  lam[m] = 0.5 * (a + b);
+  if (active && sl == 0) lam[m] = 0.5 * (a + b);
+}
+
+// Lanes per eigenvalue for k_bisect.  A round costs one Sturm pass (n dependent steps of about
+// 150 cycles) when the SM sub-partitions are idle, and n L / 32 warp passes of about 22 issue
+// cycles per step spread over 4 nsm sub-partitions when they are full; rounds ~ 53 / log2(L+1).
+int bisect_lanes(long long n, int nsm) {
+  int best = 1;
+  double bt = 1e300;
+  for (int L = 1; L <= 32; L *= 2) {
+    const double rounds = std::ceil(53.0 / std::log2((double)L + 1.0));
+    const double lat = 150.0 * (double)n;
+    const double thr = 22.0 * (double)n * (double)n * (double)L / 32.0 / (4.0 * std::max(nsm, 1));
+    const double t = rounds * std::max(lat, thr);
+    if (t < bt) {
+      bt = t;
+      best = L;
+    }
+  }
+  return best;
 }
 
 __device__ __forceinline__ double start_value(long long m, long long k) {
@@ -98,10 +134,15 @@ __global__ void __launch_bounds__(128) k_inviter(InvArgs a) {
   if (cs == 0) return;
   const long long n = a.n;
   const int M = a.M;
-  double* X = a.ws;
-  double* U1 = a.ws + n * M;
-  double* U2 = a.ws + 2 * n * M;
-  double* U3 = a.ws + 3 * n * M;
+  // four disjoint slices of the workspace: declared non-aliasing so that the loads of the next
+  // elimination / substitution steps can be issued ahead of this step's stores (the steps form a
+  // dependent chain through one division each; the loads do not depend on it)
+  double* __restrict__ X = a.ws;
+  double* __restrict__ U1 = a.ws + n * M;
+  double* __restrict__ U2 = a.ws + 2 * n * M;
+  double* __restrict__ U3 = a.ws + 3 * n * M;
+  const double* __restrict__ dd_ = a.d;
+  const double* __restrict__ ee_ = a.e;
   const double pert = a.pert;
   for (int s = 0; s < cs; ++s) {
     const long long mm = m + s;
@@ -111,13 +152,14 @@ __global__ void __launch_bounds__(128) k_inviter(InvArgs a) {
     for (long long k = 0; k < n; ++k) X[k * M + jj] = start_value(mm, k);
     for (int it = 0; it < 3; ++it) {
       // factor T - lam I with partial pivoting, eliminating the right-hand side on the fly
-      double diag = a.d[0] - lam;
-      double sup = (n > 1) ? a.e[0] : 0.0;
+      double diag = dd_[0] - lam;
+      double sup = (n > 1) ? ee_[0] : 0.0;
       double cur = X[jj] * sc;
+#pragma unroll 4
       for (long long k = 0; k < n - 1; ++k) {
-        const double sub = a.e[k];
-        const double nd = a.d[k + 1] - lam;
-        const double nsup = (k + 1 < n - 1) ? a.e[k + 1] : 0.0;
+        const double sub = ee_[k];
+        const double nd = dd_[k + 1] - lam;
+        const double nsup = (k + 1 < n - 1) ? ee_[k + 1] : 0.0;
         const double nxt = X[(k + 1) * M + jj] * sc;
         if (fabs(diag) >= fabs(sub)) {
           if (fabs(diag) < pert) diag = copysign(pert, diag);
@@ -145,6 +187,7 @@ __global__ void __launch_bounds__(128) k_inviter(InvArgs a) {
       double x2 = 0.0, x1 = cur / diag;
       X[(n - 1) * M + jj] = x1;
       double nrm = x1 * x1;
+#pragma unroll 4
       for (long long k = n - 2; k >= 0; --k) {
         const double xk = (X[k * M + jj] - U2[k * M + jj] * x1 - U3[k * M + jj] * x2) / U1[k * M + jj];
         X[k * M + jj] = xk;
@@ -374,7 +417,10 @@ static int tridiagonal_solve_body(wtbg_ctx* ctx, int dtfull, int cpol, bool vect
     k_e2<<<(int)((n + 255) / 256), 256, 0, s>>>(ctx->e.as<double>(), n, e2); WTBG_COUNT(ctx, 1);
     CKL("k_e2");
   }
-  k_bisect<<<(int)((n + 127) / 128), 128, 0, s>>>(ctx->d.as<double>(), e2, n, lo, hi, pivmin, ctx->lam.as<double>()); WTBG_COUNT(ctx, 1);
+  if (ctx->nsm <= 0) cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+  const int lanes = bisect_lanes(n, ctx->nsm);
+  k_bisect<<<(int)((n * lanes + 127) / 128), 128, 0, s>>>(ctx->d.as<double>(), e2, n, lo, hi, pivmin, lanes,
+                                                       ctx->lam.as<double>()); WTBG_COUNT(ctx, 1);
   CKL("k_bisect");
   ctx->lam_host.resize(n);
   CK(cudaMemcpyAsync(ctx->lam_host.data(), ctx->lam.as<double>(), n * 8, cudaMemcpyDeviceToHost, s));

@@ -67,37 +67,37 @@ __device__ __forceinline__ unsigned long long globaltimer() {
 }
 constexpr unsigned long long kWaitNs = 2000000000ull;   // 2 s bound on every spin wait
 
-// Grid barrier among the co-resident CTAs of a cooperative launch: arrival counter plus a
-// generation word.  The wait is bounded (2 s of %globaltimer); on time-out (or when another
-// CTA has already failed) the CTA sets *err and the barrier reports failure, after which every
-// CTA leaves the kernel.
-struct GridBar {
-  unsigned int count;
-  unsigned int gen;
-};
-__device__ bool grid_barrier(GridBar* gb, int* err) {
+// Bounded acquire-wait until *p >= need.  The error flag and the clock are read every 64 polls,
+// so that a detection costs one L2 round trip; after 2 s, or when another CTA or warp has
+// failed, the flag is set and the wait reports failure.
+__device__ __forceinline__ bool wait_at_least(const unsigned int* p, unsigned int need, int* err) {
+  unsigned int spins = 0;
+  unsigned long long t0 = 0;
+  while (ld_acquire(p) < need) {
+    if ((++spins & 63u) == 0u) {
+      if (t0 == 0) t0 = globaltimer();
+      if (ld_acquire(reinterpret_cast<unsigned int*>(err)) != 0u || globaltimer() - t0 > kWaitNs) {
+        atomicExch(err, 1);
+        return false;
+      }
+    }
+  }
+  return true;
+}
+
+// Grid barrier among the co-resident CTAs of a cooperative launch.  Each launch has its own
+// arrival counter, zeroed before the launch; barrier k of the launch is passed when the counter
+// reaches k * gridDim.x.  Thread 0 arrives with a release reduction (no returned value, no reset
+// step) and polls with acquire loads; the CTA barrier around it orders the other threads' memory
+// operations (as in a cooperative-groups grid sync).  The wait is bounded (2 s of %globaltimer);
+// on time-out (or when another CTA has already failed) the CTA sets *err and the barrier reports
+// failure, after which every CTA leaves the kernel.
+__device__ bool grid_sync(unsigned int* cnt, unsigned int target, int* err) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned int g = ld_acquire(&gb->gen);
-    __threadfence();
-    const unsigned int arrived = atomicAdd(&gb->count, 1u);
-    int ok = 1;
-    if (arrived == gridDim.x - 1) {
-      atomicExch(&gb->count, 0u);
-      __threadfence();
-      st_release(&gb->gen, g + 1u);
-    } else {
-      const unsigned long long t0 = globaltimer();
-      while (ld_acquire(&gb->gen) == g) {
-        if (ld_acquire(reinterpret_cast<unsigned int*>(err)) != 0u || globaltimer() - t0 > kWaitNs) {
-          atomicExch(err, 1);
-          ok = 0;
-          break;
-        }
-      }
-    }
-    s_ok = ok;
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
+    s_ok = wait_at_least(cnt, target, err) ? 1 : 0;
   }
   __syncthreads();
   return s_ok != 0;
@@ -108,6 +108,10 @@ __device__ bool grid_barrier(GridBar* gb, int* err) {
 // memory as P[col][row] (row fastest).  Per column p: ZLARFG from the grid-reduced norm (every
 // CTA sums the same partials in the same order, so all hold identical scalars), then the
 // reflector is applied to the panel's remaining columns with grid-reduced dot products.
+// The column step is one latency chain (grid barrier, reduction of the CTAs' partials, scalars,
+// update, next partials), so every part of it uses all threads: 8 threads per column reduce the
+// partials and form the next ones (fixed order, width-8 shuffle tree), every thread evaluates
+// the reflector scalars itself, and the update runs over (row, 8-column chunk) items.
 struct PanelArgs {
   double2* A;
   long long N;
@@ -123,7 +127,7 @@ struct PanelArgs {
   double2* partG;      // [grid][32*32]
   double2* partVg;     // [grid][32*NGMAX]
   double2* alpha;      // [2][32] posted row k0 + p (alpha = its column-p entry), by parity of p
-  GridBar* bar;
+  unsigned int* cnt;   // this launch's grid-barrier arrival counter (zero at launch)
   int* err;
 };
 
@@ -133,61 +137,83 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
   extern __shared__ __align__(16) double2 P[];   // [jb][R]
   __shared__ double2 s_tau[BW];
   __shared__ double2 s_w[BW];
-  __shared__ double2 s_scal;
-  __shared__ double s_beta;
+  __shared__ double2 s_S[BW];    // grid-reduced S_q of the current column (q >= p)
+  __shared__ double2 s_al[BW];   // posted row k0 + p
   __shared__ double2 s_T[BW * BW];
   __shared__ double2 s_y[BW * NGMAX];
-  const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-  constexpr int NW = PQ_THREADS / 32;
+  const int tid = threadIdx.x;
   const int R = a.R, jb = a.jb;
   const long long N = a.N;
   const int G = (int)gridDim.x;
   const long long rbeg = (long long)a.k0 + (long long)blockIdx.x * R;
   const long long rend = min((long long)a.k0 + (long long)(blockIdx.x + 1) * R, N);
   const int nr = (int)max(0LL, rend - rbeg);
+  unsigned int nbar = 0;
+  auto sync_grid = [&]() -> bool {
+    ++nbar;
+    return grid_sync(a.cnt, nbar * (unsigned int)G, a.err);
+  };
   for (int q = 0; q < jb; ++q)
     for (int i = tid; i < R; i += PQ_THREADS)
       P[(size_t)q * R + i] = (i < nr) ? a.A[(rbeg + i) + (long long)(a.j0 + q) * N] : make_double2(0, 0);
   __syncthreads();
 
+  // width-8 sum over the aligned lane groups of 8 (every lane of a group ends with the same sum)
+  auto sum8 = [](double2 v) {
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+      v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+      v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    return v;
+  };
+  const int qq = tid >> 3, sl = tid & 7;   // column offset and slice of the 8-thread groups
+
   // Partials of column p over the own rows below row k0 + p, one reduction for both the norm
   // and the unscaled dot products: S_q = sum_{r > k0+p} conj(P[r,p]) P[r,q] for q = p .. jb-1
-  // (S_p = |x|^2).  The owner of row k0 + p posts that row (alpha = P[k0+p, p] and P[k0+p, q]).
-  // Buffers alternate with the parity of p: a CTA writes the partials of column p+1 while others
-  // may still read those of p, but never those of p+2 before everyone passed the barrier of p+1.
+  // (S_p = |x|^2); thread slice sl takes the rows i = sl (mod 8).  The owner of row k0 + p
+  // posts that row (alpha = P[k0+p, p] and P[k0+p, q]).  Buffers alternate with the parity of
+  // p: a CTA writes the partials of column p+1 while others may still read those of p, but
+  // never those of p+2 before everyone passed the barrier of p+1.
   auto partials = [&](int p) {
     const long long rp = (long long)a.k0 + p;
     const int buf = p & 1;
-    for (int q = p + wp; q < jb; q += NW) {
-      double2 sacc = make_double2(0, 0);
-      for (int i = lane; i < nr; i += 32)
-        if (rbeg + i > rp) sacc = cadd(sacc, cmulc(P[(size_t)p * R + i], P[(size_t)q * R + i]));
-      sacc = warp_sum2(sacc);
-      if (lane == 0) a.partW[((size_t)buf * G + blockIdx.x) * BW + q] = sacc;
+    double2 sacc = make_double2(0, 0);
+    if (qq < jb - p) {
+      const double2* Pp = P + (size_t)p * R;
+      const double2* Pq = P + (size_t)(p + qq) * R;
+      const int i0 = (int)max(0LL, rp + 1 - rbeg);
+      for (int i = i0 + ((sl - i0) & 7); i < nr; i += 8) sacc = cadd(sacc, cmulc(Pp[i], Pq[i]));
     }
+    sacc = sum8(sacc);
+    if (qq < jb - p && sl == 0) a.partW[((size_t)buf * G + blockIdx.x) * BW + p + qq] = sacc;
     if (rp >= rbeg && rp < rend)
       for (int q = p + tid; q < jb; q += PQ_THREADS) a.alpha[buf * BW + q] = P[(size_t)q * R + (rp - rbeg)];
   };
 
   partials(0);
   for (int p = 0; p < a.nref; ++p) {
-    if (!grid_barrier(a.bar, a.err)) return;
+    if (!sync_grid()) return;
     const long long rp = (long long)a.k0 + p;
     const int buf = p & 1;
-    const int nq = jb - p;   // columns p .. jb-1
-    for (int qq = wp; qq < nq; qq += NW) {
-      const int q = p + qq;
+    // grid reduction of S_q (q = p + qq): slice sl sums the CTAs c = sl (mod 8) in order
+    {
       double2 sacc = make_double2(0, 0);
-      for (int c = lane; c < G; c += 32) sacc = cadd(sacc, ldcg2(a.partW + ((size_t)buf * G + c) * BW + q));
-      sacc = warp_sum2(sacc);
-      if (lane == 0) s_w[q] = sacc;
+      if (qq < jb - p)
+        for (int c = sl; c < G; c += 8) sacc = cadd(sacc, ldcg2(a.partW + ((size_t)buf * G + c) * BW + p + qq));
+      sacc = sum8(sacc);
+      if (qq < jb - p) {
+        if (sl == 0) s_S[p + qq] = sacc;
+        else if (sl == 1) s_al[p + qq] = ldcg2(a.alpha + buf * BW + p + qq);
+      }
     }
     __syncthreads();
-    if (tid == 0) {
-      const double xn2 = s_w[p].x;
-      const double2 al = ldcg2(a.alpha + buf * BW + p);
-      double2 tau, scal;
-      double beta;
+    // ZLARFG scalars, evaluated by every thread from the same shared values
+    double2 tau, scal;
+    double beta;
+    {
+      const double xn2 = s_S[p].x;
+      const double2 al = s_al[p];
       if (xn2 == 0.0 && al.y == 0.0) {
         tau = make_double2(0, 0);
         scal = make_double2(0, 0);
@@ -199,37 +225,33 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
         const double dd = den.x * den.x + den.y * den.y;
         scal = make_double2(den.x / dd, -den.y / dd);
       }
-      s_tau[p] = tau;
-      s_scal = scal;
-      s_beta = beta;
     }
-    __syncthreads();
-    // w_q = sum_{r >= k0+p} conj(v_r) P[r,q] = P[k0+p, q] + conj(scal) S_q   (q > p)
-    if (tid > p && tid < jb) s_w[tid] = cadd(ldcg2(a.alpha + buf * BW + tid), cmul(cconj(s_scal), s_w[tid]));
-    __syncthreads();
+    if (tid == 0) s_tau[p] = tau;
+    // P[r,q] -= conj(tau) v_r w_q (r >= k0+p, q > p), with v_r = P[r,p] scal (v = 1 at row
+    // k0+p) and w_q = sum_{r >= k0+p} conj(v_r) P[r,q] = P[k0+p, q] + conj(scal) S_q
     {
-      const double2 scal = s_scal;
-      const double2 ct = cconj(s_tau[p]);
-      const int nu = jb - p - 1;
-      for (int i = tid; i < nr; i += PQ_THREADS) {
+      const double2 ct = cconj(tau);
+      const int nch = (jb - p - 1 + 7) >> 3;
+      for (int it = tid; it < nr * nch; it += PQ_THREADS) {
+        const int i = it % nr, ch = it / nr;
         const long long r = rbeg + i;
         if (r < rp) continue;
-        double2 v;
-        if (r == rp) {
-          v = make_double2(1.0, 0.0);
-          P[(size_t)p * R + i] = make_double2(s_beta, 0.0);
-        } else {
-          v = cmul(P[(size_t)p * R + i], scal);
-          P[(size_t)p * R + i] = v;
-        }
+        const double2 v = (r == rp) ? make_double2(1.0, 0.0) : cmul(P[(size_t)p * R + i], scal);
         const double2 cv = cmul(ct, v);
-        for (int u = 0; u < nu; ++u) {
-          const int q = p + 1 + u;
-          P[(size_t)q * R + i] = csub(P[(size_t)q * R + i], cmul(cv, s_w[q]));
+        const int q0 = p + 1 + ch * 8, q1 = min(q0 + 8, jb);
+        for (int q = q0; q < q1; ++q) {
+          const double2 wq = cadd(s_al[q], cmul(cconj(scal), s_S[q]));
+          P[(size_t)q * R + i] = csub(P[(size_t)q * R + i], cmul(cv, wq));
         }
       }
     }
     __syncthreads();
+    // column p becomes v (beta on row k0+p), then the partials of column p+1
+    for (int i = tid; i < nr; i += PQ_THREADS) {
+      const long long r = rbeg + i;
+      if (r == rp) P[(size_t)p * R + i] = make_double2(beta, 0.0);
+      else if (r > rp) P[(size_t)p * R + i] = cmul(P[(size_t)p * R + i], scal);
+    }
     if (p + 1 < a.nref) partials(p + 1);
   }
   __syncthreads();
@@ -261,7 +283,7 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
       for (int i = 0; i < nr; ++i) s = cadd(s, cmul(vval(q, i), a.g[(long long)al * N + rbeg + i]));
     a.partVg[(size_t)blockIdx.x * BW * NGMAX + e] = s;
   }
-  if (!grid_barrier(a.bar, a.err)) return;
+  if (!sync_grid()) return;
   // T factor (ZLARFT forward columnwise): T[i][i] = tau_i, T[0:i, i] = -tau_i T[0:i, 0:i] G[0:i, i]
   if (blockIdx.x == 0) {
     for (int e = tid; e < BW * BW; e += PQ_THREADS) {
@@ -291,7 +313,7 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
     // s_T now holds T upper triangular; G entries below the diagonal were overwritten with 0
     for (int e = tid; e < BW * BW; e += PQ_THREADS) a.Tout[e] = s_T[e];
   }
-  if (!grid_barrier(a.bar, a.err)) return;
+  if (!sync_grid()) return;
   // g <- g - conj(V) T^T (V^T g)
   for (int e = tid; e < BW * BW; e += PQ_THREADS) s_T[e] = ldcg2(a.Tout + e);
   for (int e = tid; e < BW * a.ng; e += PQ_THREADS) {
@@ -894,21 +916,12 @@ __global__ void __launch_bounds__(32 * BG_WARPS, 1) k_bulge(BulgeArgs a) {
       if (s > 0) {
         const unsigned int need = (unsigned int)min(t + 3, nprev);
         int bad = 0;
-        if (lane == 0) {
-          const unsigned long long t0 = globaltimer();
-          while (ld_acquire(prog + s - 1) < need) {
-            if (ld_acquire(reinterpret_cast<unsigned int*>(a.err)) != 0u || globaltimer() - t0 > kWaitNs) {
-              atomicExch(a.err, 1);
-              bad = 1;
-              break;
-            }
-          }
-        }
+        if (lane == 0) bad = wait_at_least(prog + s - 1, need, a.err) ? 0 : 1;
         bad = __shfl_sync(0xffffffffu, bad, 0);
         if (bad) return;
       }
       bulge_step(b, s, t, Bs, Ds, B1s, vs, ws);
-      __threadfence();
+      // publish: the warp barrier orders the lanes' writes before lane 0's release store
       __syncwarp();
       if (lane == 0) st_release(prog + s, (unsigned int)(t + 1));
     }
@@ -1106,25 +1119,11 @@ __global__ void __launch_bounds__(B4_THREADS) k_bulge4(BulgeArgs a) {
     const long long ns = nsteps_of(N, s);
     const long long nprev = (s > 0) ? nsteps_of(N, s - 1) : 0;
     for (long long t = 0; t < ns; ++t) {
-      if (tid == 0) {
-        int bad = 0;
-        if (s > 0) {
-          const unsigned int need = (unsigned int)min(t + 3, nprev);
-          const unsigned long long t0 = globaltimer();
-          while (ld_acquire(prog + s - 1) < need) {
-            if (ld_acquire(reinterpret_cast<unsigned int*>(a.err)) != 0u || globaltimer() - t0 > kWaitNs) {
-              atomicExch(a.err, 1);
-              bad = 1;
-              break;
-            }
-          }
-        }
-        s_bad = bad;
-      }
+      if (tid == 0) s_bad = (s > 0 && !wait_at_least(prog + s - 1, (unsigned int)min(t + 3, nprev), a.err)) ? 1 : 0;
       __syncthreads();
       if (s_bad) return;
       bulge_step4(b, s, t, b4sm);
-      __threadfence();
+      // publish: the CTA barrier orders every thread's writes before thread 0's release store
       __syncthreads();
       if (tid == 0) st_release(prog + s, (unsigned int)(t + 1));
     }
@@ -1155,16 +1154,7 @@ __global__ void __launch_bounds__(32 * BG_WARPS, 1) k_bulge_back(const double2* 
       if (s + 1 < N - 1) {
         const unsigned int need = (unsigned int)min(t + 1, nnext);
         int bad = 0;
-        if (lane == 0) {
-          const unsigned long long t0 = globaltimer();
-          while (ld_acquire(prog + s + 1) < need) {
-            if (ld_acquire(reinterpret_cast<unsigned int*>(err)) != 0u || globaltimer() - t0 > kWaitNs) {
-              atomicExch(err, 1);
-              bad = 1;
-              break;
-            }
-          }
-        }
+        if (lane == 0) bad = wait_at_least(prog + s + 1, need, err) ? 0 : 1;
         bad = __shfl_sync(0xffffffffu, bad, 0);
         if (bad) return;
       }
@@ -1178,7 +1168,6 @@ __global__ void __launch_bounds__(32 * BG_WARPS, 1) k_bulge_back(const double2* 
         const double2 sv = warp_sum2(cmulc(v, xv));   // v^H x
         if (lane < L) xp[lane] = csub(xv, cmul(tau, cmul(v, sv)));
       }
-      __threadfence();
       __syncwarp();
       if (lane == 0) st_release(prog + s, (unsigned int)(t + 1));
     }
@@ -1280,7 +1269,8 @@ static int two_stage_buffers(wtbg_ctx* ctx, int nband) {
   ENSURE(ctx->t2G, (size_t)nI * 1024 * 16 + 1024 * 16 + (size_t)nI * 2 * (LOOKAHEAD - 1) * 1024 * 16 +
                         (size_t)2 * (LOOKAHEAD - 1) * 1024 * 16);
   ENSURE(ctx->t2T, (size_t)std::max<long long>(npan, 1) * 1024 * 16);
-  ENSURE(ctx->t2P, (size_t)nsm * (16 + 2 * 16 * BW + 16 * BW * BW + 16 * BW * NGMAX) + 4096);
+  ENSURE(ctx->t2P, (size_t)nsm * (16 + 2 * 16 * BW + 16 * BW * BW + 16 * BW * NGMAX) + 4096 +
+                        (size_t)std::max<long long>(npan, 1) * 4);
   ENSURE(ctx->t2AB, (size_t)nband * N * LDB * 16);
   ENSURE(ctx->t2prog, (size_t)nband * N * 4 + 64);
   ENSURE(ctx->triErr, 16);
@@ -1313,9 +1303,9 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
   double2* partG = partW + (size_t)2 * nsm * BW;
   double2* partVg = partG + (size_t)nsm * BW * BW;
   double2* alpha = partVg + (size_t)nsm * BW * NGMAX;
-  GridBar* bar = reinterpret_cast<GridBar*>(alpha + 2 * BW);
+  unsigned int* cnt = reinterpret_cast<unsigned int*>(alpha + 2 * BW);   // one barrier counter per panel launch
   int* err = ctx->triErr.as<int>();
-  CK(cudaMemsetAsync(bar, 0, sizeof(GridBar), s));
+  CK(cudaMemsetAsync(cnt, 0, (size_t)std::max<long long>(npan, 1) * 4, s));
   CK(cudaFuncSetAttribute(k_hemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HM_SMEM));
   CK(cudaFuncSetAttribute(k_xreduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XR_SMEM));
   // profiling: event pairs around the panel QR, the Hermitian product and the rank-2k update
@@ -1358,7 +1348,7 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
     pa.partG = partG;
     pa.partVg = partVg;
     pa.alpha = alpha;
-    pa.bar = bar;
+    pa.cnt = cnt + pnl;
     pa.err = err;
     const size_t psm = (size_t)BW * R * 16;
     CK(cudaFuncSetAttribute(k_panel_qr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
