@@ -1,10 +1,13 @@
 """Exciton band structure in one call (the Q loop of bsebnds, bse_kpath-tool.f90:246-435):
-every Q of a path through wtbg_bse_q_batch, whose tridiagonalisation is one captured CUDA
-graph replayed per Q with the autotuned mat-vec chunk.
+every Q of a path through wtbg_bse_q_batch.  Below N = 2048 the one-stage tridiagonalisation of
+each Q is replayed from one captured CUDA graph (autotuned mat-vec chunk); from N = 2048 the Q
+points run in groups, each Q's build and dense -> band stage leaving its band in a slot and one
+persistent bulge-chasing launch reducing the whole group's bands.
 
 Parity: the batch gives exactly what one wtbg_bse_q_eigenvalues call per Q gives (same kernels,
-same launch parameters, replayed from the graph), and the Q eigenvalues agree with the oracle's
-dense eigvalsh of its own Q kernel to 1e-9 eV.
+same launch parameters; graph replay or grouped bands), the two-stage group agrees with the
+one-stage reduction to 1e-9 eV, and the Q eigenvalues agree with the oracle's dense eigvalsh of
+its own Q kernel to 1e-9 eV.  The config-4 size (64 Q, N = 8100) is timed.
 """
 import time
 

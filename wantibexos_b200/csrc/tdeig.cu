@@ -125,7 +125,9 @@ struct InvArgs {
   long long zs0, zs1;
 };
 
-__global__ void __launch_bounds__(128) k_inviter(InvArgs a) {
+constexpr int SB = 8;   // inverse-iteration steps whose loads are issued together
+
+__global__ void __launch_bounds__(64) k_inviter(InvArgs a) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= a.M) return;
   const long long m = a.m0 + j;
@@ -134,9 +136,10 @@ __global__ void __launch_bounds__(128) k_inviter(InvArgs a) {
   if (cs == 0) return;
   const long long n = a.n;
   const int M = a.M;
-  // four disjoint slices of the workspace: declared non-aliasing so that the loads of the next
-  // elimination / substitution steps can be issued ahead of this step's stores (the steps form a
-  // dependent chain through one division each; the loads do not depend on it)
+  // Four disjoint slices of the workspace, laid out [k][slot]: each step of the elimination and
+  // of the substitution is one link of a chain through a division, while its workspace loads
+  // (one DRAM round trip each) do not depend on the chain; so the loads of SB steps are issued
+  // together before the SB dependent steps run (same arithmetic, one round trip per SB steps).
   double* __restrict__ X = a.ws;
   double* __restrict__ U1 = a.ws + n * M;
   double* __restrict__ U2 = a.ws + 2 * n * M;
@@ -155,31 +158,47 @@ __global__ void __launch_bounds__(128) k_inviter(InvArgs a) {
       double diag = dd_[0] - lam;
       double sup = (n > 1) ? ee_[0] : 0.0;
       double cur = X[jj] * sc;
-#pragma unroll 4
-      for (long long k = 0; k < n - 1; ++k) {
-        const double sub = ee_[k];
-        const double nd = dd_[k + 1] - lam;
-        const double nsup = (k + 1 < n - 1) ? ee_[k + 1] : 0.0;
-        const double nxt = X[(k + 1) * M + jj] * sc;
-        if (fabs(diag) >= fabs(sub)) {
-          if (fabs(diag) < pert) diag = copysign(pert, diag);
-          const double mult = sub / diag;
-          U1[k * M + jj] = diag;
-          U2[k * M + jj] = sup;
-          U3[k * M + jj] = 0.0;
-          X[k * M + jj] = cur;
-          cur = nxt - mult * cur;
-          diag = nd - mult * sup;
-          sup = nsup;
-        } else {
-          const double mult = diag / sub;
-          U1[k * M + jj] = sub;
-          U2[k * M + jj] = nd;
-          U3[k * M + jj] = nsup;
-          X[k * M + jj] = nxt;
-          cur = cur - mult * nxt;
-          diag = sup - mult * nd;
-          sup = -mult * nsup;
+      for (long long k0 = 0; k0 < n - 1; k0 += SB) {
+        // the block's operands first (independent of the chain), then its SB dependent steps
+        double xs[SB], es[SB + 1], ds[SB];
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+          const long long k = k0 + q;
+          if (k < n - 1) {
+            xs[q] = X[(k + 1) * M + jj];
+            es[q] = ee_[k];
+            ds[q] = dd_[k + 1];
+          }
+        }
+        es[SB] = (k0 + SB < n - 1) ? ee_[k0 + SB] : 0.0;
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+          const long long k = k0 + q;
+          if (k >= n - 1) break;
+          const double sub = es[q];
+          const double nd = ds[q] - lam;
+          const double nsup = (k + 1 < n - 1) ? es[q + 1] : 0.0;
+          const double nxt = xs[q] * sc;
+          if (fabs(diag) >= fabs(sub)) {
+            if (fabs(diag) < pert) diag = copysign(pert, diag);
+            const double mult = sub / diag;
+            U1[k * M + jj] = diag;
+            U2[k * M + jj] = sup;
+            U3[k * M + jj] = 0.0;
+            X[k * M + jj] = cur;
+            cur = nxt - mult * cur;
+            diag = nd - mult * sup;
+            sup = nsup;
+          } else {
+            const double mult = diag / sub;
+            U1[k * M + jj] = sub;
+            U2[k * M + jj] = nd;
+            U3[k * M + jj] = nsup;
+            X[k * M + jj] = nxt;
+            cur = cur - mult * nxt;
+            diag = sup - mult * nd;
+            sup = -mult * nsup;
+          }
         }
       }
       if (fabs(diag) < pert) diag = copysign(pert, diag);
@@ -187,13 +206,28 @@ __global__ void __launch_bounds__(128) k_inviter(InvArgs a) {
       double x2 = 0.0, x1 = cur / diag;
       X[(n - 1) * M + jj] = x1;
       double nrm = x1 * x1;
-#pragma unroll 4
-      for (long long k = n - 2; k >= 0; --k) {
-        const double xk = (X[k * M + jj] - U2[k * M + jj] * x1 - U3[k * M + jj] * x2) / U1[k * M + jj];
-        X[k * M + jj] = xk;
-        nrm += xk * xk;
-        x2 = x1;
-        x1 = xk;
+      for (long long kb = n - 2; kb >= 0; kb -= SB) {
+        double xs[SB], u1[SB], u2[SB], u3[SB];
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+          const long long k = kb - q;
+          if (k >= 0) {
+            xs[q] = X[k * M + jj];
+            u1[q] = U1[k * M + jj];
+            u2[q] = U2[k * M + jj];
+            u3[q] = U3[k * M + jj];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+          const long long k = kb - q;
+          if (k < 0) break;
+          const double xk = (xs[q] - u2[q] * x1 - u3[q] * x2) / u1[q];
+          X[k * M + jj] = xk;
+          nrm += xk * xk;
+          x2 = x1;
+          x1 = xk;
+        }
       }
       sc = 1.0 / sqrt(nrm);
       // orthogonalise against the earlier members of the cluster (normalised, in slots j..jj-1)
@@ -214,18 +248,27 @@ __global__ void __launch_bounds__(128) k_inviter(InvArgs a) {
     for (int al = 0; al < NG; ++al) sg[al] = make_double2(0, 0);
     const bool keep = (a.zsel != nullptr && mm >= a.zs0 && mm <= a.zs1);
     const int ng = a.ng;
-    for (long long k = 0; k < n; ++k) {
-      const double x = X[k * M + jj] * sc;
-      X[k * M + jj] = x;
+    for (long long k0 = 0; k0 < n; k0 += SB) {
+      double xs[SB];
 #pragma unroll
-      for (int al = 0; al < NG; ++al) {
-        if (al < ng) {
-          const double2 gk = a.g[al * n + k];
-          sg[al].x += x * gk.x;
-          sg[al].y += x * gk.y;
+      for (int q = 0; q < SB; ++q)
+        if (k0 + q < n) xs[q] = X[(k0 + q) * M + jj];
+#pragma unroll
+      for (int q = 0; q < SB; ++q) {
+        const long long k = k0 + q;
+        if (k >= n) break;
+        const double x = xs[q] * sc;
+        X[k * M + jj] = x;
+#pragma unroll
+        for (int al = 0; al < NG; ++al) {
+          if (al < ng) {
+            const double2 gk = a.g[al * n + k];
+            sg[al].x += x * gk.x;
+            sg[al].y += x * gk.y;
+          }
         }
+        if (keep) a.zsel[(mm - a.zs0) * n + k] = x;
       }
-      if (keep) a.zsel[(mm - a.zs0) * n + k] = x;
     }
     // act(a, b) = Re[(z^T g_a) conj(z^T g'_b)], g' = g (dielbsev/dielbsep) or the f-weighted
     // vectors with temperature (dielbseptemp)
@@ -480,7 +523,7 @@ static int tridiagonal_solve_body(wtbg_ctx* ctx, int dtfull, int cpol, bool vect
     a.m1 = m1;
     a.M = (int)M;
     const int cnt = (int)(m1 - m0);
-    k_inviter<<<(cnt + 127) / 128, 128, 0, s>>>(a); WTBG_COUNT(ctx, 1);
+    k_inviter<<<(cnt + 63) / 64, 64, 0, s>>>(a); WTBG_COUNT(ctx, 1);
     CKL("k_inviter");
     m0 = m1;
   }
@@ -527,7 +570,7 @@ int run_eigvecs(wtbg_ctx* ctx, int n0, int n1, double2* d_out) {
     a.zsel = ctx->zsel.as<double>();
     a.zs0 = n0 - 1;
     a.zs1 = n1 - 1;
-    k_inviter<<<(int)((M + 127) / 128), 128, 0, s>>>(a); WTBG_COUNT(ctx, 1);
+    k_inviter<<<(int)((M + 63) / 64), 64, 0, s>>>(a); WTBG_COUNT(ctx, 1);
     CKL("k_inviter(eigvecs)");
   }
   const long long cnt = (long long)nvec * n;

@@ -937,11 +937,13 @@ constexpr int B4_THREADS = 128;
 constexpr int B4_TILE = 3 * BW * BG_LD + 4 * BW + 8;   // Bs, Ds, B1s, v, w1, w2, scalars (double2)
 constexpr size_t B4_SMEM = (size_t)B4_TILE * 16;
 
-__device__ void bulge_step4(const BulgeArgs& a, long long s, long long t, double2* sm) {
-  double2* Bs = sm;
-  double2* Ds = Bs + BW * BG_LD;
-  double2* B1s = Ds + BW * BG_LD;
-  double2* vs = B1s + BW * BG_LD;
+// Bs, Ds, B1s: the bulge block, the diagonal block and the block below; gv: warp 0's rows of the
+// velocity vectors.  With pre, the previous step of the sweep has already placed them (Bs is its
+// block below, updated in place; Ds, B1s and gv prefetched) except the corner of B1s, which the
+// predecessor sweep's step t + 3 writes and which is read here after the wait.
+__device__ void bulge_step4(const BulgeArgs& a, long long s, long long t, double2* Bs, double2* Ds, double2* B1s,
+                            double2* tail, double2 (&gv)[NGMAX], bool pre) {
+  double2* vs = tail;
   double2* w1 = vs + BW;
   double2* w2 = w1 + BW;
   double2* sc = w2 + BW;   // [0] tau, [1] (beta, 0)
@@ -954,22 +956,25 @@ __device__ void bulge_step4(const BulgeArgs& a, long long s, long long t, double
   const long long r1 = r0 + L;
   const int L1 = (r1 < N) ? (int)min((long long)BW, N - r1) : 0;
   // ---- fetch (element e of each tile: row e % 32, column e / 32)
-  if (t > 0)
+  if (!pre) {
+    if (t > 0)
+      for (int e = tid; e < BW * BW; e += B4_THREADS) {
+        const int i = e & 31, q = e >> 5;
+        cpa16(Bs + i * BG_LD + q, AB + (c0 + q) * LDB + (BW + i - q), i < L);
+      }
     for (int e = tid; e < BW * BW; e += B4_THREADS) {
       const int i = e & 31, q = e >> 5;
-      cpa16(Bs + i * BG_LD + q, AB + (c0 + q) * LDB + (BW + i - q), i < L);
+      if (q < L) {
+        const bool ok = i >= q && i < L;
+        cpa16(Ds + i * BG_LD + q, ok ? AB + (r0 + q) * LDB + (i - q) : AB, ok);
+        cpa16(B1s + i * BG_LD + q, AB + (r0 + q) * LDB + (L + i - q), i < L1);
+      }
     }
-  for (int e = tid; e < BW * BW; e += B4_THREADS) {
-    const int i = e & 31, q = e >> 5;
-    if (q < L) {
-      const bool ok = i >= q && i < L;
-      cpa16(Ds + i * BG_LD + q, ok ? AB + (r0 + q) * LDB + (i - q) : AB, ok);
-      cpa16(B1s + i * BG_LD + q, AB + (r0 + q) * LDB + (L + i - q), i < L1);
-    }
+  } else if (tid == 0 && L == BW && L1 == BW) {
+    cpa16(B1s + (BW - 1) * BG_LD + (BW - 1), AB + (r0 + BW - 1) * LDB + L, true);
   }
   asm volatile("cp.async.commit_group;" ::: "memory");
-  double2 gv[NGMAX];
-  if (wid == 0) {
+  if (wid == 0 && !pre) {
 #pragma unroll
     for (int al2 = 0; al2 < NGMAX; ++al2)
       gv[al2] = (al2 < a.ng && lane < L) ? __ldcg(a.g + (long long)al2 * N + r0 + lane) : make_double2(0, 0);
@@ -1098,8 +1103,13 @@ __device__ void bulge_step4(const BulgeArgs& a, long long s, long long t, double
     }
     z = cadd(cadd(z, z1), cadd(z2, z3));
     const double2 tz = cmul(tau, z);
+    // also in place: the next step's bulge block
 #pragma unroll 4
-    for (int q = 0; q < L; ++q) AB[(r0 + q) * LDB + (L + lane - q)] = csub(B1s[lane * BG_LD + q], cmul(tz, cconj(vs[q])));
+    for (int q = 0; q < L; ++q) {
+      const double2 nb = csub(B1s[lane * BG_LD + q], cmul(tz, cconj(vs[q])));
+      AB[(r0 + q) * LDB + (L + lane - q)] = nb;
+      B1s[lane * BG_LD + q] = nb;
+    }
   }
 }
 
@@ -1118,14 +1128,55 @@ __global__ void __launch_bounds__(B4_THREADS) k_bulge4(BulgeArgs a) {
     unsigned int* prog = a.prog + q * a.prog_stride;
     const long long ns = nsteps_of(N, s);
     const long long nprev = (s > 0) ? nsteps_of(N, s - 1) : 0;
+    double2* Bb = b4sm;                // roles of the three tiles rotate between steps
+    double2* Db = b4sm + BW * BG_LD;
+    double2* B1b = Db + BW * BG_LD;
+    double2* tail = b4sm + 3 * BW * BG_LD;
+    double2 gv[NGMAX];
+    bool pre = false;
     for (long long t = 0; t < ns; ++t) {
       if (tid == 0) s_bad = (s > 0 && !wait_at_least(prog + s - 1, (unsigned int)min(t + 3, nprev), a.err)) ? 1 : 0;
       __syncthreads();
       if (s_bad) return;
-      bulge_step4(b, s, t, b4sm);
-      // publish: the CTA barrier orders every thread's writes before thread 0's release store
+      bulge_step4(b, s, t, Bb, Db, B1b, tail, gv, pre);
+      // publish: the CTA barrier orders every thread's writes before the release store, issued
+      // by warp 3 so that its latency overlaps thread 0's wait for the next step
       __syncthreads();
-      if (tid == 0) st_release(prog + s, (unsigned int)(t + 1));
+      if (tid == 96) st_release(prog + s, (unsigned int)(t + 1));
+      pre = false;
+      if (t + 1 < ns) {
+        // Prefetch for step t + 1 (rows r0n = r0 + 32 on): its bulge block is this step's block
+        // below (updated in place); its diagonal block, its block below and the velocity rows
+        // are final already: the predecessor sweep's steps <= t + 2 that write them are done
+        // (this step waited for t + 3), this step wrote none of them, and of the predecessor's
+        // step t + 3 only the corner (31, 31) of the block below overlaps (read after the wait).
+        // The successor sweep runs at most step t - 1 from now on and touches rows above.
+        double2* tmp = Bb;
+        Bb = B1b;
+        B1b = tmp;
+        const long long r0n = s + 1 + (t + 1) * BW;
+        const int Ln = (int)min((long long)BW, N - r0n);
+        const long long r1n = r0n + Ln;
+        const int L1n = (r1n < N) ? (int)min((long long)BW, N - r1n) : 0;
+        if (tid < 96) {
+          for (int e = tid; e < BW * BW; e += 96) {
+            const int i = e & 31, q = e >> 5;
+            if (q < Ln) {
+              const bool ok = i >= q && i < Ln;
+              cpa16(Db + i * BG_LD + q, ok ? b.AB + (r0n + q) * LDB + (i - q) : b.AB, ok);
+              if (!(i == BW - 1 && q == BW - 1 && Ln == BW && L1n == BW))
+                cpa16(B1b + i * BG_LD + q, b.AB + (r0n + q) * LDB + (Ln + i - q), i < L1n);
+            }
+          }
+          asm volatile("cp.async.commit_group;" ::: "memory");
+        }
+        if (tid < 32) {
+#pragma unroll
+          for (int al2 = 0; al2 < NGMAX; ++al2)
+            gv[al2] = (al2 < a.ng && tid < Ln) ? __ldcg(a.g + (long long)al2 * N + r0n + tid) : make_double2(0, 0);
+        }
+        pre = true;
+      }
     }
   }
 }
