@@ -75,13 +75,13 @@ def build_driver(force: bool = False, verbose: bool = False) -> str:
         return DRIVER_LIB
     gxx = shutil.which("g++") or "g++"
     rpath = "-Wl,-rpath,$ORIGIN"
-    cmd = [gxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-I" + os.path.join(ROOT, "include"), src,
+    cmd = [gxx, "-O2", "-std=c++17", "-pthread", "-fPIC", "-shared", "-I" + os.path.join(ROOT, "include"), src,
            "-o", DRIVER_LIB + ".tmp", "-L" + HERE, "-lwtbgpu", rpath]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
     os.replace(DRIVER_LIB + ".tmp", DRIVER_LIB)
-    cmd = [gxx, "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), main, "-o", DRIVER_EXE + ".tmp",
+    cmd = [gxx, "-O2", "-std=c++17", "-pthread", "-I" + os.path.join(ROOT, "include"), main, "-o", DRIVER_EXE + ".tmp",
            "-L" + HERE, "-lwtbdriver", "-lwtbgpu", rpath]
     if verbose:
         print(" ".join(cmd))

@@ -31,6 +31,7 @@
 #include <stdexcept>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/wtbgpu.h"
@@ -448,6 +449,42 @@ std::string F(double x, int w, int d) {
   return s;
 }
 
+// F(x, w, d) appended to out without temporaries (the large per-state tables)
+void append_F(std::string& out, double x, int w, int d) {
+  if (std::isnan(x) || std::isinf(x)) {
+    out += F(x, w, d);
+    return;
+  }
+  char buf[64];
+  const int n = snprintf(buf, sizeof buf, "%*.*f", w, d, x);
+  if (n > w || n < 0) out.append((size_t)w, '*');
+  else out.append(buf, (size_t)n);
+}
+
+// Rows [0, n) of a table formatted by fmt(i, out) on several host threads, joined in row order
+// (the text is the same as one sequential pass).
+template <class Fn>
+std::string format_rows(long long n, size_t per_row, Fn fmt) {
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int nt = (int)std::max<long long>(1, std::min<long long>(std::min<unsigned>(hw ? hw : 1u, 32u), n / 2048 + 1));
+  std::vector<std::string> part(nt);
+  auto work = [&](int t) {
+    const long long a = n * t / nt, b = n * (t + 1) / nt;
+    part[t].reserve((size_t)(b - a) * per_row);
+    for (long long i = a; i < b; ++i) fmt(i, part[t]);
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; ++t) th.emplace_back(work, t);
+  work(0);
+  for (auto& x : th) x.join();
+  size_t tot = 0;
+  for (auto& q : part) tot += q.size();
+  std::string out;
+  out.reserve(tot);
+  for (auto& q : part) out += q;
+  return out;
+}
+
 // Ew.d with the 0.dddd mantissa of Fortran output
 std::string E(double x, int w, int d) {
   if (std::isnan(x) || std::isinf(x)) {
@@ -708,26 +745,33 @@ void write_sp_tables(const Deck& d, int nk, long long N, const std::vector<float
     return k == 0 ? std::string(10, ' ') : I(k, 10);
   };
   {
-    std::string b401, b403, b402, b404;
-    b401.reserve(N * 106);
-    b403.reserve(N * 91);
-    for (long long i = 0; i < N; ++i) {
-      b401 += F(col(i, 6), 15, 4) + F(col(i, 7), 15, 4) + F(col(i, 8), 15, 4) + F(col(i, 9), 15, 4) +
-              F(col(i, 10), 15, 4) + F(col(i, 11), 15, 4) + F(col(i, 12), 15, 4) + "\n";
-      b403 += F(col(i, 6), 15, 4) + F(col(i, 7), 15, 4) + F(col(i, 8), 15, 4) + F(col(i, 9), 15, 4) +
-              F(col(i, 13), 15, 4) + F(col(i, 14), 15, 4) + "\n";
-      if (d.tmcoef) {
-        std::string head = F(col(i, 0), 10, 4) + F(col(i, 1), 10, 4) + F(col(i, 2), 10, 4) + i100(col(i, 3)) +
-                           i100(col(i, 4)) + i100(col(i, 5)) + F(col(i, 6), 10, 4) + F(col(i, 7), 10, 4) +
-                           F(col(i, 8), 10, 4) + F(col(i, 9), 10, 4);
-        b402 += head + F(col(i, 10), 10, 4) + F(col(i, 11), 10, 4) + F(col(i, 12), 10, 4) + "\n";
-        b404 += head + F(col(i, 13), 10, 4) + F(col(i, 14), 10, 4) + "\n";
-      }
-    }
+    const std::string b401 = format_rows(N, 106, [&](long long i, std::string& o) {
+      for (int c = 6; c <= 12; ++c) append_F(o, col(i, c), 15, 4);
+      o += '\n';
+    });
     fputs(b401.c_str(), f401.f);
+    const std::string b403 = format_rows(N, 91, [&](long long i, std::string& o) {
+      for (int c : {6, 7, 8, 9, 13, 14}) append_F(o, col(i, c), 15, 4);
+      o += '\n';
+    });
     fputs(b403.c_str(), f403.f);
     if (d.tmcoef) {
+      auto head = [&](long long i, std::string& o) {
+        for (int c = 0; c < 3; ++c) append_F(o, col(i, c), 10, 4);
+        for (int c = 3; c < 6; ++c) o += i100(col(i, c));
+        for (int c = 6; c < 10; ++c) append_F(o, col(i, c), 10, 4);
+      };
+      const std::string b402 = format_rows(N, 131, [&](long long i, std::string& o) {
+        head(i, o);
+        for (int c = 10; c <= 12; ++c) append_F(o, col(i, c), 10, 4);
+        o += '\n';
+      });
       fputs(b402.c_str(), f402);
+      const std::string b404 = format_rows(N, 121, [&](long long i, std::string& o) {
+        head(i, o);
+        for (int c = 13; c <= 14; ++c) append_F(o, col(i, c), 10, 4);
+        o += '\n';
+      });
       fputs(b404.c_str(), f404);
     }
   }
@@ -981,20 +1025,20 @@ RunState bsesolver(wtbg_ctx* ctx, const Deck& d, const Model& m, Timings* tm) {
   log.line(" optics finished");
   log.flush();
   {
-    std::string b301, b302;
-    b301.reserve(rows * 106);
-    for (long long i = 0; i < rows; ++i) {
-      b301 += F(W[i], 15, 4);
-      for (int c = 0; c < 6; ++c) b301 += F(act[i + (size_t)rows * c], 15, 4);
-      b301 += "\n";
-      if (d.cpol) {
-        b302 += F(W[i], 15, 4) + F(act[i], 15, 4) + F(act[i + (size_t)rows], 15, 4) +
-                F(act[i + 2 * (size_t)rows], 15, 4) + F(act[i + 6 * (size_t)rows], 15, 4) +
-                F(act[i + 7 * (size_t)rows], 15, 4) + "\n";
-      }
-    }
+    const std::string b301 = format_rows(rows, 106, [&](long long i, std::string& o) {
+      append_F(o, W[i], 15, 4);
+      for (int c = 0; c < 6; ++c) append_F(o, act[i + (size_t)rows * c], 15, 4);
+      o += '\n';
+    });
     fputs(b301.c_str(), f301.f);
-    fputs(b302.c_str(), f302.f);
+    if (d.cpol) {
+      const std::string b302 = format_rows(rows, 91, [&](long long i, std::string& o) {
+        append_F(o, W[i], 15, 4);
+        for (int c : {0, 1, 2, 6, 7}) append_F(o, act[i + (size_t)rows * c], 15, 4);
+        o += '\n';
+      });
+      fputs(b302.c_str(), f302.f);
+    }
   }
   log.line("");
   log.line(stamp("end"));
