@@ -118,6 +118,7 @@ struct PanelArgs {
   int j0, k0, jb;      // panel columns j0 .. j0+jb-1, first panel row k0
   int nref;            // reflectors: min(jb, N - k0)
   int R;               // rows per CTA
+  int RS;              // column stride of the panel slice in shared memory (R rounded up to odd)
   double2* Vp;         // [32][N] dense V (rows k0.. written, explicit unit and zeros)
   double2* Tout;       // [32][32] column-major T factor
   double2* g;          // [ng][N]
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
   __shared__ double2 s_T[BW * BW];
   __shared__ double2 s_y[BW * NGMAX];
   const int tid = threadIdx.x;
-  const int R = a.R, jb = a.jb;
+  const int R = a.R, RS = a.RS, jb = a.jb;   // rows per CTA; shared-memory column stride (odd)
   const long long N = a.N;
   const int G = (int)gridDim.x;
   const long long rbeg = (long long)a.k0 + (long long)blockIdx.x * R;
@@ -155,7 +156,7 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
   };
   for (int q = 0; q < jb; ++q)
     for (int i = tid; i < R; i += PQ_THREADS)
-      P[(size_t)q * R + i] = (i < nr) ? a.A[(rbeg + i) + (long long)(a.j0 + q) * N] : make_double2(0, 0);
+      P[(size_t)q * RS + i] = (i < nr) ? a.A[(rbeg + i) + (long long)(a.j0 + q) * N] : make_double2(0, 0);
   __syncthreads();
 
   // width-8 sum over the aligned lane groups of 8 (every lane of a group ends with the same sum)
@@ -180,15 +181,15 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
     const int buf = p & 1;
     double2 sacc = make_double2(0, 0);
     if (qq < jb - p) {
-      const double2* Pp = P + (size_t)p * R;
-      const double2* Pq = P + (size_t)(p + qq) * R;
+      const double2* Pp = P + (size_t)p * RS;
+      const double2* Pq = P + (size_t)(p + qq) * RS;
       const int i0 = (int)max(0LL, rp + 1 - rbeg);
       for (int i = i0 + ((sl - i0) & 7); i < nr; i += 8) sacc = cadd(sacc, cmulc(Pp[i], Pq[i]));
     }
     sacc = sum8(sacc);
     if (qq < jb - p && sl == 0) a.partW[((size_t)buf * G + blockIdx.x) * BW + p + qq] = sacc;
     if (rp >= rbeg && rp < rend)
-      for (int q = p + tid; q < jb; q += PQ_THREADS) a.alpha[buf * BW + q] = P[(size_t)q * R + (rp - rbeg)];
+      for (int q = p + tid; q < jb; q += PQ_THREADS) a.alpha[buf * BW + q] = P[(size_t)q * RS + (rp - rbeg)];
   };
 
   partials(0);
@@ -236,12 +237,12 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
         const int i = it % nr, ch = it / nr;
         const long long r = rbeg + i;
         if (r < rp) continue;
-        const double2 v = (r == rp) ? make_double2(1.0, 0.0) : cmul(P[(size_t)p * R + i], scal);
+        const double2 v = (r == rp) ? make_double2(1.0, 0.0) : cmul(P[(size_t)p * RS + i], scal);
         const double2 cv = cmul(ct, v);
         const int q0 = p + 1 + ch * 8, q1 = min(q0 + 8, jb);
         for (int q = q0; q < q1; ++q) {
           const double2 wq = cadd(s_al[q], cmul(cconj(scal), s_S[q]));
-          P[(size_t)q * R + i] = csub(P[(size_t)q * R + i], cmul(cv, wq));
+          P[(size_t)q * RS + i] = csub(P[(size_t)q * RS + i], cmul(cv, wq));
         }
       }
     }
@@ -249,8 +250,8 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
     // column p becomes v (beta on row k0+p), then the partials of column p+1
     for (int i = tid; i < nr; i += PQ_THREADS) {
       const long long r = rbeg + i;
-      if (r == rp) P[(size_t)p * R + i] = make_double2(beta, 0.0);
-      else if (r > rp) P[(size_t)p * R + i] = cmul(P[(size_t)p * R + i], scal);
+      if (r == rp) P[(size_t)p * RS + i] = make_double2(beta, 0.0);
+      else if (r > rp) P[(size_t)p * RS + i] = cmul(P[(size_t)p * RS + i], scal);
     }
     if (p + 1 < a.nref) partials(p + 1);
   }
@@ -260,43 +261,80 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
     const long long r = rbeg + i, rq = (long long)a.k0 + q;
     if (q >= a.nref || r < rq) return make_double2(0, 0);
     if (r == rq) return make_double2(1.0, 0.0);
-    return P[(size_t)q * R + i];
+    return P[(size_t)q * RS + i];
   };
   for (int q = 0; q < jb; ++q)
     for (int i = tid; i < nr; i += PQ_THREADS) {
-      a.A[(rbeg + i) + (long long)(a.j0 + q) * N] = P[(size_t)q * R + i];
+      a.A[(rbeg + i) + (long long)(a.j0 + q) * N] = P[(size_t)q * RS + i];
       a.Vp[(rbeg + i) + (long long)q * N] = vval(q, i);
     }
-  // Gram partial V^H V over the own rows, and V^T g
+  // P becomes the explicit V (unit on row k0+q, zeros above it and in columns >= nref), so that
+  // the Gram and velocity sums below run without branches
+  __syncthreads();
   const int nref = a.nref;
-  for (int e = tid; e < BW * BW; e += PQ_THREADS) {
-    const int qi = e % BW, qj = e / BW;
-    double2 s = make_double2(0, 0);
-    if (qi < nref && qj < nref)
-      for (int i = 0; i < nr; ++i) s = cadd(s, cmulc(vval(qi, i), vval(qj, i)));
-    a.partG[(size_t)blockIdx.x * BW * BW + e] = s;
+  for (int q = 0; q < jb; ++q)
+    for (int i = tid; i < nr; i += PQ_THREADS) {
+      const long long r = rbeg + i, rq = (long long)a.k0 + q;
+      if (q >= nref || r < rq) P[(size_t)q * RS + i] = make_double2(0, 0);
+      else if (r == rq) P[(size_t)q * RS + i] = make_double2(1.0, 0.0);
+    }
+  __syncthreads();
+  // Gram partial V^H V over the own rows: thread t sums the four entries (t mod 32, t/32 + 8k) in
+  // one pass (one column per lane, the odd stride keeps the 32 lanes on distinct banks; the
+  // other column is a broadcast), rows in order
+  {
+    const int qi = tid & (BW - 1), qj0 = tid >> 5;
+    double2 s4[4] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+    const double2* Pi = P + (size_t)qi * RS;
+    for (int i = 0; i < nr; ++i) {
+      const double2 vi = Pi[i];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s4[k] = cadd(s4[k], cmulc(vi, P[(size_t)(qj0 + 8 * k) * RS + i]));
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) a.partG[(size_t)blockIdx.x * BW * BW + tid + PQ_THREADS * k] = s4[k];
   }
+  // V^T g over the own rows, rows in order; the loads of 16 rows are issued together
   for (int e = tid; e < BW * a.ng; e += PQ_THREADS) {
     const int q = e % BW, al = e / BW;
+    const double2* gp = a.g + (long long)al * N + rbeg;
     double2 s = make_double2(0, 0);
-    if (q < nref)
-      for (int i = 0; i < nr; ++i) s = cadd(s, cmul(vval(q, i), a.g[(long long)al * N + rbeg + i]));
+    for (int i0 = 0; i0 < nr; i0 += 16) {
+      double2 gv[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) gv[u] = (i0 + u < nr) ? __ldcg(gp + i0 + u) : make_double2(0, 0);
+#pragma unroll
+      for (int u = 0; u < 16; ++u)
+        if (i0 + u < nr) s = cadd(s, cmul(P[(size_t)q * RS + i0 + u], gv[u]));
+    }
     a.partVg[(size_t)blockIdx.x * BW * NGMAX + e] = s;
   }
   if (!sync_grid()) return;
+  // Sum of the CTAs' partials in CTA order, the loads of 8 partials issued together
+  auto sum_parts = [&](const double2* base, size_t stride, int e) {
+    double2 s = make_double2(0, 0);
+    for (int c0 = 0; c0 < G; c0 += 8) {
+      double2 pv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) pv[u] = (c0 + u < G) ? ldcg2(base + (size_t)(c0 + u) * stride + e) : make_double2(0, 0);
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (c0 + u < G) s = cadd(s, pv[u]);
+    }
+    return s;
+  };
+  // every CTA: y = V^T g (needed after the T factor; reduced while CTA 0 forms T)
+  for (int e = tid; e < BW * a.ng; e += PQ_THREADS) s_y[e] = sum_parts(a.partVg, (size_t)BW * NGMAX, e);   // [q + al*BW]
   // T factor (ZLARFT forward columnwise): T[i][i] = tau_i, T[0:i, i] = -tau_i T[0:i, 0:i] G[0:i, i]
   if (blockIdx.x == 0) {
-    for (int e = tid; e < BW * BW; e += PQ_THREADS) {
-      double2 s = make_double2(0, 0);
-      for (int c = 0; c < G; ++c) s = cadd(s, ldcg2(a.partG + (size_t)c * BW * BW + e));
-      s_T[e] = s;   // G for now, column-major (qi + qj * BW)
-    }
+    for (int e = tid; e < BW * BW; e += PQ_THREADS) s_T[e] = sum_parts(a.partG, (size_t)BW * BW, e);   // G for now (qi + qj * BW)
     __syncthreads();
-    // column by column; column i of T is built in s_w from G(:, i) before T(:, i) is stored
-    for (int i = 0; i < BW; ++i) {
-      if (tid < BW) s_w[tid] = (tid < i && i < nref) ? s_T[tid + i * BW] : make_double2(0, 0);
-      __syncthreads();
-      if (tid < BW) {
+    // column by column on one warp; column i of T is built in s_w from G(:, i) before T(:, i) is
+    // stored
+    if (tid < BW) {
+      for (int i = 0; i < BW; ++i) {
+        s_w[tid] = (tid < i && i < nref) ? s_T[tid + i * BW] : make_double2(0, 0);
+        __syncwarp();
         double2 t = make_double2(0, 0);
         if (i < nref && tid < i) {
           for (int l = tid; l < i; ++l) t = cadd(t, cmul(s_T[tid + l * BW], s_w[l]));   // T[tid][l] for l < i
@@ -307,20 +345,16 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
         // column i of the G storage is no longer needed below the diagonal: the T entries of
         // rows < i overwrite G(0:i, i); rows >= i become T's diagonal and zeros
         s_T[tid + i * BW] = t;
+        __syncwarp();
       }
-      __syncthreads();
     }
+    __syncthreads();
     // s_T now holds T upper triangular; G entries below the diagonal were overwritten with 0
     for (int e = tid; e < BW * BW; e += PQ_THREADS) a.Tout[e] = s_T[e];
   }
   if (!sync_grid()) return;
   // g <- g - conj(V) T^T (V^T g)
   for (int e = tid; e < BW * BW; e += PQ_THREADS) s_T[e] = ldcg2(a.Tout + e);
-  for (int e = tid; e < BW * a.ng; e += PQ_THREADS) {
-    double2 s = make_double2(0, 0);
-    for (int c = 0; c < G; ++c) s = cadd(s, ldcg2(a.partVg + (size_t)c * BW * NGMAX + e));
-    s_y[e] = s;   // (V^T g)[q][al] at q + al*BW
-  }
   __syncthreads();
   // z = T^T y into s_w-sized scratch: z[j][al] = sum_{i <= j} T[i][j] y[i][al]
   __shared__ double2 s_z[BW * NGMAX];
@@ -1390,6 +1424,7 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
     pa.jb = BW;
     pa.nref = nref;
     pa.R = R;
+    pa.RS = R | 1;
     pa.Vp = V;
     pa.Tout = Tbuf + (size_t)pnl * 1024;
     pa.g = g;
@@ -1401,7 +1436,7 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
     pa.alpha = alpha;
     pa.cnt = cnt + pnl;
     pa.err = err;
-    const size_t psm = (size_t)BW * R * 16;
+    const size_t psm = (size_t)BW * (R | 1) * 16;
     CK(cudaFuncSetAttribute(k_panel_qr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
     mark(pnl, 0);
     {
