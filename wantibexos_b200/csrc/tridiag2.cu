@@ -36,6 +36,7 @@ namespace {
 
 constexpr int BW = 32;            // band width b of the two-stage reduction (= WTBG_PANEL)
 constexpr int PQ_THREADS = 256;   // threads of the panel QR kernel
+constexpr int PQ_MAXG = 160;      // largest panel-QR grid (one CTA per SM; the host checks)
 constexpr int NGMAX = 10;         // velocity vectors carried through (x, y, z, sp, sm [, times f])
 
 __device__ __forceinline__ double2 warp_sum2(double2 v) {
@@ -197,11 +198,21 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
     if (!sync_grid()) return;
     const long long rp = (long long)a.k0 + p;
     const int buf = p & 1;
-    // grid reduction of S_q (q = p + qq): slice sl sums the CTAs c = sl (mod 8) in order
+    // grid reduction of S_q (q = p + qq): slice sl sums the CTAs c = sl (mod 8) in order, its
+    // (at most PQ_MAXG / 8) loads issued together
     {
       double2 sacc = make_double2(0, 0);
-      if (qq < jb - p)
-        for (int c = sl; c < G; c += 8) sacc = cadd(sacc, ldcg2(a.partW + ((size_t)buf * G + c) * BW + p + qq));
+      if (qq < jb - p) {
+        double2 pv[PQ_MAXG / 8];
+#pragma unroll
+        for (int u = 0; u < PQ_MAXG / 8; ++u) {
+          const int c = sl + 8 * u;
+          pv[u] = (c < G) ? ldcg2(a.partW + ((size_t)buf * G + c) * BW + p + qq) : make_double2(0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < PQ_MAXG / 8; ++u)
+          if (sl + 8 * u < G) sacc = cadd(sacc, pv[u]);
+      }
       sacc = sum8(sacc);
       if (qq < jb - p) {
         if (sl == 0) s_S[p + qq] = sacc;
@@ -528,15 +539,17 @@ __global__ void __launch_bounds__(256, 2) k_hemm2(const double2* __restrict__ A,
     }
 }
 
-constexpr size_t XR_SMEM = (size_t)(32 * 64 + 32 * 32 + 32 * 64) * sizeof(double2);
+constexpr int XR_LD = 65;   // row stride of sX, sV: odd, so the Gram loads of 32 columns hit distinct banks
+constexpr size_t XR_SMEM = (size_t)(32 * XR_LD + 32 * 32 + 32 * XR_LD) * sizeof(double2);
 // X = sum of the split partials; Y = X T into Wp; partial G_b = V_b^H Y_b over the 64 rows of
-// this block (Gpart[b][i + 32 j]).
+// this block (Gpart[b][i + 32 j]).  Every sum keeps its order; the independent sums of a thread
+// are interleaved and the split partials' loads issued together (the kernel is latency-bound).
 __global__ void __launch_bounds__(256) k_xreduce(const double2* __restrict__ Xpart, int S, long long N, long long k0,
                                                  const double2* __restrict__ T, const double2* __restrict__ V,
                                                  double2* __restrict__ Wp, double2* __restrict__ Gpart) {
-  extern __shared__ __align__(16) double2 xsm[];   // sX [32][64], sT [32][32], sV [32][64]
+  extern __shared__ __align__(16) double2 xsm[];   // sX [32][XR_LD], sT [32][32], sV [32][XR_LD]
   double2* sX = xsm;
-  double2* sT = sX + 32 * 64;
+  double2* sT = sX + 32 * XR_LD;
   double2* sV = sT + 32 * 32;
   const long long m = N - k0;
   const long long rb = (long long)blockIdx.x * 64;
@@ -547,34 +560,48 @@ __global__ void __launch_bounds__(256) k_xreduce(const double2* __restrict__ Xpa
     const long long rr = rb + r;
     double2 x = make_double2(0, 0), v = make_double2(0, 0);
     if (rr < m) {
-      for (int s = 0; s < S; ++s) x = cadd(x, Xpart[((size_t)s * 32 + c) * (size_t)m + rr]);
+      double2 xp[8];
+#pragma unroll
+      for (int s = 0; s < 8; ++s) xp[s] = (s < S) ? Xpart[((size_t)s * 32 + c) * (size_t)m + rr] : make_double2(0, 0);
+#pragma unroll
+      for (int s = 0; s < 8; ++s)
+        if (s < S) x = cadd(x, xp[s]);
       v = V[k0 + rr + (long long)c * N];
     }
-    sX[e] = x;
-    sV[e] = v;
+    sX[c * XR_LD + r] = x;
+    sV[c * XR_LD + r] = v;
   }
   __syncthreads();
+  // y[u] = sum_{i <= j_u} X[r][i] T[i][j_u], j_u = tid/64 + 4u, the eight chains interleaved
   double2 y[8];
-  for (int u = 0; u < 8; ++u) {
-    const int e = tid + u * 256;
-    const int r = e & 63, j = e >> 6;
-    double2 t = make_double2(0, 0);
-    for (int i = 0; i <= j; ++i) t = cadd(t, cmul(sX[i * 64 + r], sT[i + j * 32]));
-    y[u] = t;
+  const int r = tid & 63, jb0 = tid >> 6;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) y[u] = make_double2(0, 0);
+  for (int i = 0; i <= jb0 + 28; ++i) {
+    const double2 xi = sX[i * XR_LD + r];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (i <= jb0 + 4 * u) y[u] = cadd(y[u], cmul(xi, sT[i + (jb0 + 4 * u) * 32]));
   }
   __syncthreads();
+#pragma unroll
   for (int u = 0; u < 8; ++u) {
-    const int e = tid + u * 256;
-    const int r = e & 63, j = e >> 6;
-    sX[e] = y[u];
+    const int j = jb0 + 4 * u;
+    sX[j * XR_LD + r] = y[u];
     if (rb + r < m) Wp[k0 + rb + r + (long long)j * N] = y[u];
   }
   __syncthreads();
-  for (int e = tid; e < 32 * 32; e += 256) {
-    const int i = e & 31, j = e >> 5;
-    double2 t = make_double2(0, 0);
-    for (int r = 0; r < 64; ++r) t = cadd(t, cmulc(sV[i * 64 + r], sX[j * 64 + r]));
-    Gpart[(size_t)blockIdx.x * 1024 + i + 32 * j] = t;
+  // G[i][j] = sum_r conj(V[r][i]) Y[r][j]: thread t takes (i, j) = (t mod 32, t/32 + 8k), k < 4
+  {
+    const int i = tid & 31, j0 = tid >> 5;
+    double2 g4[4] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+    for (int rr = 0; rr < 64; ++rr) {
+      const double2 vi = sV[i * XR_LD + rr];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) g4[k] = cadd(g4[k], cmulc(vi, sX[(j0 + 8 * k) * XR_LD + rr]));
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) Gpart[(size_t)blockIdx.x * 1024 + i + 32 * (j0 + 8 * k)] = g4[k];
   }
 }
 
@@ -585,7 +612,14 @@ __global__ void __launch_bounds__(1024) k_mform(const double2* __restrict__ Gpar
   __shared__ double2 sT[1024];
   const int e = threadIdx.x;
   double2 t = make_double2(0, 0);
-  for (int b = 0; b < nb; ++b) t = cadd(t, Gpart[(size_t)b * 1024 + e]);
+  for (int b0 = 0; b0 < nb; b0 += 8) {   // in block order, 8 loads issued together
+    double2 pv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) pv[u] = (b0 + u < nb) ? __ldcg(Gpart + (size_t)(b0 + u) * 1024 + e) : make_double2(0, 0);
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (b0 + u < nb) t = cadd(t, pv[u]);
+  }
   sG[e] = t;
   sT[e] = T[e];
   __syncthreads();
@@ -595,18 +629,36 @@ __global__ void __launch_bounds__(1024) k_mform(const double2* __restrict__ Gpar
   M[i + 32 * j] = s;
 }
 
-// W = Y - 1/2 V M (in place in Wp, rows k0..N-1)
+// W = Y - 1/2 V M (in place in Wp, rows k0..N-1): 32 rows per CTA, V staged column by column
+// with coalesced loads; element (r, j) sums i in order as before
+constexpr int WF_LD = 33;
 __global__ void __launch_bounds__(256) k_wform(long long N, long long k0, const double2* __restrict__ V,
                                                const double2* __restrict__ M, double2* __restrict__ Wp) {
   __shared__ double2 sM[1024];
-  for (int e = threadIdx.x; e < 1024; e += 256) sM[e] = M[e];
+  __shared__ double2 sVb[32 * WF_LD];
+  const int tid = threadIdx.x;
+  const long long r0 = k0 + (long long)blockIdx.x * 32;
+  for (int e = tid; e < 1024; e += 256) sM[e] = M[e];
+  for (int e = tid; e < 32 * 32; e += 256) {
+    const int rr = e & 31, i = e >> 5;
+    sVb[i * WF_LD + rr] = (r0 + rr < N) ? V[r0 + rr + (long long)i * N] : make_double2(0, 0);
+  }
   __syncthreads();
-  const long long r = k0 + (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
-  const int j = threadIdx.x & 31;
-  if (r >= N) return;
-  double2 t = make_double2(0, 0);
-  for (int i = 0; i < 32; ++i) t = cadd(t, cmul(V[r + (long long)i * N], sM[i + 32 * j]));
-  Wp[r + (long long)j * N] = csub(Wp[r + (long long)j * N], cscale(t, 0.5));
+  const int rr = tid & 31, jg = tid >> 5;   // columns j = jg + 8u, u < 4
+  if (r0 + rr >= N) return;
+  double2 t[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) t[u] = make_double2(0, 0);
+  for (int i = 0; i < 32; ++i) {
+    const double2 vi = sVb[i * WF_LD + rr];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) t[u] = cadd(t[u], cmul(vi, sM[i + 32 * (jg + 8 * u)]));
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    double2* w = Wp + r0 + rr + (long long)(jg + 8 * u) * N;
+    *w = csub(*w, cscale(t[u], 0.5));
+  }
 }
 
 
@@ -1438,6 +1490,7 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
     pa.err = err;
     const size_t psm = (size_t)BW * (R | 1) * 16;
     CK(cudaFuncSetAttribute(k_panel_qr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+    if (G > PQ_MAXG) return set_err(ctx, WTBG_ERR_UNSUPPORTED, "panel QR: more CTAs than the column reduction holds");
     mark(pnl, 0);
     {
       void* args[] = {&pa};
@@ -1464,7 +1517,7 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
     }
     k_xreduce<<<nIm, 256, XR_SMEM, s>>>(Xpart, S, N, k0, Tbuf + (size_t)pnl * 1024, V, Wout, Gpart);
     k_mform<<<1, 1024, 0, s>>>(Gpart, nIm, Tbuf + (size_t)pnl * 1024, Mbuf);
-    k_wform<<<(int)((m + 7) / 8), 256, 0, s>>>(N, k0, V, Mbuf, Wout);
+    k_wform<<<(int)((m + 31) / 32), 256, 0, s>>>(N, k0, V, Mbuf, Wout);
     WTBG_COUNT(ctx, 6);
     CKL("two-stage panel");
     return 0;
