@@ -697,32 +697,35 @@ __global__ void __launch_bounds__(256) k_strip_update(double2* __restrict__ A, l
 
 // Correction Gram matrices over 64-row blocks from row k1: which = 0: C1 = Wacc^H V2,
 // which = 1: C2 = Vacc^H V2 (K x 32 each, part[b][which][i + K j]).  Rows staged in shared memory.
+constexpr int CP_LD = 65;
 __global__ void __launch_bounds__(256) k_cpart(long long N, long long k1, int K, const double2* __restrict__ Vacc,
                                                const double2* __restrict__ Wacc, const double2* __restrict__ V2,
                                                double2* __restrict__ part) {
-  extern __shared__ __align__(16) double2 csm[];   // sL [K][64], sV [32][64]
+  // sL [K][CP_LD], sV [32][CP_LD]: the odd row stride keeps a warp's K different rows of sL on
+  // distinct banks
+  extern __shared__ __align__(16) double2 csm[];
   const int which = blockIdx.y;
   const double2* L = which ? Vacc : Wacc;
   double2* sL = csm;
-  double2* sV = csm + (size_t)K * 64;
+  double2* sV = csm + (size_t)K * CP_LD;
   const long long rb = k1 + (long long)blockIdx.x * 64;
   for (int e = threadIdx.x; e < K * 64; e += 256) {
     const int u = e & 63, i = e >> 6;
     const long long r = rb + u;
-    sL[e] = r < N ? L[r + (long long)i * N] : make_double2(0, 0);
+    sL[i * CP_LD + u] = r < N ? L[r + (long long)i * N] : make_double2(0, 0);
   }
   for (int e = threadIdx.x; e < 32 * 64; e += 256) {
     const int u = e & 63, j = e >> 6;
     const long long r = rb + u;
-    sV[e] = r < N ? V2[r + (long long)j * N] : make_double2(0, 0);
+    sV[j * CP_LD + u] = r < N ? V2[r + (long long)j * N] : make_double2(0, 0);
   }
   __syncthreads();
   for (int e = threadIdx.x; e < K * 32; e += 256) {
     const int i = e % K, j = e / K;
     double2 t0 = make_double2(0, 0), t1 = t0;
     for (int u = 0; u < 64; u += 2) {
-      t0 = cadd(t0, cmulc(sL[i * 64 + u], sV[j * 64 + u]));
-      t1 = cadd(t1, cmulc(sL[i * 64 + u + 1], sV[j * 64 + u + 1]));
+      t0 = cadd(t0, cmulc(sL[i * CP_LD + u], sV[j * CP_LD + u]));
+      t1 = cadd(t1, cmulc(sL[i * CP_LD + u + 1], sV[j * CP_LD + u + 1]));
     }
     part[((size_t)blockIdx.x * 2 + which) * K * 32 + e] = cadd(t0, t1);
   }
@@ -745,20 +748,41 @@ __global__ void __launch_bounds__(256) k_creduce(const double2* __restrict__ par
 __global__ void __launch_bounds__(256) k_xcorr(double2* __restrict__ X0, long long N, long long k1, int K,
                                                const double2* __restrict__ Vacc, const double2* __restrict__ Wacc,
                                                const double2* __restrict__ C12) {
-  extern __shared__ __align__(16) double2 xsm2[];   // C1 [K][32] (i + K j), C2
-  for (int e = threadIdx.x; e < 2 * K * 32; e += 256) xsm2[e] = C12[e];
-  __syncthreads();
+  // C1 [K][32] (i + K j), C2, then the 32 rows of Vacc and Wacc [K][33] (staged with coalesced
+  // loads); element (rr, c) sums i in order as before, 32 rows per CTA, lanes along the rows
+  extern __shared__ __align__(16) double2 xsm2[];
+  double2* sVa = xsm2 + 2 * K * 32;
+  double2* sWa = sVa + (size_t)K * 33;
   const long long m = N - k1;
-  const long long rr = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
-  const int c = threadIdx.x & 31;
-  if (rr >= m) return;
-  const long long r = k1 + rr;
-  double2 t0 = make_double2(0, 0), t1 = t0;
-  for (int i = 0; i < K; ++i) {
-    t0 = cadd(t0, cmul(Vacc[r + (long long)i * N], xsm2[i + K * c]));
-    t1 = cadd(t1, cmul(Wacc[r + (long long)i * N], xsm2[K * 32 + i + K * c]));
+  const long long rr0 = (long long)blockIdx.x * 32;
+  for (int e = threadIdx.x; e < 2 * K * 32; e += 256) xsm2[e] = C12[e];
+  for (int e = threadIdx.x; e < K * 32; e += 256) {
+    const int u = e & 31, i = e >> 5;
+    const bool ok = rr0 + u < m;
+    sVa[i * 33 + u] = ok ? Vacc[k1 + rr0 + u + (long long)i * N] : make_double2(0, 0);
+    sWa[i * 33 + u] = ok ? Wacc[k1 + rr0 + u + (long long)i * N] : make_double2(0, 0);
   }
-  X0[(size_t)c * m + rr] = csub(X0[(size_t)c * m + rr], cadd(t0, t1));
+  __syncthreads();
+  const int u = threadIdx.x & 31, cg = threadIdx.x >> 5;   // columns c = cg + 8v, v < 4
+  const long long rr = rr0 + u;
+  if (rr >= m) return;
+  double2 t0[4], t1[4];
+#pragma unroll
+  for (int v = 0; v < 4; ++v) t0[v] = t1[v] = make_double2(0, 0);
+  for (int i = 0; i < K; ++i) {
+    const double2 va = sVa[i * 33 + u], wa = sWa[i * 33 + u];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int c = cg + 8 * v;
+      t0[v] = cadd(t0[v], cmul(va, xsm2[i + K * c]));
+      t1[v] = cadd(t1[v], cmul(wa, xsm2[K * 32 + i + K * c]));
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    const int c = cg + 8 * v;
+    X0[(size_t)c * m + rr] = csub(X0[(size_t)c * m + rr], cadd(t0[v], t1[v]));
+  }
 }
 
 // ----------------------------------------------------------------------------- stage 2
@@ -1507,12 +1531,12 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
     k_hemm2<<<dim3(nIm, S), 256, HM_SMEM, s>>>(A, N, k0, Dsym, V, nIm, chunkJ, Xpart);
     mark(pnl, 3);
     if (K > 0) {
-      const size_t cps = ((size_t)K * 64 + 32 * 64) * 16, xcs = (size_t)2 * K * 32 * 16;
+      const size_t cps = ((size_t)K * CP_LD + 32 * CP_LD) * 16, xcs = ((size_t)2 * K * 32 + 2 * (size_t)K * 33) * 16;
       CK(cudaFuncSetAttribute(k_cpart, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cps));
       CK(cudaFuncSetAttribute(k_xcorr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xcs));
       k_cpart<<<dim3(nIm, 2), 256, cps, s>>>(N, k0, K, Vp, Wp, V, Cpart);
       k_creduce<<<(2 * K * 32 + 255) / 256, 256, 0, s>>>(Cpart, nIm, K, Cbuf);
-      k_xcorr<<<(int)((m + 7) / 8), 256, xcs, s>>>(Xpart, N, k0, K, Vp, Wp, Cbuf);
+      k_xcorr<<<(int)((m + 31) / 32), 256, xcs, s>>>(Xpart, N, k0, K, Vp, Wp, Cbuf);
       WTBG_COUNT(ctx, 3);
     }
     k_xreduce<<<nIm, 256, XR_SMEM, s>>>(Xpart, S, N, k0, Tbuf + (size_t)pnl * 1024, V, Wout, Gpart);
