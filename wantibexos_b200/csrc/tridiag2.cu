@@ -388,18 +388,28 @@ __global__ void __launch_bounds__(PQ_THREADS, 1) k_panel_qr(PanelArgs a) {
 
 // Diagonal 64 x 64 tiles of A22 made full Hermitian (lower stored, upper = conj of lower,
 // diagonal real), column-major per tile: Dsym[I][c*64 + r].  Rows/columns past N are zero.
+constexpr int SD_LD = 65;
+constexpr size_t SD_SMEM = (size_t)64 * SD_LD * sizeof(double2);
 __global__ void __launch_bounds__(256) k_symdiag(const double2* __restrict__ A, long long N, long long k0,
                                                  double2* __restrict__ Dsym) {
+  // the tile's lower half read once with coalesced loads into sL [c][r], then written out full
+  extern __shared__ __align__(16) double2 sL[];
   const long long I0 = k0 + (long long)blockIdx.x * 64;
   double2* D = Dsym + (size_t)blockIdx.x * 64 * 64;
   for (int e = threadIdx.x; e < 64 * 64; e += 256) {
     const int r = e & 63, c = e >> 6;
     const long long gr = I0 + r, gc = I0 + c;
+    sL[c * SD_LD + r] = (r >= c && gr < N && gc < N) ? A[gr + gc * N] : make_double2(0, 0);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 64 * 64; e += 256) {
+    const int r = e & 63, c = e >> 6;
+    const long long gr = I0 + r, gc = I0 + c;
     double2 v = make_double2(0, 0);
     if (gr < N && gc < N) {
-      if (r > c) v = A[gr + gc * N];
-      else if (r < c) v = cconj(A[gc + gr * N]);
-      else v = make_double2(A[gr + gc * N].x, 0.0);
+      if (r > c) v = sL[c * SD_LD + r];
+      else if (r < c) v = cconj(sL[r * SD_LD + c]);
+      else v = make_double2(sL[c * SD_LD + r].x, 0.0);
     }
     D[e] = v;
   }
@@ -670,29 +680,41 @@ __global__ void __launch_bounds__(256) k_wform(long long N, long long k0, const 
 // One warp per row (lane = column); the column rows of V and W in shared memory.
 __global__ void __launch_bounds__(256) k_strip_update(double2* __restrict__ A, long long N, long long c0, int K,
                                                       const double2* __restrict__ V, const double2* __restrict__ W) {
-  extern __shared__ __align__(16) double2 ssm[];   // sVc [K][32], sWc [K][32]
+  // sVc, sWc [K][32]: the strip's column rows; sVr, sWr [K][33]: this CTA's 32 rows (coalesced
+  // loads); thread (lane = row, warp w) takes the columns w + 8v; sums in the order as before
+  extern __shared__ __align__(16) double2 ssm[];
   double2* sVc = ssm;
   double2* sWc = ssm + (size_t)K * 32;
+  double2* sVr = sWc + (size_t)K * 32;
+  double2* sWr = sVr + (size_t)K * 33;
+  const long long rb = c0 + (long long)blockIdx.x * 32;
   for (int e = threadIdx.x; e < K * 32; e += 256) {
     const int q = e >> 5, c = e & 31;
-    const long long rc = c0 + c;
+    const long long rc = c0 + c, rr = rb + c;
     sVc[e] = rc < N ? V[rc + (long long)q * N] : make_double2(0, 0);
     sWc[e] = rc < N ? W[rc + (long long)q * N] : make_double2(0, 0);
+    sVr[q * 33 + c] = rr < N ? V[rr + (long long)q * N] : make_double2(0, 0);
+    sWr[q * 33 + c] = rr < N ? W[rr + (long long)q * N] : make_double2(0, 0);
   }
   __syncthreads();
-  const long long r = c0 + (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
-  const int c = threadIdx.x & 31;
-  if (r >= N || c0 + c >= N || r < c0 + c) return;
-  double2 t0 = make_double2(0, 0), t1 = t0;
-  for (int q = 0; q < K; q += 2) {
-    t0 = cadd(t0, cadd(cmulc(sWc[q * 32 + c], V[r + (long long)q * N]), cmulc(sVc[q * 32 + c], W[r + (long long)q * N])));
-    t1 = cadd(t1, cadd(cmulc(sWc[(q + 1) * 32 + c], V[r + (long long)(q + 1) * N]),
-                       cmulc(sVc[(q + 1) * 32 + c], W[r + (long long)(q + 1) * N])));
+  const int u = threadIdx.x & 31, cg = threadIdx.x >> 5;
+  const long long r = rb + u;
+  if (r >= N) return;
+#pragma unroll
+  for (int v = 0; v < 4; ++v) {
+    const int c = cg + 8 * v;
+    if (c0 + c >= N || r < c0 + c) continue;
+    double2 t0 = make_double2(0, 0), t1 = t0;
+    for (int q = 0; q < K; q += 2) {
+      t0 = cadd(t0, cadd(cmulc(sWc[q * 32 + c], sVr[q * 33 + u]), cmulc(sVc[q * 32 + c], sWr[q * 33 + u])));
+      t1 = cadd(t1, cadd(cmulc(sWc[(q + 1) * 32 + c], sVr[(q + 1) * 33 + u]),
+                         cmulc(sVc[(q + 1) * 32 + c], sWr[(q + 1) * 33 + u])));
+    }
+    const long long idx = r + (c0 + c) * N;
+    double2 a = csub(A[idx], cadd(t0, t1));
+    if (r == c0 + c) a.y = 0.0;
+    A[idx] = a;
   }
-  const long long idx = r + (c0 + c) * N;
-  double2 a = csub(A[idx], cadd(t0, t1));
-  if (r == c0 + c) a.y = 0.0;
-  A[idx] = a;
 }
 
 // Correction Gram matrices over 64-row blocks from row k1: which = 0: C1 = Wacc^H V2,
@@ -1469,6 +1491,7 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
   CK(cudaMemsetAsync(cnt, 0, (size_t)std::max<long long>(npan, 1) * 4, s));
   CK(cudaFuncSetAttribute(k_hemm2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HM_SMEM));
   CK(cudaFuncSetAttribute(k_xreduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)XR_SMEM));
+  CK(cudaFuncSetAttribute(k_symdiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SD_SMEM));
   // profiling: event pairs around the panel QR, the Hermitian product and the rank-2k update
   // of every panel (read after the stage), and around the stage
   const bool prof = ctx->profiling != 0;
@@ -1522,7 +1545,7 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
     }
     mark(pnl, 1);
     const int nIm = (int)((m + 63) / 64);
-    k_symdiag<<<nIm, 256, 0, s>>>(A, N, k0, Dsym);
+    k_symdiag<<<nIm, 256, SD_SMEM, s>>>(A, N, k0, Dsym);
     int S = (int)std::min<long long>(SMAX, std::max<long long>(1, (4LL * nsm + nIm - 1) / nIm));
     S = std::min(S, nIm);
     const int chunkJ = (nIm + S - 1) / S;
@@ -1558,10 +1581,10 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
       if (j > 0) {
         const long long c0 = pnl * BW;   // the panel's first column (= the previous panel's k0)
         const long long mc = N - c0;
-        const size_t sss = (size_t)2 * 32 * j * 32 * 16;
+        const size_t sss = ((size_t)2 * 32 * j * 32 + (size_t)2 * 32 * j * 33) * 16;
         CK(cudaFuncSetAttribute(k_strip_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sss));
         mark(pnl - 1, 4);
-        k_strip_update<<<(int)((mc + 7) / 8), 256, sss, s>>>(A, N, c0, 32 * j, Vp, Wp);
+        k_strip_update<<<(int)((mc + 31) / 32), 256, sss, s>>>(A, N, c0, 32 * j, Vp, Wp);
         WTBG_COUNT(ctx, 1);
         mark(pnl - 1, 5);
         her2k_flops[pnl - 1] = 8.0 * (double)mc * 32 * 2 * 32 * j;
