@@ -482,10 +482,11 @@ static int tridiagonal_solve_body(wtbg_ctx* ctx, int dtfull, int cpol, bool vect
     maxc = std::max(maxc, jx - i);
     i = jx;
   }
-  // chunk size: bounded workspace
+  // chunk size: the vectors of one launch run their chains side by side, so one launch for all
+  // of them where the workspace fits (43.5 GB at N = 36864), else chunks
   size_t freeb = 0, totb = 0;
   CK(cudaMemGetInfo(&freeb, &totb));
-  const double budget = std::min((double)freeb * 0.5 + (double)ctx->ws.bytes, 24e9);
+  const double budget = std::min((double)freeb * 0.6 + (double)ctx->ws.bytes, 96e9);
   long long M = (long long)(budget / (4.0 * 8.0 * (double)n));
   M = std::max<long long>(M, maxc);
   M = std::min<long long>(M, n);
