@@ -148,7 +148,7 @@ int wtbg_destroy(wtbg_ctx* ctx) {
   DevBuf* bufs[] = {&ctx->HR, &ctx->Rcart, &ctx->Rf32, &ctx->invdeg, &ctx->isR0, &ctx->kpt, &ctx->eig, &ctx->U,
                     &ctx->nocp, &ctx->kstat, &ctx->kptq, &ctx->eigq, &ctx->Uq, &ctx->nocpq, &ctx->h, &ctx->H,
                     &ctx->d, &ctx->e, &ctx->tau, &ctx->g, &ctx->fdeh, &ctx->Wp, &ctx->slots, &ctx->part, &ctx->scal,
-                    &ctx->yv, &ctx->lam, &ctx->ws, &ctx->act, &ctx->zsel, &ctx->csz, &ctx->sp_in, &ctx->sp_out,
+                    &ctx->yv, &ctx->lam, &ctx->bgrid, &ctx->ws, &ctx->act, &ctx->zsel, &ctx->csz, &ctx->sp_in, &ctx->sp_out,
                     &ctx->sp_om, &ctx->tmp, &ctx->tmp2, &ctx->istat, &ctx->pOpA, &ctx->pOpB,
                     &ctx->pHk, &ctx->pOc, &ctx->pOv, &ctx->pErr, &ctx->triErr, &ctx->gwork,
                     &ctx->t2V, &ctx->t2X, &ctx->t2D, &ctx->t2G, &ctx->t2T, &ctx->t2P, &ctx->t2AB, &ctx->t2prog, &ctx->t2de};

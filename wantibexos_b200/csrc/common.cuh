@@ -64,6 +64,7 @@ struct wtbg_ctx {
   DevBuf scal;             // per-column scalars
   DevBuf yv;               // hemv result
   DevBuf lam;              // eigenvalues
+  DevBuf bgrid;            // coarse multisection grid: points and Sturm counts
   DevBuf ws;               // inverse-iteration workspace
   DevBuf act;              // oscillator strengths [8][N]
   DevBuf zsel;             // selected tridiagonal eigenvectors (for eigvecs)

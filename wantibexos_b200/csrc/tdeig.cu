@@ -6,8 +6,9 @@
 //   f_n = |sum_j A_jn h_j|^2 = |z_n^T g|^2,  g = Q^T h,  A = Q Z,
 // so after the reduction only the tridiagonal eigenvectors z_n are needed, and only inside
 // the dot products with the five g vectors.
-//   * eigenvalues: Sturm-count multisection, L lanes per eigenvalue index (L = 1: bisection),
-//     to full precision;
+//   * eigenvalues: one coarse round of Sturm counts at 32769 points of the Gershgorin interval
+//     gives every eigenvalue index its starting cell; then Sturm-count multisection, L lanes
+//     per eigenvalue index (L = 1: bisection), to full precision;
 //   * eigenvectors: inverse iteration with a partial-pivoting tridiagonal LU, three steps
 //     from a deterministic pseudo-random start vector; eigenvalues closer than
 //     1e-7 * ||T|| form a cluster that one thread processes in sequence with modified
@@ -54,13 +55,38 @@ __global__ void k_e2(const double* e, long long n, double* e2) {
 // at the midpoint, for L = 1: plain bisection), so the chain of dependent Sturm passes per
 // eigenvalue is log2(L + 1) times shorter, for L times more total passes; the host picks L.
 // Stopping rule as in bisection: width <= 2 eps max(|a|, |b|) + pivmin, or no double between.
+// Coarse round: Sturm counts at the P + 1 points x_j = lo + (hi - lo) j / P of the Gershgorin
+// interval (count 0 at lo and n at hi by construction), one thread per point.
+constexpr int BIS_P = 32768;
+__global__ void k_bisect_grid(const double* __restrict__ d, const double* __restrict__ e2, long long n, double lo,
+                              double hi, double pivmin, double* __restrict__ xg, int* __restrict__ cg) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > BIS_P) return;
+  const double x = (j == BIS_P) ? hi : lo + (hi - lo) * ((double)j / (double)BIS_P);
+  xg[j] = x;
+  cg[j] = (j == 0) ? 0 : (j == BIS_P ? (int)n : sturm_count(d, e2, n, x, pivmin));
+}
+
 __global__ void __launch_bounds__(128) k_bisect(const double* __restrict__ d, const double* __restrict__ e2, long long n,
-                                                double lo, double hi, double pivmin, int L, double* lam) {
+                                                const double* __restrict__ xg, const int* __restrict__ cg,
+                                                double pivmin, int L, double* lam) {
   const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long m = gt / L;
   const int lane = threadIdx.x & 31, sl = lane & (L - 1), base = lane - sl;
   const bool active = m < n;
-  double a = lo, b = hi;
+  // start from the coarse cell [x_j, x_{j+1}] with count(x_j) <= m < count(x_{j+1}) (binary
+  // search keeping that invariant; cg[0] = 0 <= m < n = cg[P])
+  double a = xg[0], b = xg[BIS_P];
+  if (active) {
+    int jl = 0, jh = BIS_P;
+    while (jh - jl > 1) {
+      const int jm = (jl + jh) >> 1;
+      if (cg[jm] <= m) jl = jm;
+      else jh = jm;
+    }
+    a = xg[jl];
+    b = xg[jh];
+  }
   for (int it = 0; it < 256; ++it) {
     const double mid = 0.5 * (a + b);
     const bool done = !active || !(mid > a && mid < b) || (b - a <= 2.0 * DBL_EPSILON * fmax(fabs(a), fabs(b)) + pivmin);
@@ -80,15 +106,17 @@ __global__ void __launch_bounds__(128) k_bisect(const double* __restrict__ d, co
 }
 
 // Lanes per eigenvalue for k_bisect.  A round costs one Sturm pass (n dependent steps of about
-// 150 cycles) when the SM sub-partitions are idle, and n L / 32 warp passes of about 22 issue
-// cycles per step spread over 4 nsm sub-partitions when they are full; rounds ~ 53 / log2(L+1).
+// 170 cycles) when the SM sub-partitions are idle, and n L / 32 warp passes of about 50 issue
+// cycles per step spread over 4 nsm sub-partitions when they are full; after the coarse round
+// (15 bits) rounds ~ 38 / log2(L+1).  (Constants fitted to B200 timings at N = 2304 and 9216
+// over L = 4 .. 32.)
 int bisect_lanes(long long n, int nsm) {
   int best = 1;
   double bt = 1e300;
   for (int L = 1; L <= 32; L *= 2) {
-    const double rounds = std::ceil(53.0 / std::log2((double)L + 1.0));
-    const double lat = 150.0 * (double)n;
-    const double thr = 22.0 * (double)n * (double)n * (double)L / 32.0 / (4.0 * std::max(nsm, 1));
+    const double rounds = std::ceil(38.0 / std::log2((double)L + 1.0));
+    const double lat = 170.0 * (double)n;
+    const double thr = 50.0 * (double)n * (double)n * (double)L / 32.0 / (4.0 * std::max(nsm, 1));
     const double t = rounds * std::max(lat, thr);
     if (t < bt) {
       bt = t;
@@ -462,8 +490,13 @@ static int tridiagonal_solve_body(wtbg_ctx* ctx, int dtfull, int cpol, bool vect
   }
   if (ctx->nsm <= 0) cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
   const int lanes = bisect_lanes(n, ctx->nsm);
-  k_bisect<<<(int)((n * lanes + 127) / 128), 128, 0, s>>>(ctx->d.as<double>(), e2, n, lo, hi, pivmin, lanes,
-                                                       ctx->lam.as<double>()); WTBG_COUNT(ctx, 1);
+  ENSURE(ctx->bgrid, (size_t)(BIS_P + 1) * (8 + 4) + 64);
+  double* xg = ctx->bgrid.as<double>();
+  int* cg = reinterpret_cast<int*>(xg + BIS_P + 1);
+  k_bisect_grid<<<(BIS_P + 1 + 255) / 256, 256, 0, s>>>(ctx->d.as<double>(), e2, n, lo, hi, pivmin, xg, cg);
+  CKL("k_bisect_grid");
+  k_bisect<<<(int)((n * lanes + 127) / 128), 128, 0, s>>>(ctx->d.as<double>(), e2, n, xg, cg, pivmin, lanes,
+                                                       ctx->lam.as<double>()); WTBG_COUNT(ctx, 2);
   CKL("k_bisect");
   ctx->lam_host.resize(n);
   CK(cudaMemcpyAsync(ctx->lam_host.data(), ctx->lam.as<double>(), n * 8, cudaMemcpyDeviceToHost, s));
