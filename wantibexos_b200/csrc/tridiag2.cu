@@ -1421,7 +1421,14 @@ __global__ void __launch_bounds__(256) k_bt1_apply(const double2* __restrict__ A
 // Largest N whose panels fit the aggregate shared memory of the panel QR (one CTA per SM,
 // at most PQ_MAX_R rows of the 32-wide panel each).
 constexpr int PQ_MAX_R = 384;
-constexpr int LOOKAHEAD = 2;   // panels applied per rank-2k update (K = 64)
+constexpr long long LA_FOUR_FROM = 20000;   // N from which groups of four are used
+constexpr int LOOKAHEAD = 4;   // largest number of panels applied per rank-2k update (K = 128)
+// the look-ahead corrections stage K = 32 (group - 1) rows in shared memory (200 KB at 4)
+static_assert(LOOKAHEAD >= 1 && LOOKAHEAD <= 4, "look-ahead groups of 1 to 4 panels");
+// Group size per reduction: the wider update pays off where the trailing matrices are large
+// (config 2, N = 36864: fours 11.75 s, pairs 11.86 s per step); at N = 8100 the update rate does
+// not rise and the corrections cost more (fours 228 ms, pairs 223 ms per config-4 Q).
+inline int lookahead_group(long long N) { return N >= LA_FOUR_FROM ? 4 : 2; }
 static bool two_stage_fits(wtbg_ctx* ctx, long long N) {
   if (ctx->nsm <= 0) cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->device);
   return N > BW + 1 && (N + ctx->nsm - 1) / ctx->nsm <= PQ_MAX_R;
@@ -1569,13 +1576,14 @@ static int run_stage1(wtbg_ctx* ctx, int ng, int band) {
     CKL("two-stage panel");
     return 0;
   };
-  // Panels in look-ahead groups of up to LOOKAHEAD: panel j of a group first gets the pending
+  // Panels in look-ahead groups of la (up to LOOKAHEAD): panel j of a group first gets the pending
   // updates of the group's earlier panels on its own 32 columns (strip), is factored, and forms
   // its product from the matrix that still lacks those updates (corrected); one rank-2k update
   // with K = 32 x (panels in the group) then applies the whole group to the trailing matrix.
   std::vector<double> her2k_flops(npan, 0.0);
-  for (long long p0 = 0; p0 < npan; p0 += LOOKAHEAD) {
-    const int gsz = (int)std::min<long long>(LOOKAHEAD, npan - p0);
+  const int la = std::min(LOOKAHEAD, lookahead_group(N));
+  for (long long p0 = 0; p0 < npan; p0 += la) {
+    const int gsz = (int)std::min<long long>(la, npan - p0);
     for (int j = 0; j < gsz; ++j) {
       const long long pnl = p0 + j;
       if (j > 0) {
