@@ -442,7 +442,8 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // Warp (wr, wc): rows 16 wr .. +16, columns 16 wc .. +16 (two 8-wide n blocks).
 constexpr int HM_LDA = 66;   // sA[k][row], 64 rows + 2 (conflict-free fragment loads)
 constexpr int HM_LDT = 36;   // sAT[row][k], 32 k + 4
-constexpr int HM_LDV = 34;   // sV[k][col], 32 columns + 2
+constexpr int HM_LDV = 36;   // sV[col][k], 32 k + 4 (the staging writes along k and the fragment
+                             // reads of 8 columns x 4 k both fall on distinct banks)
 constexpr int HM_ABUF = 64 * HM_LDT;   // >= 32 * HM_LDA; union of the two A layouts
 constexpr int HM_STAGE = HM_ABUF + 32 * HM_LDV;
 constexpr size_t HM_SMEM = 2 * (size_t)HM_STAGE * sizeof(double2);
@@ -495,7 +496,7 @@ __global__ void __launch_bounds__(256, 2) k_hemm2(const double2* __restrict__ A,
       const int k = e & 31, col = e >> 5;
       const long long gr = cJ + k;
       const bool ok = gr < N;
-      cp_async16(sV + k * HM_LDV + col, ok ? V + gr + (long long)col * N : V, ok);
+      cp_async16(sV + col * HM_LDV + k, ok ? V + gr + (long long)col * N : V, ok);
     }
     cp_async_commit();
   };
@@ -529,7 +530,7 @@ __global__ void __launch_bounds__(256, 2) k_hemm2(const double2* __restrict__ A,
 #pragma unroll
       for (int nb = 0; nb < 2; ++nb) {
         const int col = wc * 16 + nb * 8 + gq;
-        const double2 v0 = sV[ka * HM_LDV + col], v1 = sV[kb * HM_LDV + col];
+        const double2 v0 = sV[col * HM_LDV + ka], v1 = sV[col * HM_LDV + kb];
         const double bre[4] = {v0.x, v1.x, -v0.y, -v1.y};
         const double bim[4] = {v0.y, v1.y, v0.x, v1.x};
         dmma16(accr[nb], a, bre);
