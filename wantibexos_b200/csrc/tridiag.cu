@@ -494,10 +494,12 @@ __global__ void __launch_bounds__(RB) k_wfix_last(const double2* A, long long N,
 // One CTA per 64x64 tile of the lower triangle. The panel columns arrive in chunks of HK
 // through a two-stage cp.async ring (the next chunk loads while the current one multiplies),
 // and the tile of A itself is prefetched into L2 at the start so that the read-modify-write
-// epilogue does not wait on HBM.
+// epilogue does not wait on HBM.  Each staged operand is k-major, [q][row] with row stride
+// HLD = 66: the copying lanes step along the rows (consecutive 16-byte slots) and a fragment
+// load's 8-lane phase (rows r, r+1 at k .. k+3) falls on 8 distinct bank groups.
 constexpr int HK = 8;         // q-chunk staged per step
-constexpr int HKP = HK + 4;   // padded row stride (bank-conflict free 16-byte loads)
-constexpr int HSTAGE = 4 * TB * HKP;   // double2 per stage (Vr, Wr, Vc, Wc)
+constexpr int HLD = TB + 2;   // row stride of a staged [q][row] operand
+constexpr int HSTAGE = 4 * HK * HLD;   // double2 per stage (Vr, Wr, Vc, Wc)
 constexpr size_t HER2K_SMEM = 2 * (size_t)HSTAGE * sizeof(double2);
 
 // D += A B with A 16x16 (k = tq + 4*(i/2) for a_i, row gq + 8*(i%2)) and B 16x8 (k = tq + 4*j for
@@ -548,9 +550,9 @@ __global__ void __launch_bounds__(256, 2) k_her2k(double2* A, long long N, const
 
   auto stage = [&](int c, int buf) {
     double2* sVr = hsm + (size_t)buf * HSTAGE;
-    double2* sWr = sVr + TB * HKP;
-    double2* sVc = sWr + TB * HKP;
-    double2* sWc = sVc + TB * HKP;
+    double2* sWr = sVr + HK * HLD;
+    double2* sVc = sWr + HK * HLD;
+    double2* sWc = sVc + HK * HLD;
     const int qc = c * HK;
     for (int it = tid; it < TB * HK; it += 256) {
       const int rr = it % TB, q = it / TB;
@@ -558,10 +560,10 @@ __global__ void __launch_bounds__(256, 2) k_her2k(double2* A, long long N, const
       const bool qv = (qc + q) < jb;
       const long long qcol = (long long)(vc0 + qc + q);
       const bool vr = qv && rg < N, vc = qv && cg < N;
-      cp_async16(sVr + rr * HKP + q, vr ? Vs + rg + qcol * N : Vs, vr);
-      cp_async16(sWr + rr * HKP + q, vr ? Wp + rg + (long long)(qc + q) * N : Wp, vr);
-      cp_async16(sVc + rr * HKP + q, vc ? Vs + cg + qcol * N : Vs, vc);
-      cp_async16(sWc + rr * HKP + q, vc ? Wp + cg + (long long)(qc + q) * N : Wp, vc);
+      cp_async16(sVr + q * HLD + rr, vr ? Vs + rg + qcol * N : Vs, vr);
+      cp_async16(sWr + q * HLD + rr, vr ? Wp + rg + (long long)(qc + q) * N : Wp, vr);
+      cp_async16(sVc + q * HLD + rr, vc ? Vs + cg + qcol * N : Vs, vc);
+      cp_async16(sWc + q * HLD + rr, vc ? Wp + cg + (long long)(qc + q) * N : Wp, vc);
     }
     cp_async_commit();
   };
@@ -580,21 +582,21 @@ __global__ void __launch_bounds__(256, 2) k_her2k(double2* A, long long N, const
     else cp_async_wait<0>();
     __syncthreads();
     const double2* sVr = hsm + (size_t)(c & 1) * HSTAGE;
-    const double2* sWr = sVr + TB * HKP;
-    const double2* sVc = sWr + TB * HKP;
-    const double2* sWc = sVc + TB * HKP;
+    const double2* sWr = sVr + HK * HLD;
+    const double2* sVc = sWr + HK * HLD;
+    const double2* sWc = sVc + HK * HLD;
 #pragma unroll
     for (int kk = 0; kk < HK; kk += 4) {
       const int row = wr * 16 + gq;
-      const double2 v0 = sVr[row * HKP + kk + tq], v1 = sVr[(row + 8) * HKP + kk + tq];
-      const double2 w0 = sWr[row * HKP + kk + tq], w1 = sWr[(row + 8) * HKP + kk + tq];
+      const double2 v0 = sVr[(kk + tq) * HLD + row], v1 = sVr[(kk + tq) * HLD + row + 8];
+      const double2 w0 = sWr[(kk + tq) * HLD + row], w1 = sWr[(kk + tq) * HLD + row + 8];
       // k segments: [Vr | Vi | Wr | Wi] (re) and [Vi | -Vr | Wi | -Wr] (im) against [Wr; Wi; Vr; Vi]
       const double are[8] = {v0.x, v1.x, v0.y, v1.y, w0.x, w1.x, w0.y, w1.y};
       const double aim[8] = {v0.y, v1.y, -v0.x, -v1.x, w0.y, w1.y, -w0.x, -w1.x};
 #pragma unroll
       for (int n = 0; n < 4; ++n) {
         const int col = wc * 32 + n * 8 + gq;
-        const double2 bw = sWc[col * HKP + kk + tq], bv = sVc[col * HKP + kk + tq];
+        const double2 bw = sWc[(kk + tq) * HLD + col], bv = sVc[(kk + tq) * HLD + col];
         const double b[4] = {bw.x, bw.y, bv.x, bv.y};
         dmma16(accr[n], are, b);
         dmma16(acci[n], aim, b);
